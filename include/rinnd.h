@@ -1,0 +1,185 @@
+/*
+ * rinnd.h -- C ABI of the B200-native NN-Descent engine (librinnd_b200.so).
+ *
+ * Drop-in boundary for lmcinnes/rinnd's build/query path.  Plain pointers and
+ * sizes only.  Every call returns RINND_OK (0) or a negative RINND_ERR_* code;
+ * rinnd_last_error() returns a thread-local message for the last failure.
+ * Host pointers are read/written synchronously unless a name says "device".
+ *
+ * Reference interfaces replaced (paths relative to the reference root; core/ =
+ * crates/rinnd-core/src/):
+ *   NNDescentBuilder::new + setters + build_with_distance   core/index.rs:449-733
+ *   NNDescentIndex::query / query_one                        core/index.rs:389-439
+ *   NNDescentIndex::query_one_quantized_i8_with_workspace    core/index.rs:283-334
+ *   RINND(...) constructor / query / neighbor_graph / search_graph / storage_info
+ *                                                            crates/rinnd/src/lib.rs:616-1103
+ */
+#ifndef RINND_H
+#define RINND_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RINND_EXPORT __attribute__((visibility("default")))
+#else
+#define RINND_EXPORT
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define RINND_OK 0
+#define RINND_ERR_INVALID (-1)   /* bad argument (reference: ValueError / assert!) */
+#define RINND_ERR_OOM (-2)       /* device allocation failed (MemoryError)          */
+#define RINND_ERR_CUDA (-3)      /* CUDA runtime failure (RuntimeError)             */
+#define RINND_ERR_NO_DEVICE (-4) /* no CUDA device visible                         */
+#define RINND_ERR_INTERNAL (-5)
+
+/* ---- distance kinds: the reference's build distances and proxies -------- */
+#define RINND_DIST_SQEUCLIDEAN 0        /* core/distance/euclidean.rs:14-93    */
+#define RINND_DIST_MANHATTAN 1          /* core/distance/minkowski.rs:11-83    */
+#define RINND_DIST_COSINE 2             /* core/distance/cosine.rs:20-113      */
+#define RINND_DIST_ALT_COSINE 3         /* core/distance/alternatives.rs:200-231 */
+#define RINND_DIST_ALT_DOT 4            /* core/distance/alternatives.rs:15-124  */
+#define RINND_DIST_DIRECT_COSINE 5      /* core/distance/alternatives.rs:131-154 */
+#define RINND_DIST_INNER_PRODUCT 6      /* core/distance/inner_product.rs:96-107 */
+#define RINND_DIST_ALT_INNER_PRODUCT 7  /* core/distance/alternatives.rs:160-193 */
+
+/* ---- corrections applied to reported distances -------------------------- */
+#define RINND_CORR_NONE 0
+#define RINND_CORR_SQRT 1        /* index.rs:587                    */
+#define RINND_CORR_ALT_COSINE 2  /* alternatives.rs:273-277          */
+#define RINND_CORR_ALT_IP 3      /* alternatives.rs:279-287          */
+
+/* ---- int8 encodings (crates/rinnd/src/lib.rs:151-156) ------------------- */
+#define RINND_Q8_PER_VECTOR_COSINE 0  /* "int8"  */
+#define RINND_Q8_GLOBAL_SYMMETRIC 1   /* "sq8u"  */
+#define RINND_Q8_PER_VECTOR_SYMMETRIC 2 /* "sq8p" */
+
+/* Mirrors NNDescentBuilder's fields (core/index.rs:449-494) plus the metric
+ * dispatch decisions the Python layer makes (crates/rinnd/src/lib.rs:1175-1297). */
+typedef struct rinnd_build_params {
+  int32_t n_neighbors;              /* default 30                                  */
+  int32_t n_trees;                  /* default 8                                   */
+  int32_t n_search_trees;           /* default 1                                   */
+  int32_t search_tree_leaf_budget;  /* default 1 (only 1 is implemented)           */
+  int32_t leaf_size;                /* <= 0: clamp(5k, 60, 256)  (index.rs:617-619) */
+  int32_t max_candidates;           /* <= 0: min(k, 60)          (index.rs:620-622) */
+  int32_t n_iters;                  /* <= 0: max(5, ceil(log2 N)) (index.rs:623-625) */
+  float delta;                      /* default 0.001                               */
+  uint64_t random_seed;             /* default 42                                  */
+  float diversify_prob;             /* default 1.0 (only 1.0 is implemented)       */
+  float pruning_degree_multiplier;  /* default 1.5                                 */
+  int32_t angular;                  /* angular RP splits (index.rs:606-614)        */
+  int32_t distance_kind;            /* RINND_DIST_*                                */
+  int32_t correction;               /* RINND_CORR_*                                */
+  int32_t normalize;                /* L2-normalize rows before build (lib.rs:710-712) */
+  int32_t verbose;
+  int32_t device;                   /* CUDA device ordinal, default 0              */
+  int32_t reserved[7];
+} rinnd_build_params;
+
+typedef struct rinnd_index rinnd_index;
+
+/* Per-phase timings and counters of the last build. */
+typedef struct rinnd_build_info {
+  int32_t iterations;
+  int32_t forest_levels;
+  int64_t n_leaves;
+  double ms_forest, ms_leaf_init, ms_iterations, ms_candidates, ms_join, ms_sort, ms_graph, ms_total;
+  uint64_t pairs_evaluated;      /* local-join pair distances over all iterations */
+  uint64_t pushes_accepted;      /* heap changes over all iterations              */
+  uint64_t push_contention;      /* pushes abandoned after the bounded retry count */
+  int64_t search_graph_nnz;
+  float min_distance;
+} rinnd_build_info;
+
+/* ---- lifecycle ------------------------------------------------------------ */
+RINND_EXPORT int rinnd_params_default(rinnd_build_params* p);
+/* NNDescentBuilder::build_with_distance (core/index.rs:601-733) from host rows (n x d f32). */
+RINND_EXPORT int rinnd_build(const float* data, int64_t n, int32_t d, const rinnd_build_params* p,
+                rinnd_index** out);
+/* Same, with the rows already on the device (row stride `ld` floats, ld >= d). */
+RINND_EXPORT int rinnd_build_device(const float* d_data, int64_t n, int32_t d, int64_t ld,
+                       const rinnd_build_params* p, rinnd_index** out);
+RINND_EXPORT int rinnd_free(rinnd_index* idx);
+RINND_EXPORT int rinnd_build_info_get(const rinnd_index* idx, rinnd_build_info* info);
+RINND_EXPORT int rinnd_index_shape(const rinnd_index* idx, int64_t* n, int32_t* d, int32_t* k);
+
+/* ---- queries -------------------------------------------------------------- */
+/* NNDescentIndex::query (core/index.rs:406-439): nq x d host queries -> nq x k
+ * results in original ids, corrected distances, (-1, +inf) padding.  Query i
+ * uses random stream seed + qid_base + i (index.rs:165). */
+RINND_EXPORT int rinnd_query(rinnd_index* idx, const float* queries, int64_t nq, int32_t k, float epsilon,
+                int32_t* out_idx, float* out_dist);
+/* NNDescentIndex::query_one (core/index.rs:390-392): stream seed + 0. */
+RINND_EXPORT int rinnd_query_one(rinnd_index* idx, const float* query, int32_t k, float epsilon,
+                    int32_t* out_idx, float* out_dist);
+/* Device-resident queries/results (row stride d rounded up to 4 floats is NOT
+ * required: rows are `ld` floats apart). */
+RINND_EXPORT int rinnd_query_device(rinnd_index* idx, const float* d_queries, int64_t nq, int64_t ld,
+                       int32_t k, float epsilon, uint64_t qid_base, int32_t* d_out_idx,
+                       float* d_out_dist, void* stream);
+
+/* ---- graph exports ----------------------------------------------------------- */
+/* neighbor_graph property (crates/rinnd/src/lib.rs:1087-1103): n x k ids and
+ * corrected distances sorted ascending. */
+RINND_EXPORT int rinnd_neighbor_graph(const rinnd_index* idx, int32_t* out_idx, float* out_dist);
+/* search_graph property (lib.rs:1013-1025, index.rs:137-141): CSR in original id order. */
+RINND_EXPORT int rinnd_search_graph_nnz(const rinnd_index* idx, int64_t* nnz);
+RINND_EXPORT int rinnd_search_graph(const rinnd_index* idx, int32_t* indptr, int32_t* indices,
+                       float* min_distance);
+/* Internal (search-layout) vertex order: vertex_order[internal] = original id (index.rs:679-715). */
+RINND_EXPORT int rinnd_vertex_order(const rinnd_index* idx, int32_t* out);
+
+/* ---- int8 serving (crates/rinnd/src/lib.rs:159-416, core/index.rs:283-334) -- */
+/* Encodes the index rows (must be built with RINND_DIST_DIRECT_COSINE on
+ * normalized rows) with one of RINND_Q8_*. */
+RINND_EXPORT int rinnd_quantize(rinnd_index* idx, int32_t encoding);
+/* Quantized greedy search + optional exact FP32 rerank; width rules of
+ * core/index.rs:55-89.  Uses random stream seed + 0 for every query (index.rs:298). */
+RINND_EXPORT int rinnd_query_quantized(rinnd_index* idx, const float* queries, int64_t nq, int32_t k,
+                          float epsilon, int32_t candidate_width, int32_t rerank_width,
+                          int32_t* out_idx, float* out_dist);
+
+/* ---- storage info (crates/rinnd/src/lib.rs:1028-1077) ---------------------- */
+typedef struct rinnd_storage_info {
+  char encoding[32];
+  int64_t code_bytes, metadata_bytes, retained_fp32_bytes;
+  double encode_seconds;
+  int64_t device_bytes;
+} rinnd_storage_info;
+RINND_EXPORT int rinnd_storage_info_get(const rinnd_index* idx, rinnd_storage_info* info);
+
+/* ---- component entry points (parity tests, tools) -------------------------- */
+/* out[i] = distance(kind, a[i], b[i]) over n_pairs row pairs (host, n x d each);
+ * reference accumulation order, core/distance/*.rs. */
+RINND_EXPORT int rinnd_distance_pairs(int32_t kind, const float* a, const float* b, int64_t n_pairs, int32_t d,
+                         float* out);
+/* SearchGraph::from_dense_diversified (core/graph/search_graph.rs:263-360) on a
+ * host kNN graph (n x k, ascending rows, -1 padding) over host data (n x d).
+ * indices must hold n * round(mult * k) entries; *nnz receives the edge count. */
+RINND_EXPORT int rinnd_search_graph_from_knn(const int32_t* knn_idx, const float* knn_dist, const float* data,
+                                int32_t n, int32_t k, int32_t d, int32_t kind, float mult,
+                                int32_t* indptr, int32_t* indices, int64_t* nnz,
+                                float* min_distance);
+/* Concurrent NeighborHeap::checked_flagged_push (core/heap/neighbor_heap.rs:149-177):
+ * applies n_ops pushes (row, id, dist, is_new) to an empty n x k heap on the
+ * device, all at once, then sort_all (:293-320).  Returns accepted pushes. */
+RINND_EXPORT int rinnd_heap_push_batch(int32_t n, int32_t k, int64_t n_ops, const int32_t* rows,
+                          const int32_t* ids, const float* dists, const uint8_t* flags,
+                          int32_t* out_idx, float* out_dist, uint8_t* out_flags,
+                          int64_t* n_accepted);
+
+/* ---- misc ------------------------------------------------------------------- */
+RINND_EXPORT const char* rinnd_last_error(void);
+RINND_EXPORT const char* rinnd_version(void);
+RINND_EXPORT int rinnd_device_count(int32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RINND_H */

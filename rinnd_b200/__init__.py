@@ -1,0 +1,281 @@
+"""rinnd_b200 -- B200-native NN-Descent engine behind the reference's ``rinnd.RINND`` API.
+
+``RINND`` mirrors the PyO3 class of lmcinnes/rinnd (crates/rinnd/src/lib.rs:61-1103):
+the same constructor keywords and defaults, metric dispatch, ``ValueError``
+messages, output dtypes (int32 ids, float32 distances) and methods.  All compute
+runs in librinnd_b200.so (hand-written sm_100a CUDA) through the C ABI in
+include/rinnd.h; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib as L
+
+__all__ = ["RINND", "version", "simd_info", "device_count"]
+
+# Metric::from_str aliases (core/distance/mod.rs:203-247).
+_ALIASES = {
+    "euclidean": "euclidean", "l2": "euclidean",
+    "sqeuclidean": "sqeuclidean", "squared_euclidean": "sqeuclidean",
+    "manhattan": "manhattan", "taxicab": "manhattan", "l1": "manhattan",
+    "cosine": "cosine", "inner_product": "inner_product", "ip": "inner_product", "dot": "dot",
+}
+# Metrics the reference knows that this engine does not implement (outside the hot path).
+_KNOWN_OTHER = {
+    "chebyshev", "linfinity", "linfty", "linf", "canberra", "braycurtis", "correlation", "true_angular",
+    "tsss", "hamming", "jaccard", "dice", "matching", "kulsinski", "rogerstanimoto", "russellrao",
+    "sokalsneath", "sokalmichener", "yule", "hellinger", "jensen_shannon", "jensen-shannon",
+    "symmetric_kl", "symmetric-kl", "symmetric_kullback_liebler",
+}
+_ANGULAR = {"cosine", "inner_product", "dot"}  # index.rs:606-614
+
+_ENCODINGS = {"int8": L.Q8_PER_VECTOR_COSINE, "sq8u": L.Q8_GLOBAL_SYMMETRIC, "sq8p": L.Q8_PER_VECTOR_SYMMETRIC}
+
+
+def version() -> str:
+    """Library version (crates/rinnd/src/lib.rs:1301-1304)."""
+    return L.lib.rinnd_version().decode()
+
+
+def simd_info() -> str:
+    """Compute backend description (crates/rinnd/src/lib.rs:1307-1336)."""
+    n = L.device_count()
+    return f"CUDA sm_100a ({n} device{'s' if n != 1 else ''})"
+
+
+def device_count() -> int:
+    return L.device_count()
+
+
+def _as_f32_2d(a, what="data") -> np.ndarray:
+    a = np.asarray(a)
+    if a.dtype != np.float32:
+        raise TypeError(f"{what} must be a float32 array, got {a.dtype}")
+    if a.ndim != 2:
+        raise ValueError(f"{what} must be 2-dimensional")
+    return np.ascontiguousarray(a)
+
+
+def _validate_quantized_widths(k: int, candidate_width: int, rerank_width: int) -> None:
+    """crates/rinnd/src/lib.rs:1148-1172."""
+    if candidate_width == 0:
+        return
+    if candidate_width < k:
+        raise ValueError(f"candidate_width {candidate_width} must be at least k ({k})")
+    if rerank_width > candidate_width:
+        raise ValueError(f"rerank_width {rerank_width} must not exceed candidate_width {candidate_width}")
+    if 0 < rerank_width < k:
+        raise ValueError(f"rerank_width {rerank_width} must be zero or at least k ({k})")
+
+
+class RINND:
+    """NNDescent index built and queried on the GPU (crates/rinnd/src/lib.rs:616-755)."""
+
+    def __init__(self, data, metric="euclidean", n_neighbors=30, n_trees=None, n_search_trees=1,
+                 search_tree_leaf_budget=1, leaf_size=None, max_candidates=None, n_iters=None, delta=0.001,
+                 random_state=None, diversify_prob=1.0, pruning_degree_multiplier=1.5, verbose=False,
+                 normalize=False, cosine_distance_mode="log", quantized_candidate_width=0,
+                 quantized_rerank_width=0, tree_quantization="none", retain_fp32_data=None, device=0):
+        self._h = None
+        data = _as_f32_2d(data)
+        n_points, dim = data.shape
+        if quantized_candidate_width > 0 and quantized_rerank_width > quantized_candidate_width:
+            raise ValueError("quantized_rerank_width must not exceed quantized_candidate_width when candidate "
+                             "width is explicit")
+        name = metric.lower()
+        if name not in _ALIASES:
+            if name in _KNOWN_OTHER:
+                raise ValueError(f"Metric '{metric}' is not implemented by the B200 engine")
+            raise ValueError(f"Unknown metric: {metric}")
+        name = _ALIASES[name]
+        normalize_cosine = bool(normalize) and name == "cosine"
+        modes = {"log": (False, None), "direct": (True, None)}
+        modes.update({m: (True, e) for m, e in _ENCODINGS.items()})
+        if cosine_distance_mode not in modes:
+            raise ValueError(f"Unknown cosine_distance_mode: {cosine_distance_mode}; expected 'log', 'direct', "
+                             "'int8', 'sq8u', or 'sq8p'")
+        direct_cosine, encoding = modes[cosine_distance_mode]
+        if tree_quantization not in ("none", "int8"):
+            raise ValueError(f"Unknown tree_quantization: {tree_quantization}; expected 'none' or 'int8'")
+        quantize_trees = tree_quantization == "int8"
+        if quantize_trees and encoding is None:
+            raise ValueError("tree_quantization='int8' is available only with a quantized cosine_distance_mode")
+        if quantize_trees and encoding == L.Q8_GLOBAL_SYMMETRIC:
+            raise ValueError("tree_quantization='int8' is incompatible with cosine_distance_mode='sq8u'; use "
+                             "tree_quantization='none'")
+        if direct_cosine and not normalize_cosine:
+            raise ValueError("direct and quantized cosine modes require metric='cosine' and normalize=True")
+        if quantize_trees:
+            raise ValueError("tree_quantization='int8' is not implemented by the B200 engine")
+        if retain_fp32_data is None:
+            retain_fp32_data = (not quantize_trees) or quantized_rerank_width > 0
+
+        # lib.rs:1200-1204 n_trees default: clamp(round(2 log10 N), 3, 12)
+        if n_trees is None:
+            v = 2.0 * math.log10(n_points) if n_points > 0 else float("-inf")
+            n_trees = int(min(max(math.floor(v + 0.5) if math.isfinite(v) else 0, 3), 12))
+
+        # lib.rs:1239-1294 metric -> build distance + correction
+        if name == "euclidean":
+            kind, corr = L.DIST_SQEUCLIDEAN, L.CORR_SQRT
+        elif name == "sqeuclidean":
+            kind, corr = L.DIST_SQEUCLIDEAN, L.CORR_NONE
+        elif name == "manhattan":
+            kind, corr = L.DIST_MANHATTAN, L.CORR_NONE
+        elif name == "cosine":
+            if normalize_cosine:
+                if encoding is not None or direct_cosine:
+                    kind, corr = L.DIST_DIRECT_COSINE, L.CORR_NONE
+                else:
+                    kind, corr = L.DIST_ALT_DOT, L.CORR_ALT_COSINE
+            else:
+                kind, corr = L.DIST_ALT_COSINE, L.CORR_ALT_COSINE
+        elif name == "dot":
+            kind, corr = L.DIST_ALT_DOT, L.CORR_ALT_COSINE
+        else:  # inner_product
+            kind, corr = L.DIST_ALT_INNER_PRODUCT, L.CORR_ALT_IP
+
+        p = L.BuildParams()
+        L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
+        p.n_neighbors = int(n_neighbors)
+        p.n_trees = int(n_trees)
+        p.n_search_trees = int(n_search_trees)
+        p.search_tree_leaf_budget = max(int(search_tree_leaf_budget), 1)
+        p.leaf_size = int(leaf_size) if leaf_size is not None else 0
+        p.max_candidates = int(max_candidates) if max_candidates is not None else 0
+        p.n_iters = int(n_iters) if n_iters is not None else 0
+        p.delta = float(delta)
+        p.random_seed = int(random_state) if random_state is not None else 42
+        p.diversify_prob = float(diversify_prob)
+        p.pruning_degree_multiplier = float(pruning_degree_multiplier)
+        p.angular = int(name in _ANGULAR)
+        p.distance_kind = kind
+        p.correction = corr
+        p.normalize = int(normalize_cosine)
+        p.verbose = int(bool(verbose))
+        p.device = int(device)
+
+        h = ctypes.c_void_p()
+        L.check(L.lib.rinnd_build(L.ptr(data), n_points, dim, ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self.n_points, self.dim, self.n_neighbors = n_points, dim, int(n_neighbors)
+        self.metric = metric
+        self._encoding = encoding
+        self._candidate_width = int(quantized_candidate_width)
+        self._rerank_width = int(quantized_rerank_width)
+        self._retain_fp32 = bool(retain_fp32_data)
+        if encoding is not None:
+            L.check(L.lib.rinnd_quantize(self._h, encoding))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            L.lib.rinnd_free(h)
+            self._h = None
+
+    # ---- queries (lib.rs:775-1010) -------------------------------------------------
+    def _check_dim(self, qdim: int) -> None:
+        if qdim != self.dim:
+            raise ValueError(f"Query dimension {qdim} does not match data dimension {self.dim}")
+
+    def _run_query(self, q: np.ndarray, k: int, epsilon: float):
+        n = q.shape[0]
+        idx = np.empty((n, k), np.int32)
+        dist = np.empty((n, k), np.float32)
+        if self._encoding is not None:
+            L.check(L.lib.rinnd_query_quantized(self._h, L.ptr(q), n, k, float(epsilon), self._candidate_width,
+                                                self._rerank_width, L.ptr(idx), L.ptr(dist)))
+        else:
+            L.check(L.lib.rinnd_query(self._h, L.ptr(q), n, k, float(epsilon), L.ptr(idx), L.ptr(dist)))
+        return idx, dist
+
+    def query(self, query_data, k=10, epsilon=0.1):
+        """Approximate k nearest neighbours of each query row (lib.rs:775-821)."""
+        q = _as_f32_2d(query_data, "query_data")
+        self._check_dim(q.shape[1])
+        return self._run_query(q, int(k), epsilon)
+
+    def query_quantized(self, query_data, k=10, epsilon=0.1, candidate_width=0, rerank_width=0):
+        """Quantized query with query-time widths (lib.rs:825-874)."""
+        _validate_quantized_widths(k, candidate_width, rerank_width)
+        if self._encoding is None:
+            raise ValueError("query-time quantized widths require a quantized cosine_distance_mode")
+        q = _as_f32_2d(query_data, "query_data")
+        self._check_dim(q.shape[1])
+        n = q.shape[0]
+        idx = np.empty((n, k), np.int32)
+        dist = np.empty((n, k), np.float32)
+        L.check(L.lib.rinnd_query_quantized(self._h, L.ptr(q), n, int(k), float(epsilon), int(candidate_width),
+                                            int(rerank_width), L.ptr(idx), L.ptr(dist)))
+        return idx, dist
+
+    def query_one(self, query, k=10, epsilon=0.1):
+        """Single-vector query (lib.rs:877-912); same random stream as query row 0."""
+        q = np.asarray(query)
+        if q.dtype != np.float32:
+            raise TypeError(f"query must be a float32 array, got {q.dtype}")
+        if q.ndim != 1:
+            raise ValueError("query must be 1-dimensional")
+        self._check_dim(q.shape[0])
+        idx, dist = self._run_query(np.ascontiguousarray(q[None, :]), int(k), epsilon)
+        return idx[0], dist[0]
+
+    def query_one_indices(self, query, k=10, epsilon=0.1):
+        """Single-vector query returning ids only (lib.rs:918-951)."""
+        return self.query_one(query, k, epsilon)[0]
+
+    def query_one_indices_quantized(self, query, k=10, epsilon=0.1, candidate_width=0, rerank_width=0):
+        """lib.rs:959-1010."""
+        _validate_quantized_widths(k, candidate_width, rerank_width)
+        q = np.asarray(query, dtype=np.float32)
+        self._check_dim(q.shape[0])
+        return self.query_quantized(q[None, :], k, epsilon, candidate_width, rerank_width)[0][0]
+
+    # ---- exports -------------------------------------------------------------------
+    @property
+    def neighbor_graph(self):
+        """(int32[N,k], float32[N,k]) sorted ascending, corrected distances (lib.rs:1087-1103)."""
+        idx = np.empty((self.n_points, self.n_neighbors), np.int32)
+        dist = np.empty((self.n_points, self.n_neighbors), np.float32)
+        L.check(L.lib.rinnd_neighbor_graph(self._h, L.ptr(idx), L.ptr(dist)))
+        return idx, dist
+
+    @property
+    def search_graph(self):
+        """(indptr int32, indices int32, min_distance) in original id order (lib.rs:1013-1025)."""
+        nnz = ctypes.c_int64(0)
+        L.check(L.lib.rinnd_search_graph_nnz(self._h, ctypes.byref(nnz)))
+        indptr = np.empty(self.n_points + 1, np.int32)
+        indices = np.empty(max(nnz.value, 1), np.int32)
+        md = ctypes.c_float(0)
+        L.check(L.lib.rinnd_search_graph(self._h, L.ptr(indptr), L.ptr(indices), ctypes.byref(md)))
+        return indptr, indices[: nnz.value], float(md.value)
+
+    @property
+    def vertex_order(self):
+        out = np.empty(self.n_points, np.int32)
+        L.check(L.lib.rinnd_vertex_order(self._h, L.ptr(out)))
+        return out
+
+    @property
+    def build_info(self) -> dict:
+        info = L.BuildInfo()
+        L.check(L.lib.rinnd_build_info_get(self._h, ctypes.byref(info)))
+        return {f: getattr(info, f) for f, _ in L.BuildInfo._fields_}
+
+    def storage_info(self) -> dict:
+        """Storage/encoding metadata (lib.rs:1028-1077) plus device bytes."""
+        s = L.StorageInfo()
+        L.check(L.lib.rinnd_storage_info_get(self._h, ctypes.byref(s)))
+        info = {
+            "encoding": s.encoding.decode(), "code_bytes": int(s.code_bytes),
+            "metadata_bytes": int(s.metadata_bytes), "retained_fp32_bytes": int(s.retained_fp32_bytes),
+            "encode_seconds": float(s.encode_seconds), "device_bytes": int(s.device_bytes),
+        }
+        info["allocated_bytes"] = info["code_bytes"] + info["metadata_bytes"] + info["retained_fp32_bytes"]
+        info["bytes_per_vector"] = info["allocated_bytes"] / self.n_points
+        return info

@@ -1,0 +1,615 @@
+// api.cu -- C ABI and host orchestration of the B200 NN-Descent engine.
+//
+// rinnd_build follows NNDescentBuilder::build_with_distance (core/index.rs:601-733):
+// parameter defaults (:617-625), RP forest + leaf init + NN-Descent iterations
+// with the delta convergence test (core/nndescent/mod.rs:137-163), sorted kNN
+// rows (:653), the diversified CSR (:656-666), corrected neighbor distances
+// (:669-673) and the physical reorder by the first tree's leaf order (:679-715).
+// Everything stays resident on the device; host copies are made only for
+// exports.  There is no CPU fallback: without a CUDA device every entry point
+// fails with RINND_ERR_NO_DEVICE.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/rinnd.h"
+#include "common.cuh"
+#include "engine.h"
+
+using namespace rinnd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct NoDevice : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return RINND_OK;
+  } catch (const std::invalid_argument& e) {
+    return fail(RINND_ERR_INVALID, e.what());
+  } catch (const NoDevice& e) {
+    return fail(RINND_ERR_NO_DEVICE, e.what());
+  } catch (const std::bad_alloc& e) {
+    return fail(RINND_ERR_OOM, "host allocation failed");
+  } catch (const CudaError& e) {
+    std::string m = e.what();
+    int code = (m.find("out of memory") != std::string::npos) ? RINND_ERR_OOM : RINND_ERR_CUDA;
+    return fail(code, m);
+  } catch (const std::exception& e) {
+    return fail(RINND_ERR_INTERNAL, e.what());
+  }
+}
+
+void require(bool cond, const std::string& msg) {
+  if (!cond) throw std::invalid_argument(msg);
+}
+
+void ensure_device(int dev) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    throw NoDevice("no CUDA device is available: the B200 engine has no CPU fallback");
+  }
+  require(dev >= 0 && dev < n, "device ordinal out of range");
+  RINND_CUDA(cudaSetDevice(dev));
+}
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct StreamGuard {
+  cudaStream_t s = nullptr;
+  StreamGuard() { RINND_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+  ~StreamGuard() {
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+// Copies n rows of d floats (row stride ld) into a zero-padded n x Dp device buffer.
+void load_rows(const float* src, bool src_device, int64_t n, int d, int64_t ld, int Dp, DVec<float>& dst,
+               cudaStream_t st) {
+  dst.alloc((size_t)n * Dp, st);
+  if (Dp != d) dst.fill_bytes(0);
+  RINND_CUDA(cudaMemcpy2DAsync(dst.p, sizeof(float) * Dp, src, sizeof(float) * ld, sizeof(float) * d,
+                               (size_t)n, src_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                               st));
+}
+
+bool kind_uses_norms(int kind) { return kind != DK_SQEUCLIDEAN && kind != DK_MANHATTAN; }
+
+__global__ void k_tree_idx(const int32_t* perm, const int32_t* inverse, long long total, int32_t* out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = inverse[perm[i]];
+}
+
+__global__ void k_iota(int32_t* p, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = i;
+}
+
+}  // namespace
+
+struct rinnd_index {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int64_t N = 0;
+  int D = 0, Dp = 0, k = 0;
+  rinnd_build_params p{};
+  int kind = 0, corr = 0;
+  bool normalize = false;
+  DVec<float> X;                 // internal order, N x Dp
+  DVec<int32_t> vertex_order;    // internal -> original
+  DVec<int32_t> inverse;         // original -> internal
+  Csr graph_int, graph_orig;
+  Forest forest;
+  DVec<int32_t> tree_idx, tree_roots;
+  int n_search_trees = 0;
+  DVec<int32_t> knn_idx;
+  DVec<float> knn_dist;          // corrected
+  float min_distance = 0.f;
+  rinnd_build_info info{};
+  DVec<unsigned long long> search_stats;
+  // int8 serving
+  int encoding = -1;
+  DVec<int8_t> codes;
+  DVec<float> inv_norms;
+  float global_mult = 0.f;
+  int Dq = 0;
+  double encode_seconds = 0.0;
+  std::mutex mu;
+  ~rinnd_index() {
+    if (st) {
+      cudaSetDevice(device);
+      cudaStreamSynchronize(st);
+    }
+  }
+  SearchIndex search_view() const {
+    SearchIndex s;
+    s.N = (int)N;
+    s.D = D;
+    s.Dp = Dp;
+    s.kind = kind;
+    s.corr = corr;
+    s.X = X.p;
+    s.indptr = graph_int.indptr.p;
+    s.indices = graph_int.indices.p;
+    s.min_distance = min_distance;
+    s.n_trees = n_search_trees;
+    s.tree_roots = tree_roots.p;
+    s.children = forest.children.p;
+    s.offsets = forest.offsets.p;
+    s.hyperplanes = forest.hyperplanes.p;
+    s.tree_idx = tree_idx.p;
+    s.leaf_budget = p.search_tree_leaf_budget;
+    s.vertex_order = vertex_order.p;
+    s.seed = p.random_seed;
+    s.codes = codes.p;
+    s.inv_norms = inv_norms.p;
+    s.Dq = Dq;
+    return s;
+  }
+};
+
+namespace {
+
+void validate_params(const rinnd_build_params* p, int64_t n, int d) {
+  require(p != nullptr, "params must not be null");
+  require(n >= 1, "data must contain at least one point");
+  require(n < (int64_t)INT32_MAX - 1, "at most 2^31-2 points are supported");
+  require(d >= 1, "data dimension must be positive");
+  require(p->n_neighbors >= 1 && p->n_neighbors <= 128, "n_neighbors must be in [1, 128]");
+  require(p->n_trees >= 0 && p->n_trees <= 64, "n_trees must be in [0, 64]");
+  require(p->n_search_trees >= 0, "n_search_trees must be >= 0");
+  require(p->search_tree_leaf_budget <= 1, "search_tree_leaf_budget > 1 is not implemented");
+  require(p->distance_kind >= 0 && p->distance_kind < DK_COUNT, "unknown distance kind");
+  require(p->correction >= 0 && p->correction <= CK_ALT_IP, "unknown correction");
+  require(p->diversify_prob >= 1.0f, "diversify_prob < 1 is not implemented");
+  require(p->pruning_degree_multiplier > 0.f, "pruning_degree_multiplier must be positive");
+}
+
+void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
+                const rinnd_build_params* pin, rinnd_index** out) {
+  require(out != nullptr, "out must not be null");
+  require(data != nullptr, "data must not be null");
+  validate_params(pin, n, d);
+  require(ld >= d, "row stride must be >= dimension");
+  ensure_device(pin->device);
+  double t_start = now_ms();
+  std::unique_ptr<rinnd_index> ix(new rinnd_index());
+  ix->device = pin->device;
+  ix->p = *pin;
+  RINND_CUDA(cudaStreamCreateWithFlags(&ix->st, cudaStreamNonBlocking));
+  cudaStream_t st = ix->st;
+  const int N = (int)n, D = d, Dp = round_up(d, 4), k = pin->n_neighbors;
+  ix->N = n;
+  ix->D = D;
+  ix->Dp = Dp;
+  ix->k = k;
+  ix->kind = pin->distance_kind;
+  ix->corr = pin->correction;
+  ix->normalize = pin->normalize != 0;
+  // index.rs:617-625 defaults
+  int leaf_size = pin->leaf_size > 0 ? pin->leaf_size : std::max(60, std::min(5 * k, 256));
+  int max_cand = pin->max_candidates > 0 ? pin->max_candidates : std::min(k, 60);
+  int n_iters = pin->n_iters > 0 ? pin->n_iters : std::max(5, (int)std::ceil(std::log2((double)N)));
+  int c = std::min(std::min(max_cand, 60), k);  // nndescent/mod.rs:89
+  ix->p.leaf_size = leaf_size;
+  ix->p.max_candidates = max_cand;
+  ix->p.n_iters = n_iters;
+  ix->p.search_tree_leaf_budget = std::max(1, pin->search_tree_leaf_budget);
+
+  TempStorage tmp;
+  DVec<float> X0;
+  load_rows(data, on_device, n, d, ld, Dp, X0, st);
+  if (ix->normalize) normalize_rows(X0.p, n, D, Dp, st);
+  KnnState ks;
+  if (kind_uses_norms(ix->kind)) {
+    ks.norms.alloc((size_t)N, st);
+    compute_norms(X0.p, N, D, Dp, ks.norms.p, st);
+  }
+  RINND_CUDA(cudaStreamSynchronize(st));
+  double t0 = now_ms();
+  build_forest(X0.p, N, D, Dp, std::max(pin->n_trees, 0), leaf_size, pin->angular != 0, 200,
+               pin->random_seed, st, tmp, ix->forest);
+  RINND_CUDA(cudaStreamSynchronize(st));
+  double t1 = now_ms();
+  knn_init(ks, N, k, c, st);
+  leaf_init(ks, ix->forest, X0.p, D, Dp, ix->kind, st);
+  RINND_CUDA(cudaStreamSynchronize(st));
+  double t2 = now_ms();
+  const size_t conv = (size_t)(pin->delta * (float)k * (float)N);  // mod.rs:157
+  uint64_t pairs_total = 0, pushes_total = 0;
+  double ms_cand = 0, ms_join = 0;
+  int iters = 0;
+  for (int it = 0; it < n_iters; ++it) {
+    iters = it + 1;
+    double a = now_ms();
+    build_candidates(ks, pin->random_seed, it, st);
+    RINND_CUDA(cudaStreamSynchronize(st));
+    double b = now_ms();
+    unsigned long long pairs = 0;
+    unsigned long long changes = local_join(ks, X0.p, D, Dp, ix->kind, st, &pairs);
+    double e = now_ms();
+    ms_cand += b - a;
+    ms_join += e - b;
+    pairs_total += pairs;
+    pushes_total += changes;
+    if (pin->verbose) std::printf("Iteration %d: %llu updates (%llu pairs)\n", it + 1, changes, pairs);
+    if ((size_t)changes <= conv) break;
+  }
+  double t3 = now_ms();
+  // sorted kNN rows (index.rs:653)
+  DVec<int32_t> knn_idx((size_t)N * k, st);
+  DVec<float> knn_raw((size_t)N * k, st);
+  finalize_knn(ks, knn_idx.p, knn_raw.p, st);
+  unsigned long long hc[4];
+  RINND_CUDA(cudaMemcpyAsync(hc, ks.counters.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+  ks = KnnState();  // release heap and candidate rows
+  RINND_CUDA(cudaStreamSynchronize(st));
+  double t4 = now_ms();
+  // diversified CSR (index.rs:656-666) on the original order
+  float min_d = 0.f;
+  build_search_graph(knn_idx.p, knn_raw.p, X0.p, N, k, D, Dp, ix->kind, pin->pruning_degree_multiplier, st,
+                     tmp, ix->graph_orig, &min_d);
+  ix->min_distance = min_d;
+  // corrected neighbor distances (index.rs:669-673)
+  apply_correction_dev(knn_raw.p, (int64_t)N * k, ix->corr, st);
+  ix->knn_idx = std::move(knn_idx);
+  ix->knn_dist = std::move(knn_raw);
+  // vertex order = first retained tree's leaf order (index.rs:679-715)
+  ix->n_search_trees = std::min(std::max(pin->n_search_trees, 0), std::max(pin->n_trees, 0));
+  ix->vertex_order.alloc((size_t)N, st);
+  if (ix->n_search_trees > 0) {
+    RINND_CUDA(cudaMemcpyAsync(ix->vertex_order.p, ix->forest.perm.p, sizeof(int32_t) * N,
+                               cudaMemcpyDeviceToDevice, st));
+  } else {
+    k_iota<<<grid_for(N, 256), 256, 0, st>>>(ix->vertex_order.p, N);
+    RINND_LAUNCH_CHECK();
+  }
+  ix->inverse.alloc((size_t)N, st);
+  invert_permutation(ix->vertex_order.p, N, ix->inverse.p, st);
+  ix->X.alloc((size_t)N * Dp, st);
+  gather_rows(X0.p, ix->vertex_order.p, N, Dp, ix->X.p, st);
+  X0.release();
+  reorder_csr(ix->graph_orig, ix->vertex_order.p, ix->inverse.p, st, tmp, ix->graph_int);
+  if (ix->n_search_trees > 0) {
+    long long tot = (long long)ix->n_search_trees * N;
+    ix->tree_idx.alloc((size_t)tot, st);
+    k_tree_idx<<<grid_for(tot, 256, 148 * 64), 256, 0, st>>>(ix->forest.perm.p, ix->inverse.p, tot,
+                                                              ix->tree_idx.p);
+    RINND_LAUNCH_CHECK();
+    std::vector<int32_t> roots(ix->n_search_trees);
+    for (int t = 0; t < ix->n_search_trees; ++t) roots[t] = t;
+    ix->tree_roots.alloc(roots.size(), st);
+    ix->tree_roots.from_host(roots.data(), roots.size());
+  }
+  ix->forest.perm.release();
+  ix->forest.leaves.release();
+  ix->search_stats.alloc(4, st);
+  ix->search_stats.fill_bytes(0);
+  RINND_CUDA(cudaStreamSynchronize(st));
+  double t5 = now_ms();
+  rinnd_build_info& inf = ix->info;
+  inf.iterations = iters;
+  inf.forest_levels = ix->forest.levels;
+  inf.n_leaves = ix->forest.n_leaves;
+  inf.ms_forest = t1 - t0;
+  inf.ms_leaf_init = t2 - t1;
+  inf.ms_iterations = t3 - t2;
+  inf.ms_candidates = ms_cand;
+  inf.ms_join = ms_join;
+  inf.ms_sort = t4 - t3;
+  inf.ms_graph = t5 - t4;
+  inf.ms_total = t5 - t_start;
+  inf.pairs_evaluated = pairs_total;
+  inf.pushes_accepted = pushes_total;
+  inf.push_contention = hc[1];
+  inf.search_graph_nnz = ix->graph_orig.nnz;
+  inf.min_distance = ix->min_distance;
+  *out = ix.release();
+}
+
+void check_index(const rinnd_index* idx) { require(idx != nullptr, "index must not be null"); }
+
+void query_impl(rinnd_index* ix, const float* q, bool on_device, int64_t nq, int64_t ld, int k, float eps,
+                uint64_t qid_base, int32_t* out_idx, float* out_dist, bool out_device, cudaStream_t user_st) {
+  check_index(ix);
+  require(nq >= 0, "number of queries must be >= 0");
+  require(k >= 1 && k <= 256, "k must be in [1, 256]");
+  if (nq == 0) return;
+  require(q != nullptr && out_idx != nullptr && out_dist != nullptr, "query/output pointers must not be null");
+  std::lock_guard<std::mutex> lock(ix->mu);
+  RINND_CUDA(cudaSetDevice(ix->device));
+  cudaStream_t st = user_st ? user_st : ix->st;
+  DVec<float> Q;
+  load_rows(q, on_device, nq, ix->D, ld, ix->Dp, Q, st);
+  if (ix->normalize) normalize_rows(Q.p, nq, ix->D, ix->Dp, st);
+  SearchIndex sv = ix->search_view();
+  if (out_device) {
+    greedy_search(sv, Q.p, (int)nq, k, eps, qid_base, out_idx, out_dist, st, ix->search_stats.p);
+  } else {
+    DVec<int32_t> oi((size_t)nq * k, st);
+    DVec<float> od((size_t)nq * k, st);
+    greedy_search(sv, Q.p, (int)nq, k, eps, qid_base, oi.p, od.p, st, ix->search_stats.p);
+    oi.to_host(out_idx, (size_t)nq * k);
+    od.to_host(out_dist, (size_t)nq * k);
+    RINND_CUDA(cudaStreamSynchronize(st));
+  }
+  Q.release();
+}
+
+}  // namespace
+
+extern "C" {
+
+int rinnd_params_default(rinnd_build_params* p) {
+  if (!p) return fail(RINND_ERR_INVALID, "params must not be null");
+  std::memset(p, 0, sizeof(*p));
+  p->n_neighbors = 30;  // index.rs:475-494
+  p->n_trees = 8;
+  p->n_search_trees = 1;
+  p->search_tree_leaf_budget = 1;
+  p->delta = 0.001f;
+  p->random_seed = 42;
+  p->diversify_prob = 1.0f;
+  p->pruning_degree_multiplier = 1.5f;
+  p->distance_kind = RINND_DIST_SQEUCLIDEAN;
+  p->correction = RINND_CORR_SQRT;
+  return RINND_OK;
+}
+
+int rinnd_build(const float* data, int64_t n, int32_t d, const rinnd_build_params* p, rinnd_index** out) {
+  return guarded([&] { build_impl(data, false, n, d, d, p, out); });
+}
+
+int rinnd_build_device(const float* d_data, int64_t n, int32_t d, int64_t ld, const rinnd_build_params* p,
+                       rinnd_index** out) {
+  return guarded([&] { build_impl(d_data, true, n, d, ld, p, out); });
+}
+
+int rinnd_free(rinnd_index* idx) {
+  return guarded([&] {
+    if (idx) {
+      cudaSetDevice(idx->device);
+      delete idx;
+    }
+  });
+}
+
+int rinnd_build_info_get(const rinnd_index* idx, rinnd_build_info* info) {
+  return guarded([&] {
+    check_index(idx);
+    require(info != nullptr, "info must not be null");
+    *info = idx->info;
+  });
+}
+
+int rinnd_index_shape(const rinnd_index* idx, int64_t* n, int32_t* d, int32_t* k) {
+  return guarded([&] {
+    check_index(idx);
+    if (n) *n = idx->N;
+    if (d) *d = idx->D;
+    if (k) *k = idx->k;
+  });
+}
+
+int rinnd_query(rinnd_index* idx, const float* queries, int64_t nq, int32_t k, float epsilon,
+                int32_t* out_idx, float* out_dist) {
+  return guarded([&] {
+    check_index(idx);
+    query_impl(idx, queries, false, nq, idx->D, k, epsilon, 0, out_idx, out_dist, false, nullptr);
+  });
+}
+
+int rinnd_query_one(rinnd_index* idx, const float* query, int32_t k, float epsilon, int32_t* out_idx,
+                    float* out_dist) {
+  return guarded([&] {
+    check_index(idx);
+    query_impl(idx, query, false, 1, idx->D, k, epsilon, 0, out_idx, out_dist, false, nullptr);
+  });
+}
+
+int rinnd_query_device(rinnd_index* idx, const float* d_queries, int64_t nq, int64_t ld, int32_t k,
+                       float epsilon, uint64_t qid_base, int32_t* d_out_idx, float* d_out_dist, void* stream) {
+  return guarded([&] {
+    check_index(idx);
+    require(ld >= idx->D, "query row stride must be >= dimension");
+    query_impl(idx, d_queries, true, nq, ld, k, epsilon, qid_base, d_out_idx, d_out_dist, true,
+               reinterpret_cast<cudaStream_t>(stream));
+  });
+}
+
+int rinnd_neighbor_graph(const rinnd_index* idx, int32_t* out_idx, float* out_dist) {
+  return guarded([&] {
+    check_index(idx);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    size_t nk = (size_t)idx->N * idx->k;
+    if (out_idx) idx->knn_idx.to_host(out_idx, nk);
+    if (out_dist) idx->knn_dist.to_host(out_dist, nk);
+    RINND_CUDA(cudaStreamSynchronize(idx->st));
+  });
+}
+
+int rinnd_search_graph_nnz(const rinnd_index* idx, int64_t* nnz) {
+  return guarded([&] {
+    check_index(idx);
+    require(nnz != nullptr, "nnz must not be null");
+    *nnz = idx->graph_orig.nnz;
+  });
+}
+
+int rinnd_search_graph(const rinnd_index* idx, int32_t* indptr, int32_t* indices, float* min_distance) {
+  return guarded([&] {
+    check_index(idx);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    if (indptr) idx->graph_orig.indptr.to_host(indptr, (size_t)idx->N + 1);
+    if (indices) idx->graph_orig.indices.to_host(indices, (size_t)idx->graph_orig.nnz);
+    if (min_distance) *min_distance = idx->min_distance;
+    RINND_CUDA(cudaStreamSynchronize(idx->st));
+  });
+}
+
+int rinnd_vertex_order(const rinnd_index* idx, int32_t* out) {
+  return guarded([&] {
+    check_index(idx);
+    require(out != nullptr, "out must not be null");
+    RINND_CUDA(cudaSetDevice(idx->device));
+    idx->vertex_order.to_host(out, (size_t)idx->N);
+    RINND_CUDA(cudaStreamSynchronize(idx->st));
+  });
+}
+
+int rinnd_storage_info_get(const rinnd_index* idx, rinnd_storage_info* info) {
+  return guarded([&] {
+    check_index(idx);
+    require(info != nullptr, "info must not be null");
+    std::memset(info, 0, sizeof(*info));
+    static const char* names[] = {"int8_per_vector_cosine", "sq8u_global_symmetric", "sq8p_per_vector_symmetric"};
+    const char* enc = idx->encoding >= 0 ? names[idx->encoding] : "fp32";
+    std::snprintf(info->encoding, sizeof(info->encoding), "%s", enc);
+    if (idx->encoding >= 0) {
+      info->code_bytes = (int64_t)idx->N * idx->D;
+      info->metadata_bytes = (int64_t)idx->N * 4;
+      info->retained_fp32_bytes = (int64_t)idx->N * idx->D * 4 + (int64_t)idx->N * idx->k * 4;
+      info->encode_seconds = idx->encode_seconds;
+    } else {
+      info->code_bytes = (int64_t)idx->N * idx->D * 4;
+    }
+    info->device_bytes = (int64_t)(idx->X.n * 4 + idx->graph_int.indices.n * 4 + idx->graph_orig.indices.n * 4 +
+                                   idx->knn_idx.n * 4 + idx->knn_dist.n * 4 + idx->codes.n + idx->inv_norms.n * 4 +
+                                   idx->forest.hyperplanes.n * 4 + idx->tree_idx.n * 4);
+  });
+}
+
+int rinnd_distance_pairs(int32_t kind, const float* a, const float* b, int64_t n_pairs, int32_t d, float* out) {
+  return guarded([&] {
+    require(kind >= 0 && kind < DK_COUNT, "unknown distance kind");
+    require(d >= 1 && n_pairs >= 0, "invalid shape");
+    if (n_pairs == 0) return;
+    require(a && b && out, "pointers must not be null");
+    ensure_device(0);
+    StreamGuard sg;
+    int Dp = round_up(d, 4);
+    DVec<float> A, B;
+    load_rows(a, false, n_pairs, d, d, Dp, A, sg.s);
+    load_rows(b, false, n_pairs, d, d, Dp, B, sg.s);
+    DVec<float> O((size_t)n_pairs, sg.s);
+    distance_pairs(kind, A.p, B.p, n_pairs, d, Dp, O.p, sg.s);
+    O.to_host(out, (size_t)n_pairs);
+    RINND_CUDA(cudaStreamSynchronize(sg.s));
+  });
+}
+
+int rinnd_search_graph_from_knn(const int32_t* knn_idx, const float* knn_dist, const float* data, int32_t n,
+                                int32_t k, int32_t d, int32_t kind, float mult, int32_t* indptr,
+                                int32_t* indices, int64_t* nnz, float* min_distance) {
+  return guarded([&] {
+    require(n >= 1 && k >= 1 && d >= 1, "invalid shape");
+    require(kind >= 0 && kind < DK_COUNT, "unknown distance kind");
+    require(knn_idx && knn_dist && data && indptr && indices, "pointers must not be null");
+    ensure_device(0);
+    StreamGuard sg;
+    cudaStream_t st = sg.s;
+    int Dp = round_up(d, 4);
+    DVec<float> X;
+    load_rows(data, false, n, d, d, Dp, X, st);
+    DVec<int32_t> ki((size_t)n * k, st);
+    DVec<float> kd((size_t)n * k, st);
+    ki.from_host(knn_idx, (size_t)n * k);
+    kd.from_host(knn_dist, (size_t)n * k);
+    TempStorage tmp;
+    Csr g;
+    float md = 0.f;
+    build_search_graph(ki.p, kd.p, X.p, n, k, d, Dp, kind, mult, st, tmp, g, &md);
+    g.indptr.to_host(indptr, (size_t)n + 1);
+    g.indices.to_host(indices, (size_t)g.nnz);
+    RINND_CUDA(cudaStreamSynchronize(st));
+    if (nnz) *nnz = g.nnz;
+    if (min_distance) *min_distance = md;
+  });
+}
+
+int rinnd_heap_push_batch(int32_t n, int32_t k, int64_t n_ops, const int32_t* rows, const int32_t* ids,
+                          const float* dists, const uint8_t* flags, int32_t* out_idx, float* out_dist,
+                          uint8_t* out_flags, int64_t* n_accepted) {
+  return guarded([&] {
+    require(n >= 1 && k >= 1 && k <= 512 && n_ops >= 0, "invalid shape");
+    require(out_idx && out_dist, "output pointers must not be null");
+    std::vector<int32_t> hr(rows, rows + n_ops), hi(ids, ids + n_ops);
+    for (int64_t i = 0; i < n_ops; ++i) {
+      require(hr[(size_t)i] >= 0 && hr[(size_t)i] < n, "push row out of range");
+      require(hi[(size_t)i] >= 0 && hi[(size_t)i] < INT32_MAX - 1, "push id out of range");
+    }
+    ensure_device(0);
+    StreamGuard sg;
+    cudaStream_t st = sg.s;
+    KnnState s;
+    knn_init(s, n, k, 1, st);
+    DVec<int32_t> dr((size_t)std::max<int64_t>(n_ops, 1), st), di((size_t)std::max<int64_t>(n_ops, 1), st);
+    DVec<float> dd((size_t)std::max<int64_t>(n_ops, 1), st);
+    DVec<uint8_t> df((size_t)std::max<int64_t>(n_ops, 1), st);
+    dr.from_host(rows, (size_t)n_ops);
+    di.from_host(ids, (size_t)n_ops);
+    dd.from_host(dists, (size_t)n_ops);
+    if (flags) df.from_host(flags, (size_t)n_ops);
+    else df.fill_bytes(0);
+    unsigned long long acc = n_ops ? heap_push_batch(s, n_ops, dr.p, di.p, dd.p, df.p, st) : 0ull;
+    DVec<int32_t> oi((size_t)n * k, st);
+    DVec<float> od((size_t)n * k, st);
+    DVec<uint8_t> of((size_t)n * k, st);
+    finalize_rows(s.slots.p, n, k, oi.p, od.p, of.p, st);
+    oi.to_host(out_idx, (size_t)n * k);
+    od.to_host(out_dist, (size_t)n * k);
+    if (out_flags) of.to_host(out_flags, (size_t)n * k);
+    RINND_CUDA(cudaStreamSynchronize(st));
+    if (n_accepted) *n_accepted = (int64_t)acc;
+  });
+}
+
+const char* rinnd_last_error(void) { return g_last_error.c_str(); }
+
+const char* rinnd_version(void) { return "0.1.0-b200"; }
+
+int rinnd_device_count(int32_t* count) {
+  return guarded([&] {
+    require(count != nullptr, "count must not be null");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      n = 0;
+    }
+    *count = n;
+  });
+}
+
+int rinnd_quantize(rinnd_index* idx, int32_t encoding) {
+  return fail(RINND_ERR_INVALID, "int8 quantization is not available in this build");
+}
+
+int rinnd_query_quantized(rinnd_index* idx, const float* queries, int64_t nq, int32_t k, float epsilon,
+                          int32_t candidate_width, int32_t rerank_width, int32_t* out_idx, float* out_dist) {
+  return fail(RINND_ERR_INVALID, "int8 quantization is not available in this build");
+}
+
+}  // extern "C"

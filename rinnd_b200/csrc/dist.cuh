@@ -1,0 +1,238 @@
+// dist.cuh -- per-pair distance functions.
+//
+// The `exact_*` functions reproduce the reference's AVX2+FMA code path
+// bit-for-bit: eight (or 4x8) FMA lanes over chunks of 8 (or 32) elements, the
+// same horizontal-sum tree, and a separately rounded multiply-add remainder
+// (__fmul_rn/__fadd_rn prevent contraction).  They are used wherever an
+// individual distance decides a comparison the reference makes: the pair
+// distance kernel, RNG-style diversification, tree margins and graph search.
+//
+// References (core/ = crates/rinnd-core/src/):
+//   sqeuclidean core/distance/euclidean.rs:66-110
+//   manhattan   core/distance/minkowski.rs:57-83
+//   cosine      core/distance/cosine.rs:41-80
+//   alt cosine  core/distance/alternatives.rs:207-226
+//   alt dot / direct normalized cosine  alternatives.rs:38-150 (normalized_dot_avx2)
+//   inner product  core/distance/inner_product.rs:61-101
+//   alt inner product  alternatives.rs:163-187
+#pragma once
+#include "common.cuh"
+
+namespace rinnd {
+
+// euclidean.rs:95-110 hsum256_ps_avx
+__device__ __forceinline__ float hsum_a(const float* s) {
+  float a0 = __fadd_rn(s[4], s[0]), a1 = __fadd_rn(s[5], s[1]);
+  float a2 = __fadd_rn(s[6], s[2]), a3 = __fadd_rn(s[7], s[3]);
+  return __fadd_rn(__fadd_rn(a0, a1), __fadd_rn(a2, a3));
+}
+// alternatives.rs:92-103 horizontal_sum_avx
+__device__ __forceinline__ float hsum_b(const float* s) {
+  float a0 = __fadd_rn(s[0], s[4]), a1 = __fadd_rn(s[1], s[5]);
+  float a2 = __fadd_rn(s[2], s[6]), a3 = __fadd_rn(s[3], s[7]);
+  return __fadd_rn(__fadd_rn(a0, a2), __fadd_rn(a1, a3));
+}
+
+// Rows are 16-byte aligned (row stride is a multiple of 4 floats), so each
+// chunk of 8 is read as two float4 loads.
+__device__ __forceinline__ void load8(const float* p, float* v) {
+  float4 x = *reinterpret_cast<const float4*>(p);
+  float4 y = *reinterpret_cast<const float4*>(p + 4);
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+}
+
+__device__ __forceinline__ float exact_sqeuclid(const float* a, const float* b, int n) {
+  float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int chunks = n >> 3;
+  for (int c = 0; c < chunks; ++c) {
+    float x[8], y[8];
+    load8(a + 8 * c, x);
+    load8(b + 8 * c, y);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+      float d = __fsub_rn(x[l], y[l]);
+      s[l] = __fmaf_rn(d, d, s[l]);
+    }
+  }
+  float r = hsum_a(s);
+  for (int i = chunks * 8; i < n; ++i) {
+    float d = __fsub_rn(a[i], b[i]);
+    r = __fadd_rn(r, __fmul_rn(d, d));
+  }
+  return r;
+}
+
+__device__ __forceinline__ float exact_manhattan(const float* a, const float* b, int n) {
+  float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int chunks = n >> 3;
+  for (int c = 0; c < chunks; ++c) {
+    float x[8], y[8];
+    load8(a + 8 * c, x);
+    load8(b + 8 * c, y);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) s[l] = __fadd_rn(s[l], fabsf(__fsub_rn(x[l], y[l])));
+  }
+  float r = hsum_a(s);
+  for (int i = chunks * 8; i < n; ++i) r = __fadd_rn(r, fabsf(__fsub_rn(a[i], b[i])));
+  return r;
+}
+
+__device__ __forceinline__ float exact_dot_a(const float* a, const float* b, int n) {
+  float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int chunks = n >> 3;
+  for (int c = 0; c < chunks; ++c) {
+    float x[8], y[8];
+    load8(a + 8 * c, x);
+    load8(b + 8 * c, y);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) s[l] = __fmaf_rn(x[l], y[l], s[l]);
+  }
+  float r = hsum_a(s);
+  for (int i = chunks * 8; i < n; ++i) r = __fadd_rn(r, __fmul_rn(a[i], b[i]));
+  return r;
+}
+
+__device__ __forceinline__ float exact_dot_b(const float* a, const float* b, int n) {
+  float t0[8] = {0, 0, 0, 0, 0, 0, 0, 0}, t1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  float t2[8] = {0, 0, 0, 0, 0, 0, 0, 0}, t3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int chunks = n >> 5;
+  for (int c = 0; c < chunks; ++c) {
+    const float* pa = a + 32 * c;
+    const float* pb = b + 32 * c;
+    float x[8], y[8];
+    load8(pa, x); load8(pb, y);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) t0[l] = __fmaf_rn(x[l], y[l], t0[l]);
+    load8(pa + 8, x); load8(pb + 8, y);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) t1[l] = __fmaf_rn(x[l], y[l], t1[l]);
+    load8(pa + 16, x); load8(pb + 16, y);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) t2[l] = __fmaf_rn(x[l], y[l], t2[l]);
+    load8(pa + 24, x); load8(pb + 24, y);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) t3[l] = __fmaf_rn(x[l], y[l], t3[l]);
+  }
+  float s[8];
+#pragma unroll
+  for (int l = 0; l < 8; ++l) s[l] = __fadd_rn(__fadd_rn(t0[l], t1[l]), __fadd_rn(t2[l], t3[l]));
+  float r = hsum_b(s);
+  for (int i = chunks * 32; i < n; ++i) r = __fadd_rn(r, __fmul_rn(a[i], b[i]));
+  return r;
+}
+
+__device__ __forceinline__ float exact_dot_c(const float* a, const float* b, int n) {
+  float dot = 0.f;
+  int chunks = n >> 2;
+  for (int c = 0; c < chunks; ++c) {
+    float4 x = *reinterpret_cast<const float4*>(a + 4 * c);
+    float4 y = *reinterpret_cast<const float4*>(b + 4 * c);
+    float p = __fmul_rn(x.x, y.x);
+    p = __fadd_rn(p, __fmul_rn(x.y, y.y));
+    p = __fadd_rn(p, __fmul_rn(x.z, y.z));
+    p = __fadd_rn(p, __fmul_rn(x.w, y.w));
+    dot = __fadd_rn(dot, p);
+  }
+  for (int i = chunks * 4; i < n; ++i) dot = __fadd_rn(dot, __fmul_rn(a[i], b[i]));
+  return dot;
+}
+
+__device__ __forceinline__ float exact_cosine(const float* a, const float* b, int n) {
+  float sd[8] = {0, 0, 0, 0, 0, 0, 0, 0}, sa[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  float sb[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int chunks = n >> 3;
+  for (int c = 0; c < chunks; ++c) {
+    float x[8], y[8];
+    load8(a + 8 * c, x);
+    load8(b + 8 * c, y);
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+      sd[l] = __fmaf_rn(x[l], y[l], sd[l]);
+      sa[l] = __fmaf_rn(x[l], x[l], sa[l]);
+      sb[l] = __fmaf_rn(y[l], y[l], sb[l]);
+    }
+  }
+  float dot = hsum_a(sd), na = hsum_a(sa), nb = hsum_a(sb);
+  for (int i = chunks * 8; i < n; ++i) {
+    dot = __fadd_rn(dot, __fmul_rn(a[i], b[i]));
+    na = __fadd_rn(na, __fmul_rn(a[i], a[i]));
+    nb = __fadd_rn(nb, __fmul_rn(b[i], b[i]));
+  }
+  float denom = __fsqrt_rn(__fmul_rn(na, nb));
+  if (denom < 1e-12f) return 1.0f;
+  float sim = fminf(fmaxf(__fdiv_rn(dot, denom), -1.0f), 1.0f);
+  return __fsub_rn(1.0f, sim);
+}
+
+__device__ __forceinline__ float exact_alt_cosine(const float* a, const float* b, int n) {
+  float dot = 0.f, na = 0.f, nb = 0.f;
+  for (int i = 0; i < n; ++i) {
+    dot = __fadd_rn(dot, __fmul_rn(a[i], b[i]));
+    na = __fadd_rn(na, __fmul_rn(a[i], a[i]));
+    nb = __fadd_rn(nb, __fmul_rn(b[i], b[i]));
+  }
+  if (na == 0.f && nb == 0.f) return 0.f;
+  if (na == 0.f || nb == 0.f) return FLT_MAX;
+  if (dot <= 0.f) return FLT_MAX;
+  return log2f(__fdiv_rn(__fsqrt_rn(__fmul_rn(na, nb)), dot));
+}
+
+// Dispatch.  `n` is the true dimension; rows may be padded beyond it.
+__device__ __forceinline__ float exact_distance(int kind, const float* a, const float* b, int n) {
+  switch (kind) {
+    case DK_SQEUCLIDEAN: return exact_sqeuclid(a, b, n);
+    case DK_MANHATTAN: return exact_manhattan(a, b, n);
+    case DK_COSINE: return exact_cosine(a, b, n);
+    case DK_ALT_COSINE: return exact_alt_cosine(a, b, n);
+    case DK_ALT_DOT: {
+      float dot = exact_dot_b(a, b, n);
+      return dot <= 0.f ? FLT_MAX : -log2f(dot);
+    }
+    case DK_DIRECT_COSINE: {
+      float dot = exact_dot_b(a, b, n);
+      return __fsub_rn(1.0f, fminf(fmaxf(dot, -1.0f), 1.0f));
+    }
+    case DK_INNER_PRODUCT: return -exact_dot_a(a, b, n);
+    case DK_ALT_INNER_PRODUCT: {
+      float dot = exact_dot_c(a, b, n);
+      return dot <= 0.f ? FLT_MAX : __fdiv_rn(1.0f, dot);
+    }
+  }
+  return __int_as_float(0x7fc00000);
+}
+
+// Metrics evaluated from (dot, |a|^2, |b|^2) in the tiled join kernels.
+__device__ __forceinline__ bool kind_is_dot(int kind) {
+  return kind != DK_SQEUCLIDEAN && kind != DK_MANHATTAN;
+}
+__device__ __forceinline__ float finalize_dot(int kind, float dot, float na, float nb) {
+  switch (kind) {
+    case DK_COSINE: {
+      float denom = sqrtf(na * nb);
+      if (denom < 1e-12f) return 1.0f;
+      return 1.0f - fminf(fmaxf(dot / denom, -1.0f), 1.0f);
+    }
+    case DK_ALT_COSINE:
+      if (na == 0.f && nb == 0.f) return 0.f;
+      if (na == 0.f || nb == 0.f || dot <= 0.f) return FLT_MAX;
+      return log2f(sqrtf(na * nb) / dot);
+    case DK_ALT_DOT: return dot <= 0.f ? FLT_MAX : -log2f(dot);
+    case DK_DIRECT_COSINE: return 1.0f - fminf(fmaxf(dot, -1.0f), 1.0f);
+    case DK_INNER_PRODUCT: return -dot;
+    case DK_ALT_INNER_PRODUCT: return dot <= 0.f ? FLT_MAX : 1.0f / dot;
+  }
+  return dot;
+}
+
+// alternatives.rs:273-287, index.rs:587
+__host__ __device__ __forceinline__ float apply_correction(int corr, float d) {
+  switch (corr) {
+    case CK_SQRT: return sqrtf(d);
+    case CK_ALT_COSINE: return 1.0f - exp2f(-d);
+    case CK_ALT_IP: return d >= FLT_MAX ? 0.0f : -1.0f / d;
+  }
+  return d;
+}
+
+}  // namespace rinnd

@@ -1,0 +1,119 @@
+// engine.h -- internal interfaces between the kernel files and the C ABI layer.
+#pragma once
+#include <stdint.h>
+
+#include "devmem.cuh"
+
+namespace rinnd {
+
+// ---- RP forest (forest.cu) -------------------------------------------------
+// Level-synchronous batched construction of all trees at once.  Node ids are
+// global across the forest; roots are 0..T-1.  children[2*node] = {left,right}
+// for internal nodes (always > 0) and {-start, -end} (positions within the
+// tree's `perm` slice) for leaves, the reference FlatTree encoding
+// (core/tree/flat_tree.rs:14-28).
+struct Forest {
+  int T = 0, N = 0, Dp = 0;
+  DVec<int32_t> perm;         // T*N, leaf order per tree
+  DVec<int32_t> children;     // 2 * n_nodes
+  DVec<float> offsets;        // n_nodes
+  DVec<float> hyperplanes;    // n_nodes * Dp (zeros for leaves)
+  DVec<int4> leaves;          // (tree, start, end, node)
+  int64_t n_nodes = 0;
+  int64_t n_leaves = 0;
+  int max_leaf = 0;
+  int levels = 0;
+};
+void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bool angular,
+                  int max_depth, uint64_t seed, cudaStream_t st, TempStorage& tmp, Forest& out);
+
+// ---- NN-Descent (nndescent.cu) ---------------------------------------------
+struct BuildStats {
+  int iterations = 0;
+  unsigned long long changes[64] = {};
+  unsigned long long pairs[64] = {};
+  unsigned long long contention = 0;
+  double ms_forest = 0, ms_leaf = 0, ms_iters = 0, ms_sort = 0, ms_graph = 0, ms_total = 0;
+  double ms_candidates = 0, ms_join = 0;
+};
+
+struct KnnState {
+  int N = 0, k = 0, c = 0;
+  DVec<uint64_t> slots;      // N*k neighbor slots
+  DVec<uint32_t> thr;        // N upper bounds of fkey(row max)
+  DVec<uint64_t> cand_new;   // N*c
+  DVec<uint64_t> cand_old;   // N*c
+  DVec<float> norms;         // N squared norms (dot-form metrics)
+  DVec<unsigned long long> counters;  // [0] changes, [1] contention, [2] pairs
+};
+
+void knn_init(KnnState& s, int N, int k, int c, cudaStream_t st);
+void compute_norms(const float* X, int N, int D, int Dp, float* norms, cudaStream_t st);
+void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int kind,
+               cudaStream_t st);
+void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st);
+unsigned long long local_join(KnnState& s, const float* X, int D, int Dp, int kind,
+                              cudaStream_t st, unsigned long long* pairs_out);
+// Sorted output: idx (-1 empty), raw distance (+inf empty).
+void finalize_knn(const KnnState& s, int32_t* out_idx, float* out_dist, cudaStream_t st);
+void finalize_rows(const uint64_t* slots, int N, int k, int32_t* out_idx, float* out_dist,
+                   uint8_t* out_flags, cudaStream_t st);
+unsigned long long heap_push_batch(KnnState& s, long long n_ops, const int32_t* rows,
+                                   const int32_t* ids, const float* dists, const uint8_t* flags,
+                                   cudaStream_t st);
+
+// ---- search graph (graph.cu) -----------------------------------------------
+struct Csr {
+  int N = 0;
+  DVec<int32_t> indptr;   // N+1
+  DVec<int32_t> indices;  // nnz
+  int64_t nnz = 0;
+};
+// search_graph.rs:263-360 from a sorted dense kNN graph (raw distances).
+void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const float* X, int N,
+                        int k, int D, int Dp, int kind, float mult, cudaStream_t st,
+                        TempStorage& tmp, Csr& out, float* min_distance_host);
+// search_graph.rs:199-229: row new_v = old row order[new_v], neighbors mapped by inverse.
+void reorder_csr(const Csr& in, const int32_t* order, const int32_t* inverse, cudaStream_t st,
+                 TempStorage& tmp, Csr& out);
+
+// ---- greedy search (search.cu) ----------------------------------------------
+struct SearchIndex {
+  int N = 0, D = 0, Dp = 0, kind = 0, corr = 0;
+  const float* X = nullptr;              // internal order, N x Dp
+  const int32_t* indptr = nullptr;
+  const int32_t* indices = nullptr;
+  float min_distance = 0.f;
+  int n_trees = 0;
+  const int32_t* tree_roots = nullptr;   // n_trees
+  const int32_t* children = nullptr;
+  const float* offsets = nullptr;
+  const float* hyperplanes = nullptr;
+  const int32_t* tree_idx = nullptr;     // n_trees * N leaf order (internal ids)
+  int leaf_budget = 1;
+  const int32_t* vertex_order = nullptr; // internal -> original id
+  uint64_t seed = 42;
+  // int8 codes (optional)
+  const int8_t* codes = nullptr;         // N x Dq (Dq = round_up(D,16))
+  const float* inv_norms = nullptr;
+  int Dq = 0;
+};
+struct SearchStats {
+  unsigned long long evals = 0, expansions = 0, visited_overflow = 0;
+};
+// Q: nq x Dp device queries.  Results already remapped to original ids.
+void greedy_search(const SearchIndex& ix, const float* Q, int nq, int k, float eps,
+                   uint64_t qid_base, int32_t* out_idx, float* out_dist, cudaStream_t st,
+                   unsigned long long* dstats);
+
+// ---- utilities (util.cu) ------------------------------------------------------
+void distance_pairs(int kind, const float* A, const float* B, int64_t n, int D, int Dp,
+                    float* out, cudaStream_t st);
+void pad_rows(const float* src, int64_t n, int D, int Dp, float* dst, cudaStream_t st);
+void gather_rows(const float* src, const int32_t* order, int64_t n, int Dp, float* dst,
+                 cudaStream_t st);
+void normalize_rows(float* X, int64_t n, int D, int Dp, cudaStream_t st);
+void invert_permutation(const int32_t* order, int N, int32_t* inverse, cudaStream_t st);
+void apply_correction_dev(float* d, int64_t n, int corr, cudaStream_t st);
+
+}  // namespace rinnd

@@ -1,0 +1,369 @@
+// graph.cu -- diversified, pruned CSR search graph.
+//
+// Restates SearchGraph::from_dense_diversified (core/graph/search_graph.rs:263-360):
+//   1. forward diversify every sorted kNN row (diversify_row :432-473): keep j
+//      unless a retained c has d_ic > f32::MIN_POSITIVE and d(c, j) < d_ij;
+//   2. transpose the forward rows with their distances (transpose_csr :526-567)
+//      and order each reverse row by (distance, source id);
+//   3. diversify the reverse rows (diversify_sorted_csr :478-523);
+//   4. union forward and reverse rows (weighted_union_pruned :368-426): drop
+//      -1, self loops and non-finite distances, merge duplicate ids with the
+//      max distance, keep the max_degree nearest by (distance, id), emit by id;
+//   5. min_distance = min forward distance (0 -> f32::EPSILON), :353-357.
+// With diversify_prob = 1 (the default) no randomness is involved and the
+// output equals the reference's for the same input graph: the d(c, j)
+// comparisons use the reference's exact accumulation order (dist.cuh), and the
+// reverse-row order (distance, then source id) equals the reference's whenever
+// a reverse row has no tied distances.
+#include <cub/cub.cuh>
+
+#include "dist.cuh"
+#include "engine.h"
+
+namespace rinnd {
+namespace {
+
+constexpr int WARPS = 4;
+
+// Warp-cooperative RNG-style prune step: does any retained c (in smem) prune j?
+__device__ __forceinline__ bool pruned_by_retained(const int32_t* ret_id, const float* ret_d, int nret,
+                                                   int32_t j, float dij, const float* X, int D,
+                                                   int Dp, int kind) {
+  const int lane = threadIdx.x & 31;
+  for (int r0 = 0; r0 < nret; r0 += 32) {
+    int r = r0 + lane;
+    bool pr = false;
+    if (r < nret) {
+      float dic = ret_d[r];
+      if (dic > FLT_MIN) {
+        float dcj = exact_distance(kind, X + (size_t)ret_id[r] * Dp, X + (size_t)j * Dp, D);
+        pr = dcj < dij;
+      }
+    }
+    if (__any_sync(0xffffffffu, pr)) return true;
+  }
+  return false;
+}
+
+template <int MAXR>
+__global__ void k_diversify_fwd(const int32_t* knn_idx, const float* knn_dist, int N, int k,
+                                const float* X, int D, int Dp, int kind, int max_degree,
+                                int32_t* fwd_idx, float* fwd_dist, int32_t* fwd_cnt,
+                                uint32_t* min_key) {
+  __shared__ int32_t s_id[WARPS][MAXR];
+  __shared__ float s_d[WARPS][MAXR];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * WARPS + w;
+  if (row >= N) return;
+  int nret = 0;
+  uint32_t local_min = KEY_INF;
+  for (int pos = 0; pos < k; ++pos) {
+    int32_t j = knn_idx[(size_t)row * k + pos];
+    if (j < 0) break;
+    float dij = knn_dist[(size_t)row * k + pos];
+    bool pruned = pruned_by_retained(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind);
+    if (!pruned) {
+      if (lane == 0) {
+        s_id[w][nret] = j;
+        s_d[w][nret] = dij;
+      }
+      __syncwarp();
+      ++nret;
+      float v = dij == 0.f ? FLT_EPSILON : dij;
+      if (isfinite(v)) local_min = min(local_min, fkey(v));
+      if (nret >= max_degree) break;
+    }
+  }
+  for (int r = lane; r < nret; r += 32) {
+    fwd_idx[(size_t)row * k + r] = s_id[w][r];
+    fwd_dist[(size_t)row * k + r] = s_d[w][r];
+  }
+  if (lane == 0) {
+    fwd_cnt[row] = nret;
+    if (local_min != KEY_INF) atomicMin(min_key, local_min);
+  }
+}
+
+__global__ void k_indegree(const int32_t* fwd_idx, const int32_t* fwd_cnt, int N, int k,
+                           int32_t* indeg) {
+  long long total = (long long)N * k;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(e / k), r = (int)(e % k);
+    if (r < fwd_cnt[i]) atomicAdd(&indeg[fwd_idx[e]], 1);
+  }
+}
+
+__global__ void k_transpose(const int32_t* fwd_idx, const float* fwd_dist, const int32_t* fwd_cnt,
+                            int N, int k, int32_t* cursor, uint64_t* rev_key) {
+  long long total = (long long)N * k;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(e / k), r = (int)(e % k);
+    if (r >= fwd_cnt[i]) continue;
+    int32_t j = fwd_idx[e];
+    int pos = atomicAdd(&cursor[j], 1);
+    rev_key[pos] = ((uint64_t)fkey(fwd_dist[e]) << 32) | (uint32_t)i;
+  }
+}
+
+template <int MAXR>
+__global__ void k_diversify_rev(const int32_t* rev_ptr, const uint64_t* rev_key, int N,
+                                const float* X, int D, int Dp, int kind, int max_degree,
+                                int32_t* rret_idx, float* rret_dist, int32_t* rret_cnt) {
+  __shared__ int32_t s_id[WARPS][MAXR];
+  __shared__ float s_d[WARPS][MAXR];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * WARPS + w;
+  if (row >= N) return;
+  int nret = 0;
+  for (int e = rev_ptr[row]; e < rev_ptr[row + 1]; ++e) {
+    uint64_t key = rev_key[e];
+    int32_t j = (int32_t)(uint32_t)key;
+    float dij = fkey_inv((uint32_t)(key >> 32));
+    bool pruned = pruned_by_retained(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind);
+    if (!pruned) {
+      if (lane == 0) {
+        s_id[w][nret] = j;
+        s_d[w][nret] = dij;
+      }
+      __syncwarp();
+      ++nret;
+      if (nret >= max_degree) break;
+    }
+  }
+  for (int r = lane; r < nret; r += 32) {
+    rret_idx[(size_t)row * max_degree + r] = s_id[w][r];
+    rret_dist[(size_t)row * max_degree + r] = s_d[w][r];
+  }
+  if (lane == 0) rret_cnt[row] = nret;
+}
+
+template <int P>
+__device__ __forceinline__ void warp_bitonic(uint64_t* b) {
+  const int lane = threadIdx.x & 31;
+  for (int size = 2; size <= P; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int j = lane; j < P; j += 32) {
+        int partner = j ^ stride;
+        if (partner > j) {
+          bool up = (j & size) == 0;
+          uint64_t x = b[j], y = b[partner];
+          if ((x > y) == up) {
+            b[j] = y;
+            b[partner] = x;
+          }
+        }
+      }
+      __syncwarp();
+    }
+}
+
+// search_graph.rs:368-426 weighted_union_pruned, one warp per vertex.
+template <int P>
+__global__ void k_union(const int32_t* fwd_idx, const float* fwd_dist, const int32_t* fwd_cnt, int k,
+                        const int32_t* rret_idx, const float* rret_dist, const int32_t* rret_cnt,
+                        int N, int max_degree, int32_t* out_idx, int32_t* out_cnt) {
+  __shared__ uint64_t buf[WARPS][P];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int v = blockIdx.x * WARPS + w;
+  if (v >= N) return;
+  uint64_t* b = buf[w];
+  const int nf = fwd_cnt[v], nr = rret_cnt[v];
+  // (id, distance) keys; dropped entries become ~0.
+  for (int e = lane; e < P; e += 32) {
+    uint64_t key = ~0ull;
+    int32_t id = -1;
+    float d = 0.f;
+    if (e < nf) {
+      id = fwd_idx[(size_t)v * k + e];
+      d = fwd_dist[(size_t)v * k + e];
+    } else if (e < nf + nr) {
+      id = rret_idx[(size_t)v * max_degree + (e - nf)];
+      d = rret_dist[(size_t)v * max_degree + (e - nf)];
+    }
+    if (id >= 0 && id != v && isfinite(d)) key = ((uint64_t)(uint32_t)id << 32) | fkey(d);
+    b[e] = key;
+  }
+  __syncwarp();
+  warp_bitonic<P>(b);
+  // keep the last (max distance) entry of each id run; re-key by (distance, id)
+  uint64_t nk[P / 32];
+#pragma unroll
+  for (int t = 0; t < P / 32; ++t) {
+    int e = t * 32 + lane;
+    uint64_t key = b[e];
+    uint64_t out = ~0ull;
+    if (key != ~0ull) {
+      uint64_t nxt = e + 1 < P ? b[e + 1] : ~0ull;
+      bool last = nxt == ~0ull || (nxt >> 32) != (key >> 32);
+      if (last) out = ((key & 0xFFFFFFFFull) << 32) | (key >> 32);
+    }
+    nk[t] = out;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < P / 32; ++t) b[t * 32 + lane] = nk[t];
+  __syncwarp();
+  warp_bitonic<P>(b);
+  // first max_degree valid entries, re-keyed by id
+#pragma unroll
+  for (int t = 0; t < P / 32; ++t) {
+    int e = t * 32 + lane;
+    uint64_t key = b[e];
+    nk[t] = (e < max_degree && key != ~0ull) ? (key & 0xFFFFFFFFull) : ~0ull;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < P / 32; ++t) b[t * 32 + lane] = nk[t];
+  __syncwarp();
+  warp_bitonic<P>(b);
+  int cnt = 0;
+#pragma unroll
+  for (int t = 0; t < P / 32; ++t) {
+    int e = t * 32 + lane;
+    uint64_t key = b[e];
+    bool valid = key != ~0ull;
+    cnt += __popc(__ballot_sync(0xffffffffu, valid));
+    if (valid) out_idx[(size_t)v * max_degree + e] = (int32_t)key;
+  }
+  if (lane == 0) out_cnt[v] = cnt;
+}
+
+__global__ void k_compact(const int32_t* rows, int width, const int32_t* cnt, const int32_t* ptr,
+                          int N, int32_t* out) {
+  long long total = (long long)N * width;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    int v = (int)(e / width), r = (int)(e % width);
+    if (r < cnt[v]) out[ptr[v] + r] = rows[e];
+  }
+}
+
+__global__ void k_reorder_count(const int32_t* in_ptr, const int32_t* order, int N, int32_t* cnt) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < N) cnt[v] = in_ptr[order[v] + 1] - in_ptr[order[v]];
+}
+__global__ void k_reorder_fill(const int32_t* in_ptr, const int32_t* in_idx, const int32_t* order,
+                               const int32_t* inverse, const int32_t* out_ptr, int N,
+                               int32_t* out_idx) {
+  int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= N) return;
+  int ov = order[w];
+  int s = in_ptr[ov], e = in_ptr[ov + 1], o = out_ptr[w];
+  for (int t = s + lane; t < e; t += 32) out_idx[o + (t - s)] = inverse[in_idx[t]];
+}
+
+template <class T>
+void exclusive_scan(const T* in, T* out, long long n, TempStorage& tmp, cudaStream_t st) {
+  size_t bytes = 0;
+  RINND_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, st));
+  void* p = tmp.ensure(bytes, st);
+  RINND_CUDA(cub::DeviceScan::ExclusiveSum(p, bytes, in, out, n, st));
+}
+
+}  // namespace
+
+void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const float* X, int N,
+                        int k, int D, int Dp, int kind, float mult, cudaStream_t st,
+                        TempStorage& tmp, Csr& out, float* min_distance_host) {
+  const int max_degree = (int)roundf(mult * (float)k);  // f32::round (:276)
+  if (k > 128 || max_degree < 1 || max_degree > 384)
+    throw std::invalid_argument("search graph supports n_neighbors <= 128 and 1 <= round(mult * k) <= 384");
+  const int blocks = (N + WARPS - 1) / WARPS;
+  DVec<int32_t> fwd_idx((size_t)N * k, st), fwd_cnt((size_t)N, st);
+  DVec<float> fwd_dist((size_t)N * k, st);
+  DVec<uint32_t> min_key(1, st);
+  RINND_CUDA(cudaMemcpyAsync(min_key.p, &KEY_INF, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  if (k <= 32)
+    k_diversify_fwd<32><<<blocks, 32 * WARPS, 0, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind,
+                                                      max_degree, fwd_idx.p, fwd_dist.p, fwd_cnt.p,
+                                                      min_key.p);
+  else
+    k_diversify_fwd<128><<<blocks, 32 * WARPS, 0, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind,
+                                                       max_degree, fwd_idx.p, fwd_dist.p, fwd_cnt.p,
+                                                       min_key.p);
+  RINND_LAUNCH_CHECK();
+  // transpose
+  DVec<int32_t> indeg((size_t)N + 1, st), rev_ptr((size_t)N + 1, st), cursor((size_t)N + 1, st);
+  indeg.fill_bytes(0);
+  k_indegree<<<grid_for((long long)N * k, 256, 148 * 64), 256, 0, st>>>(fwd_idx.p, fwd_cnt.p, N, k, indeg.p);
+  RINND_LAUNCH_CHECK();
+  exclusive_scan(indeg.p, rev_ptr.p, (long long)N + 1, tmp, st);
+  int32_t n_rev = 0;
+  RINND_CUDA(cudaMemcpyAsync(&n_rev, rev_ptr.p + N, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  RINND_CUDA(cudaMemcpyAsync(cursor.p, rev_ptr.p, sizeof(int32_t) * ((size_t)N + 1),
+                             cudaMemcpyDeviceToDevice, st));
+  RINND_CUDA(cudaStreamSynchronize(st));
+  DVec<uint64_t> rev_key((size_t)std::max(n_rev, 1), st), rev_sorted((size_t)std::max(n_rev, 1), st);
+  k_transpose<<<grid_for((long long)N * k, 256, 148 * 64), 256, 0, st>>>(fwd_idx.p, fwd_dist.p, fwd_cnt.p,
+                                                                        N, k, cursor.p, rev_key.p);
+  RINND_LAUNCH_CHECK();
+  if (n_rev > 0) {
+    size_t bytes = 0;
+    RINND_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, bytes, rev_key.p, rev_sorted.p, n_rev, N,
+                                                  rev_ptr.p, rev_ptr.p + 1, st));
+    void* p = tmp.ensure(bytes, st);
+    RINND_CUDA(cub::DeviceSegmentedSort::SortKeys(p, bytes, rev_key.p, rev_sorted.p, n_rev, N,
+                                                  rev_ptr.p, rev_ptr.p + 1, st));
+  }
+  DVec<int32_t> rret_idx((size_t)N * max_degree, st), rret_cnt((size_t)N, st);
+  DVec<float> rret_dist((size_t)N * max_degree, st);
+  if (max_degree <= 32)
+    k_diversify_rev<32><<<blocks, 32 * WARPS, 0, st>>>(rev_ptr.p, rev_sorted.p, N, X, D, Dp, kind,
+                                                      max_degree, rret_idx.p, rret_dist.p, rret_cnt.p);
+  else
+    k_diversify_rev<384><<<blocks, 32 * WARPS, 0, st>>>(rev_ptr.p, rev_sorted.p, N, X, D, Dp, kind,
+                                                       max_degree, rret_idx.p, rret_dist.p, rret_cnt.p);
+  RINND_LAUNCH_CHECK();
+  // union + prune
+  DVec<int32_t> rows((size_t)N * max_degree, st), cnt((size_t)N + 1, st);
+  RINND_CUDA(cudaMemsetAsync(cnt.p + N, 0, sizeof(int32_t), st));
+  int need = k + max_degree;
+  if (need <= 64)
+    k_union<64><<<blocks, 32 * WARPS, 0, st>>>(fwd_idx.p, fwd_dist.p, fwd_cnt.p, k, rret_idx.p,
+                                              rret_dist.p, rret_cnt.p, N, max_degree, rows.p, cnt.p);
+  else if (need <= 128)
+    k_union<128><<<blocks, 32 * WARPS, 0, st>>>(fwd_idx.p, fwd_dist.p, fwd_cnt.p, k, rret_idx.p,
+                                               rret_dist.p, rret_cnt.p, N, max_degree, rows.p, cnt.p);
+  else if (need <= 256)
+    k_union<256><<<blocks, 32 * WARPS, 0, st>>>(fwd_idx.p, fwd_dist.p, fwd_cnt.p, k, rret_idx.p,
+                                               rret_dist.p, rret_cnt.p, N, max_degree, rows.p, cnt.p);
+  else
+    k_union<512><<<blocks, 32 * WARPS, 0, st>>>(fwd_idx.p, fwd_dist.p, fwd_cnt.p, k, rret_idx.p,
+                                               rret_dist.p, rret_cnt.p, N, max_degree, rows.p, cnt.p);
+  RINND_LAUNCH_CHECK();
+  out.N = N;
+  out.indptr.alloc((size_t)N + 1, st);
+  exclusive_scan(cnt.p, out.indptr.p, (long long)N + 1, tmp, st);
+  int32_t nnz = 0;
+  uint32_t mk = KEY_INF;
+  RINND_CUDA(cudaMemcpyAsync(&nnz, out.indptr.p + N, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  RINND_CUDA(cudaMemcpyAsync(&mk, min_key.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  RINND_CUDA(cudaStreamSynchronize(st));
+  out.nnz = nnz;
+  out.indices.alloc((size_t)std::max(nnz, 1), st);
+  k_compact<<<grid_for((long long)N * max_degree, 256, 148 * 64), 256, 0, st>>>(rows.p, max_degree, cnt.p,
+                                                                               out.indptr.p, N, out.indices.p);
+  RINND_LAUNCH_CHECK();
+  *min_distance_host = fkey_inv(mk);
+}
+
+void reorder_csr(const Csr& in, const int32_t* order, const int32_t* inverse, cudaStream_t st,
+                 TempStorage& tmp, Csr& out) {
+  const int N = in.N;
+  out.N = N;
+  out.nnz = in.nnz;
+  DVec<int32_t> cnt((size_t)N + 1, st);
+  RINND_CUDA(cudaMemsetAsync(cnt.p + N, 0, sizeof(int32_t), st));
+  k_reorder_count<<<grid_for(N, 256), 256, 0, st>>>(in.indptr.p, order, N, cnt.p);
+  RINND_LAUNCH_CHECK();
+  out.indptr.alloc((size_t)N + 1, st);
+  exclusive_scan(cnt.p, out.indptr.p, (long long)N + 1, tmp, st);
+  out.indices.alloc((size_t)std::max<int64_t>(in.nnz, 1), st);
+  k_reorder_fill<<<grid_for((long long)N * 32, 256), 256, 0, st>>>(in.indptr.p, in.indices.p, order,
+                                                                   inverse, out.indptr.p, N, out.indices.p);
+  RINND_LAUNCH_CHECK();
+}
+
+}  // namespace rinnd

@@ -1,0 +1,381 @@
+// search.cu -- warp-per-query greedy graph search.
+//
+// Restates the reference query path (core/search/greedy.rs:70-241, 365-413;
+// core/index.rs:157-202, 283-334) with one warp per query:
+//   * tree seeding: hard descent of each retained RP tree (flat_tree.rs:253-273;
+//     margin = dot(q, hyperplane) + offset in the reference dot order, |m| < 1e-8
+//     -> random side), every unvisited leaf point pushed to results and seeds;
+//   * fill_random up to k seeds (greedy.rs:148-163);
+//   * traverse (greedy.rs:165-201): pop the nearest seed; stop when the result
+//     list is full and the seed is >= bound, bound = max + eps * (max - min_distance)
+//     evaluated with separately rounded ops; expand CSR neighbors not yet
+//     visited, push those with d < bound (results bounded to k, seeds
+//     unbounded), recomputing the bound after every result insertion.
+// Distances use the reference's exact accumulation order (dist.cuh), or the
+// exact int8 dot with the reference's scaling (quantized.rs:26-40, greedy.rs:384-390).
+//
+// Per-warp state lives in shared memory: the query, the result list (sorted by
+// (distance, id)), the seed set as a sorted array merged warp-parallel with each
+// batch of accepted neighbors, and an open-addressing visited table.
+// Deviations, all bounded and counted: the seed set keeps at most S entries
+// (the farthest are dropped), and a visited table that cannot place an id after
+// 32 probes treats the id as unvisited (results are still deduplicated).
+// Neighbor and tie order follow (distance, id); the reference's BinaryHeap
+// orders exact distance ties by its internal layout.
+#include "dist.cuh"
+#include "engine.h"
+
+namespace rinnd {
+namespace {
+
+constexpr int WPB = 4;  // warps per block
+constexpr int HASH_PROBES = 32;
+
+struct WarpLayout {
+  int dp, kmax, s, h;
+  __host__ __device__ size_t q_off() const { return 0; }
+  __host__ __device__ size_t res_off() const { return (size_t)dp * 4; }
+  __host__ __device__ size_t seed_off() const { return res_off() + (size_t)kmax * 8; }
+  __host__ __device__ size_t batch_off() const { return seed_off() + (size_t)2 * s * 8; }
+  __host__ __device__ size_t vis_off() const { return batch_off() + 32 * 8; }
+  __host__ __device__ size_t bytes() const { return vis_off() + (size_t)h * 4; }
+};
+
+__device__ __forceinline__ uint64_t rkey(float d, int32_t id) {
+  return ((uint64_t)fkey(d) << 32) | (uint32_t)id;
+}
+
+struct QRng {  // counter-based per-query stream (seed + query id, as index.rs:165)
+  uint64_t base, ctr;
+  __device__ uint64_t next() { return mix64(base ^ mix64(++ctr)); }
+  __device__ bool next_bool() { return (next() >> 63) != 0; }
+  __device__ uint32_t next_index(uint32_t n) { return (uint32_t)(((next() >> 32) * (uint64_t)n) >> 32); }
+};
+
+// Visited table: returns true if id was already present (VisitedSet::check_and_mark).
+__device__ __forceinline__ bool visited_check_and_mark(int32_t* tab, int h, int32_t id,
+                                                       unsigned long long* overflow) {
+  uint32_t pos = ((uint32_t)id * 2654435761u) & (uint32_t)(h - 1);
+  for (int p = 0; p < HASH_PROBES; ++p) {
+    int32_t old = atomicCAS(&tab[pos], -1, id);
+    if (old == -1) return false;
+    if (old == id) return true;
+    pos = (pos + 1) & (uint32_t)(h - 1);
+  }
+  atomicAdd(overflow, 1ull);
+  return false;
+}
+
+template <bool QUANT>
+__device__ __forceinline__ float dist_to(const SearchIndex& ix, const float* q, const int8_t* q8,
+                                         float qinv, int32_t id) {
+  if (QUANT) {
+    const int* a = reinterpret_cast<const int*>(q8);
+    const int* b = reinterpret_cast<const int*>(ix.codes + (size_t)id * ix.Dq);
+    int acc = 0;
+    for (int t = 0; t < ix.Dq / 4; ++t) acc = __dp4a(a[t], __ldg(b + t), acc);
+    float sim = __fmul_rn(__fmul_rn((float)acc, qinv), ix.inv_norms[id]);
+    return __fsub_rn(1.0f, fminf(fmaxf(sim, -1.0f), 1.0f));
+  }
+  return exact_distance(ix.kind, q, ix.X + (size_t)id * ix.Dp, ix.D);
+}
+
+// Warp-parallel insertion into the sorted result list (BoundedHeap::push,
+// candidate_heap.rs:97-113).  Returns true if inserted.  Uniform across the warp.
+__device__ __forceinline__ bool result_push(uint64_t* res, int& rc, int k, float d, int32_t id) {
+  const int lane = threadIdx.x & 31;
+  uint64_t key = rkey(d, id);
+  if (rc >= k) {
+    float mx = fkey_inv((uint32_t)(res[rc - 1] >> 32));
+    if (!(d < mx)) return false;
+  }
+  // duplicate guard (only reachable after a visited-table overflow)
+  bool dup = false;
+  for (int e = lane; e < rc; e += 32) dup |= ((uint32_t)res[e] == (uint32_t)id);
+  if (__any_sync(0xffffffffu, dup)) return false;
+  int pos = 0;
+  for (int e0 = 0; e0 < rc; e0 += 32) {
+    int e = e0 + lane;
+    pos += __popc(__ballot_sync(0xffffffffu, e < rc && res[e] < key));
+  }
+  int last = rc < k ? rc : k - 1;  // entries [pos, last) shift right by one
+  uint64_t tmp[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    int e = pos + lane + 32 * t;
+    tmp[t] = e < last ? res[e] : 0;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    int e = pos + lane + 32 * t;
+    if (e < last) res[e + 1] = tmp[t];
+  }
+  __syncwarp();
+  if (lane == 0) res[pos] = key;
+  __syncwarp();
+  if (rc < k) ++rc;
+  return true;
+}
+
+__device__ __forceinline__ float result_max(const uint64_t* res, int rc) {
+  return rc > 0 ? fkey_inv((uint32_t)(res[rc - 1] >> 32)) : __int_as_float(0x7f800000);
+}
+
+// Sort 32 keys held one per lane (ascending), bitonic via shuffles.
+__device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
+  const int lane = threadIdx.x & 31;
+  for (int size = 2; size <= 32; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      uint64_t o = __shfl_xor_sync(0xffffffffu, v, stride);
+      bool up = (lane & size) == 0;
+      bool lower = (lane & stride) == 0;
+      uint64_t mn = v < o ? v : o, mx = v < o ? o : v;
+      v = (lower == up) ? mn : mx;
+    }
+  return v;
+}
+
+// Merge the sorted batch (one key per lane, ascending, ~0 = none; nb valid) into
+// the sorted seed array A[head, tail) -> C[0, min(na + nb, S)).
+__device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int S, int& cur,
+                                            int& head, int& tail, uint64_t bkey, int nb) {
+  const int lane = threadIdx.x & 31;
+  if (nb == 0) return;
+  bbuf[lane] = bkey;
+  __syncwarp();
+  const uint64_t* A = seeds + (size_t)cur * S;
+  uint64_t* C = seeds + (size_t)(cur ^ 1) * S;
+  const int na = tail - head;
+  for (int i = lane; i < na; i += 32) {  // out = i + #(b < a)
+    uint64_t a = A[head + i];
+    int lo = 0, hi = nb;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (bbuf[mid] < a) lo = mid + 1; else hi = mid;
+    }
+    int o = i + lo;
+    if (o < S) C[o] = a;
+  }
+  if (lane < nb) {  // out = j + #(a <= b)
+    uint64_t b = bkey;
+    int lo = 0, hi = na;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (A[head + mid] <= b) lo = mid + 1; else hi = mid;
+    }
+    int o = lane + lo;
+    if (o < S) C[o] = b;
+  }
+  __syncwarp();
+  cur ^= 1;
+  head = 0;
+  tail = min(na + nb, S);
+}
+
+template <bool QUANT>
+__device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_t* Q8row,
+                           float qinv, int qid, uint64_t seed_base, int k, float eps,
+                           const WarpLayout& L, unsigned char* wsm, int32_t* out_idx,
+                           float* out_dist, unsigned long long* stats) {
+  const int lane = threadIdx.x & 31;
+  float* q = reinterpret_cast<float*>(wsm + L.q_off());
+  uint64_t* res = reinterpret_cast<uint64_t*>(wsm + L.res_off());
+  uint64_t* seeds = reinterpret_cast<uint64_t*>(wsm + L.seed_off());
+  int32_t* vis = reinterpret_cast<int32_t*>(wsm + L.vis_off());
+  uint64_t* bbuf = reinterpret_cast<uint64_t*>(wsm + L.batch_off());
+  int8_t* q8 = reinterpret_cast<int8_t*>(q);  // QUANT: codes stored in the query slot
+  if (QUANT) {
+    for (int t = lane; t < ix.Dq / 4; t += 32)
+      reinterpret_cast<int*>(q8)[t] = reinterpret_cast<const int*>(Q8row)[t];
+  } else {
+    for (int t = lane; t < ix.Dp; t += 32) q[t] = t < ix.D ? Qrow[t] : 0.f;
+  }
+  for (int t = lane; t < L.h; t += 32) vis[t] = -1;
+  __syncwarp();
+  QRng rng{seed_base + (uint64_t)qid, 0};
+  int rc = 0, cur = 0, head = 0, tail = 0;
+  unsigned long long evals = 0, expansions = 0;
+  unsigned long long* overflow = &stats[2];
+  const float min_d = ix.min_distance;
+  auto bound_of = [&](float mx) { return __fadd_rn(mx, __fmul_rn(eps, __fsub_rn(mx, min_d))); };
+
+  // ---- unconditional pushes of a list of candidate ids (leaves, random fill) ----
+  auto push_all = [&](int32_t my_id, bool have) {
+    bool fresh = false;
+    float d = 0.f;
+    if (have) {
+      fresh = !visited_check_and_mark(vis, L.h, my_id, overflow);
+      if (fresh) d = dist_to<QUANT>(ix, q, q8, qinv, my_id);
+    }
+    unsigned m = __ballot_sync(0xffffffffu, fresh);
+    evals += __popc(m);
+    uint64_t bkey = fresh ? rkey(d, my_id) : ~0ull;
+    unsigned mm = m;
+    while (mm) {
+      int j = __ffs(mm) - 1;
+      mm &= mm - 1;
+      float dj = __shfl_sync(0xffffffffu, d, j);
+      int32_t ij = __shfl_sync(0xffffffffu, my_id, j);
+      result_push(res, rc, k, dj, ij);
+    }
+    uint64_t sorted = warp_sort32(bkey);
+    seeds_merge(seeds, bbuf, L.s, cur, head, tail, sorted, __popc(m));
+  };
+
+  // ---- tree seeding (greedy.rs:70-99, leaf budget 1) ----
+  for (int t = 0; t < ix.n_trees; ++t) {
+    int node = ix.tree_roots[t];
+    while (ix.children[2 * (size_t)node] > 0) {
+      float margin = __fadd_rn(exact_dot_a(QUANT ? Qrow : q, ix.hyperplanes + (size_t)node * ix.Dp, ix.D),
+                               ix.offsets[node]);
+      int side;
+      if (fabsf(margin) < 1e-8f) side = rng.next_bool() ? 1 : 0;
+      else side = margin > 0.f ? 1 : 0;
+      node = ix.children[2 * (size_t)node + side];
+    }
+    int start = -ix.children[2 * (size_t)node], end = -ix.children[2 * (size_t)node + 1];
+    const int32_t* tidx = ix.tree_idx + (size_t)t * ix.N;
+    for (int p0 = start; p0 < end; p0 += 32) {
+      int p = p0 + lane;
+      int32_t id = p < end ? tidx[p] : -1;
+      push_all(id, id >= 0);
+    }
+  }
+  // ---- fill_random (greedy.rs:148-163) ----
+  {
+    int need = k - (tail - head);
+    for (int r0 = 0; r0 < need; r0 += 32) {
+      int32_t id = -1;
+      // draws in sequence order (every lane runs the stream); lane r takes draw r0 + r
+      for (int r = 0; r < 32 && r0 + r < need; ++r) {
+        uint32_t x = rng.next_index((uint32_t)ix.N);
+        if (r == lane) id = (int32_t)x;
+      }
+      // mark in draw order so a repeated draw is skipped like check_and_mark
+      bool fresh = false;
+      for (int r = 0; r < 32 && r0 + r < need; ++r) {
+        int32_t x = __shfl_sync(0xffffffffu, id, r);
+        bool f = false;
+        if (lane == 0) f = !visited_check_and_mark(vis, L.h, x, overflow);
+        f = __shfl_sync(0xffffffffu, f, 0);
+        if (lane == r) fresh = f;
+      }
+      __syncwarp();
+      float d = fresh ? dist_to<QUANT>(ix, q, q8, qinv, id) : 0.f;
+      unsigned m = __ballot_sync(0xffffffffu, fresh);
+      evals += __popc(m);
+      unsigned mm = m;
+      while (mm) {
+        int j = __ffs(mm) - 1;
+        mm &= mm - 1;
+        result_push(res, rc, k, __shfl_sync(0xffffffffu, d, j), __shfl_sync(0xffffffffu, id, j));
+      }
+      uint64_t sorted = warp_sort32(fresh ? rkey(d, id) : ~0ull);
+      seeds_merge(seeds, bbuf, L.s, cur, head, tail, sorted, __popc(m));
+    }
+  }
+  // ---- traverse (greedy.rs:165-201) ----
+  float mx = result_max(res, rc);
+  float bound = bound_of(mx);
+  while (head < tail) {
+    uint64_t top = seeds[(size_t)cur * L.s + head];
+    ++head;
+    float vd = fkey_inv((uint32_t)(top >> 32));
+    int32_t v = (int32_t)(uint32_t)top;
+    if (rc >= k && vd >= bound) break;
+    // With an exact visited set every node is expanded at most once; the cap
+    // only matters after a visited-table overflow, where it bounds the loop.
+    if (expansions >= (unsigned long long)ix.N + 64) break;
+    ++expansions;
+    int s = ix.indptr[v], e = ix.indptr[v + 1];
+    for (int c0 = s; c0 < e; c0 += 32) {
+      int c = c0 + lane;
+      int32_t nb = c < e ? ix.indices[c] : -1;
+      bool fresh = nb >= 0 && !visited_check_and_mark(vis, L.h, nb, overflow);
+      float d = fresh ? dist_to<QUANT>(ix, q, q8, qinv, nb) : 0.f;
+      unsigned m = __ballot_sync(0xffffffffu, fresh);
+      evals += __popc(m);
+      unsigned acc_mask = 0;
+      unsigned mm = m;
+      while (mm) {
+        int j = __ffs(mm) - 1;
+        mm &= mm - 1;
+        float dj = __shfl_sync(0xffffffffu, d, j);
+        if (dj < bound) {
+          int32_t ij = __shfl_sync(0xffffffffu, nb, j);
+          acc_mask |= 1u << j;
+          if (result_push(res, rc, k, dj, ij)) {
+            mx = result_max(res, rc);
+            bound = bound_of(mx);
+          }
+        }
+      }
+      bool acc = (acc_mask >> lane) & 1u;
+      uint64_t sorted = warp_sort32(acc ? rkey(d, nb) : ~0ull);
+      seeds_merge(seeds, bbuf, L.s, cur, head, tail, sorted, __popc(acc_mask));
+    }
+  }
+  // ---- output (index.rs:182-199) ----
+  for (int j = lane; j < k; j += 32) {
+    if (j < rc) {
+      uint64_t key = res[j];
+      int32_t id = (int32_t)(uint32_t)key;
+      float d = fkey_inv((uint32_t)(key >> 32));
+      out_idx[(size_t)qid * k + j] = ix.vertex_order ? ix.vertex_order[id] : id;
+      out_dist[(size_t)qid * k + j] = QUANT ? d : apply_correction(ix.corr, d);
+    } else {
+      out_idx[(size_t)qid * k + j] = -1;
+      out_dist[(size_t)qid * k + j] = __int_as_float(0x7f800000);
+    }
+  }
+  if (lane == 0) {
+    atomicAdd(&stats[0], evals);
+    atomicAdd(&stats[1], expansions);
+  }
+  __syncwarp();
+}
+
+template <bool QUANT>
+__global__ void __launch_bounds__(WPB * 32)
+    k_search(SearchIndex ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k,
+             float eps, uint64_t qid_base, WarpLayout L, int32_t* out_idx, float* out_dist,
+             unsigned long long* stats) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int w = threadIdx.x >> 5;
+  unsigned char* wsm = smem + (size_t)w * L.bytes();
+  const int total_warps = gridDim.x * WPB;
+  for (int qi = blockIdx.x * WPB + w; qi < nq; qi += total_warps) {
+    search_one<QUANT>(ix, Q + (size_t)qi * ix.Dp, QUANT ? Q8 + (size_t)qi * ix.Dq : nullptr,
+                      QUANT ? qinv[qi] : 0.f, qi, ix.seed + qid_base, k, eps, L, wsm, out_idx,
+                      out_dist, stats);
+  }
+}
+
+}  // namespace
+
+void greedy_search(const SearchIndex& ix, const float* Q, int nq, int k, float eps,
+                   uint64_t qid_base, int32_t* out_idx, float* out_dist, cudaStream_t st,
+                   unsigned long long* dstats) {
+  if (nq <= 0) return;
+  if (k > 256) throw std::invalid_argument("k must be <= 256");
+  WarpLayout L;
+  L.dp = ix.Dp;
+  L.kmax = k <= 32 ? 32 : (k <= 128 ? 128 : 256);
+  L.s = L.kmax <= 32 ? 256 : 4 * L.kmax;
+  L.h = 4096;
+  size_t bytes = L.bytes() * WPB;
+  static bool attr_set = false;
+  if (!attr_set) {
+    RINND_CUDA(cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    RINND_CUDA(cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr_set = true;
+  }
+  if (bytes > 200 * 1024) throw std::invalid_argument("query dimension too large for search shared memory");
+  int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
+  k_search<false><<<blocks, WPB * 32, bytes, st>>>(ix, Q, nullptr, nullptr, nq, k, eps, qid_base, L,
+                                                   out_idx, out_dist, dstats);
+  RINND_LAUNCH_CHECK();
+}
+
+}  // namespace rinnd
