@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""Benchmark: k-NN graph build throughput (points/s) and query QPS.
+
+Workload: N = 1,000,000 x D = 128 f32 points from a Gaussian mixture of 100
+isotropic clusters (centers ~ N(0, 10^2 I), within-cluster std 1), squared
+Euclidean, n_neighbors = 30, 8 RP trees, leaf size 30, <= 10 NN-Descent
+iterations, delta 0.001; 10,000 queries from the same mixture, k = 10,
+epsilon = 0.1.  Synthetic data (numpy seeded), generated on the host.
+
+One step = one full index build (forest, leaf init, NN-Descent iterations,
+sorted kNN rows, diversified CSR, search layout) over resident device data.
+`value` = points built per second over all ranks; `e2e` = the same through
+the C ABI from pinned host memory with the neighbor graph copied back.
+Multi-GPU: one independent index per rank (weak scaling, no collective on the
+data path); the max over ranks of the device-timed region is reported.
+
+--impl reference: the reference's CPU algorithm (the C++ restatement under
+oracle/, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "k-NN graph build pts/sec & QPS at fixed recall@k; vs plain FP32 GPU, % roofline"
+N_FULL, DIM, N_CLUSTERS, K = 1_000_000, 128, 100, 30
+N_TREES, LEAF, N_ITERS, DELTA = 8, 30, 10, 0.001
+N_QUERIES, QK, EPS = 10_000, 10, 0.1
+CPU_SAMPLE = 250_000
+WORKLOAD = ("nndescent-build 1M x 128 f32 GMM(100 clusters, center std 10, unit std), sqeuclidean, "
+            "k=30, 8 RP trees, leaf 30, <=10 iters, delta 0.001; 10k queries k=10 eps=0.1")
+
+
+def gen_mixture(n, d, seed, n_clusters=N_CLUSTERS):
+    rng = np.random.default_rng(seed)
+    centers = rng.normal(0.0, 10.0, (n_clusters, d)).astype(np.float32)
+    X = centers[rng.integers(0, n_clusters, n)]
+    X += rng.standard_normal((n, d), dtype=np.float32)
+    return X
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_FULL, help="points per rank")
+    ap.add_argument("--no-recall", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--parity", action="store_true",
+                    help="also build the oracle (CPU restatement) at the full size and report its recall")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled with nvidia-smi during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                mx.append(float(parts[2].split()[0]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def join_traffic_per_row():
+    """DRAM bytes per gathered candidate row of the join kernel, from the
+    committed ncu summary (profiles/local_join_fp32.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "local_join_fp32.json")) as f:
+            return float(json.load(f)["dram_bytes_per_gathered_row"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def cpu_build(X, n_threads=0):
+    import oracle
+
+    t = time.perf_counter()
+    ix = oracle.OracleIndex(X, n_neighbors=K, n_trees=N_TREES, leaf_size=LEAF, n_iters=N_ITERS, delta=DELTA,
+                            distance_kind=oracle.SQEUCLIDEAN, correction=oracle.CORR_NONE, n_threads=n_threads)
+    dt = time.perf_counter() - t
+    return ix, dt
+
+
+def run_reference(args, rank):
+    """The reference's CPU build (restated in oracle/) on bounded samples."""
+    if rank != 0:
+        return
+    import oracle
+
+    n = min(args.n, CPU_SAMPLE)
+    X = gen_mixture(n, DIM, seed=0)
+    cores = oracle.max_threads()
+    for _ in range(args.warmup):
+        cpu_build(X)
+    times = [cpu_build(X)[1] for _ in range(args.steps)]
+    total = sum(times)
+    value = n * args.steps / total
+    sample = f"N={n} rows of the same 100-cluster mixture per step (bounded sample of the 1M workload)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_points": n, "threads": cores},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def exact_knn_torch(X_dev, Q_dev, k, chunk=512):
+    """FP64 exact kNN on the GPU (recall checker only)."""
+    import torch
+
+    Xd = X_dev.double()
+    xx = (Xd * Xd).sum(1)
+    out = []
+    for s in range(0, Q_dev.shape[0], chunk):
+        q = Q_dev[s:s + chunk].double()
+        d = (q * q).sum(1)[:, None] + xx[None, :] - 2.0 * (q @ Xd.T)
+        out.append(torch.topk(d, k, dim=1, largest=False).indices.int().cpu())
+        del d
+    return torch.cat(out).numpy()
+
+
+def recall(found, truth):
+    k = truth.shape[1]
+    hits = sum(len(set(f[f >= 0].tolist()) & set(t.tolist())) for f, t in zip(found, truth))
+    return hits / (truth.shape[0] * k)
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from rinnd_b200 import _lib as L
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+    n = args.n
+    # data and queries: independent samples of the same mixture
+    XQ = gen_mixture(n + N_QUERIES, DIM, seed=1000 * rank)
+    X, Q = XQ[:n], XQ[n:]
+    X_dev = torch.from_numpy(X).to(dev)
+    Q_dev = torch.from_numpy(Q).to(dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    p = L.BuildParams()
+    L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
+    p.n_neighbors, p.n_trees, p.leaf_size, p.n_iters, p.delta = K, N_TREES, LEAF, N_ITERS, DELTA
+    p.distance_kind, p.correction, p.random_seed, p.device = L.DIST_SQEUCLIDEAN, L.CORR_NONE, 42, local_rank
+
+    def build(src_ptr, on_device):
+        h = ctypes.c_void_p()
+        L.check(L.lib.rinnd_build_on_stream(src_ptr, on_device, n, DIM, DIM, ctypes.byref(p),
+                                            ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h)))
+        return h
+
+    def info_of(h):
+        inf = L.BuildInfo()
+        L.check(L.lib.rinnd_build_info_get(h, ctypes.byref(inf)))
+        return inf
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    xp = ctypes.c_void_p(X_dev.data_ptr())
+    for _ in range(args.warmup):
+        L.check(L.lib.rinnd_free(build(xp, 1)))
+
+    # ---- timed region: K builds over resident device data ----
+    launches0 = ctypes.c_uint64(0)
+    launches1 = ctypes.c_uint64(0)
+    infos = []
+    gpu_index = local_rank
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        gpu_index = vis.split(",")[local_rank]
+    barrier()
+    L.lib.rinnd_kernel_launches(ctypes.byref(launches0))
+    with ClockSampler(gpu_index) as clocks:
+        ev = []
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            h = build(xp, 1)
+            e1.record(stream)
+            infos.append(info_of(h))
+            L.check(L.lib.rinnd_free(h))
+            ev.append((e0, e1))
+        barrier()
+    L.lib.rinnd_kernel_launches(ctypes.byref(launches1))
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_s = max_over_ranks(sum(step_ms) / 1000.0)
+    value = n * world * args.steps / total_s
+    clk = clocks.summary()
+
+    # ---- roofline of the dominant kernel (local join) ----
+    join_ms = sum(i.ms_join_kernel for i in infos)
+    join_launches = sum(i.iterations for i in infos)
+    rows = sum(i.join_rows_gathered for i in infos)
+    c = min(K, 60)
+    alg_bytes = rows * DIM * 4 + join_launches * 2 * n * c * 8
+    achieved = alg_bytes / (join_ms / 1000.0) / 1e9 if join_ms > 0 else None
+    peak, peak_kind = measured_peaks()
+    tpr = join_traffic_per_row()
+    roofline = {
+        "kernel": "k_local_join (FP32 SIMT tile join)", "bound": "hbm", "achieved": achieved, "peak": peak,
+        "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+        "traffic": (tpr * rows / join_launches) if tpr else None,
+        "algorithmic_bytes_per_launch": alg_bytes / max(join_launches, 1),
+        "avg_launch_ms": join_ms / max(join_launches, 1),
+        "share_of_build": join_ms / sum(step_ms),
+    }
+
+    # ---- queries (resident), QPS and recall ----
+    h = build(xp, 1)
+    inf = info_of(h)
+    qi = torch.empty((N_QUERIES, QK), dtype=torch.int32, device=dev)
+    qd = torch.empty((N_QUERIES, QK), dtype=torch.float32, device=dev)
+
+    def run_queries():
+        L.check(L.lib.rinnd_query_device(h, ctypes.c_void_p(Q_dev.data_ptr()), N_QUERIES, DIM, QK, EPS, 0,
+                                         ctypes.c_void_p(qi.data_ptr()), ctypes.c_void_p(qd.data_ptr()),
+                                         ctypes.c_void_p(stream.cuda_stream)))
+
+    for _ in range(3):
+        run_queries()
+    torch.cuda.synchronize()
+    q0 = torch.cuda.Event(enable_timing=True)
+    q1 = torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(args.steps):
+        run_queries()
+    q1.record(stream)
+    torch.cuda.synchronize()
+    q_s = max_over_ranks(q0.elapsed_time(q1) / 1000.0)
+    qps = N_QUERIES * world * args.steps / q_s
+    quality = {}
+    if not args.no_recall:
+        ki = np.empty((n, K), np.int32)
+        kd = np.empty((n, K), np.float32)
+        L.check(L.lib.rinnd_neighbor_graph(h, L.ptr(ki), L.ptr(kd)))
+        sample = np.random.default_rng(7).choice(n, size=min(10_000, n), replace=False)
+        sample.sort()
+        Xd = X_dev.double()
+        xx = (Xd * Xd).sum(1)
+        truth = np.concatenate([_exact_rows(Xd, xx, sample[s:s + 512], K, dev)
+                                for s in range(0, len(sample), 512)])
+        del Xd, xx
+        quality["graph_recall@30"] = recall(ki[sample], truth)
+        qtruth = exact_knn_torch(X_dev, Q_dev, QK)
+        quality["query_recall@10"] = recall(qi.cpu().numpy(), qtruth)
+        quality["graph_recall_sample"] = f"{len(sample)} seeded rows vs FP64 exact"
+        if args.parity and rank == 0:
+            oix, odt = cpu_build(X)
+            oki, _ = oix.neighbor_graph
+            quality["oracle_graph_recall@30"] = recall(oki[sample], truth)
+            oqi, _ = oix.query(Q, k=QK, epsilon=EPS)
+            quality["oracle_query_recall@10"] = recall(oqi, qtruth)
+            quality["oracle_build_s"] = odt
+            quality["oracle_iterations"] = oix.iterations
+    L.check(L.lib.rinnd_free(h))
+
+    # ---- e2e: pinned host data -> build -> neighbor graph back to host ----
+    e2e = None
+    if not args.no_e2e:
+        X_pin = torch.from_numpy(X).pin_memory()
+        out_i = torch.empty((n, K), dtype=torch.int32).pin_memory()
+        out_d = torch.empty((n, K), dtype=torch.float32).pin_memory()
+        hp = ctypes.c_void_p(X_pin.data_ptr())
+
+        def e2e_step():
+            hh = build(hp, 0)
+            L.check(L.lib.rinnd_neighbor_graph(hh, ctypes.c_void_p(out_i.data_ptr()),
+                                               ctypes.c_void_p(out_d.data_ptr())))
+            return hh
+
+        L.check(L.lib.rinnd_free(e2e_step()))
+        barrier()
+        ee = []
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            hh = e2e_step()
+            e1.record(stream)
+            L.check(L.lib.rinnd_free(hh))
+            ee.append((e0, e1))
+        barrier()
+        e_s = max_over_ranks(sum(a.elapsed_time(b) for a, b in ee) / 1000.0)
+        e2e = {"value": n * world * args.steps / e_s, "unit": "points/s", "h2d_bytes_per_step": n * DIM * 4,
+               "d2h_bytes_per_step": n * K * 8}
+
+    # ---- CPU baseline (rank 0, single GPU only) ----
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        import oracle
+
+        m = min(n, CPU_SAMPLE)
+        _, dt = cpu_build(X[:m])
+        cpu = {"value": m / dt, "unit": "points/s", "cores": oracle.max_threads(), "kind": "port",
+               "sample": f"first {m} rows of this run's mixture, same k/trees/leaf/iters (oracle/ C++ restatement, OpenMP)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "points_per_rank": n, "parallelism": f"replicas{world}",
+                       "l2": "inputs (512 MB/rank) exceed L2 (126 MB); no flush",
+                       "iterations_per_build": [i.iterations for i in infos]},
+            "clocks": clk, "e2e": e2e, "gpu_launches": int(launches1.value - launches0.value),
+            "roofline": roofline, "cpu_baseline": cpu,
+            "query": {"qps": qps, "k": QK, "epsilon": EPS, "n_queries": N_QUERIES, **quality},
+            "timed_steps_ms": {"event": step_ms, "host_total": [i.ms_total for i in infos],
+                               "join_kernels": [i.ms_join_kernel for i in infos]},
+            "counters": {"pairs_evaluated": int(inf.pairs_evaluated), "pushes_accepted": int(inf.pushes_accepted),
+                         "push_contention": int(inf.push_contention), "join_rows": int(inf.join_rows_gathered),
+                         "iterations": int(inf.iterations), "n_leaves": int(inf.n_leaves)},
+            "phases_ms": {"forest": inf.ms_forest, "leaf_init": inf.ms_leaf_init, "iterations": inf.ms_iterations,
+                          "candidates": inf.ms_candidates, "join": inf.ms_join, "sort": inf.ms_sort,
+                          "graph": inf.ms_graph, "total": inf.ms_total},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _exact_rows(Xd, xx, rows, k, dev):
+    """FP64 exact kNN of data rows `rows` against all of X (self excluded)."""
+    import torch
+
+    r = torch.from_numpy(np.asarray(rows)).to(dev).long()
+    q = Xd[r]
+    d = (q * q).sum(1)[:, None] + xx[None, :] - 2.0 * (q @ Xd.T)
+    d[torch.arange(len(rows), device=dev), r] = float("inf")
+    return torch.topk(d, k, dim=1, largest=False).indices.int().cpu().numpy()
+
+
+if __name__ == "__main__":
+    main()

@@ -95,6 +95,9 @@ typedef struct rinnd_build_info {
   uint64_t push_contention;      /* pushes abandoned after the bounded retry count */
   int64_t search_graph_nnz;
   float min_distance;
+  uint64_t join_rows_gathered;   /* candidate rows gathered by the join kernel      */
+  double ms_join_kernel;         /* CUDA-event time of the join kernels             */
+  uint64_t kernel_launches;      /* kernels this library launched during the build  */
 } rinnd_build_info;
 
 /* ---- lifecycle ------------------------------------------------------------ */
@@ -105,6 +108,12 @@ RINND_EXPORT int rinnd_build(const float* data, int64_t n, int32_t d, const rinn
 /* Same, with the rows already on the device (row stride `ld` floats, ld >= d). */
 RINND_EXPORT int rinnd_build_device(const float* d_data, int64_t n, int32_t d, int64_t ld,
                        const rinnd_build_params* p, rinnd_index** out);
+/* General form: rows on host or device (`data_on_device`), all build work on
+ * `stream` (a cudaStream_t; NULL = a stream owned by the index).  A caller
+ * stream is adopted by the index for its later calls and must outlive it. */
+RINND_EXPORT int rinnd_build_on_stream(const float* data, int32_t data_on_device, int64_t n, int32_t d,
+                                       int64_t ld, const rinnd_build_params* p, void* stream,
+                                       rinnd_index** out);
 RINND_EXPORT int rinnd_free(rinnd_index* idx);
 RINND_EXPORT int rinnd_build_info_get(const rinnd_index* idx, rinnd_build_info* info);
 RINND_EXPORT int rinnd_index_shape(const rinnd_index* idx, int64_t* n, int32_t* d, int32_t* k);
@@ -178,6 +187,8 @@ RINND_EXPORT int rinnd_heap_push_batch(int32_t n, int32_t k, int64_t n_ops, cons
 RINND_EXPORT const char* rinnd_last_error(void);
 RINND_EXPORT const char* rinnd_version(void);
 RINND_EXPORT int rinnd_device_count(int32_t* count);
+/* Number of kernels this library has launched in the process so far. */
+RINND_EXPORT int rinnd_kernel_launches(uint64_t* count);
 
 #ifdef __cplusplus
 }

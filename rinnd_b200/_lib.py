@@ -43,7 +43,8 @@ class BuildInfo(ctypes.Structure):
         ("ms_forest", _f64), ("ms_leaf_init", _f64), ("ms_iterations", _f64), ("ms_candidates", _f64),
         ("ms_join", _f64), ("ms_sort", _f64), ("ms_graph", _f64), ("ms_total", _f64),
         ("pairs_evaluated", _u64), ("pushes_accepted", _u64), ("push_contention", _u64),
-        ("search_graph_nnz", _i64), ("min_distance", _f32),
+        ("search_graph_nnz", _i64), ("min_distance", _f32), ("join_rows_gathered", _u64),
+        ("ms_join_kernel", _f64), ("kernel_launches", _u64),
     ]
 
 
@@ -59,6 +60,7 @@ SIGNATURES = {
     "rinnd_params_default": (ctypes.c_int, [_P]),
     "rinnd_build": (ctypes.c_int, [_P, _i64, _i32, _P, _P]),
     "rinnd_build_device": (ctypes.c_int, [_P, _i64, _i32, _i64, _P, _P]),
+    "rinnd_build_on_stream": (ctypes.c_int, [_P, _i32, _i64, _i32, _i64, _P, _P, _P]),
     "rinnd_free": (ctypes.c_int, [_P]),
     "rinnd_build_info_get": (ctypes.c_int, [_P, _P]),
     "rinnd_index_shape": (ctypes.c_int, [_P, _P, _P, _P]),
@@ -78,6 +80,7 @@ SIGNATURES = {
     "rinnd_last_error": (ctypes.c_char_p, []),
     "rinnd_version": (ctypes.c_char_p, []),
     "rinnd_device_count": (ctypes.c_int, [_P]),
+    "rinnd_kernel_launches": (ctypes.c_int, [_P]),
 }
 
 if not os.path.exists(LIB_PATH):

@@ -24,6 +24,13 @@
 
 using namespace rinnd;
 
+namespace rinnd {
+std::atomic<unsigned long long>& launch_counter() {
+  static std::atomic<unsigned long long> n{0};
+  return n;
+}
+}  // namespace rinnd
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -70,6 +77,17 @@ void ensure_device(int dev) {
   }
   require(dev >= 0 && dev < n, "device ordinal out of range");
   RINND_CUDA(cudaSetDevice(dev));
+  // Keep freed stream-ordered allocations cached in the device pool instead of
+  // returning them to the driver at every synchronization: builds allocate and
+  // free large temporaries per level / per iteration.
+  static bool pool_set[64] = {};
+  if (dev < 64 && !pool_set[dev]) {
+    cudaMemPool_t pool;
+    RINND_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t threshold = UINT64_MAX;
+    RINND_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    pool_set[dev] = true;
+  }
 }
 
 double now_ms() {
@@ -112,6 +130,7 @@ __global__ void k_iota(int32_t* p, int n) {
 struct rinnd_index {
   int device = 0;
   cudaStream_t st = nullptr;
+  bool own_stream = true;
   int64_t N = 0;
   int D = 0, Dp = 0, k = 0;
   rinnd_build_params p{};
@@ -142,6 +161,10 @@ struct rinnd_index {
       cudaSetDevice(device);
       cudaStreamSynchronize(st);
     }
+  }
+  void destroy_stream() {
+    if (st && own_stream) cudaStreamDestroy(st);
+    st = nullptr;
   }
   SearchIndex search_view() const {
     SearchIndex s;
@@ -188,7 +211,7 @@ void validate_params(const rinnd_build_params* p, int64_t n, int d) {
 }
 
 void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
-                const rinnd_build_params* pin, rinnd_index** out) {
+                const rinnd_build_params* pin, cudaStream_t user_st, rinnd_index** out) {
   require(out != nullptr, "out must not be null");
   require(data != nullptr, "data must not be null");
   validate_params(pin, n, d);
@@ -198,8 +221,14 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   std::unique_ptr<rinnd_index> ix(new rinnd_index());
   ix->device = pin->device;
   ix->p = *pin;
-  RINND_CUDA(cudaStreamCreateWithFlags(&ix->st, cudaStreamNonBlocking));
+  if (user_st) {
+    ix->st = user_st;
+    ix->own_stream = false;
+  } else {
+    RINND_CUDA(cudaStreamCreateWithFlags(&ix->st, cudaStreamNonBlocking));
+  }
   cudaStream_t st = ix->st;
+  const unsigned long long launches0 = launch_counter();
   const int N = (int)n, D = d, Dp = round_up(d, 4), k = pin->n_neighbors;
   ix->N = n;
   ix->D = D;
@@ -238,8 +267,8 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   RINND_CUDA(cudaStreamSynchronize(st));
   double t2 = now_ms();
   const size_t conv = (size_t)(pin->delta * (float)k * (float)N);  // mod.rs:157
-  uint64_t pairs_total = 0, pushes_total = 0;
-  double ms_cand = 0, ms_join = 0;
+  uint64_t pairs_total = 0, pushes_total = 0, rows_total = 0;
+  double ms_cand = 0, ms_join = 0, ms_join_kernel = 0;
   int iters = 0;
   for (int it = 0; it < n_iters; ++it) {
     iters = it + 1;
@@ -247,15 +276,18 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
     build_candidates(ks, pin->random_seed, it, st);
     RINND_CUDA(cudaStreamSynchronize(st));
     double b = now_ms();
-    unsigned long long pairs = 0;
-    unsigned long long changes = local_join(ks, X0.p, D, Dp, ix->kind, st, &pairs);
+    JoinStats js = local_join(ks, X0.p, D, Dp, ix->kind, st);
     double e = now_ms();
     ms_cand += b - a;
     ms_join += e - b;
-    pairs_total += pairs;
-    pushes_total += changes;
-    if (pin->verbose) std::printf("Iteration %d: %llu updates (%llu pairs)\n", it + 1, changes, pairs);
-    if ((size_t)changes <= conv) break;
+    ms_join_kernel += js.kernel_ms;
+    pairs_total += js.pairs;
+    pushes_total += js.changes;
+    rows_total += js.rows;
+    if (pin->verbose)
+      std::printf("Iteration %d: %llu updates (%llu pairs, %.3f ms join)\n", it + 1, js.changes, js.pairs,
+                  js.kernel_ms);
+    if ((size_t)js.changes <= conv) break;
   }
   double t3 = now_ms();
   // sorted kNN rows (index.rs:653)
@@ -322,6 +354,9 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   inf.ms_graph = t5 - t4;
   inf.ms_total = t5 - t_start;
   inf.pairs_evaluated = pairs_total;
+  inf.join_rows_gathered = rows_total;
+  inf.ms_join_kernel = ms_join_kernel;
+  inf.kernel_launches = launch_counter() - launches0;
   inf.pushes_accepted = pushes_total;
   inf.push_contention = hc[1];
   inf.search_graph_nnz = ix->graph_orig.nnz;
@@ -379,19 +414,36 @@ int rinnd_params_default(rinnd_build_params* p) {
 }
 
 int rinnd_build(const float* data, int64_t n, int32_t d, const rinnd_build_params* p, rinnd_index** out) {
-  return guarded([&] { build_impl(data, false, n, d, d, p, out); });
+  return guarded([&] { build_impl(data, false, n, d, d, p, nullptr, out); });
 }
 
 int rinnd_build_device(const float* d_data, int64_t n, int32_t d, int64_t ld, const rinnd_build_params* p,
                        rinnd_index** out) {
-  return guarded([&] { build_impl(d_data, true, n, d, ld, p, out); });
+  return guarded([&] { build_impl(d_data, true, n, d, ld, p, nullptr, out); });
+}
+
+int rinnd_build_on_stream(const float* data, int32_t data_on_device, int64_t n, int32_t d, int64_t ld,
+                          const rinnd_build_params* p, void* stream, rinnd_index** out) {
+  return guarded([&] {
+    build_impl(data, data_on_device != 0, n, d, ld, p, reinterpret_cast<cudaStream_t>(stream), out);
+  });
+}
+
+int rinnd_kernel_launches(uint64_t* count) {
+  return guarded([&] {
+    require(count != nullptr, "count must not be null");
+    *count = launch_counter();
+  });
 }
 
 int rinnd_free(rinnd_index* idx) {
   return guarded([&] {
     if (idx) {
       cudaSetDevice(idx->device);
-      delete idx;
+      cudaStream_t st = idx->st;
+      bool own = idx->own_stream;
+      delete idx;  // device buffers are freed stream-ordered on st
+      if (st && own) cudaStreamDestroy(st);
     }
   });
 }
@@ -577,7 +629,7 @@ int rinnd_heap_push_batch(int32_t n, int32_t k, int64_t n_ops, const int32_t* ro
     DVec<int32_t> oi((size_t)n * k, st);
     DVec<float> od((size_t)n * k, st);
     DVec<uint8_t> of((size_t)n * k, st);
-    finalize_rows(s.slots.p, n, k, oi.p, od.p, of.p, st);
+    finalize_rows(s.slots.p, n, k, s.kp, oi.p, od.p, of.p, st);
     oi.to_host(out_idx, (size_t)n * k);
     od.to_host(out_dist, (size_t)n * k);
     if (out_flags) of.to_host(out_flags, (size_t)n * k);

@@ -5,6 +5,7 @@
 #include <stdint.h>
 #include <float.h>
 
+#include <atomic>
 #include <stdexcept>
 #include <string>
 
@@ -37,7 +38,14 @@ struct CudaError : std::runtime_error {
                                __FILE__ + ":" + std::to_string(__LINE__) + ")");           \
   } while (0)
 
-#define RINND_LAUNCH_CHECK() RINND_CUDA(cudaGetLastError())
+// Every kernel launch of this library is followed by RINND_LAUNCH_CHECK, which
+// also counts it (rinnd_kernel_launches).
+std::atomic<unsigned long long>& launch_counter();
+#define RINND_LAUNCH_CHECK()               \
+  do {                                     \
+    ++::rinnd::launch_counter();           \
+    RINND_CUDA(cudaGetLastError());        \
+  } while (0)
 
 // ---------------------------------------------------------------------------
 // Order-preserving float <-> u32 map.  -0.0 is folded onto +0.0 so that the

@@ -39,24 +39,33 @@ struct BuildStats {
 
 struct KnnState {
   int N = 0, k = 0, c = 0;
-  DVec<uint64_t> slots;      // N*k neighbor slots
+  int kp = 0, cp = 0;        // row strides (multiples of 16 slots)
+  DVec<uint64_t> slots;      // N*kp neighbor slots (first k of each row used)
   DVec<uint32_t> thr;        // N upper bounds of fkey(row max)
-  DVec<uint64_t> cand_new;   // N*c
-  DVec<uint64_t> cand_old;   // N*c
+  DVec<uint64_t> cand_new;   // N*cp
+  DVec<uint64_t> cand_old;   // N*cp
   DVec<float> norms;         // N squared norms (dot-form metrics)
-  DVec<unsigned long long> counters;  // [0] changes, [1] contention, [2] pairs
+  // [0] changes, [1] contention, [2] pairs, [3] gathered rows, [4] buffered updates
+  DVec<unsigned long long> counters;
+  DVec<uint32_t> urow;       // update buffer: destination rows
+  DVec<uint64_t> ukey;       // update buffer: slot keys
+  unsigned long long ucap = 0;
 };
 
 void knn_init(KnnState& s, int N, int k, int c, cudaStream_t st);
+void ensure_update_buffer(KnnState& s, cudaStream_t st);
 void compute_norms(const float* X, int N, int D, int Dp, float* norms, cudaStream_t st);
 void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int kind,
                cudaStream_t st);
 void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st);
-unsigned long long local_join(KnnState& s, const float* X, int D, int Dp, int kind,
-                              cudaStream_t st, unsigned long long* pairs_out);
+struct JoinStats {
+  unsigned long long changes = 0, pairs = 0, rows = 0;
+  float kernel_ms = 0.f;  // CUDA-event duration of the join kernel on its stream
+};
+JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st);
 // Sorted output: idx (-1 empty), raw distance (+inf empty).
 void finalize_knn(const KnnState& s, int32_t* out_idx, float* out_dist, cudaStream_t st);
-void finalize_rows(const uint64_t* slots, int N, int k, int32_t* out_idx, float* out_dist,
+void finalize_rows(const uint64_t* slots, int N, int k, int kp, int32_t* out_idx, float* out_dist,
                    uint8_t* out_flags, cudaStream_t st);
 unsigned long long heap_push_batch(KnnState& s, long long n_ops, const int32_t* rows,
                                    const int32_t* ids, const float* dists, const uint8_t* flags,

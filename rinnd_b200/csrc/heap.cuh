@@ -3,11 +3,13 @@
 // Restates NeighborHeap::checked_flagged_push (core/heap/neighbor_heap.rs:149-177)
 // and checked_heap_push_flat (core/nndescent/candidates.rs:433-484) for many
 // concurrent writers.  A row is k unordered 64-bit slots, key = (fkey(value) << 32) | id
-// (flag in bit 31 of the low word for neighbor rows).  A push of (v, id):
+// (flag in bit 31 of the low word for neighbor rows), stored with a stride that
+// is a multiple of ROW_ALIGN slots (128 bytes) so a row spans whole cache lines.
+// A push of (v, id):
 //   1. is rejected if v >= the row's cached upper bound `thr[row]`,
-//   2. reads a snapshot of all k slots (each 8-byte read is single-copy atomic),
-//      rejects if id is present or v >= max slot value (the reference's
-//      `distance >= root`),
+//   2. reads a snapshot of all k slots (each 8-byte read is single-copy atomic;
+//      all loads are issued before any is used), rejects if id is present or
+//      v >= max slot value (the reference's `distance >= root`),
 //   3. CASes the max slot (lowest index among equal keys) from its snapshot
 //      value to the new key; on CAS failure it retries from 2.
 // Slot values only ever decrease (a CAS always installs a strictly smaller key)
@@ -22,35 +24,46 @@
 namespace rinnd {
 
 constexpr int PUSH_MAX_RETRY = 256;
+constexpr int ROW_ALIGN = 16;  // slots per 128-byte line group
 
-__device__ __forceinline__ uint64_t ld_slot(const uint64_t* p) { return __ldcg(p); }
+__host__ __device__ __forceinline__ int row_stride(int k) { return (k + ROW_ALIGN - 1) / ROW_ALIGN * ROW_ALIGN; }
 
-// Scan `k` slots; returns max slot index (lowest index among equal keys) and
-// value; sets *dup if the low 31 bits of some slot equal `id`.
-__device__ __forceinline__ int scan_row(const uint64_t* row, int k, uint32_t id, uint64_t* vmax,
-                                        bool* dup) {
-  uint64_t best = 0;
-  int m = 0;
-  bool d = false;
-  if ((k & 1) == 0 && ((reinterpret_cast<uintptr_t>(row) & 15) == 0)) {
-    const ulonglong2* r2 = reinterpret_cast<const ulonglong2*>(row);
-    for (int j = 0; j < (k >> 1); ++j) {
-      ulonglong2 v = __ldcg(r2 + j);
-      d |= (((uint32_t)v.x) & 0x7FFFFFFFu) == id;
-      d |= (((uint32_t)v.y) & 0x7FFFFFFFu) == id;
-      if (j == 0 || v.x > best) { best = v.x; m = 2 * j; }
-      if (v.y > best) { best = v.y; m = 2 * j + 1; }
-    }
-  } else {
-    for (int j = 0; j < k; ++j) {
-      uint64_t v = ld_slot(row + j);
-      d |= (((uint32_t)v) & 0x7FFFFFFFu) == id;
-      if (j == 0 || v > best) { best = v; m = j; }
+struct RowScan {
+  uint64_t vmax;  // largest key (lowest index among equal keys)
+  uint64_t v2;    // largest key among the other slots
+  int m;
+  bool dup;
+};
+
+// Scans the k valid slots of a row whose storage holds row_stride(k) slots
+// (16-byte aligned).  Loads are issued 16 slots at a time, unconditionally
+// within the padded stride, and masked afterwards.
+__device__ __forceinline__ RowScan scan_row(const uint64_t* row, int k, uint32_t id) {
+  RowScan r{0, 0, 0, false};
+  const ulonglong2* r2 = reinterpret_cast<const ulonglong2*>(row);
+  bool first = true;
+  for (int j0 = 0; j0 < k; j0 += ROW_ALIGN) {
+    ulonglong2 v[ROW_ALIGN / 2];
+#pragma unroll
+    for (int t = 0; t < ROW_ALIGN / 2; ++t) v[t] = __ldcg(r2 + j0 / 2 + t);
+#pragma unroll
+    for (int t = 0; t < ROW_ALIGN; ++t) {
+      int j = j0 + t;
+      if (j < k) {
+        uint64_t x = (t & 1) ? v[t >> 1].y : v[t >> 1].x;
+        r.dup |= (((uint32_t)x) & 0x7FFFFFFFu) == id;
+        if (first || x > r.vmax) {
+          r.v2 = first ? 0 : r.vmax;
+          r.vmax = x;
+          r.m = j;
+          first = false;
+        } else if (x > r.v2) {
+          r.v2 = x;
+        }
+      }
     }
   }
-  *vmax = best;
-  *dup = d;
-  return m;
+  return r;
 }
 
 // Returns 1 if inserted.  `key` = (fkey(v) << 32) | lo, lo's low 31 bits = id.
@@ -61,26 +74,19 @@ __device__ __forceinline__ int row_push(uint64_t* row, int k, uint32_t* thr, uin
   if (thr != nullptr && vk >= __ldcg(thr)) return 0;
   const uint32_t id = ((uint32_t)key) & 0x7FFFFFFFu;
   for (int attempt = 0; attempt < PUSH_MAX_RETRY; ++attempt) {
-    uint64_t vmax;
-    bool dup;
-    int m = scan_row(row, k, id, &vmax, &dup);
-    if (dup) return 0;
-    if (vk >= (uint32_t)(vmax >> 32)) {
-      if (thr != nullptr) atomicMin(thr, (uint32_t)(vmax >> 32));
+    RowScan s = scan_row(row, k, id);
+    if (s.dup) return 0;
+    if (vk >= (uint32_t)(s.vmax >> 32)) {
+      if (thr != nullptr) atomicMin(thr, (uint32_t)(s.vmax >> 32));
       return 0;
     }
-    unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long*>(row + m),
-                                       (unsigned long long)vmax, (unsigned long long)key);
-    if (old == vmax) {
+    unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long*>(row + s.m),
+                                       (unsigned long long)s.vmax, (unsigned long long)key);
+    if (old == s.vmax) {
       if (thr != nullptr) {
-        // Upper bound of the new row max: snapshot values can only be >= the
-        // current ones, so max(snapshot without m, key) bounds the true max.
-        uint64_t nm = key;
-        for (int j = 0; j < k; ++j)
-          if (j != m) {
-            uint64_t v = ld_slot(row + j);
-            nm = v > nm ? v : nm;
-          }
+        // Upper bound of the new row max: snapshot values are >= the current
+        // ones, so max(runner-up of the snapshot, key) bounds the true max.
+        uint64_t nm = s.v2 > key ? s.v2 : key;
         atomicMin(thr, (uint32_t)(nm >> 32));
       }
       return 1;

@@ -29,7 +29,6 @@
 namespace rinnd {
 namespace {
 
-enum JoinMode : int { MODE_JOIN = 0, MODE_TRI = 1, MODE_RECT = 2 };
 
 __global__ void k_fill_u64(uint64_t* p, size_t n, uint64_t v) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -53,41 +52,56 @@ __global__ void k_norms(const float* X, int N, int D, int Dp, float* norms) {
 }
 
 // ---------------------------------------------------------------------------
-// Tile join: A ids (na <= MA) x B ids (nb <= MB), dimensions chunked by DC.
+// Pair join.  A job is a set A (na <= MAXA ids) against a set B (nb <= MAXB
+// ids); the pairs are the rectangle A x B minus, where A is a prefix of B, the
+// diagonal and lower triangle of A x A, and in a vertex job the new x old pairs
+// with equal ids.  Rows are staged in shared memory JDC dimensions at a time,
+// row-major with a 4-float pad (conflict-free 16-byte loads); each thread owns
+// up to PPT pairs and accumulates their distances in registers.  Pairs that
+// beat an endpoint's threshold are appended to a global update buffer (one
+// atomic per warp); k_apply_updates performs the lock-free pushes in a
+// separate, fully parallel launch.  Updates beyond the buffer capacity are
+// pushed directly by the join thread.
 // ---------------------------------------------------------------------------
-template <int MA, int MB, int DC>
-struct __align__(16) JoinSmem {
-  int32_t aid[MA];
-  int32_t bid[MB];
-  uint32_t athr[MA];
-  uint32_t bthr[MB];
-  float an[MA];
-  float bn[MB];
-  float a[DC * MA];  // dimension-major, used only when A is not a prefix of B
-  float b[DC * MB];
-  unsigned int pushes;
+constexpr int JDC = 64;        // dimensions per staged chunk
+constexpr int JROW = JDC + 4;  // staged row stride in floats
+
+enum JoinMode : int { MODE_JOIN = 0, MODE_TRI = 1, MODE_RECT = 2 };
+
+template <int MAXA, int MAXB, int AROWS = MAXA>
+struct __align__(16) PairSmem {
+  int32_t aid[MAXA];
+  int32_t bid[MAXB];
+  uint32_t athr[MAXA];
+  uint32_t bthr[MAXB];
+  float an[MAXA];
+  float bn[MAXB];
+  float rows[(MAXB + AROWS) * JROW];  // B rows, then A rows (RECT only; AROWS = 0 when A prefixes B)
   unsigned int pairs;
+  int na, nb;
 };
 
-template <int DC>
-__device__ __forceinline__ void gather_chunk(const float* __restrict__ X, int Dp, int c0,
-                                             const int32_t* ids, int n, int M, float* dst) {
-  constexpr int Q = DC / 4;
-  for (int e = threadIdx.x; e < M * Q; e += blockDim.x) {
-    int r = e % M, q = e / M;
+struct UpdateBuf {
+  uint32_t* row;
+  uint64_t* key;
+  unsigned long long* count;  // total appended (may exceed cap)
+  unsigned long long cap;
+};
+
+__device__ __forceinline__ void stage_rows(const float* __restrict__ X, int Dp, int c0, const int32_t* ids,
+                                           int n, float* dst) {
+  constexpr int Q = JDC / 4;
+  for (int e = threadIdx.x; e < n * Q; e += blockDim.x) {
+    int r = e / Q, q = e % Q;
     int d = c0 + 4 * q;
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (r < n && d < Dp) v = __ldg(reinterpret_cast<const float4*>(X + (size_t)ids[r] * Dp + d));
-    dst[(4 * q + 0) * M + r] = v.x;
-    dst[(4 * q + 1) * M + r] = v.y;
-    dst[(4 * q + 2) * M + r] = v.z;
-    dst[(4 * q + 3) * M + r] = v.w;
+    if (d < Dp) v = __ldg(reinterpret_cast<const float4*>(X + (size_t)ids[r] * Dp + d));
+    *reinterpret_cast<float4*>(dst + r * JROW + 4 * q) = v;
   }
 }
 
-// Loads ids' thresholds / norms into shared memory (threads < n).
-template <int MA, int MB, int DC>
-__device__ __forceinline__ void load_meta(JoinSmem<MA, MB, DC>& sm, int na, int nb, bool a_prefix,
+template <int MAXA, int MAXB, int AROWS>
+__device__ __forceinline__ void load_meta(PairSmem<MAXA, MAXB, AROWS>& sm, int na, int nb, bool a_prefix,
                                           const uint32_t* thr, const float* norms) {
   for (int t = threadIdx.x; t < nb; t += blockDim.x) {
     sm.bthr[t] = __ldcg(thr + sm.bid[t]);
@@ -100,137 +114,140 @@ __device__ __forceinline__ void load_meta(JoinSmem<MA, MB, DC>& sm, int na, int 
     }
 }
 
-template <int MA, int MB, int DC>
-__device__ __forceinline__ void join_tile(JoinSmem<MA, MB, DC>& sm, int na, int nb, int mode,
-                                          const float* __restrict__ X, int Dp, int kind,
-                                          uint64_t* slots, uint32_t* thr, int k,
-                                          unsigned long long* contention) {
-  constexpr int TX = MB / 4;  // threads along B
-  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
-  const int i0 = ty * 4, j0 = tx * 4;
-  const bool a_prefix = (mode != MODE_RECT);
-  const float* sa = a_prefix ? sm.b : sm.a;
-  const int astride = a_prefix ? MB : MA;
-  bool active = i0 < na && j0 < nb;
-  if (active && mode != MODE_RECT) {
-    // skip 4x4 blocks that lie entirely on/below the diagonal of the A x A part
-    bool any_tri = (j0 + 3 > i0) && (j0 < na);
-    bool any_rect = (mode == MODE_JOIN) && (j0 + 3 >= na);
-    active = any_tri || any_rect;
+template <int MAXA, int MAXB, int AROWS, int NT>
+__device__ __forceinline__ void join_pairs(PairSmem<MAXA, MAXB, AROWS>& sm, int na, int nb, int mode,
+                                           const float* __restrict__ X, int Dp, int kind, uint64_t* slots,
+                                           uint32_t* thr, int k, int kp, UpdateBuf ub,
+                                           unsigned long long* counters) {
+  constexpr int PPT = (MAXA * MAXB + NT - 1) / NT;
+  const bool a_prefix = mode != MODE_RECT;
+  const float* rowsB = sm.rows;
+  const float* rowsA = a_prefix ? sm.rows : sm.rows + MAXB * JROW;
+  const int npairs = na * nb;
+  const int tid = threadIdx.x;
+  // validity mask of this thread's pairs
+  unsigned valid_mask = 0;
+#pragma unroll
+  for (int s = 0; s < PPT; ++s) {
+    int t = tid + s * NT;
+    if (t < npairs) {
+      int i = t / nb, j = t % nb;
+      bool v;
+      if (mode == MODE_RECT) v = true;
+      else if (j < na) v = j > i;                               // A x A: q after p (mod.rs:396)
+      else v = (mode == MODE_JOIN) && (sm.bid[j] != sm.bid[i]);  // new x old: q != p (mod.rs:424)
+      if (v) valid_mask |= 1u << s;
+    }
   }
-  const bool is_dot = kind_is_dot(kind);
-  float acc[4][4];
+  float acc[PPT];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-
-  for (int c0 = 0; c0 < Dp; c0 += DC) {
+  for (int s = 0; s < PPT; ++s) acc[s] = 0.f;
+  for (int c0 = 0; c0 < Dp; c0 += JDC) {
     __syncthreads();
-    gather_chunk<DC>(X, Dp, c0, sm.bid, nb, MB, sm.b);
-    if (!a_prefix) gather_chunk<DC>(X, Dp, c0, sm.aid, na, MA, sm.a);
+    stage_rows(X, Dp, c0, sm.bid, nb, sm.rows);
+    if (AROWS > 0 && !a_prefix) stage_rows(X, Dp, c0, sm.aid, na, sm.rows + MAXB * JROW);
     __syncthreads();
-    if (active) {
-      if (kind == DK_SQEUCLIDEAN) {
-#pragma unroll 8
-        for (int d = 0; d < DC; ++d) {
-          float4 av = *reinterpret_cast<const float4*>(sa + d * astride + i0);
-          float4 bv = *reinterpret_cast<const float4*>(sm.b + d * MB + j0);
-          float a4[4] = {av.x, av.y, av.z, av.w};
-          float b4[4] = {bv.x, bv.y, bv.z, bv.w};
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
+    for (int s = 0; s < PPT; ++s) {
+      if (valid_mask & (1u << s)) {
+        int t = tid + s * NT;
+        const float4* a = reinterpret_cast<const float4*>(rowsA + (t / nb) * JROW);
+        const float4* b = reinterpret_cast<const float4*>(rowsB + (t % nb) * JROW);
+        float x = acc[s];
+        if (kind == DK_SQEUCLIDEAN) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              float t = a4[i] - b4[j];
-              acc[i][j] = fmaf(t, t, acc[i][j]);
-            }
+          for (int q = 0; q < JDC / 4; ++q) {
+            float4 u = a[q], w = b[q];
+            float d0 = u.x - w.x, d1 = u.y - w.y, d2 = u.z - w.z, d3 = u.w - w.w;
+            x = fmaf(d0, d0, x); x = fmaf(d1, d1, x); x = fmaf(d2, d2, x); x = fmaf(d3, d3, x);
+          }
+        } else if (kind == DK_MANHATTAN) {
+#pragma unroll
+          for (int q = 0; q < JDC / 4; ++q) {
+            float4 u = a[q], w = b[q];
+            x += fabsf(u.x - w.x) + fabsf(u.y - w.y) + fabsf(u.z - w.z) + fabsf(u.w - w.w);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < JDC / 4; ++q) {
+            float4 u = a[q], w = b[q];
+            x = fmaf(u.x, w.x, x); x = fmaf(u.y, w.y, x); x = fmaf(u.z, w.z, x); x = fmaf(u.w, w.w, x);
+          }
         }
-      } else if (kind == DK_MANHATTAN) {
-#pragma unroll 8
-        for (int d = 0; d < DC; ++d) {
-          float4 av = *reinterpret_cast<const float4*>(sa + d * astride + i0);
-          float4 bv = *reinterpret_cast<const float4*>(sm.b + d * MB + j0);
-          float a4[4] = {av.x, av.y, av.z, av.w};
-          float b4[4] = {bv.x, bv.y, bv.z, bv.w};
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] += fabsf(a4[i] - b4[j]);
-        }
-      } else {
-#pragma unroll 8
-        for (int d = 0; d < DC; ++d) {
-          float4 av = *reinterpret_cast<const float4*>(sa + d * astride + i0);
-          float4 bv = *reinterpret_cast<const float4*>(sm.b + d * MB + j0);
-          float a4[4] = {av.x, av.y, av.z, av.w};
-          float b4[4] = {bv.x, bv.y, bv.z, bv.w};
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a4[i], b4[j], acc[i][j]);
-        }
+        acc[s] = x;
       }
     }
   }
-  unsigned int my_pairs = 0, my_push = 0;
-  if (active) {
+  // ---- filter, then emit updates (warp-aggregated append) ----
+  const bool is_dot = kind_is_dot(kind);
+  uint32_t kd[PPT];
+  unsigned emit_p = 0, emit_q = 0;
+  int n_emit = 0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      int ia = i0 + i;
-      if (ia >= na) break;
+  for (int s = 0; s < PPT; ++s) {
+    kd[s] = 0;
+    if (valid_mask & (1u << s)) {
+      int t = tid + s * NT;
+      int i = t / nb, j = t % nb;
+      float d = acc[s];
+      if (is_dot) d = finalize_dot(kind, d, a_prefix ? sm.bn[i] : sm.an[i], sm.bn[j]);
+      kd[s] = fkey(d);
+      uint32_t tp = a_prefix ? sm.bthr[i] : sm.athr[i];
+      if (kd[s] < tp) { emit_p |= 1u << s; ++n_emit; }
+      if (kd[s] < sm.bthr[j]) { emit_q |= 1u << s; ++n_emit; }
+    }
+  }
+  const int lane = tid & 31;
+  int incl = n_emit;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        int jb = j0 + j;
-        if (jb >= nb) break;
-        int32_t p = a_prefix ? sm.bid[ia] : sm.aid[ia], q = sm.bid[jb];
-        bool valid;
-        if (mode == MODE_RECT) valid = true;
-        else if (jb < na) valid = jb > ia;            // new x new, q after p (mod.rs:396)
-        else valid = (mode == MODE_JOIN) && (q != p);  // new x old, q != p (mod.rs:424)
-        if (!valid) continue;
-        ++my_pairs;
-        float d = acc[i][j];
-        if (is_dot) d = finalize_dot(kind, d, a_prefix ? sm.bn[ia] : sm.an[ia], sm.bn[jb]);
-        uint32_t kd = fkey(d);
-        uint32_t tp = a_prefix ? sm.bthr[ia] : sm.athr[ia];
-        if (kd < tp)
-          my_push += row_push(slots + (size_t)p * k, k, thr + p,
-                              ((uint64_t)kd << 32) | (uint32_t)q | 0x80000000u, contention);
-        if (kd < sm.bthr[jb])
-          my_push += row_push(slots + (size_t)q * k, k, thr + q,
-                              ((uint64_t)kd << 32) | (uint32_t)p | 0x80000000u, contention);
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  int warp_total = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 0 && warp_total) base = atomicAdd(ub.count, (unsigned long long)warp_total);
+  base = __shfl_sync(0xffffffffu, base, 0) + (unsigned long long)(incl - n_emit);
+  unsigned int my_pairs = __popc(valid_mask);
+#pragma unroll
+  for (int s = 0; s < PPT; ++s) {
+    if ((emit_p | emit_q) & (1u << s)) {
+      int t = tid + s * NT;
+      int i = t / nb, j = t % nb;
+      int32_t p = a_prefix ? sm.bid[i] : sm.aid[i], q = sm.bid[j];
+      for (int side = 0; side < 2; ++side) {
+        if (!((side == 0 ? emit_p : emit_q) & (1u << s))) continue;
+        uint32_t row = side == 0 ? (uint32_t)p : (uint32_t)q;
+        uint64_t key = ((uint64_t)kd[s] << 32) | (uint32_t)(side == 0 ? q : p) | 0x80000000u;
+        if (base < ub.cap) {
+          ub.row[base] = row;
+          ub.key[base] = key;
+        } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
+          atomicAdd(&counters[0], 1ull);
+        }
+        ++base;
       }
     }
   }
   if (my_pairs) atomicAdd(&sm.pairs, my_pairs);
-  if (my_push) atomicAdd(&sm.pushes, my_push);
 }
 
-// One CTA per vertex (grid-stride): A = new candidates, B = new ++ old.
-template <int MA, int MB, int DC>
-__global__ void __launch_bounds__((MA / 4) * (MB / 4))
-    k_local_join(const uint64_t* cand_new, const uint64_t* cand_old, int N, int c,
-                 const float* __restrict__ X, int Dp, int kind, const float* norms,
-                 uint64_t* slots, uint32_t* thr, int k, unsigned long long* counters) {
-  __shared__ JoinSmem<MA, MB, DC> sm;
-  __shared__ int s_cnt[2];
-  for (int v = blockIdx.x; v < N; v += gridDim.x) {
+// One CTA per vertex (grid-stride over [v0, v1)): A = new candidates, B = new ++ old.
+template <int MAXC, int NT>
+__global__ void __launch_bounds__(NT)
+    k_local_join(const uint64_t* cand_new, const uint64_t* cand_old, int v0, int v1, int c, int cp,
+                 const float* __restrict__ X, int Dp, int kind, const float* norms, uint64_t* slots,
+                 uint32_t* thr, int k, int kp, UpdateBuf ub, unsigned long long* counters) {
+  __shared__ PairSmem<MAXC, 2 * MAXC, 0> sm;
+  for (int v = v0 + blockIdx.x; v < v1; v += gridDim.x) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-      s_cnt[0] = 0;
-      s_cnt[1] = 0;
-      sm.pushes = 0;
-      sm.pairs = 0;
-    }
-    __syncthreads();
-    // compact valid ids, keeping list order: new first, then old
-    if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) sm.pairs = 0;
+    if (threadIdx.x < 32) {  // compact valid ids, new first then old
       int lane = threadIdx.x;
       int base = 0;
       for (int t0 = 0; t0 < c; t0 += 32) {
         int t = t0 + lane;
-        int32_t id = t < c ? slot_id(cand_new[(size_t)v * c + t]) : -1;
+        int32_t id = t < c ? slot_id(cand_new[(size_t)v * cp + t]) : -1;
         unsigned m = __ballot_sync(0xffffffffu, id >= 0);
         if (id >= 0) sm.bid[base + __popc(m & ((1u << lane) - 1))] = id;
         base += __popc(m);
@@ -238,27 +255,42 @@ __global__ void __launch_bounds__((MA / 4) * (MB / 4))
       int na = base;
       for (int t0 = 0; t0 < c; t0 += 32) {
         int t = t0 + lane;
-        int32_t id = t < c ? slot_id(cand_old[(size_t)v * c + t]) : -1;
+        int32_t id = t < c ? slot_id(cand_old[(size_t)v * cp + t]) : -1;
         unsigned m = __ballot_sync(0xffffffffu, id >= 0);
         if (id >= 0) sm.bid[base + __popc(m & ((1u << lane) - 1))] = id;
         base += __popc(m);
       }
       if (lane == 0) {
-        s_cnt[0] = na;
-        s_cnt[1] = base;
+        sm.na = na;
+        sm.nb = base;
       }
     }
     __syncthreads();
-    int na = s_cnt[0], nb = s_cnt[1];
-    if (na == 0) continue;  // no new candidates: nothing to join (uniform across CTA)
-    load_meta<MA, MB, DC>(sm, na, nb, true, thr, kind_is_dot(kind) ? norms : nullptr);
-    join_tile<MA, MB, DC>(sm, na, nb, MODE_JOIN, X, Dp, kind, slots, thr, k, &counters[1]);
+    const int na = sm.na, nb = sm.nb;
+    if (na == 0) continue;  // uniform across the CTA
+    load_meta(sm, na, nb, true, thr, kind_is_dot(kind) ? norms : nullptr);
+    join_pairs<MAXC, 2 * MAXC, 0, NT>(sm, na, nb, MODE_JOIN, X, Dp, kind, slots, thr, k, kp, ub, counters);
     __syncthreads();
     if (threadIdx.x == 0) {
-      if (sm.pushes) atomicAdd(&counters[0], (unsigned long long)sm.pushes);
-      if (sm.pairs) atomicAdd(&counters[2], (unsigned long long)sm.pairs);
+      atomicAdd(&counters[2], (unsigned long long)sm.pairs);
+      atomicAdd(&counters[3], (unsigned long long)nb);
     }
   }
+}
+
+// Lock-free pushes of buffered updates (heap.cuh protocol).
+__global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, const unsigned long long* count,
+                                unsigned long long cap, uint64_t* slots, uint32_t* thr, int k, int kp,
+                                unsigned long long* counters) {
+  const unsigned long long n = min(*count, cap);
+  unsigned int mine = 0;
+  for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
+       e += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t r = urow[e];
+    mine += row_push(slots + (size_t)r * kp, k, thr + r, ukey[e], &counters[1]);
+  }
+  for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&counters[0], (unsigned long long)mine);
 }
 
 // Leaf jobs: blocks of BS points of one leaf, (a, b) with a <= b.
@@ -284,13 +316,13 @@ __global__ void k_leaf_job_emit(const int4* leaves, long long nl, int BS, const 
 }
 
 // nndescent/mod.rs:203-300 initialize_from_leaves, one CTA per (leaf, block pair).
-template <int BS, int DC>
-__global__ void __launch_bounds__((BS / 4) * (BS / 4))
-    k_leaf_join(const int4* jobs, long long njobs, const int4* leaves, const int32_t* perm, int N,
-                const float* __restrict__ X, int Dp, int kind, const float* norms,
-                uint64_t* slots, uint32_t* thr, int k, unsigned long long* counters) {
-  __shared__ JoinSmem<BS, BS, DC> sm;
-  for (long long jb = blockIdx.x; jb < njobs; jb += gridDim.x) {
+template <int BS, int NT>
+__global__ void __launch_bounds__(NT)
+    k_leaf_join(const int4* jobs, long long j0, long long j1, const int4* leaves, const int32_t* perm, int N,
+                const float* __restrict__ X, int Dp, int kind, const float* norms, uint64_t* slots,
+                uint32_t* thr, int k, int kp, UpdateBuf ub, unsigned long long* counters) {
+  __shared__ PairSmem<BS, BS, BS> sm;
+  for (long long jb = j0 + blockIdx.x; jb < j1; jb += gridDim.x) {
     int4 job = jobs[jb];
     int4 leaf = leaves[job.x];
     const int32_t* P = perm + (size_t)leaf.x * N + leaf.y;
@@ -299,57 +331,52 @@ __global__ void __launch_bounds__((BS / 4) * (BS / 4))
     int na = min(BS, L - a0), nb = min(BS, L - b0);
     int mode = job.y == job.z ? MODE_TRI : MODE_RECT;
     __syncthreads();
-    if (threadIdx.x == 0) {
-      sm.pushes = 0;
-      sm.pairs = 0;
-    }
+    if (threadIdx.x == 0) sm.pairs = 0;
     for (int t = threadIdx.x; t < nb; t += blockDim.x) sm.bid[t] = P[b0 + t];
     for (int t = threadIdx.x; t < na; t += blockDim.x) sm.aid[t] = P[a0 + t];
     __syncthreads();
-    load_meta<BS, BS, DC>(sm, na, nb, mode != MODE_RECT, thr, kind_is_dot(kind) ? norms : nullptr);
-    join_tile<BS, BS, DC>(sm, na, nb, mode, X, Dp, kind, slots, thr, k, &counters[1]);
+    load_meta(sm, na, nb, mode != MODE_RECT, thr, kind_is_dot(kind) ? norms : nullptr);
+    join_pairs<BS, BS, BS, NT>(sm, na, nb, mode, X, Dp, kind, slots, thr, k, kp, ub, counters);
     __syncthreads();
-    if (threadIdx.x == 0) {
-      if (sm.pushes) atomicAdd(&counters[0], (unsigned long long)sm.pushes);
-      if (sm.pairs) atomicAdd(&counters[2], (unsigned long long)sm.pairs);
-    }
+    if (threadIdx.x == 0) atomicAdd(&counters[2], (unsigned long long)sm.pairs);
   }
 }
 
 // candidates.rs:153-351: each heap edge offered forward and reverse with one priority.
-__global__ void k_candidates(const uint64_t* slots, int N, int k, int c, uint64_t* cnew,
+__global__ void k_candidates(const uint64_t* slots, int N, int k, int kp, int c, int cp, uint64_t* cnew,
                              uint64_t* cold, uint64_t seed, int iter,
                              unsigned long long* contention) {
   long long total = (long long)N * k;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
-    uint64_t s = slots[e];
+    int32_t i = (int32_t)(e / k);
+    int j = (int)(e % k);
+    uint64_t s = slots[(size_t)i * kp + j];
     int32_t id = slot_id(s);
     if (id < 0) continue;
-    int32_t i = (int32_t)(e / k);
     uint64_t* lists = slot_new(s) ? cnew : cold;
     uint32_t prio = (uint32_t)(hash3(seed, 0xC0DE0000ull + (uint64_t)iter, (uint64_t)e) >> 33);
     uint64_t hi = (uint64_t)prio << 32;
-    row_push(lists + (size_t)i * c, c, nullptr, hi | (uint32_t)id, contention);
-    row_push(lists + (size_t)id * c, c, nullptr, hi | (uint32_t)i, contention);
+    row_push(lists + (size_t)i * cp, c, nullptr, hi | (uint32_t)id, contention);
+    row_push(lists + (size_t)id * cp, c, nullptr, hi | (uint32_t)i, contention);
   }
 }
 
 // candidates.rs:354-417 mark_old_flags, one warp per row.
-__global__ void k_mark_old(uint64_t* slots, int N, int k, const uint64_t* cnew, int c) {
+__global__ void k_mark_old(uint64_t* slots, int N, int k, int kp, const uint64_t* cnew, int c, int cp) {
   int row = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
   int lane = threadIdx.x & 31;
   if (row >= N) return;
-  const uint64_t* nl = cnew + (size_t)row * c;
+  const uint64_t* nl = cnew + (size_t)row * cp;
   for (int j0 = 0; j0 < k; j0 += 32) {
     int j = j0 + lane;
-    uint64_t s = j < k ? slots[(size_t)row * k + j] : SLOT_EMPTY;
+    uint64_t s = j < k ? slots[(size_t)row * kp + j] : SLOT_EMPTY;
     int32_t id = slot_id(s);
     bool hit = false;
     if (id >= 0 && slot_new(s))
       for (int t = 0; t < c; ++t)
         if (slot_id(nl[t]) == id) { hit = true; break; }
-    if (hit) slots[(size_t)row * k + j] = s & ~(1ull << 31);
+    if (hit) slots[(size_t)row * kp + j] = s & ~(1ull << 31);
   }
 }
 
@@ -357,7 +384,7 @@ __global__ void k_mark_old(uint64_t* slots, int N, int k, const uint64_t* cnew, 
 // one warp per row, bitonic sort of P = next_pow2(k) keys in shared memory.
 // Sort key = (fkey(d) << 32) | (id << 1) | flag; empty = ~0.
 template <int P>
-__global__ void k_finalize(const uint64_t* slots, int N, int k, int32_t* out_idx, float* out_dist,
+__global__ void k_finalize(const uint64_t* slots, int N, int k, int kp, int32_t* out_idx, float* out_dist,
                            uint8_t* out_flags) {
   __shared__ uint64_t buf[4][P];
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -367,7 +394,7 @@ __global__ void k_finalize(const uint64_t* slots, int N, int k, int32_t* out_idx
   for (int j = lane; j < P; j += 32) {
     uint64_t key = ~0ull;
     if (j < k) {
-      uint64_t s = slots[(size_t)row * k + j];
+      uint64_t s = slots[(size_t)row * kp + j];
       uint32_t lo = (uint32_t)s;
       if (lo != LO_EMPTY) key = (s & 0xFFFFFFFF00000000ull) | (((lo & 0x7FFFFFFFu) << 1) | (lo >> 31));
     }
@@ -413,13 +440,15 @@ void knn_init(KnnState& s, int N, int k, int c, cudaStream_t st) {
   s.N = N;
   s.k = k;
   s.c = c;
-  s.slots.alloc((size_t)N * k, st);
+  s.kp = row_stride(k);
+  s.cp = row_stride(c);
+  s.slots.alloc((size_t)N * s.kp, st);
   s.thr.alloc((size_t)N, st);
-  s.cand_new.alloc((size_t)N * c, st);
-  s.cand_old.alloc((size_t)N * c, st);
-  s.counters.alloc(4, st);
+  s.cand_new.alloc((size_t)N * s.cp, st);
+  s.cand_old.alloc((size_t)N * s.cp, st);
+  s.counters.alloc(8, st);
   s.counters.fill_bytes(0);
-  k_fill_u64<<<grid_for((long long)N * k, 256, 148 * 32), 256, 0, st>>>(s.slots.p, s.slots.n, SLOT_EMPTY);
+  k_fill_u64<<<grid_for((long long)N * s.kp, 256, 148 * 32), 256, 0, st>>>(s.slots.p, s.slots.n, SLOT_EMPTY);
   k_fill_u32<<<grid_for(N, 256, 148 * 32), 256, 0, st>>>(s.thr.p, s.thr.n, KEY_INF);
   RINND_LAUNCH_CHECK();
 }
@@ -429,10 +458,27 @@ void compute_norms(const float* X, int N, int D, int Dp, float* norms, cudaStrea
   RINND_LAUNCH_CHECK();
 }
 
+void ensure_update_buffer(KnnState& s, cudaStream_t st) {
+  if (s.ucap) return;
+  s.ucap = std::max<unsigned long long>(1ull << 22, 64ull * (unsigned long long)s.N);
+  s.urow.alloc(s.ucap, st);
+  s.ukey.alloc(s.ucap, st);
+}
+
+namespace {
+void apply_pending(KnnState& s, cudaStream_t st) {
+  k_apply_updates<<<148 * 16, 256, 0, st>>>(s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap, s.slots.p, s.thr.p,
+                                            s.k, s.kp, s.counters.p);
+  RINND_LAUNCH_CHECK();
+}
+UpdateBuf update_buf(KnnState& s) { return UpdateBuf{s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap}; }
+}  // namespace
+
 void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int kind,
                cudaStream_t st) {
   (void)D;
   if (f.n_leaves == 0) return;
+  ensure_update_buffer(s, st);
   const int BS = f.max_leaf <= 32 ? 32 : 64;
   TempStorage tmp;
   DVec<int32_t> cnt((size_t)f.n_leaves + 1, st), off((size_t)f.n_leaves + 1, st);
@@ -448,71 +494,101 @@ void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int 
   k_leaf_job_emit<<<grid_for(f.n_leaves, 256, 148 * 32), 256, 0, st>>>(f.leaves.p, f.n_leaves, BS, off.p, jobs.p);
   RINND_LAUNCH_CHECK();
   const float* norms = s.norms.p;
-  int grid = (int)std::min<long long>(njobs, 148LL * 16);
-  if (BS == 32)
-    k_leaf_join<32, 32><<<grid, 64, 0, st>>>(jobs.p, njobs, f.leaves.p, f.perm.p, f.N, X, Dp, kind,
-                                             norms, s.slots.p, s.thr.p, s.k, s.counters.p);
-  else
-    k_leaf_join<64, 32><<<grid, 256, 0, st>>>(jobs.p, njobs, f.leaves.p, f.perm.p, f.N, X, Dp, kind,
-                                              norms, s.slots.p, s.thr.p, s.k, s.counters.p);
-  RINND_LAUNCH_CHECK();
+  // Worst case 2 * BS^2 updates per job: batches never overflow the buffer.
+  const long long per_batch = std::max<long long>(1, (long long)(s.ucap / (2ull * BS * BS)));
+  for (long long j0 = 0; j0 < njobs; j0 += per_batch) {
+    long long j1 = std::min<long long>(njobs, j0 + per_batch);
+    RINND_CUDA(cudaMemsetAsync(s.counters.p + 4, 0, sizeof(unsigned long long), st));
+    int grid = (int)std::min<long long>(j1 - j0, 148LL * 16);
+    if (BS == 32)
+      k_leaf_join<32, 128><<<grid, 128, 0, st>>>(jobs.p, j0, j1, f.leaves.p, f.perm.p, f.N, X, Dp, kind, norms,
+                                                 s.slots.p, s.thr.p, s.k, s.kp, update_buf(s), s.counters.p);
+    else
+      k_leaf_join<64, 256><<<grid, 256, 0, st>>>(jobs.p, j0, j1, f.leaves.p, f.perm.p, f.N, X, Dp, kind, norms,
+                                                 s.slots.p, s.thr.p, s.k, s.kp, update_buf(s), s.counters.p);
+    RINND_LAUNCH_CHECK();
+    apply_pending(s, st);
+  }
 }
 
 void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st) {
   s.cand_new.fill_bytes(0xFF);
   s.cand_old.fill_bytes(0xFF);
   long long total = (long long)s.N * s.k;
-  k_candidates<<<grid_for(total, 256, 148 * 64), 256, 0, st>>>(s.slots.p, s.N, s.k, s.c, s.cand_new.p,
-                                                              s.cand_old.p, seed, iter, &s.counters.p[1]);
+  k_candidates<<<grid_for(total, 256, 148 * 64), 256, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp,
+                                                              s.cand_new.p, s.cand_old.p, seed, iter,
+                                                              &s.counters.p[1]);
   RINND_LAUNCH_CHECK();
-  k_mark_old<<<grid_for((long long)s.N * 32, 256), 256, 0, st>>>(s.slots.p, s.N, s.k, s.cand_new.p, s.c);
+  k_mark_old<<<grid_for((long long)s.N * 32, 256), 256, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.cand_new.p,
+                                                                 s.c, s.cp);
   RINND_LAUNCH_CHECK();
 }
 
-unsigned long long local_join(KnnState& s, const float* X, int D, int Dp, int kind,
-                              cudaStream_t st, unsigned long long* pairs_out) {
+JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st) {
   (void)D;
+  ensure_update_buffer(s, st);
   RINND_CUDA(cudaMemsetAsync(s.counters.p, 0, sizeof(unsigned long long), st));
-  RINND_CUDA(cudaMemsetAsync(s.counters.p + 2, 0, sizeof(unsigned long long), st));
-  int grid = std::min(s.N, 148 * 16);
-  if (s.c <= 32)
-    k_local_join<32, 64, 32><<<grid, 128, 0, st>>>(s.cand_new.p, s.cand_old.p, s.N, s.c, X, Dp, kind,
-                                                   s.norms.p, s.slots.p, s.thr.p, s.k, s.counters.p);
-  else
-    k_local_join<64, 128, 32><<<grid, 512, 0, st>>>(s.cand_new.p, s.cand_old.p, s.N, s.c, X, Dp, kind,
-                                                    s.norms.p, s.slots.p, s.thr.p, s.k, s.counters.p);
-  RINND_LAUNCH_CHECK();
-  unsigned long long h[4];
+  RINND_CUDA(cudaMemsetAsync(s.counters.p + 2, 0, 2 * sizeof(unsigned long long), st));
+  cudaEvent_t e0, e1;
+  RINND_CUDA(cudaEventCreate(&e0));
+  RINND_CUDA(cudaEventCreate(&e1));
+  // Worst case 4 c^2 updates per vertex (2 directions x c new x 2c candidates).
+  const long long per_batch =
+      std::max<long long>(1, (long long)(s.ucap / (4ull * (unsigned long long)s.c * (unsigned long long)s.c)));
+  RINND_CUDA(cudaEventRecord(e0, st));
+  for (long long v0 = 0; v0 < s.N; v0 += per_batch) {
+    int v1 = (int)std::min<long long>(s.N, v0 + per_batch);
+    RINND_CUDA(cudaMemsetAsync(s.counters.p + 4, 0, sizeof(unsigned long long), st));
+    int grid = (int)std::min<long long>(v1 - v0, 148LL * 16);
+    if (s.c <= 32)
+      k_local_join<32, 128><<<grid, 128, 0, st>>>(s.cand_new.p, s.cand_old.p, (int)v0, v1, s.c, s.cp, X, Dp, kind,
+                                                  s.norms.p, s.slots.p, s.thr.p, s.k, s.kp, update_buf(s),
+                                                  s.counters.p);
+    else
+      k_local_join<64, 256><<<grid, 256, 0, st>>>(s.cand_new.p, s.cand_old.p, (int)v0, v1, s.c, s.cp, X, Dp, kind,
+                                                  s.norms.p, s.slots.p, s.thr.p, s.k, s.kp, update_buf(s),
+                                                  s.counters.p);
+    RINND_LAUNCH_CHECK();
+    apply_pending(s, st);
+  }
+  RINND_CUDA(cudaEventRecord(e1, st));
+  unsigned long long h[5];
   RINND_CUDA(cudaMemcpyAsync(h, s.counters.p, sizeof(h), cudaMemcpyDeviceToHost, st));
   RINND_CUDA(cudaStreamSynchronize(st));
-  if (pairs_out) *pairs_out = h[2];
-  return h[0];
+  JoinStats js;
+  RINND_CUDA(cudaEventElapsedTime(&js.kernel_ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  js.changes = h[0];
+  js.pairs = h[2];
+  js.rows = h[3];
+  return js;
 }
 
 void finalize_knn(const KnnState& s, int32_t* out_idx, float* out_dist, cudaStream_t st) {
-  finalize_rows(s.slots.p, s.N, s.k, out_idx, out_dist, nullptr, st);
+  finalize_rows(s.slots.p, s.N, s.k, s.kp, out_idx, out_dist, nullptr, st);
 }
 
-void finalize_rows(const uint64_t* slots, int N, int k, int32_t* out_idx, float* out_dist,
+void finalize_rows(const uint64_t* slots, int N, int k, int kp, int32_t* out_idx, float* out_dist,
                    uint8_t* out_flags, cudaStream_t st) {
   int grid = (N + 3) / 4;
-  if (k <= 32) k_finalize<32><<<grid, 128, 0, st>>>(slots, N, k, out_idx, out_dist, out_flags);
-  else if (k <= 64) k_finalize<64><<<grid, 128, 0, st>>>(slots, N, k, out_idx, out_dist, out_flags);
-  else if (k <= 128) k_finalize<128><<<grid, 128, 0, st>>>(slots, N, k, out_idx, out_dist, out_flags);
-  else if (k <= 512) k_finalize<512><<<grid, 128, 0, st>>>(slots, N, k, out_idx, out_dist, out_flags);
+  if (k <= 32) k_finalize<32><<<grid, 128, 0, st>>>(slots, N, k, kp, out_idx, out_dist, out_flags);
+  else if (k <= 64) k_finalize<64><<<grid, 128, 0, st>>>(slots, N, k, kp, out_idx, out_dist, out_flags);
+  else if (k <= 128) k_finalize<128><<<grid, 128, 0, st>>>(slots, N, k, kp, out_idx, out_dist, out_flags);
+  else if (k <= 512) k_finalize<512><<<grid, 128, 0, st>>>(slots, N, k, kp, out_idx, out_dist, out_flags);
   else throw std::invalid_argument("n_neighbors must be <= 512");
   RINND_LAUNCH_CHECK();
 }
 
 // Applies (row, id, dist, flag) pushes concurrently to rows initialised empty.
-__global__ void k_push_batch(uint64_t* slots, uint32_t* thr, int k, long long n_ops,
+__global__ void k_push_batch(uint64_t* slots, uint32_t* thr, int k, int kp, long long n_ops,
                              const int32_t* rows, const int32_t* ids, const float* dists,
                              const uint8_t* flags, unsigned long long* counters) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_ops;
        i += (long long)gridDim.x * blockDim.x) {
     int32_t r = rows[i];
     uint64_t key = slot_pack(dists[i], ids[i], flags[i]);
-    if (row_push(slots + (size_t)r * k, k, thr + r, key, &counters[1])) atomicAdd(&counters[0], 1ull);
+    if (row_push(slots + (size_t)r * kp, k, thr + r, key, &counters[1])) atomicAdd(&counters[0], 1ull);
   }
 }
 
@@ -520,7 +596,7 @@ unsigned long long heap_push_batch(KnnState& s, long long n_ops, const int32_t* 
                                    const int32_t* ids, const float* dists, const uint8_t* flags,
                                    cudaStream_t st) {
   s.counters.fill_bytes(0);
-  k_push_batch<<<grid_for(n_ops, 256, 148 * 32), 256, 0, st>>>(s.slots.p, s.thr.p, s.k, n_ops, rows, ids,
+  k_push_batch<<<grid_for(n_ops, 256, 148 * 32), 256, 0, st>>>(s.slots.p, s.thr.p, s.k, s.kp, n_ops, rows, ids,
                                                               dists, flags, s.counters.p);
   RINND_LAUNCH_CHECK();
   unsigned long long h[4];

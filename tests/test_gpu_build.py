@@ -17,25 +17,30 @@ RECALL_TOL = 0.005
     ("gmm20k_euclid", "euclidean", 0, 1, False),
 ])
 def test_build_recall_not_below_oracle(rb, orc, name, metric, kind, corr, angular):
+    """Built-graph recall@k and query recall@10 vs FP64 exact, averaged over three
+    seeds, no more than 0.5 points below the oracle's at the same parameters."""
     if name.startswith("uniform"):
         X, k, kw = uniform(10000, 128, seed=0), 15, {}
+        Q = uniform(1000, 128, seed=11)
     else:
         X, k, kw = gmm(20000, 64, 50, seed=1), 30, {"n_trees": 8, "leaf_size": 30, "n_iters": 10}
+        Q = gmm(21000, 64, 50, seed=1)[20000:]
     truth, _ = orc.exact_knn_f64(kind, X, X, k, exclude_self=True)
-    oix = orc.OracleIndex(X, n_neighbors=k, distance_kind=kind, correction=corr, angular=angular,
-                          n_trees=kw.get("n_trees", 8), leaf_size=kw.get("leaf_size"), n_iters=kw.get("n_iters"))
-    gix = rb.RINND(X, metric=metric, n_neighbors=k, random_state=42, **kw)
-    o_rec = recall(oix.neighbor_graph[0], truth)
-    g_rec = recall(gix.neighbor_graph[0], truth)
-    print(f"{name}: graph recall@{k} gpu={g_rec:.4f} oracle={o_rec:.4f}")
-    assert g_rec >= o_rec - RECALL_TOL
-    # queries: held-out points from the same distribution
-    Q = uniform(1000, 128, seed=11) if name.startswith("uniform") else gmm(1000, 64, 50, seed=1)[::-1].copy()
     qtruth, _ = orc.exact_knn_f64(kind, X, Q, 10)
-    q_o = recall(oix.query(Q, k=10, epsilon=0.1)[0], qtruth)
-    q_g = recall(gix.query(Q, k=10, epsilon=0.1)[0], qtruth)
-    print(f"{name}: query recall@10 gpu={q_g:.4f} oracle={q_o:.4f}")
-    assert q_g >= q_o - 0.02
+    g_rec, o_rec, q_g, q_o = [], [], [], []
+    for seed in (42, 7, 1234):
+        oix = orc.OracleIndex(X, n_neighbors=k, distance_kind=kind, correction=corr, angular=angular,
+                              n_trees=kw.get("n_trees", 8), leaf_size=kw.get("leaf_size"),
+                              n_iters=kw.get("n_iters"), random_seed=seed)
+        gix = rb.RINND(X, metric=metric, n_neighbors=k, random_state=seed, **kw)
+        o_rec.append(recall(oix.neighbor_graph[0], truth))
+        g_rec.append(recall(gix.neighbor_graph[0], truth))
+        q_o.append(recall(oix.query(Q, k=10, epsilon=0.1)[0], qtruth))
+        q_g.append(recall(gix.query(Q, k=10, epsilon=0.1)[0], qtruth))
+    g, o, qg, qo = map(np.mean, (g_rec, o_rec, q_g, q_o))
+    print(f"{name}: graph recall@{k} gpu={g:.4f} oracle={o:.4f}; query recall@10 gpu={qg:.4f} oracle={qo:.4f}")
+    assert g >= o - RECALL_TOL
+    assert qg >= qo - RECALL_TOL
 
 
 def test_neighbor_graph_invariants(rb, orc):
@@ -130,12 +135,13 @@ def test_rejects_unknown_metric_and_query_dimension(rb):
 def test_all_hot_metrics_build_and_query(rb, orc, metric):
     X = np.abs(gmm(4000, 48, 20, seed=6)) + np.float32(0.01)
     kind = {"euclidean": 0, "sqeuclidean": 0, "manhattan": 1, "cosine": 3, "dot": 4, "inner_product": 7}[metric]
-    truth_kind = {0: 0, 1: 1, 3: 2, 4: 2, 7: 6}[kind]
+    # AlternativeDot / AlternativeInnerProduct rank by inner product on unnormalized rows
+    truth_kind = {0: 0, 1: 1, 3: 2, 4: 6, 7: 6}[kind]
     ix = rb.RINND(X, metric=metric, n_neighbors=15, n_trees=4, random_state=1)
     truth, _ = orc.exact_knn_f64(truth_kind, X, X, 15, exclude_self=True)
     rec = recall(ix.neighbor_graph[0], truth)
     print(metric, rec)
-    assert rec > (0.5 if metric == "inner_product" else 0.9)
+    assert rec > (0.5 if metric in ("inner_product", "dot") else 0.9)
     qi, qd = ix.query(X[:100], k=10)
     assert qi.shape == (100, 10)
 

@@ -62,7 +62,7 @@ def test_heap_push_batch_matches_sequential(rb, orc):
     # one distance per (row, id), as in NN-Descent where d(p, q) is a function of the pair
     h = (rows.astype(np.uint64) * np.uint64(2654435761) + ids.astype(np.uint64) * np.uint64(40503)) % np.uint64(1 << 20)
     dists = (h.astype(np.float32) / np.float32(1 << 20)) * np.float32(10.0)
-    flags = (rng.random(n_ops) < 0.5).astype(np.uint8)
+    flags = ((h >> np.uint64(7)) & np.uint64(1)).astype(np.uint8)  # also a function of the pair
     oi, od, of, _ = orc.neighbor_heap_apply(n, k, rows, ids, dists, flags)
     gi = np.empty((n, k), np.int32)
     gd = np.empty((n, k), np.float32)
