@@ -47,6 +47,9 @@ struct KnnState {
   DVec<float> norms;         // N squared norms (dot-form metrics)
   // [0] changes, [1] contention, [2] pairs, [3] gathered rows, [4] buffered updates
   DVec<unsigned long long> counters;
+  DVec<uint32_t> cthr;       // 2N candidate-list priority bounds (new, old)
+  DVec<int> err;             // device error flag of pipelined kernels
+  bool use_tma = true;       // bulk-copy pipelined join when shared memory allows
   DVec<uint32_t> urow;       // update buffer: destination rows
   DVec<uint64_t> ukey;       // update buffer: slot keys
   unsigned long long ucap = 0;
@@ -63,6 +66,8 @@ struct JoinStats {
   float kernel_ms = 0.f;  // CUDA-event duration of the join kernel on its stream
 };
 JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st);
+bool join_tma_supported(int c, int Dp);
+void join_tma_batch(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st);
 // Sorted output: idx (-1 empty), raw distance (+inf empty).
 void finalize_knn(const KnnState& s, int32_t* out_idx, float* out_dist, cudaStream_t st);
 void finalize_rows(const uint64_t* slots, int N, int k, int kp, int32_t* out_idx, float* out_dist,

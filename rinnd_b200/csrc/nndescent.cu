@@ -342,23 +342,95 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
-// candidates.rs:153-351: each heap edge offered forward and reverse with one priority.
-__global__ void k_candidates(const uint64_t* slots, int N, int k, int kp, int c, int cp, uint64_t* cnew,
-                             uint64_t* cold, uint64_t seed, int iter,
-                             unsigned long long* contention) {
+// candidates.rs:153-351: each heap edge i->j is offered to i's list (forward)
+// and to j's list (reverse) with one random priority; a list keeps the c
+// lowest priorities with distinct ids.  Forward offers to list i all come from
+// row i, so one warp per row selects them without atomics (k_cand_forward) and
+// records the list's priority bound; reverse offers then go through the
+// lock-free push with that bound as a pre-filter (k_cand_reverse).
+__device__ __forceinline__ uint32_t cand_priority(uint64_t seed, int iter, long long e) {
+  return (uint32_t)(mix64(seed ^ mix64(0xC0DE0000ull + (uint64_t)iter) ^ (uint64_t)e) >> 33);
+}
+
+template <int P>
+__global__ void k_cand_forward(const uint64_t* slots, int N, int k, int kp, int c, int cp, uint64_t* cnew,
+                               uint64_t* cold, uint32_t* thr_new, uint32_t* thr_old, uint64_t seed, int iter) {
+  __shared__ uint64_t buf[4][P];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * 4 + w;
+  if (row >= N) return;
+  uint64_t* b = buf[w];
+  for (int flag = 1; flag >= 0; --flag) {
+    int n = 0;
+    for (int j0 = 0; j0 < P; j0 += 32) {
+      int j = j0 + lane;
+      uint64_t key = ~0ull;
+      if (j < k) {
+        uint64_t sl = slots[(size_t)row * kp + j];
+        int32_t id = slot_id(sl);
+        if (id >= 0 && slot_new(sl) == flag)
+          key = ((uint64_t)cand_priority(seed, iter, (long long)row * k + j) << 32) | (uint32_t)id;
+      }
+      n += __popc(__ballot_sync(0xffffffffu, key != ~0ull));
+      b[j] = key;
+    }
+    __syncwarp();
+    if (n > c) {  // keep the c lowest priorities (bitonic sort of P keys)
+      for (int size = 2; size <= P; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          for (int j = lane; j < P; j += 32) {
+            int partner = j ^ stride;
+            if (partner > j) {
+              bool up = (j & size) == 0;
+              uint64_t x = b[j], y = b[partner];
+              if ((x > y) == up) { b[j] = y; b[partner] = x; }
+            }
+          }
+          __syncwarp();
+        }
+    } else {  // compact in slot order
+      uint64_t keep[P / 32];
+#pragma unroll
+      for (int t = 0; t < P / 32; ++t) keep[t] = b[t * 32 + lane];
+      __syncwarp();
+      int base = 0;
+#pragma unroll
+      for (int t = 0; t < P / 32; ++t) {
+        unsigned m = __ballot_sync(0xffffffffu, keep[t] != ~0ull);
+        if (keep[t] != ~0ull) b[base + __popc(m & ((1u << lane) - 1))] = keep[t];
+        base += __popc(m);
+      }
+      __syncwarp();
+    }
+    uint64_t* list = (flag ? cnew : cold) + (size_t)row * cp;
+    const int kept = min(n, c);
+    for (int t = lane; t < c; t += 32) list[t] = t < kept ? b[t] : CAND_EMPTY;
+    uint32_t bound = 0xFFFFFFFFu;  // accepts any priority until the list is full
+    if (kept == c) {
+      uint32_t mx = 0;
+      for (int t = lane; t < kept; t += 32) mx = max(mx, (uint32_t)(b[t] >> 32));
+      for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      bound = mx;
+    }
+    if (lane == 0) (flag ? thr_new : thr_old)[row] = bound;
+    __syncwarp();
+  }
+}
+
+__global__ void k_cand_reverse(const uint64_t* slots, int N, int k, int kp, int c, int cp, uint64_t* cnew,
+                               uint64_t* cold, uint32_t* thr_new, uint32_t* thr_old, uint64_t seed, int iter,
+                               unsigned long long* contention) {
   long long total = (long long)N * k;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     int32_t i = (int32_t)(e / k);
     int j = (int)(e % k);
-    uint64_t s = slots[(size_t)i * kp + j];
-    int32_t id = slot_id(s);
+    uint64_t sl = slots[(size_t)i * kp + j];
+    int32_t id = slot_id(sl);
     if (id < 0) continue;
-    uint64_t* lists = slot_new(s) ? cnew : cold;
-    uint32_t prio = (uint32_t)(hash3(seed, 0xC0DE0000ull + (uint64_t)iter, (uint64_t)e) >> 33);
-    uint64_t hi = (uint64_t)prio << 32;
-    row_push(lists + (size_t)i * cp, c, nullptr, hi | (uint32_t)id, contention);
-    row_push(lists + (size_t)id * cp, c, nullptr, hi | (uint32_t)i, contention);
+    const bool nw = slot_new(sl);
+    uint64_t key = ((uint64_t)cand_priority(seed, iter, e) << 32) | (uint32_t)i;
+    row_push((nw ? cnew : cold) + (size_t)id * cp, c, (nw ? thr_new : thr_old) + id, key, contention);
   }
 }
 
@@ -512,12 +584,24 @@ void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int 
 }
 
 void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st) {
-  s.cand_new.fill_bytes(0xFF);
-  s.cand_old.fill_bytes(0xFF);
+  if (s.cthr.n < 2 * (size_t)s.N) s.cthr.alloc(2 * (size_t)s.N, st);
+  uint32_t* thr_new = s.cthr.p;
+  uint32_t* thr_old = s.cthr.p + s.N;
+  const int grid = (s.N + 3) / 4;
+  if (s.k <= 32)
+    k_cand_forward<32><<<grid, 128, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p,
+                                             thr_new, thr_old, seed, iter);
+  else if (s.k <= 64)
+    k_cand_forward<64><<<grid, 128, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p,
+                                             thr_new, thr_old, seed, iter);
+  else
+    k_cand_forward<128><<<grid, 128, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p,
+                                              thr_new, thr_old, seed, iter);
+  RINND_LAUNCH_CHECK();
   long long total = (long long)s.N * s.k;
-  k_candidates<<<grid_for(total, 256, 148 * 64), 256, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp,
-                                                              s.cand_new.p, s.cand_old.p, seed, iter,
-                                                              &s.counters.p[1]);
+  k_cand_reverse<<<grid_for(total, 256, 148 * 64), 256, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp,
+                                                                s.cand_new.p, s.cand_old.p, thr_new, thr_old,
+                                                                seed, iter, &s.counters.p[1]);
   RINND_LAUNCH_CHECK();
   k_mark_old<<<grid_for((long long)s.N * 32, 256), 256, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.cand_new.p,
                                                                  s.c, s.cp);
@@ -532,6 +616,11 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
   cudaEvent_t e0, e1;
   RINND_CUDA(cudaEventCreate(&e0));
   RINND_CUDA(cudaEventCreate(&e1));
+  const bool use_tma = s.use_tma && join_tma_supported(s.c, Dp);
+  if (s.err.n == 0) {
+    s.err.alloc(1, st);
+    s.err.fill_bytes(0);
+  }
   // Worst case 4 c^2 updates per vertex (2 directions x c new x 2c candidates).
   const long long per_batch =
       std::max<long long>(1, (long long)(s.ucap / (4ull * (unsigned long long)s.c * (unsigned long long)s.c)));
@@ -540,21 +629,28 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
     int v1 = (int)std::min<long long>(s.N, v0 + per_batch);
     RINND_CUDA(cudaMemsetAsync(s.counters.p + 4, 0, sizeof(unsigned long long), st));
     int grid = (int)std::min<long long>(v1 - v0, 148LL * 16);
-    if (s.c <= 32)
+    if (use_tma) {
+      join_tma_batch(s, X, Dp, kind, (int)v0, v1, s.err.p, st);
+    } else if (s.c <= 32) {
       k_local_join<32, 128><<<grid, 128, 0, st>>>(s.cand_new.p, s.cand_old.p, (int)v0, v1, s.c, s.cp, X, Dp, kind,
                                                   s.norms.p, s.slots.p, s.thr.p, s.k, s.kp, update_buf(s),
                                                   s.counters.p);
-    else
+      RINND_LAUNCH_CHECK();
+    } else {
       k_local_join<64, 256><<<grid, 256, 0, st>>>(s.cand_new.p, s.cand_old.p, (int)v0, v1, s.c, s.cp, X, Dp, kind,
                                                   s.norms.p, s.slots.p, s.thr.p, s.k, s.kp, update_buf(s),
                                                   s.counters.p);
-    RINND_LAUNCH_CHECK();
+      RINND_LAUNCH_CHECK();
+    }
     apply_pending(s, st);
   }
   RINND_CUDA(cudaEventRecord(e1, st));
   unsigned long long h[5];
+  int herr = 0;
   RINND_CUDA(cudaMemcpyAsync(h, s.counters.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  RINND_CUDA(cudaMemcpyAsync(&herr, s.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   RINND_CUDA(cudaStreamSynchronize(st));
+  if (herr) throw CudaError("local join: a shared-memory pipeline stage did not complete within its wait limit");
   JoinStats js;
   RINND_CUDA(cudaEventElapsedTime(&js.kernel_ms, e0, e1));
   cudaEventDestroy(e0);
