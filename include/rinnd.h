@@ -183,6 +183,23 @@ RINND_EXPORT int rinnd_heap_push_batch(int32_t n, int32_t k, int64_t n_ops, cons
                           int32_t* out_idx, float* out_dist, uint8_t* out_flags,
                           int64_t* n_accepted);
 
+/* No counterpart in the reference.  The same operation as rinnd_heap_push_batch
+ * for callers that may not allocate device memory (a host engine that owns the
+ * whole device budget, code that must not call cudaMalloc/cudaFree): every
+ * pointer is caller-owned device memory (d_flags and d_out_flags may be NULL),
+ * `stream` is a cudaStream_t (NULL = legacy default stream), and the n x k rows
+ * live in a static device scratch of 1,048,576 slots that every device loading
+ * the library holds until exit.  Limits: n <= 65536 and n * round_up(k, 16) <=
+ * 1,048,576; larger requests fail with RINND_ERR_INVALID.  The first call on a
+ * device resolves the scratch address and should come before any stream
+ * capture.  Calls that overlap on the GPU race on the shared scratch.  Returns
+ * after the stream has finished the work (*n_accepted is read back). */
+RINND_EXPORT int rinnd_heap_push_batch_noalloc(int32_t n, int32_t k, int64_t n_ops, const int32_t* d_rows,
+                                               const int32_t* d_ids, const float* d_dists,
+                                               const uint8_t* d_flags, int32_t* d_out_idx,
+                                               float* d_out_dist, uint8_t* d_out_flags,
+                                               int64_t* n_accepted, void* stream);
+
 /* ---- misc ------------------------------------------------------------------- */
 RINND_EXPORT const char* rinnd_last_error(void);
 RINND_EXPORT const char* rinnd_version(void);

@@ -32,8 +32,17 @@ std::atomic<unsigned long long>& launch_counter() {
 }  // namespace rinnd
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
+
+namespace rinnd {
+int api_fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+}  // namespace rinnd
+
+namespace {
 
 struct NoDevice : std::runtime_error {
   using std::runtime_error::runtime_error;

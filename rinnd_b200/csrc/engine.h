@@ -4,7 +4,12 @@
 
 #include "devmem.cuh"
 
+#include <string>
+
 namespace rinnd {
+
+// Records msg as the thread's last error (rinnd_last_error) and returns code.
+int api_fail(int code, const std::string& msg);
 
 // ---- RP forest (forest.cu) -------------------------------------------------
 // Level-synchronous batched construction of all trees at once.  Node ids are

@@ -1,0 +1,81 @@
+"""The allocation-free push batch (rinnd_heap_push_batch_noalloc) against the
+allocating entry point (rinnd_heap_push_batch).
+
+This entry point exists for callers that cannot allocate device memory, e.g. a
+host engine that owns the whole device budget or code that must not call
+cudaMalloc/cudaFree: they pass their own device buffers and the heap rows live
+in the library's static scratch.  The test drives it through the C ABI with
+device buffers owned by the test, twice in a row with different inputs (the
+scratch keeps the previous call's contents, so the second call proves it is
+cleared), and requires outputs identical to the allocating entry point's.
+It sits in its own file, collected last, and works alone or after the suite.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def make_pushes(seed, n, k, n_ops, n_ids):
+    rng = np.random.default_rng(seed)
+    rows = rng.integers(0, n, n_ops).astype(np.int32)
+    ids = rng.integers(0, n_ids, n_ops).astype(np.int32)
+    # one distance and flag per (row, id), as in NN-Descent where both are functions of the pair
+    h = (rows.astype(np.uint64) * np.uint64(2654435761) + ids.astype(np.uint64) * np.uint64(40503)) % np.uint64(1 << 20)
+    dists = (h.astype(np.float32) / np.float32(1 << 20)) * np.float32(10.0)
+    flags = ((h >> np.uint64(7)) & np.uint64(1)).astype(np.uint8)
+    return rows, ids, dists, flags
+
+
+def allocating(L, n, k, rows, ids, dists, flags):
+    oi = np.empty((n, k), np.int32)
+    od = np.empty((n, k), np.float32)
+    of = np.empty((n, k), np.uint8)
+    acc = ctypes.c_int64(0)
+    L.check(L.lib.rinnd_heap_push_batch(n, k, rows.size, L.ptr(rows), L.ptr(ids), L.ptr(dists), L.ptr(flags),
+                                        L.ptr(oi), L.ptr(od), L.ptr(of), ctypes.byref(acc)))
+    return oi, od, of, acc.value
+
+
+def noalloc(L, torch, n, k, rows, ids, dists, flags):
+    dev = torch.device("cuda", 0)
+    t_rows, t_ids = torch.from_numpy(rows).to(dev), torch.from_numpy(ids).to(dev)
+    t_d, t_f = torch.from_numpy(dists).to(dev), torch.from_numpy(flags).to(dev)
+    oi = torch.empty((n, k), dtype=torch.int32, device=dev)
+    od = torch.empty((n, k), dtype=torch.float32, device=dev)
+    of = torch.empty((n, k), dtype=torch.uint8, device=dev)
+    acc = ctypes.c_int64(-1)
+    stream = torch.cuda.current_stream(dev)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    L.check(L.lib.rinnd_heap_push_batch_noalloc(n, k, rows.size, p(t_rows), p(t_ids), p(t_d), p(t_f), p(oi),
+                                                p(od), p(of), ctypes.byref(acc), ctypes.c_void_p(stream.cuda_stream)))
+    return oi.cpu().numpy(), od.cpu().numpy(), of.cpu().numpy(), acc.value
+
+
+def test_noalloc_matches_allocating_entry_point_twice():
+    torch = pytest.importorskip("torch")
+    from rinnd_b200 import _lib as L
+
+    assert L.device_count() > 0
+    for seed, (n, k, n_ops, n_ids) in [(11, (300, 12, 80000, 600)), (12, (1000, 30, 120000, 3000))]:
+        rows, ids, dists, flags = make_pushes(seed, n, k, n_ops, n_ids)
+        ai, ad, af, _ = allocating(L, n, k, rows, ids, dists, flags)
+        ni, nd, nf, nacc = noalloc(L, torch, n, k, rows, ids, dists, flags)
+        # both sort rows by (distance, id): outputs are bit-identical
+        np.testing.assert_array_equal(ni, ai)
+        np.testing.assert_array_equal(nd.view(np.uint32), ad.view(np.uint32))
+        np.testing.assert_array_equal(nf, af)
+        assert nacc >= int((ai >= 0).sum())
+
+
+def test_noalloc_rejects_oversized_requests():
+    from rinnd_b200 import _lib as L
+
+    # 70000 rows > 65536; 40000 x round_up(30, 16) = 1.28M slots > 1,048,576
+    for n, k in [(70000, 4), (40000, 30)]:
+        rc = L.lib.rinnd_heap_push_batch_noalloc(n, k, 0, None, None, None, None, ctypes.c_void_p(8),
+                                                 ctypes.c_void_p(8), None, None, None)
+        assert rc == L.ERR_INVALID
+        assert "allocation-free" in L.last_error()
