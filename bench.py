@@ -61,6 +61,7 @@ def parse_args():
     ap.add_argument("--no-recall", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--verbose", action="store_true", help="per-iteration build statistics")
     ap.add_argument("--parity", action="store_true",
                     help="also build the oracle (CPU restatement) at the full size and report its recall")
     return ap.parse_args()
@@ -233,6 +234,7 @@ def main():
     L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
     p.n_neighbors, p.n_trees, p.leaf_size, p.n_iters, p.delta = K, N_TREES, LEAF, N_ITERS, DELTA
     p.distance_kind, p.correction, p.random_seed, p.device = L.DIST_SQEUCLIDEAN, L.CORR_NONE, 42, local_rank
+    p.verbose = int(args.verbose)
 
     def build(src_ptr, on_device):
         h = ctypes.c_void_p()
@@ -408,7 +410,10 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu,
             "query": {"qps": qps, "k": QK, "epsilon": EPS, "n_queries": N_QUERIES, **quality},
             "timed_steps_ms": {"event": step_ms, "host_total": [i.ms_total for i in infos],
-                               "join_kernels": [i.ms_join_kernel for i in infos]},
+                               "join_kernels": [i.ms_join_kernel for i in infos],
+                               "phases": [{"forest": i.ms_forest, "leaf_init": i.ms_leaf_init,
+                                           "candidates": i.ms_candidates, "join": i.ms_join,
+                                           "sort": i.ms_sort, "graph": i.ms_graph} for i in infos]},
             "counters": {"pairs_evaluated": int(inf.pairs_evaluated), "pushes_accepted": int(inf.pushes_accepted),
                          "push_contention": int(inf.push_contention), "join_rows": int(inf.join_rows_gathered),
                          "iterations": int(inf.iterations), "n_leaves": int(inf.n_leaves)},

@@ -99,6 +99,44 @@ void ensure_device(int dev) {
   }
 }
 
+// Grows the device's stream-ordered pool once to `bytes` (a single mapping) when
+// this library has not yet reserved that much on the device.  Growing the pool
+// piecemeal, one new mapping per large block a build asks for, stalled 1M-point
+// builds by 0.1-1.5 s until the pool's segments happened to fit the build's
+// allocation pattern; one reservation of the working set removes the stalls.
+// The reservation is best effort: a failed allocation leaves the pool as it was.
+void reserve_pool(int dev, size_t bytes, cudaStream_t st) {
+  static std::mutex mu;
+  static size_t reserved[64] = {};
+  if (dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (bytes <= reserved[dev]) return;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  bytes = std::min(bytes, free_b / 10 * 9);
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, bytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  RINND_CUDA(cudaFreeAsync(p, st));
+  reserved[dev] = bytes;
+}
+
+// Device working set of one build: rows (input copy and search layout), forest,
+// neighbor rows, candidate lists, join descriptors, update buffer, sorted rows and
+// search-graph temporaries, plus a quarter for fragmentation.
+size_t build_working_set(int64_t n, int Dp, int k, int c, int n_trees) {
+  const double N = (double)n;
+  const int kp = round_up(k, 16), cp = round_up(c, 16), maxc = c <= 32 ? 32 : 64;
+  double b = N * Dp * 4.0 * 2 + N * std::max(n_trees, 1) * 4.0 * 2 + N * kp * 8.0 + 2 * N * cp * 8.0 +
+             N * (20 + 6 * maxc) * 4.0 + std::max(4194304.0, 96 * N) * 12.0 + N * k * 8.0 * 3 + 256.0 * (1 << 20);
+  return (size_t)(b * 1.25);
+}
+
 double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -256,6 +294,7 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   ix->p.n_iters = n_iters;
   ix->p.search_tree_leaf_budget = std::max(1, pin->search_tree_leaf_budget);
 
+  reserve_pool(pin->device, build_working_set(n, Dp, k, c, pin->n_trees), st);
   TempStorage tmp;
   DVec<float> X0;
   load_rows(data, on_device, n, d, ld, Dp, X0, st);
@@ -294,8 +333,8 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
     pushes_total += js.changes;
     rows_total += js.rows;
     if (pin->verbose)
-      std::printf("Iteration %d: %llu updates (%llu pairs, %.3f ms join)\n", it + 1, js.changes, js.pairs,
-                  js.kernel_ms);
+      std::printf("Iteration %d: %llu updates (%llu pairs, %llu rows, %llu buffered of %llu, %.3f ms join)\n",
+                  it + 1, js.changes, js.pairs, js.rows, js.updates, js.appended, js.kernel_ms);
     if ((size_t)js.changes <= conv) break;
   }
   double t3 = now_ms();

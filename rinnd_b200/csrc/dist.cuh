@@ -203,7 +203,7 @@ __device__ __forceinline__ float exact_distance(int kind, const float* a, const 
 }
 
 // Metrics evaluated from (dot, |a|^2, |b|^2) in the tiled join kernels.
-__device__ __forceinline__ bool kind_is_dot(int kind) {
+__host__ __device__ __forceinline__ bool kind_is_dot(int kind) {
   return kind != DK_SQEUCLIDEAN && kind != DK_MANHATTAN;
 }
 __device__ __forceinline__ float finalize_dot(int kind, float dot, float na, float nb) {

@@ -50,14 +50,17 @@ struct KnnState {
   DVec<uint64_t> cand_new;   // N*cp
   DVec<uint64_t> cand_old;   // N*cp
   DVec<float> norms;         // N squared norms (dot-form metrics)
-  // [0] changes, [1] contention, [2] pairs, [3] gathered rows, [4] buffered updates
+  // [0] changes, [1] contention, [2] pairs, [3] gathered rows, [4] buffered updates (batch),
+  // [5] applied buffered updates (iteration), [6] appended updates incl. overflow (iteration)
   DVec<unsigned long long> counters;
   DVec<uint32_t> cthr;       // 2N candidate-list priority bounds (new, old)
   DVec<int> err;             // device error flag of pipelined kernels
+  DVec<int32_t> desc;        // per-vertex join descriptors (counts, item prefix, ids, thresholds, norms)
   bool use_tma = true;       // bulk-copy pipelined join when shared memory allows
   DVec<uint32_t> urow;       // update buffer: destination rows
   DVec<uint64_t> ukey;       // update buffer: slot keys
   unsigned long long ucap = 0;
+  double upv_prev = -1.0;    // updates appended per vertex by the previous join (-1: none yet)
 };
 
 void knn_init(KnnState& s, int N, int k, int c, cudaStream_t st);
@@ -67,12 +70,13 @@ void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int 
                cudaStream_t st);
 void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st);
 struct JoinStats {
-  unsigned long long changes = 0, pairs = 0, rows = 0;
+  unsigned long long changes = 0, pairs = 0, rows = 0, updates = 0, appended = 0;
   float kernel_ms = 0.f;  // CUDA-event duration of the join kernel on its stream
 };
 JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st);
 bool join_tma_supported(int c, int Dp);
 void join_tma_batch(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st);
+void join_describe(KnnState& s, int kind, cudaStream_t st);
 // Sorted output: idx (-1 empty), raw distance (+inf empty).
 void finalize_knn(const KnnState& s, int32_t* out_idx, float* out_dist, cudaStream_t st);
 void finalize_rows(const uint64_t* slots, int N, int k, int kp, int32_t* out_idx, float* out_dist,

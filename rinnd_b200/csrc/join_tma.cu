@@ -1,24 +1,29 @@
-// join_tma.cu -- NN-Descent local join with bulk-copy row gathers (sm_100a).
+// join_tma.cu -- warp-specialized NN-Descent local join with bulk-copy gathers (sm_100a).
 //
 // Same pairs and push semantics as the chunked join in nndescent.cu (the
 // reference's update_iteration, core/nndescent/mod.rs:383-446): per vertex,
 // new x new (q after p) and new x old (q != p) candidate pairs, each pushed to
 // an endpoint's row when it beats that row's threshold.
 //
-// Persistent CTAs walk a strided vertex sequence through a two-stage shared
-// memory pipeline.  Warp 0 prepares the next vertex: it compacts the candidate
-// ids, caches their thresholds/norms and issues one cp.async.bulk (TMA engine)
-// copy per candidate row (Dp floats) into a padded slot of the free stage,
-// completing on that stage's mbarrier; meanwhile every warp computes the current
-// vertex from the other stage.  A thread owns (4 A rows) x (1 B row) and
-// accumulates 4 distances with 5 shared loads per 4 dimensions; consecutive
-// lanes take consecutive B rows (row stride Dp + 4 floats: conflict-free).
-// Updates that pass a threshold are appended to the device update buffer
-// (one atomic per warp) and applied by k_apply_updates.
-//
-// Waits are bounded: a stage that does not complete within the poll limit sets
-// the error flag, waits (bounded) for the other stage's copies, and the CTA
-// leaves; the host turns the flag into an error.
+// Work decomposition.  A prepass (k_cand_describe) writes one descriptor per
+// vertex: counts, the compacted candidate ids (new first), their thresholds and
+// norms, and a prefix table of the work items.  An item is (4 consecutive new
+// rows) x (1 candidate row j); items entirely on or below the new x new
+// diagonal are never generated.  Persistent CTAs of 1 producer warp + 8
+// consumer warps walk a strided vertex sequence:
+//   producer: keeps NDESC descriptors in flight (one cp.async.bulk each into a
+//     ring, completing on per-slot mbarriers); per vertex it waits for a free
+//     row stage (empty mbarrier, armed by the consumer warps), copies the
+//     descriptor and the candidates' current row thresholds into the stage and
+//     issues one cp.async.bulk per candidate row
+//     (Dp floats) into a padded slot, completing on the stage's full mbarrier;
+//   consumers: wait for the stage; each thread computes one item per round --
+//     4 distances with packed FP32x2 arithmetic from 5 conflict-free 16-byte
+//     shared loads per 4 dimensions -- and appends threshold-passing updates to
+//     the device update buffer (one atomic per warp) for k_apply_updates.
+// Every wait is bounded.  A wait that runs out sets the device error flag and a
+// shared abort flag; all warps leave, the producer first waiting (bounded) for
+// every copy it issued.  The host turns the flag into an error.
 #include "async_copy.cuh"
 #include "dist.cuh"
 #include "engine.h"
@@ -27,34 +32,45 @@
 namespace rinnd {
 namespace {
 
-constexpr uint32_t WAIT_POLLS = 1u << 22;
+constexpr uint32_t WAIT_POLLS = 1u << 21;
+constexpr int NSTAGE = 3;   // row stages
+constexpr int NDESC = 4;    // descriptor ring
+constexpr int NCONS = 8;    // consumer warps
+constexpr int NT = 32 * (1 + NCONS);
+constexpr int NQMAX = 16;   // max item quads per vertex (na <= 64)
 
-struct StageHdr {
-  int na, nb, v, pad;
+// Descriptor (ints): [0] na, [1] nb, [2] nq, [3] items, [4..20) quad item prefix,
+// [20..) ids (2*maxc), thresholds (2*maxc; filled in the stage by the producer), norms (2*maxc).
+struct Desc {
+  static constexpr int HDR = 4 + NQMAX;
+  __host__ __device__ static int ids(int) { return HDR; }
+  __host__ __device__ static int thr(int maxc) { return HDR + 2 * maxc; }
+  __host__ __device__ static int nrm(int maxc) { return HDR + 4 * maxc; }
+  __host__ __device__ static int stride(int maxc) { return (HDR + 6 * maxc + 15) / 16 * 16; }
 };
 
-struct StageLayout {
-  int maxc, dp, rs;  // rs = row stride in floats
-  __host__ __device__ size_t ids_off() const { return sizeof(StageHdr); }
-  __host__ __device__ size_t thr_off() const { return ids_off() + (size_t)2 * maxc * 4; }
-  __host__ __device__ size_t nrm_off() const { return thr_off() + (size_t)2 * maxc * 4; }
-  __host__ __device__ size_t rows_off() const { return (nrm_off() + (size_t)2 * maxc * 4 + 15) / 16 * 16; }
-  __host__ __device__ size_t bytes() const {
-    return (rows_off() + (size_t)(2 * maxc + 4) * rs * 4 + 15) / 16 * 16;
-  }
+struct Layout {
+  int maxc, dp, rs, dstride;  // rs: row stride (floats); dstride: descriptor stride (ints)
+  __host__ __device__ size_t bar_bytes() const { return 8 * (2 * NSTAGE + NDESC) + 16; }
+  __host__ __device__ size_t desc_off() const { return (bar_bytes() + 15) / 16 * 16; }
+  __host__ __device__ size_t stage_off() const { return desc_off() + (size_t)NDESC * dstride * 4; }
+  __host__ __device__ size_t rows_off() const { return (size_t)dstride * 4; }  // within a stage
+  // rows read: B rows j < nb and A quads up to row na + 3 <= 2 * maxc - 1
+  __host__ __device__ size_t stage_bytes() const { return rows_off() + (size_t)(2 * maxc) * rs * 4; }
+  __host__ __device__ size_t bytes() const { return stage_off() + NSTAGE * stage_bytes(); }
 };
 
-template <int MAXC>
-__device__ __forceinline__ void produce(unsigned char* stage, const StageLayout& L, uint64_t* bar,
-                                        const uint64_t* cand_new, const uint64_t* cand_old, int v, int c,
-                                        int cp, const float* __restrict__ X, int Dp, const uint32_t* thr,
-                                        const float* norms) {
-  const int lane = threadIdx.x & 31;
-  StageHdr* hdr = reinterpret_cast<StageHdr*>(stage);
-  int32_t* ids = reinterpret_cast<int32_t*>(stage + L.ids_off());
-  uint32_t* sthr = reinterpret_cast<uint32_t*>(stage + L.thr_off());
-  float* snrm = reinterpret_cast<float*>(stage + L.nrm_off());
-  float* rows = reinterpret_cast<float*>(stage + L.rows_off());
+Layout make_layout(int c, int Dp) {
+  const int maxc = c <= 32 ? 32 : 64;
+  return Layout{maxc, Dp, Dp + 4, Desc::stride(maxc)};
+}
+
+__global__ void k_cand_describe(const uint64_t* cand_new, const uint64_t* cand_old, int N, int c, int cp, int maxc,
+                                int dstride, const float* norms, int32_t* desc) {
+  const int v = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (v >= N) return;
+  int32_t* d = desc + (size_t)v * dstride;
+  int32_t* ids = d + Desc::ids(maxc);
   int base = 0;
   for (int t0 = 0; t0 < c; t0 += 32) {
     int t = t0 + lane;
@@ -64,7 +80,7 @@ __device__ __forceinline__ void produce(unsigned char* stage, const StageLayout&
     base += __popc(m);
   }
   const int na = base;
-  if (na > 0) {  // a vertex without new candidates contributes no pairs
+  if (na > 0)  // a vertex without new candidates contributes no pairs
     for (int t0 = 0; t0 < c; t0 += 32) {
       int t = t0 + lane;
       int32_t id = t < c ? slot_id(cand_old[(size_t)v * cp + t]) : -1;
@@ -72,152 +88,260 @@ __device__ __forceinline__ void produce(unsigned char* stage, const StageLayout&
       if (id >= 0) ids[base + __popc(m & ((1u << lane) - 1))] = id;
       base += __popc(m);
     }
-  }
   const int nb = base;
   __syncwarp();
-  for (int r = lane; r < nb; r += 32) {
-    int32_t id = ids[r];
-    sthr[r] = __ldcg(thr + id);
-    if (norms) snrm[r] = norms[id];
+  if (norms)
+    for (int r = lane; r < nb; r += 32) reinterpret_cast<float*>(d)[Desc::nrm(maxc) + r] = norms[ids[r]];
+  // items of quad iq: candidate rows j in [4 iq + 1, nb)
+  const int nq = (na + 3) >> 2;
+  int cnt = (lane < nq) ? max(0, nb - (4 * lane + 1)) : 0;
+  int incl = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
   }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  if (lane < NQMAX) d[4 + lane] = incl - cnt;
   if (lane == 0) {
-    hdr->na = na;
-    hdr->nb = nb;
-    hdr->v = v;
+    d[0] = na;
+    d[1] = nb;
+    d[2] = nq;
+    d[3] = total;
   }
-  fence_proxy_async_smem();  // earlier generic reads of this stage before the async writes
-  __syncwarp();
-  if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)nb * (uint32_t)Dp * 4u);
-  __syncwarp();
-  for (int r = lane; r < nb; r += 32)
-    bulk_g2s(rows + (size_t)r * L.rs, X + (size_t)ids[r] * Dp, (uint32_t)Dp * 4u, bar);
 }
 
-template <int MAXC, int NT>
+struct Bars {
+  uint64_t* full;   // [NSTAGE]
+  uint64_t* empty;  // [NSTAGE]
+  uint64_t* desc;   // [NDESC]
+  int* abort_flag;
+};
+
+// Bounded wait that also gives up when another warp has aborted.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  for (uint32_t i = 0; i < WAIT_POLLS; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63) == 63 && *abort_flag) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Packed FP32x2 arithmetic (each half rounded as the scalar instruction).
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ float f2_sum(unsigned long long a) {
+  return __uint_as_float((uint32_t)a) + __uint_as_float((uint32_t)(a >> 32));
+}
+
+template <int MAXC>
 __global__ void __launch_bounds__(NT)
-    k_join_tma(const uint64_t* cand_new, const uint64_t* cand_old, int v0, int v1, int c, int cp,
-               const float* __restrict__ X, int Dp, int kind, const float* norms, uint64_t* slots,
-               uint32_t* thr, int k, int kp, StageLayout L, uint32_t* urow_buf, uint64_t* ukey_buf,
-               unsigned long long* ucount, unsigned long long ucap, unsigned long long* counters, int* err) {
+    k_join_ws(const int32_t* __restrict__ desc, int v0, int v1, const float* __restrict__ X, int Dp, int kind,
+              uint64_t* slots, uint32_t* thr, int k, int kp, Layout L, uint32_t* urow_buf, uint64_t* ukey_buf,
+              unsigned long long* ucount, unsigned long long ucap, unsigned long long* counters, int* err) {
   extern __shared__ __align__(16) unsigned char smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
-  unsigned char* const stage0 = smem + 16;
-  const size_t stage_bytes = L.bytes();
+  Bars B{reinterpret_cast<uint64_t*>(smem), reinterpret_cast<uint64_t*>(smem) + NSTAGE,
+         reinterpret_cast<uint64_t*>(smem) + 2 * NSTAGE,
+         reinterpret_cast<int*>(smem + 8 * (2 * NSTAGE + NDESC))};
+  int32_t* dring = reinterpret_cast<int32_t*>(smem + L.desc_off());
+  unsigned char* stage0 = smem + L.stage_off();
+  const size_t sbytes = L.stage_bytes();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const bool is_dot = kind_is_dot(kind);
   if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int s = 0; s < NSTAGE; ++s) {
+      mbar_init(&B.full[s], 1);
+      mbar_init(&B.empty[s], NCONS);
+    }
+    for (int s = 0; s < NDESC; ++s) mbar_init(&B.desc[s], 1);
+    *B.abort_flag = 0;
     fence_mbar_init();
   }
   __syncthreads();
-  const int first = v0 + blockIdx.x;
+  const int first = v0 + (int)blockIdx.x;
   if (first >= v1) return;
-  if (warp == 0)
-    produce<MAXC>(stage0, L, &bars[0], cand_new, cand_old, first, c, cp, X, Dp, thr, is_dot ? norms : nullptr);
-  unsigned int pairs_total = 0, rows_total = 0;
-  for (int it = 0;; ++it) {
-    const int v = first + it * gridDim.x;
-    if (v >= v1) break;
-    const int s = it & 1;
-    const int vn = v + gridDim.x;
-    if (warp == 0 && vn < v1)
-      produce<MAXC>(stage0 + (size_t)(s ^ 1) * stage_bytes, L, &bars[s ^ 1], cand_new, cand_old, vn, c, cp, X, Dp, thr,
-                    is_dot ? norms : nullptr);
-    const uint32_t parity = (uint32_t)(it >> 1) & 1u;
+  const int stride = gridDim.x;
+  const int nv = (v1 - first + stride - 1) / stride;  // vertices of this CTA
+  volatile int* abort_flag = B.abort_flag;
+  const int dstride = L.dstride;
+
+  if (warp == 0) {
+    // ------------------------------ producer ------------------------------
+    const uint32_t dbytes = (uint32_t)dstride * 4u;
+    if (lane == 0)
+      for (int i = 0; i < NDESC && i < nv; ++i) {
+        mbar_arrive_expect_tx(&B.desc[i], dbytes);
+        bulk_g2s(dring + (size_t)i * dstride, desc + (size_t)(first + i * stride) * dstride, dbytes, &B.desc[i]);
+      }
     bool ok = true;
-    if (tid == 0) ok = mbar_wait_bounded(&bars[s], parity, WAIT_POLLS);
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
+    int i = 0;
+    int desc_issued = nv < NDESC ? nv : NDESC;  // descriptors issued for vertices [0, desc_issued)
+    for (; i < nv; ++i) {
+      const int ds = i % NDESC, s = i % NSTAGE;
+      ok = wait_or_abort(&B.desc[ds], (uint32_t)(i / NDESC) & 1u, abort_flag);
+      if (!ok) break;
+      if (i >= NSTAGE) {
+        ok = wait_or_abort(&B.empty[s], (uint32_t)((i / NSTAGE) - 1) & 1u, abort_flag);
+        if (!ok) break;
+      }
+      const int32_t* dsc = dring + (size_t)ds * dstride;
+      unsigned char* st = stage0 + (size_t)s * sbytes;
+      int32_t* sd = reinterpret_cast<int32_t*>(st);
+      const int nb = dsc[1];
+      for (int t = lane; t < dstride; t += 32) sd[t] = dsc[t];  // descriptor -> stage header
+      // row thresholds as of now (pushes applied by earlier batches tighten them)
+      int32_t my_ids[(2 * MAXC + 31) / 32];
+      uint32_t* sthr = reinterpret_cast<uint32_t*>(sd + Desc::thr(MAXC));
+#pragma unroll
+      for (int t = 0; t < (2 * MAXC + 31) / 32; ++t) {
+        const int r = lane + 32 * t;
+        my_ids[t] = r < nb ? dsc[Desc::ids(MAXC) + r] : 0;
+        if (r < nb) sthr[r] = __ldcg(thr + my_ids[t]);
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      // descriptor slot consumed: refill it NDESC vertices ahead
+      if (i + NDESC < nv) {
+        desc_issued = i + NDESC + 1;
+        if (lane == 0) {
+          mbar_arrive_expect_tx(&B.desc[ds], dbytes);
+          bulk_g2s(dring + (size_t)ds * dstride, desc + (size_t)(first + (i + NDESC) * stride) * dstride, dbytes,
+                   &B.desc[ds]);
+        }
+      }
+      float* rows = reinterpret_cast<float*>(st + L.rows_off());
+      if (lane == 0) mbar_arrive_expect_tx(&B.full[s], (uint32_t)nb * (uint32_t)Dp * 4u);
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < (2 * MAXC + 31) / 32; ++t) {
+        const int r = lane + 32 * t;
+        if (r < nb) bulk_g2s(rows + (size_t)r * L.rs, X + (size_t)my_ids[t] * Dp, (uint32_t)Dp * 4u, &B.full[s]);
+      }
+    }
+    if (!ok && lane == 0) {
+      *abort_flag = 1;
+      atomicExch(err, 1);
+      // drain: wait (bounded) for every descriptor and row copy this warp issued
+      for (int j = i; j < desc_issued; ++j)
+        mbar_wait_bounded(&B.desc[j % NDESC], (uint32_t)(j / NDESC) & 1u, WAIT_POLLS);
+      for (int j = (i > NSTAGE ? i - NSTAGE : 0); j < i; ++j)
+        mbar_wait_bounded(&B.full[j % NSTAGE], (uint32_t)(j / NSTAGE) & 1u, WAIT_POLLS);
+    }
+    return;
+  }
+
+  // ------------------------------ consumers ------------------------------
+  const int ct = tid - 32;
+  const bool is_dot = kind_is_dot(kind);
+  unsigned int pairs_total = 0;
+  unsigned long long rows_total = 0;
+  for (int i = 0; i < nv; ++i) {
+    const int s = i % NSTAGE;
+    if (!wait_or_abort(&B.full[s], (uint32_t)(i / NSTAGE) & 1u, abort_flag)) {
+      if (lane == 0) {
+        *abort_flag = 1;
         atomicExch(err, 1);
-        if (vn < v1) mbar_wait_bounded(&bars[s ^ 1], parity ^ ((s ^ 1) < s ? 1u : 0u), WAIT_POLLS);
       }
       return;
     }
-    mbar_try_wait(&bars[s], parity);  // acquire the completed phase in every thread
-    unsigned char* st = stage0 + (size_t)s * stage_bytes;
-    const StageHdr hdr = *reinterpret_cast<const StageHdr*>(st);
-    const int32_t* ids = reinterpret_cast<const int32_t*>(st + L.ids_off());
-    const uint32_t* sthr = reinterpret_cast<const uint32_t*>(st + L.thr_off());
-    const float* snrm = reinterpret_cast<const float*>(st + L.nrm_off());
+    const unsigned char* st = stage0 + (size_t)s * sbytes;
+    const int32_t* sd = reinterpret_cast<const int32_t*>(st);
+    const int na = sd[0], nb = sd[1], nq = sd[2], items = sd[3];
+    const int32_t* ids = sd + Desc::ids(MAXC);
+    const uint32_t* sthr = reinterpret_cast<const uint32_t*>(sd + Desc::thr(MAXC));
+    const float* snrm = reinterpret_cast<const float*>(sd + Desc::nrm(MAXC));
     const float* rows = reinterpret_cast<const float*>(st + L.rows_off());
-    const int na = hdr.na, nb = hdr.nb;
-    const int nq = (na + 3) >> 2;
-    const int items = nq * nb;
-    for (int b0 = 0; b0 < items; b0 += NT) {
-      const int item = b0 + tid;
+    if (ct == 0) rows_total += (unsigned long long)nb;
+    for (int b0 = 0; b0 < items; b0 += 32 * NCONS) {
+      const int item = b0 + ct;
       const bool active = item < items;
       int iq = 0, j = 0;
-      float acc[4] = {0.f, 0.f, 0.f, 0.f};
+      unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
       if (active) {
-        iq = item / nb;
-        j = item - iq * nb;
-        const float4* pb = reinterpret_cast<const float4*>(rows + (size_t)j * L.rs);
-        const float4* pa = reinterpret_cast<const float4*>(rows + (size_t)(4 * iq) * L.rs);
+        for (int q = 1; q < nq; ++q) iq += (sd[4 + q] <= item);
+        j = 4 * iq + 1 + (item - sd[4 + iq]);
+        const ulonglong2* pb = reinterpret_cast<const ulonglong2*>(rows + (size_t)j * L.rs);
+        const ulonglong2* pa = reinterpret_cast<const ulonglong2*>(rows + (size_t)(4 * iq) * L.rs);
         const int ars = L.rs / 4;
         if (kind == DK_SQEUCLIDEAN) {
 #pragma unroll 4
           for (int q = 0; q < Dp / 4; ++q) {
-            float4 b = pb[q];
+            const ulonglong2 b = pb[q];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-              float4 a = pa[u * ars + q];
-              float d0 = a.x - b.x, d1 = a.y - b.y, d2 = a.z - b.z, d3 = a.w - b.w;
-              acc[u] = fmaf(d0, d0, acc[u]);
-              acc[u] = fmaf(d1, d1, acc[u]);
-              acc[u] = fmaf(d2, d2, acc[u]);
-              acc[u] = fmaf(d3, d3, acc[u]);
+              const ulonglong2 a = pa[u * ars + q];
+              const unsigned long long d01 = f2_sub(a.x, b.x), d23 = f2_sub(a.y, b.y);
+              acc[u] = f2_fma(d01, d01, acc[u]);
+              acc[u] = f2_fma(d23, d23, acc[u]);
             }
           }
         } else if (kind == DK_MANHATTAN) {
+          const unsigned long long absmask = 0x7FFFFFFF7FFFFFFFull;
 #pragma unroll 4
           for (int q = 0; q < Dp / 4; ++q) {
-            float4 b = pb[q];
+            const ulonglong2 b = pb[q];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-              float4 a = pa[u * ars + q];
-              acc[u] += fabsf(a.x - b.x) + fabsf(a.y - b.y) + fabsf(a.z - b.z) + fabsf(a.w - b.w);
+              const ulonglong2 a = pa[u * ars + q];
+              acc[u] = f2_add(acc[u], f2_sub(a.x, b.x) & absmask);
+              acc[u] = f2_add(acc[u], f2_sub(a.y, b.y) & absmask);
             }
           }
         } else {
 #pragma unroll 4
           for (int q = 0; q < Dp / 4; ++q) {
-            float4 b = pb[q];
+            const ulonglong2 b = pb[q];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-              float4 a = pa[u * ars + q];
-              acc[u] = fmaf(a.x, b.x, acc[u]);
-              acc[u] = fmaf(a.y, b.y, acc[u]);
-              acc[u] = fmaf(a.z, b.z, acc[u]);
-              acc[u] = fmaf(a.w, b.w, acc[u]);
+              const ulonglong2 a = pa[u * ars + q];
+              acc[u] = f2_fma(a.x, b.x, acc[u]);
+              acc[u] = f2_fma(a.y, b.y, acc[u]);
             }
           }
         }
       }
-      // validity, thresholds -> emit masks (bit u: push to row of A[4iq+u]; bit 4+u: to B[j])
+      // validity and thresholds -> emit bits (u: push into A row; 4+u: into B row)
       uint32_t kd[4];
       unsigned emit = 0;
       int n_emit = 0;
+      const int32_t bid = active ? ids[j] : -1;
+      const uint32_t bthr = active ? sthr[j] : 0u;
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         kd[u] = 0;
-        const int i = 4 * iq + u;
-        if (active && i < na) {
-          bool valid = (j < na) ? (j > i) : (ids[j] != ids[i]);  // mod.rs:396, :424
+        const int ia = 4 * iq + u;
+        if (active && ia < na) {
+          const bool valid = (j < na) ? (j > ia) : (bid != ids[ia]);  // mod.rs:396, :424
           if (valid) {
             ++pairs_total;
-            float d = acc[u];
-            if (is_dot) d = finalize_dot(kind, d, snrm[i], snrm[j]);
+            float d = f2_sum(acc[u]);
+            if (is_dot) d = finalize_dot(kind, d, snrm[ia], snrm[j]);
             kd[u] = fkey(d);
-            if (kd[u] < sthr[i]) { emit |= 1u << u; ++n_emit; }
-            if (kd[u] < sthr[j]) { emit |= 16u << u; ++n_emit; }
+            if (kd[u] < sthr[ia]) { emit |= 1u << u; ++n_emit; }
+            if (kd[u] < bthr) { emit |= 16u << u; ++n_emit; }
           }
         }
       }
       int incl = n_emit;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += y;
       }
       const int warp_total = __shfl_sync(0xffffffffu, incl, 31);
@@ -227,12 +351,12 @@ __global__ void __launch_bounds__(NT)
       if (emit) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const int i = 4 * iq + u;
 #pragma unroll
           for (int side = 0; side < 2; ++side) {
             if (!(emit & ((side ? 16u : 1u) << u))) continue;
-            const int32_t row = side ? ids[j] : ids[i];
-            const int32_t other = side ? ids[i] : ids[j];
+            const int32_t aid = ids[4 * iq + u];
+            const int32_t row = side ? bid : aid;
+            const int32_t other = side ? aid : bid;
             const uint64_t key = ((uint64_t)kd[u] << 32) | (uint32_t)other | 0x80000000u;
             if (base < ucap) {
               urow_buf[base] = (uint32_t)row;
@@ -245,43 +369,47 @@ __global__ void __launch_bounds__(NT)
         }
       }
     }
-    if (tid == 0) rows_total += nb;
-    __syncthreads();  // stage s fully consumed before warp 0 refills it
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&B.empty[s]);  // this warp is done with stage s
   }
   for (int o = 16; o; o >>= 1) pairs_total += __shfl_xor_sync(0xffffffffu, pairs_total, o);
   if (lane == 0 && pairs_total) atomicAdd(&counters[2], (unsigned long long)pairs_total);
-  if (tid == 0 && rows_total) atomicAdd(&counters[3], (unsigned long long)rows_total);
+  if (ct == 0 && rows_total) atomicAdd(&counters[3], rows_total);
 }
 
-template <int MAXC, int NT>
-void launch_join(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, cudaStream_t st,
-                 const StageLayout& L, int* err) {
-  size_t smem = 16 + 2 * L.bytes();
-  static bool attr[2] = {false, false};
-  bool& done = attr[MAXC == 64];
-  if (!done) {
-    RINND_CUDA(cudaFuncSetAttribute(k_join_tma<MAXC, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    done = true;
+template <int MAXC>
+void launch_join(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, cudaStream_t st, const Layout& L,
+                 int* err) {
+  const size_t smem = L.bytes();
+  static bool attr_done = false;
+  if (!attr_done) {
+    RINND_CUDA(cudaFuncSetAttribute(k_join_ws<MAXC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_done = true;
   }
-  int per_sm = std::max(1, (int)((220 * 1024) / smem));
-  int grid = std::min(v1 - v0, 148 * per_sm);
+  const int per_sm = std::max(1, (int)((227 * 1024) / (smem + 1024)));
+  const int grid = std::min(v1 - v0, 148 * per_sm);
   if (grid <= 0) return;
-  k_join_tma<MAXC, NT><<<grid, NT, smem, st>>>(s.cand_new.p, s.cand_old.p, v0, v1, s.c, s.cp, X, Dp, kind,
-                                               s.norms.p, s.slots.p, s.thr.p, s.k, s.kp, L, s.urow.p, s.ukey.p,
-                                               s.counters.p + 4, s.ucap, s.counters.p, err);
+  k_join_ws<MAXC><<<grid, NT, smem, st>>>(s.desc.p, v0, v1, X, Dp, kind, s.slots.p, s.thr.p, s.k, s.kp, L,
+                                          s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap, s.counters.p, err);
   RINND_LAUNCH_CHECK();
 }
 
 }  // namespace
 
-bool join_tma_supported(int c, int Dp) {
-  StageLayout L{c <= 32 ? 32 : 64, Dp, Dp + 4};
-  return 16 + 2 * L.bytes() <= 200 * 1024;
+bool join_tma_supported(int c, int Dp) { return make_layout(c, Dp).bytes() <= 220 * 1024; }
+
+void join_describe(KnnState& s, int kind, cudaStream_t st) {
+  const Layout L = make_layout(s.c, 4);
+  if (s.desc.n < (size_t)s.N * L.dstride) s.desc.alloc((size_t)s.N * L.dstride, st);
+  k_cand_describe<<<grid_for((long long)s.N * 32, 256), 256, 0, st>>>(
+      s.cand_new.p, s.cand_old.p, s.N, s.c, s.cp, L.maxc, L.dstride, kind_is_dot(kind) ? s.norms.p : nullptr, s.desc.p);
+  RINND_LAUNCH_CHECK();
 }
 
 void join_tma_batch(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st) {
-  if (s.c <= 32) launch_join<32, 128>(s, X, Dp, kind, v0, v1, st, StageLayout{32, Dp, Dp + 4}, err);
-  else launch_join<64, 256>(s, X, Dp, kind, v0, v1, st, StageLayout{64, Dp, Dp + 4}, err);
+  const Layout L = make_layout(s.c, Dp);
+  if (L.maxc == 32) launch_join<32>(s, X, Dp, kind, v0, v1, st, L, err);
+  else launch_join<64>(s, X, Dp, kind, v0, v1, st, L, err);
 }
 
 }  // namespace rinnd

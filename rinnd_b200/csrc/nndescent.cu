@@ -283,6 +283,10 @@ __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, cons
                                 unsigned long long cap, uint64_t* slots, uint32_t* thr, int k, int kp,
                                 unsigned long long* counters) {
   const unsigned long long n = min(*count, cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicAdd(&counters[5], n);
+    atomicAdd(&counters[6], *count);  // appended, including overflow pushed directly
+  }
   unsigned int mine = 0;
   for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
        e += (unsigned long long)gridDim.x * blockDim.x) {
@@ -532,7 +536,9 @@ void compute_norms(const float* X, int N, int D, int Dp, float* norms, cudaStrea
 
 void ensure_update_buffer(KnnState& s, cudaStream_t st) {
   if (s.ucap) return;
-  s.ucap = std::max<unsigned long long>(1ull << 22, 64ull * (unsigned long long)s.N);
+  // Sized for one whole join iteration: at most ~70 buffered updates per vertex were
+  // seen on 1M-point mixtures (k = 30); overflow falls back to direct pushes.
+  s.ucap = std::max<unsigned long long>(1ull << 22, 96ull * (unsigned long long)s.N);
   s.urow.alloc(s.ucap, st);
   s.ukey.alloc(s.ucap, st);
 }
@@ -613,6 +619,7 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
   ensure_update_buffer(s, st);
   RINND_CUDA(cudaMemsetAsync(s.counters.p, 0, sizeof(unsigned long long), st));
   RINND_CUDA(cudaMemsetAsync(s.counters.p + 2, 0, 2 * sizeof(unsigned long long), st));
+  RINND_CUDA(cudaMemsetAsync(s.counters.p + 5, 0, 2 * sizeof(unsigned long long), st));
   cudaEvent_t e0, e1;
   RINND_CUDA(cudaEventCreate(&e0));
   RINND_CUDA(cudaEventCreate(&e1));
@@ -621,10 +628,19 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
     s.err.alloc(1, st);
     s.err.fill_bytes(0);
   }
-  // Worst case 4 c^2 updates per vertex (2 directions x c new x 2c candidates).
-  const long long per_batch =
+  // The chunked kernel batches for its worst case, 4 c^2 updates per vertex (2 directions x
+  // c new x 2c candidates).  The pipelined kernel batches for the expected count: the
+  // previous iteration's appended updates per vertex (1.2 c^2 before the first), with
+  // the buffer filled to 80%; rows tightened by one batch's pushes filter the next.
+  long long per_batch =
       std::max<long long>(1, (long long)(s.ucap / (4ull * (unsigned long long)s.c * (unsigned long long)s.c)));
+  if (use_tma) {
+    const double upv = s.upv_prev >= 0 ? 1.1 * s.upv_prev : 1.2 * (double)s.c * (double)s.c;
+    const double nbatch = std::max(1.0, std::ceil(upv * (double)s.N / (0.8 * (double)s.ucap)));
+    per_batch = std::max<long long>(1, (long long)std::ceil((double)s.N / nbatch));
+  }
   RINND_CUDA(cudaEventRecord(e0, st));
+  if (use_tma) join_describe(s, kind, st);
   for (long long v0 = 0; v0 < s.N; v0 += per_batch) {
     int v1 = (int)std::min<long long>(s.N, v0 + per_batch);
     RINND_CUDA(cudaMemsetAsync(s.counters.p + 4, 0, sizeof(unsigned long long), st));
@@ -645,7 +661,7 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
     apply_pending(s, st);
   }
   RINND_CUDA(cudaEventRecord(e1, st));
-  unsigned long long h[5];
+  unsigned long long h[7];
   int herr = 0;
   RINND_CUDA(cudaMemcpyAsync(h, s.counters.p, sizeof(h), cudaMemcpyDeviceToHost, st));
   RINND_CUDA(cudaMemcpyAsync(&herr, s.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -658,6 +674,9 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
   js.changes = h[0];
   js.pairs = h[2];
   js.rows = h[3];
+  js.updates = h[5];
+  js.appended = h[6];
+  s.upv_prev = (double)h[6] / (double)s.N;
   return js;
 }
 
