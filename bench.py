@@ -39,6 +39,8 @@ N_FULL, DIM, N_CLUSTERS, K = 1_000_000, 128, 100, 30
 N_TREES, LEAF, N_ITERS, DELTA = 8, 30, 10, 0.001
 N_QUERIES, QK, EPS = 10_000, 10, 0.1
 CPU_SAMPLE = 250_000
+# FP32 SIMT peak for context: 148 SMs x 128 FP32 lanes x 2 flops (FMA) x 1.965 GHz.
+FP32_SIMT_NOMINAL_TFLOPS = 74.4
 WORKLOAD = ("nndescent-build 1M x 128 f32 GMM(100 clusters, center std 10, unit std), sqeuclidean, "
             "k=30, 8 RP trees, leaf 30, <=10 iters, delta 0.001; 10k queries k=10 eps=0.1")
 
@@ -291,22 +293,33 @@ def main():
     value = n * world * args.steps / total_s
     clk = clocks.summary()
 
-    # ---- roofline of the dominant kernel (local join) ----
+    # ---- roofline of the dominant kernel (the local join, k_join_ws) ----
+    # Algorithmic bytes of the join over a build: every gathered candidate row
+    # (D x 4 B) plus the new/old candidate lists (2 N c x 4 B x 2) per iteration;
+    # the heap row traffic belongs to k_apply_updates.  Durations: CUDA events
+    # around each join launch on the build stream, summed over the timed builds.
     join_ms = sum(i.ms_join_kernel for i in infos)
-    join_launches = sum(i.iterations for i in infos)
+    join_launches = sum(i.join_kernel_launches for i in infos)
+    iters = sum(i.iterations for i in infos)
     rows = sum(i.join_rows_gathered for i in infos)
+    pairs = sum(i.pairs_evaluated for i in infos)
     c = min(K, 60)
-    alg_bytes = rows * DIM * 4 + join_launches * 2 * n * c * 8
+    alg_bytes = rows * DIM * 4 + iters * 2 * n * c * 4 * 2
     achieved = alg_bytes / (join_ms / 1000.0) / 1e9 if join_ms > 0 else None
     peak, peak_kind = measured_peaks()
     tpr = join_traffic_per_row()
     roofline = {
-        "kernel": "k_local_join (FP32 SIMT tile join)", "bound": "hbm", "achieved": achieved, "peak": peak,
-        "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+        "kernel": "k_join_ws (local join, FP32 SIMT, bulk-copy row gathers)", "bound": "hbm",
+        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+        "peak_source": peak_kind,
         "traffic": (tpr * rows / join_launches) if tpr else None,
         "algorithmic_bytes_per_launch": alg_bytes / max(join_launches, 1),
         "avg_launch_ms": join_ms / max(join_launches, 1),
+        "launches_per_build": join_launches / max(len(infos), 1),
         "share_of_build": join_ms / sum(step_ms),
+        "fp32_simt": {"achieved_tflops": 2.0 * DIM * pairs / (join_ms / 1000.0) / 1e12 if join_ms > 0 else None,
+                      "nominal_peak_tflops": FP32_SIMT_NOMINAL_TFLOPS,
+                      "flops": "2 x D per evaluated pair"},
     }
 
     # ---- queries (resident), QPS and recall ----

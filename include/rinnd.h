@@ -96,8 +96,10 @@ typedef struct rinnd_build_info {
   int64_t search_graph_nnz;
   float min_distance;
   uint64_t join_rows_gathered;   /* candidate rows gathered by the join kernel      */
-  double ms_join_kernel;         /* CUDA-event time of the join kernels             */
+  double ms_join_kernel;         /* CUDA-event time of the local-join kernel launches */
   uint64_t kernel_launches;      /* kernels this library launched during the build  */
+  uint64_t join_kernel_launches; /* local-join kernel launches (ms_join_kernel covers these) */
+  uint64_t join_updates;         /* updates the join kernels appended for the heap pushes */
 } rinnd_build_info;
 
 /* ---- lifecycle ------------------------------------------------------------ */
@@ -153,6 +155,11 @@ RINND_EXPORT int rinnd_quantize(rinnd_index* idx, int32_t encoding);
 RINND_EXPORT int rinnd_query_quantized(rinnd_index* idx, const float* queries, int64_t nq, int32_t k,
                           float epsilon, int32_t candidate_width, int32_t rerank_width,
                           int32_t* out_idx, float* out_dist);
+/* Row encoder of QuantizedI8Index::new (lib.rs:159-223) on the GPU for host rows
+ * (n x d f32): codes (n x d int8), per-row scales (inv_norms) and the global
+ * multiplier 127 / max|x|. */
+RINND_EXPORT int rinnd_quantize_rows(const float* data, int64_t n, int32_t d, int32_t encoding, int8_t* codes,
+                                     float* scales, float* global_multiplier);
 
 /* ---- storage info (crates/rinnd/src/lib.rs:1028-1077) ---------------------- */
 typedef struct rinnd_storage_info {

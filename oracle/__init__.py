@@ -79,6 +79,8 @@ def lib():
             "orc_query_one": (None, [_P, _P, _i32, _f32, _P, _P]),
             "orc_quantize_rows": (None, [_P, _i64, _i32, _i32, _P, _P, _P]),
             "orc_query_quantized": (_i32, [_P, _P, _i64, _i32, _f32, _i32, _i32, _i32, _P, _P]),
+            "orc_quantize_queries": (None, [_P, _i64, _i32, _i32, _f32, _P, _P]),
+            "orc_normalize_rows": (None, [_P, _i64, _i32]),
             "orc_exact_knn_f64": (None, [ctypes.c_int, _P, _i64, _P, _i64, _i32, _i32, _i32, _P, _P]),
             "orc_max_threads": (_i32, []),
         }
@@ -251,6 +253,21 @@ def quantize_rows(data, encoding):
     gm = ctypes.c_float(0)
     lib().orc_quantize_rows(_p(data), n, d, encoding, _p(codes), _p(inv), ctypes.byref(gm))
     return codes, inv, gm.value
+
+
+def quantize_queries(queries, encoding, global_mult):
+    queries = _f(queries)
+    n, d = queries.shape
+    codes = np.empty((n, d), np.int8)
+    scales = np.empty(n, np.float32)
+    lib().orc_quantize_queries(_p(queries), n, d, encoding, global_mult, _p(codes), _p(scales))
+    return codes, scales
+
+
+def normalize_rows(data):
+    out = np.array(data, dtype=np.float32, order="C", copy=True)
+    lib().orc_normalize_rows(_p(out), out.shape[0], out.shape[1])
+    return out
 
 
 def exact_knn_f64(kind, data, queries, k, exclude_self=False):

@@ -1621,6 +1621,44 @@ void orc_quantize_rows(const float* data, int64_t n, int32_t dim, int32_t encodi
   *global_mult = gm;
 }
 
+// lib.rs:325-358 quantize_query: the row multiplier of the per-vector encodings or
+// the index's global multiplier (sq8u); scale = 1/sqrt(sum code^2), 1/multiplier
+// or the global dequantization scale.
+void orc_quantize_queries(const float* queries, int64_t nq, int32_t dim, int32_t encoding, float global_mult,
+                          int8_t* codes, float* scales) {
+  const float gds = global_mult > 0.f ? 1.0f / global_mult : 0.f;
+  for (int64_t r = 0; r < nq; ++r) {
+    const float* q = queries + r * dim;
+    float mult = global_mult;
+    if (encoding != 1) {
+      float mx = 0.f;
+      for (int j = 0; j < dim; ++j) mx = std::max(mx, std::fabs(q[j]));
+      mult = mx > 0.f ? 127.0f / mx : 0.f;
+    }
+    int8_t* c = codes + r * dim;
+    for (int j = 0; j < dim; ++j) {
+      float v = std::round(q[j] * mult);
+      c[j] = (int8_t)std::min(std::max(v, -127.0f), 127.0f);
+    }
+    int32_t nsq = i8_dot(c, c, dim);
+    scales[r] = encoding == 0 ? (nsq > 0 ? 1.0f / std::sqrt((float)nsq) : 0.f)
+                              : (encoding == 1 ? gds : (mult > 0.f ? 1.0f / mult : 0.f));
+  }
+}
+
+// lib.rs:1131-1146 normalize_rows_inplace: sequential f32 sum of squares; rows
+// with norm^2 <= 1e-12 are left unchanged; x *= 1/sqrt(norm^2).
+void orc_normalize_rows(float* data, int64_t n, int32_t dim) {
+  for (int64_t r = 0; r < n; ++r) {
+    float* row = data + r * dim;
+    float nsq = 0.f;
+    for (int j = 0; j < dim; ++j) nsq += row[j] * row[j];
+    if (nsq <= 1e-12f) continue;
+    float inv = 1.0f / std::sqrt(nsq);
+    for (int j = 0; j < dim; ++j) row[j] *= inv;
+  }
+}
+
 // lib.rs:325-358 quantize_query + index.rs:283-334 + greedy.rs:365-413 + index.rs:103-126.
 // The index must have been built with ORC_DIRECT_COSINE on normalized rows.  Search
 // trees are the FP32 trees (tree_quantization="none").  Returns 0, or -1 when the

@@ -146,6 +146,12 @@ void orc_query_one(const orc_index* idx, const float* query, int32_t k, float ep
 /* encoding: 0 int8 per-vector cosine, 1 sq8u global symmetric, 2 sq8p per-vector. */
 void orc_quantize_rows(const float* data, int64_t n, int32_t dim, int32_t encoding,
                        int8_t* codes, float* inv_norms, float* global_mult);
+/* quantize_query (lib.rs:325-358) with the index's global multiplier `global_mult`
+ * (used by encoding 1 only): codes nq x dim, per-query scale (query_inv_norm). */
+void orc_quantize_queries(const float* queries, int64_t nq, int32_t dim, int32_t encoding,
+                          float global_mult, int8_t* codes, float* scales);
+/* normalize_rows_inplace (lib.rs:1131-1146). */
+void orc_normalize_rows(float* data, int64_t n, int32_t dim);
 int32_t orc_query_quantized(const orc_index* idx, const float* queries, int64_t nq,
                             int32_t k, float epsilon, int32_t encoding,
                             int32_t candidate_width, int32_t rerank_width,

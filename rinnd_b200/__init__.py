@@ -182,11 +182,18 @@ class RINND:
         if qdim != self.dim:
             raise ValueError(f"Query dimension {qdim} does not match data dimension {self.dim}")
 
+    def _ensure_rerank_available(self, k: int, candidate_width: int, rerank_width: int) -> None:
+        """lib.rs:283-300: exact reranking needs the retained FP32 rows."""
+        requested = rerank_width > k if candidate_width == 0 else rerank_width > 0
+        if requested and not self._retain_fp32:
+            raise ValueError("exact reranking is unavailable because FP32 vector data was released")
+
     def _run_query(self, q: np.ndarray, k: int, epsilon: float):
         n = q.shape[0]
         idx = np.empty((n, k), np.int32)
         dist = np.empty((n, k), np.float32)
         if self._encoding is not None:
+            self._ensure_rerank_available(k, self._candidate_width, self._rerank_width)
             L.check(L.lib.rinnd_query_quantized(self._h, L.ptr(q), n, k, float(epsilon), self._candidate_width,
                                                 self._rerank_width, L.ptr(idx), L.ptr(dist)))
         else:
@@ -204,6 +211,7 @@ class RINND:
         _validate_quantized_widths(k, candidate_width, rerank_width)
         if self._encoding is None:
             raise ValueError("query-time quantized widths require a quantized cosine_distance_mode")
+        self._ensure_rerank_available(int(k), int(candidate_width), int(rerank_width))
         q = _as_f32_2d(query_data, "query_data")
         self._check_dim(q.shape[1])
         n = q.shape[0]

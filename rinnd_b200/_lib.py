@@ -44,7 +44,8 @@ class BuildInfo(ctypes.Structure):
         ("ms_join", _f64), ("ms_sort", _f64), ("ms_graph", _f64), ("ms_total", _f64),
         ("pairs_evaluated", _u64), ("pushes_accepted", _u64), ("push_contention", _u64),
         ("search_graph_nnz", _i64), ("min_distance", _f32), ("join_rows_gathered", _u64),
-        ("ms_join_kernel", _f64), ("kernel_launches", _u64),
+        ("ms_join_kernel", _f64), ("kernel_launches", _u64), ("join_kernel_launches", _u64),
+        ("join_updates", _u64),
     ]
 
 
@@ -73,6 +74,7 @@ SIGNATURES = {
     "rinnd_vertex_order": (ctypes.c_int, [_P, _P]),
     "rinnd_quantize": (ctypes.c_int, [_P, _i32]),
     "rinnd_query_quantized": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _i32, _i32, _P, _P]),
+    "rinnd_quantize_rows": (ctypes.c_int, [_P, _i64, _i32, _i32, _P, _P, _P]),
     "rinnd_storage_info_get": (ctypes.c_int, [_P, _P]),
     "rinnd_distance_pairs": (ctypes.c_int, [_i32, _P, _P, _i64, _i32, _P]),
     "rinnd_search_graph_from_knn": (ctypes.c_int, [_P, _P, _P, _i32, _i32, _i32, _i32, _f32, _P, _P, _P, _P]),

@@ -317,6 +317,7 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   const size_t conv = (size_t)(pin->delta * (float)k * (float)N);  // mod.rs:157
   uint64_t pairs_total = 0, pushes_total = 0, rows_total = 0;
   double ms_cand = 0, ms_join = 0, ms_join_kernel = 0;
+  uint64_t join_launches = 0, join_updates = 0;
   int iters = 0;
   for (int it = 0; it < n_iters; ++it) {
     iters = it + 1;
@@ -329,12 +330,16 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
     ms_cand += b - a;
     ms_join += e - b;
     ms_join_kernel += js.kernel_ms;
+    join_launches += (uint64_t)js.launches;
+    join_updates += js.appended;
     pairs_total += js.pairs;
     pushes_total += js.changes;
     rows_total += js.rows;
     if (pin->verbose)
-      std::printf("Iteration %d: %llu updates (%llu pairs, %llu rows, %llu buffered of %llu, %.3f ms join)\n",
-                  it + 1, js.changes, js.pairs, js.rows, js.updates, js.appended, js.kernel_ms);
+      std::printf("Iteration %d: %llu updates (%llu pairs, %llu rows, %llu buffered of %llu, %d join launches "
+                  "%.3f ms, join step %.3f ms)\n",
+                  it + 1, js.changes, js.pairs, js.rows, js.updates, js.appended, js.launches, js.kernel_ms,
+                  js.total_ms);
     if ((size_t)js.changes <= conv) break;
   }
   double t3 = now_ms();
@@ -404,6 +409,8 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   inf.pairs_evaluated = pairs_total;
   inf.join_rows_gathered = rows_total;
   inf.ms_join_kernel = ms_join_kernel;
+  inf.join_kernel_launches = join_launches;
+  inf.join_updates = join_updates;
   inf.kernel_launches = launch_counter() - launches0;
   inf.pushes_accepted = pushes_total;
   inf.push_contention = hc[1];
@@ -704,12 +711,93 @@ int rinnd_device_count(int32_t* count) {
 }
 
 int rinnd_quantize(rinnd_index* idx, int32_t encoding) {
-  return fail(RINND_ERR_INVALID, "int8 quantization is not available in this build");
+  return guarded([&] {
+    check_index(idx);
+    require(encoding >= RINND_Q8_PER_VECTOR_COSINE && encoding <= RINND_Q8_PER_VECTOR_SYMMETRIC,
+            "unknown int8 encoding");
+    require(idx->kind == DK_DIRECT_COSINE,
+            "int8 quantization requires an index built with the direct cosine distance on normalized rows");
+    std::lock_guard<std::mutex> lock(idx->mu);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    cudaStream_t st = idx->st;
+    RINND_CUDA(cudaStreamSynchronize(st));
+    const double t0 = now_ms();
+    const int Dq = round_up(idx->D, 16);
+    const float gm = quant_global_multiplier(idx->X.p, (long long)idx->N * idx->Dp, st);
+    idx->codes.alloc((size_t)idx->N * Dq, st);
+    idx->inv_norms.alloc((size_t)idx->N, st);
+    quantize_rows(idx->X.p, idx->N, idx->D, idx->Dp, Dq, encoding, gm, idx->codes.p, idx->inv_norms.p, st);
+    RINND_CUDA(cudaStreamSynchronize(st));
+    idx->Dq = Dq;
+    idx->global_mult = gm;
+    idx->encoding = encoding;
+    idx->encode_seconds = (now_ms() - t0) / 1000.0;
+  });
 }
 
 int rinnd_query_quantized(rinnd_index* idx, const float* queries, int64_t nq, int32_t k, float epsilon,
                           int32_t candidate_width, int32_t rerank_width, int32_t* out_idx, float* out_dist) {
-  return fail(RINND_ERR_INVALID, "int8 quantization is not available in this build");
+  return guarded([&] {
+    check_index(idx);
+    require(idx->encoding >= 0, "index has no int8 codes: call rinnd_quantize first");
+    require(nq >= 0, "number of queries must be >= 0");
+    require(k >= 1, "k must be >= 1");
+    require(candidate_width >= 0 && rerank_width >= 0, "quantized widths must be >= 0");
+    // resolve_quantized_candidate_width / should_rerank_quantized (index.rs:55-89)
+    const int resolved = candidate_width == 0 ? std::max(k, rerank_width) : candidate_width;
+    require(resolved >= k, "quantized candidate width must be at least k");
+    require(rerank_width <= resolved, "quantized rerank width must not exceed candidate width");
+    require(candidate_width == 0 || rerank_width == 0 || rerank_width >= k,
+            "quantized rerank width must be zero or at least k");
+    require(resolved <= 256, "quantized candidate width must be <= 256");
+    const bool rerank = candidate_width == 0 ? rerank_width > k : rerank_width > 0;
+    if (nq == 0) return;
+    require(queries && out_idx && out_dist, "query/output pointers must not be null");
+    std::lock_guard<std::mutex> lock(idx->mu);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    cudaStream_t st = idx->st;
+    DVec<float> Q;
+    load_rows(queries, false, nq, idx->D, idx->D, idx->Dp, Q, st);
+    if (idx->normalize) normalize_rows(Q.p, nq, idx->D, idx->Dp, st);
+    DVec<int8_t> Q8((size_t)nq * idx->Dq, st);
+    DVec<float> qs((size_t)nq, st);
+    quantize_rows(Q.p, nq, idx->D, idx->Dp, idx->Dq, idx->encoding, idx->global_mult, Q8.p, qs.p, st);
+    DVec<int32_t> oi((size_t)nq * k, st);
+    DVec<float> od((size_t)nq * k, st);
+    greedy_search_quantized(idx->search_view(), Q.p, Q8.p, qs.p, (int)nq, resolved, k, rerank ? rerank_width : 0,
+                            epsilon, oi.p, od.p, st, idx->search_stats.p);
+    oi.to_host(out_idx, (size_t)nq * k);
+    od.to_host(out_dist, (size_t)nq * k);
+    RINND_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int rinnd_quantize_rows(const float* data, int64_t n, int32_t d, int32_t encoding, int8_t* codes, float* scales,
+                        float* global_multiplier) {
+  return guarded([&] {
+    require(n >= 0 && d >= 1, "invalid shape");
+    require(encoding >= RINND_Q8_PER_VECTOR_COSINE && encoding <= RINND_Q8_PER_VECTOR_SYMMETRIC,
+            "unknown int8 encoding");
+    if (n == 0) {
+      if (global_multiplier) *global_multiplier = 0.f;
+      return;
+    }
+    require(data && codes && scales, "pointers must not be null");
+    ensure_device(0);
+    StreamGuard sg;
+    const int Dp = round_up(d, 4), Dq = round_up(d, 16);
+    DVec<float> X;
+    load_rows(data, false, n, d, d, Dp, X, sg.s);
+    const float gm = quant_global_multiplier(X.p, n * Dp, sg.s);
+    DVec<int8_t> C((size_t)n * Dq, sg.s);
+    DVec<float> S((size_t)n, sg.s);
+    quantize_rows(X.p, n, d, Dp, Dq, encoding, gm, C.p, S.p, sg.s);
+    RINND_CUDA(cudaMemcpy2DAsync(codes, (size_t)d, C.p, (size_t)Dq, (size_t)d, (size_t)n, cudaMemcpyDeviceToHost,
+                                 sg.s));
+    S.to_host(scales, (size_t)n);
+    RINND_CUDA(cudaStreamSynchronize(sg.s));
+    if (global_multiplier) *global_multiplier = gm;
+  });
 }
 
 }  // extern "C"

@@ -71,7 +71,9 @@ void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int 
 void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st);
 struct JoinStats {
   unsigned long long changes = 0, pairs = 0, rows = 0, updates = 0, appended = 0;
-  float kernel_ms = 0.f;  // CUDA-event duration of the join kernel on its stream
+  float kernel_ms = 0.f;   // CUDA-event duration of the join kernel launches on their stream
+  float total_ms = 0.f;    // CUDA-event duration of the whole join step (describe, joins, applies)
+  int launches = 0;        // join kernel launches
 };
 JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st);
 bool join_tma_supported(int c, int Dp);
@@ -128,6 +130,21 @@ struct SearchStats {
 void greedy_search(const SearchIndex& ix, const float* Q, int nq, int k, float eps,
                    uint64_t qid_base, int32_t* out_idx, float* out_dist, cudaStream_t st,
                    unsigned long long* dstats);
+// Quantized search (index.rs:283-334): int8 query codes Q8 (nq x Dq) with scales
+// qinv; the result list holds k_search entries; with rerank > 0 the first
+// `rerank` results are re-ordered by their exact FP32 distance to Q (index.rs:103-126);
+// k_out entries per query are written.  Every query uses the index seed alone.
+void greedy_search_quantized(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq,
+                             int k_search, int k_out, int rerank, float eps, int32_t* out_idx, float* out_dist,
+                             cudaStream_t st, unsigned long long* dstats);
+
+// ---- int8 scalar quantization (quantize.cu) -------------------------------------
+enum Q8Encoding : int { Q8_PER_VECTOR_COSINE = 0, Q8_GLOBAL_SYMMETRIC = 1, Q8_PER_VECTOR_SYMMETRIC = 2 };
+// 127 / max |x| over `total` floats (0 if all zero), lib.rs:163-174.
+float quant_global_multiplier(const float* X, long long total, cudaStream_t st);
+// Codes (n x Dq, zero-padded beyond D) and per-row scales of rows X (n x Dp).
+void quantize_rows(const float* X, long long n, int D, int Dp, int Dq, int encoding, float gmult, int8_t* codes,
+                   float* scale, cudaStream_t st);
 
 // ---- utilities (util.cu) ------------------------------------------------------
 void distance_pairs(int kind, const float* A, const float* B, int64_t n, int D, int Dp,

@@ -22,6 +22,8 @@
 // every thread accumulates a 4x4 block of pair distances in registers.
 #include <cub/cub.cuh>
 
+#include <vector>
+
 #include "dist.cuh"
 #include "engine.h"
 #include "heap.cuh"
@@ -641,10 +643,16 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
   }
   RINND_CUDA(cudaEventRecord(e0, st));
   if (use_tma) join_describe(s, kind, st);
+  std::vector<cudaEvent_t> kev;  // start/stop of every join kernel launch
   for (long long v0 = 0; v0 < s.N; v0 += per_batch) {
     int v1 = (int)std::min<long long>(s.N, v0 + per_batch);
     RINND_CUDA(cudaMemsetAsync(s.counters.p + 4, 0, sizeof(unsigned long long), st));
     int grid = (int)std::min<long long>(v1 - v0, 148LL * 16);
+    for (int e = 0; e < 2; ++e) {
+      kev.emplace_back();
+      RINND_CUDA(cudaEventCreate(&kev.back()));
+    }
+    RINND_CUDA(cudaEventRecord(kev[kev.size() - 2], st));
     if (use_tma) {
       join_tma_batch(s, X, Dp, kind, (int)v0, v1, s.err.p, st);
     } else if (s.c <= 32) {
@@ -658,6 +666,7 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
                                                   s.counters.p);
       RINND_LAUNCH_CHECK();
     }
+    RINND_CUDA(cudaEventRecord(kev.back(), st));
     apply_pending(s, st);
   }
   RINND_CUDA(cudaEventRecord(e1, st));
@@ -668,7 +677,14 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
   RINND_CUDA(cudaStreamSynchronize(st));
   if (herr) throw CudaError("local join: a shared-memory pipeline stage did not complete within its wait limit");
   JoinStats js;
-  RINND_CUDA(cudaEventElapsedTime(&js.kernel_ms, e0, e1));
+  RINND_CUDA(cudaEventElapsedTime(&js.total_ms, e0, e1));
+  for (size_t e = 0; e < kev.size(); e += 2) {
+    float ms = 0.f;
+    RINND_CUDA(cudaEventElapsedTime(&ms, kev[e], kev[e + 1]));
+    js.kernel_ms += ms;
+  }
+  js.launches = (int)(kev.size() / 2);
+  for (cudaEvent_t ev : kev) cudaEventDestroy(ev);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   js.changes = h[0];

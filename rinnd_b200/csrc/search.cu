@@ -12,7 +12,8 @@
 //     visited, push those with d < bound (results bounded to k, seeds
 //     unbounded), recomputing the bound after every result insertion.
 // Distances use the reference's exact accumulation order (dist.cuh), or the
-// exact int8 dot with the reference's scaling (quantized.rs:26-40, greedy.rs:384-390).
+// exact int8 dot with the reference's scaling (quantized.rs:26-40, greedy.rs:384-390)
+// followed by an optional exact FP32 rerank of the leading results (index.rs:103-126).
 //
 // Per-warp state lives in shared memory: the query, the result list (sorted by
 // (distance, id)), the seed set as a sorted array merged warp-parallel with each
@@ -70,10 +71,16 @@ template <bool QUANT>
 __device__ __forceinline__ float dist_to(const SearchIndex& ix, const float* q, const int8_t* q8,
                                          float qinv, int32_t id) {
   if (QUANT) {
-    const int* a = reinterpret_cast<const int*>(q8);
-    const int* b = reinterpret_cast<const int*>(ix.codes + (size_t)id * ix.Dq);
-    int acc = 0;
-    for (int t = 0; t < ix.Dq / 4; ++t) acc = __dp4a(a[t], __ldg(b + t), acc);
+    const int4* a = reinterpret_cast<const int4*>(q8);
+    const int4* b = reinterpret_cast<const int4*>(ix.codes + (size_t)id * ix.Dq);
+    int acc = 0;  // exact: |sum| <= 127^2 D
+    for (int t = 0; t < ix.Dq / 16; ++t) {
+      const int4 x = a[t], y = __ldg(b + t);
+      acc = __dp4a(x.x, y.x, acc);
+      acc = __dp4a(x.y, y.y, acc);
+      acc = __dp4a(x.z, y.z, acc);
+      acc = __dp4a(x.w, y.w, acc);
+    }
     float sim = __fmul_rn(__fmul_rn((float)acc, qinv), ix.inv_norms[id]);
     return __fsub_rn(1.0f, fminf(fmaxf(sim, -1.0f), 1.0f));
   }
@@ -173,9 +180,11 @@ __device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int
   tail = min(na + nb, S);
 }
 
+// k: result-list width; k_out: entries written per query; rerank (QUANT only):
+// number of leading results re-ordered by exact FP32 distance before output.
 template <bool QUANT>
 __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_t* Q8row,
-                           float qinv, int qid, uint64_t seed_base, int k, float eps,
+                           float qinv, int qid, uint64_t seed_base, int k, int k_out, int rerank, float eps,
                            const WarpLayout& L, unsigned char* wsm, int32_t* out_idx,
                            float* out_dist, unsigned long long* stats) {
   const int lane = threadIdx.x & 31;
@@ -186,14 +195,16 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
   uint64_t* bbuf = reinterpret_cast<uint64_t*>(wsm + L.batch_off());
   int8_t* q8 = reinterpret_cast<int8_t*>(q);  // QUANT: codes stored in the query slot
   if (QUANT) {
-    for (int t = lane; t < ix.Dq / 4; t += 32)
-      reinterpret_cast<int*>(q8)[t] = reinterpret_cast<const int*>(Q8row)[t];
+    for (int t = lane; t < ix.Dq / 16; t += 32)
+      reinterpret_cast<int4*>(q8)[t] = reinterpret_cast<const int4*>(Q8row)[t];
   } else {
     for (int t = lane; t < ix.Dp; t += 32) q[t] = t < ix.D ? Qrow[t] : 0.f;
   }
   for (int t = lane; t < L.h; t += 32) vis[t] = -1;
   __syncwarp();
-  QRng rng{seed_base + (uint64_t)qid, 0};
+  // FP32 queries seed with seed + query index (index.rs:165); quantized queries
+  // all use the seed alone (index.rs:298).
+  QRng rng{seed_base + (QUANT ? 0ull : (uint64_t)qid), 0};
   int rc = 0, cur = 0, head = 0, tail = 0;
   unsigned long long evals = 0, expansions = 0;
   unsigned long long* overflow = &stats[2];
@@ -316,17 +327,37 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
       seeds_merge(seeds, bbuf, L.s, cur, head, tail, sorted, __popc(acc_mask));
     }
   }
-  // ---- output (index.rs:182-199) ----
-  for (int j = lane; j < k; j += 32) {
-    if (j < rc) {
+  // ---- exact rerank of the first `rerank` results (index.rs:103-126): exact
+  // FP32 distance to the FP32 query, sorted by (distance, id) ----
+  int nres = rc;
+  if (QUANT && rerank > 0) {
+    const int m = min(rc, rerank);
+    uint64_t* tmp = seeds;  // the seed arrays (2 S >= 512 entries) are free after the traversal
+    for (int e = lane; e < m; e += 32) {
+      const int32_t id = (int32_t)(uint32_t)res[e];
+      tmp[e] = rkey(exact_distance(ix.kind, Qrow, ix.X + (size_t)id * ix.Dp, ix.D), id);
+    }
+    __syncwarp();
+    for (int e = lane; e < m; e += 32) {  // ids are distinct, so ranks are too
+      const uint64_t key = tmp[e];
+      int r = 0;
+      for (int j = 0; j < m; ++j) r += tmp[j] < key;
+      res[r] = key;
+    }
+    __syncwarp();
+    nres = m;
+  }
+  // ---- output (index.rs:182-199, :324-333) ----
+  for (int j = lane; j < k_out; j += 32) {
+    if (j < nres) {
       uint64_t key = res[j];
       int32_t id = (int32_t)(uint32_t)key;
       float d = fkey_inv((uint32_t)(key >> 32));
-      out_idx[(size_t)qid * k + j] = ix.vertex_order ? ix.vertex_order[id] : id;
-      out_dist[(size_t)qid * k + j] = QUANT ? d : apply_correction(ix.corr, d);
+      out_idx[(size_t)qid * k_out + j] = ix.vertex_order ? ix.vertex_order[id] : id;
+      out_dist[(size_t)qid * k_out + j] = QUANT ? d : apply_correction(ix.corr, d);
     } else {
-      out_idx[(size_t)qid * k + j] = -1;
-      out_dist[(size_t)qid * k + j] = __int_as_float(0x7f800000);
+      out_idx[(size_t)qid * k_out + j] = -1;
+      out_dist[(size_t)qid * k_out + j] = __int_as_float(0x7f800000);
     }
   }
   if (lane == 0) {
@@ -338,8 +369,8 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
 
 template <bool QUANT>
 __global__ void __launch_bounds__(WPB * 32)
-    k_search(SearchIndex ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k,
-             float eps, uint64_t qid_base, WarpLayout L, int32_t* out_idx, float* out_dist,
+    k_search(SearchIndex ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k, int k_out,
+             int rerank, float eps, uint64_t qid_base, WarpLayout L, int32_t* out_idx, float* out_dist,
              unsigned long long* stats) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = threadIdx.x >> 5;
@@ -347,9 +378,26 @@ __global__ void __launch_bounds__(WPB * 32)
   const int total_warps = gridDim.x * WPB;
   for (int qi = blockIdx.x * WPB + w; qi < nq; qi += total_warps) {
     search_one<QUANT>(ix, Q + (size_t)qi * ix.Dp, QUANT ? Q8 + (size_t)qi * ix.Dq : nullptr,
-                      QUANT ? qinv[qi] : 0.f, qi, ix.seed + qid_base, k, eps, L, wsm, out_idx,
+                      QUANT ? qinv[qi] : 0.f, qi, ix.seed + qid_base, k, k_out, rerank, eps, L, wsm, out_idx,
                       out_dist, stats);
   }
+}
+
+WarpLayout layout_for(const SearchIndex& ix, int k) {
+  if (k > 256) throw std::invalid_argument("k must be <= 256");
+  WarpLayout L;
+  L.dp = std::max(ix.Dp, ix.Dq / 4);
+  L.kmax = k <= 32 ? 32 : (k <= 128 ? 128 : 256);
+  L.s = L.kmax <= 32 ? 256 : 4 * L.kmax;
+  L.h = 4096;
+  static bool attr_set = false;
+  if (!attr_set) {
+    RINND_CUDA(cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    RINND_CUDA(cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr_set = true;
+  }
+  if (L.bytes() * WPB > 200 * 1024) throw std::invalid_argument("query dimension too large for search shared memory");
+  return L;
 }
 
 }  // namespace
@@ -358,23 +406,23 @@ void greedy_search(const SearchIndex& ix, const float* Q, int nq, int k, float e
                    uint64_t qid_base, int32_t* out_idx, float* out_dist, cudaStream_t st,
                    unsigned long long* dstats) {
   if (nq <= 0) return;
-  if (k > 256) throw std::invalid_argument("k must be <= 256");
-  WarpLayout L;
-  L.dp = ix.Dp;
-  L.kmax = k <= 32 ? 32 : (k <= 128 ? 128 : 256);
-  L.s = L.kmax <= 32 ? 256 : 4 * L.kmax;
-  L.h = 4096;
-  size_t bytes = L.bytes() * WPB;
-  static bool attr_set = false;
-  if (!attr_set) {
-    RINND_CUDA(cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    RINND_CUDA(cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr_set = true;
-  }
-  if (bytes > 200 * 1024) throw std::invalid_argument("query dimension too large for search shared memory");
+  const WarpLayout L = layout_for(ix, k);
   int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
-  k_search<false><<<blocks, WPB * 32, bytes, st>>>(ix, Q, nullptr, nullptr, nq, k, eps, qid_base, L,
-                                                   out_idx, out_dist, dstats);
+  k_search<false><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, nullptr, nullptr, nq, k, k, 0, eps, qid_base,
+                                                             L, out_idx, out_dist, dstats);
+  RINND_LAUNCH_CHECK();
+}
+
+void greedy_search_quantized(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq,
+                             int width, int k_out, int rerank, float eps, int32_t* out_idx, float* out_dist,
+                             cudaStream_t st, unsigned long long* dstats) {
+  if (nq <= 0) return;
+  if (!ix.codes || ix.Dq % 16 != 0) throw std::invalid_argument("index has no int8 codes");
+  if (k_out > width || rerank > width) throw std::invalid_argument("invalid quantized widths");
+  const WarpLayout L = layout_for(ix, width);
+  int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
+  k_search<true><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, width, k_out, rerank, eps, 0,
+                                                            L, out_idx, out_dist, dstats);
   RINND_LAUNCH_CHECK();
 }
 

@@ -149,3 +149,25 @@ def test_rng_is_xoshiro256pp(orc):
         s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3]; s[2] ^= t; s[3] = rotl(s[3], 45)
         exp.append(r)
     assert orc.rng_u64(42, 8).tolist() == exp
+
+
+def test_query_encoder_matches_row_encoder(orc):
+    """lib.rs:325-358 quantize_query uses the row encoder's arithmetic (lib.rs:185-223)."""
+    X = np.random.default_rng(3).normal(size=(300, 40)).astype(np.float32)
+    X[7] = 0.0
+    for enc in range(3):
+        codes, scales, gm = orc.quantize_rows(X, enc)
+        qc, qs = orc.quantize_queries(X, enc, gm)
+        np.testing.assert_array_equal(qc, codes)
+        np.testing.assert_array_equal(qs.view(np.uint32), scales.view(np.uint32))
+
+
+def test_normalize_rows_sequential_sum(orc):
+    """lib.rs:1131-1146: sequential f32 sum of squares; tiny rows untouched."""
+    X = np.random.default_rng(4).normal(size=(200, 33)).astype(np.float32)
+    X[5] = 1e-7
+    out = orc.normalize_rows(X)
+    nsq = np.add.accumulate(X * X, axis=1, dtype=np.float32)[:, -1]
+    inv = np.float32(1.0) / np.sqrt(nsq)
+    want = np.where((nsq <= np.float32(1e-12))[:, None], X, X * inv[:, None])
+    np.testing.assert_array_equal(out.view(np.uint32), want.astype(np.float32).view(np.uint32))
