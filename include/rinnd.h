@@ -59,6 +59,14 @@ extern "C" {
 #define RINND_Q8_GLOBAL_SYMMETRIC 1   /* "sq8u"  */
 #define RINND_Q8_PER_VECTOR_SYMMETRIC 2 /* "sq8p" */
 
+/* Local-join tile arithmetic (no counterpart in the reference, whose join is FP32):
+ * FP32 evaluates every candidate pair in FP32; BF16 filters the pairs with BF16
+ * Gram tiles on the tensor cores (FP32 accumulate) and recomputes every pair
+ * that may beat its row's threshold in exact FP32 before it is pushed.
+ * Manhattan and candidate lists longer than 32 use the FP32 tiles. */
+#define RINND_PRECISION_FP32 0
+#define RINND_PRECISION_BF16 1
+
 /* Mirrors NNDescentBuilder's fields (core/index.rs:449-494) plus the metric
  * dispatch decisions the Python layer makes (crates/rinnd/src/lib.rs:1175-1297). */
 typedef struct rinnd_build_params {
@@ -79,7 +87,8 @@ typedef struct rinnd_build_params {
   int32_t normalize;                /* L2-normalize rows before build (lib.rs:710-712) */
   int32_t verbose;
   int32_t device;                   /* CUDA device ordinal, default 0              */
-  int32_t reserved[7];
+  int32_t precision;                /* RINND_PRECISION_*: local-join tile arithmetic */
+  int32_t reserved[6];
 } rinnd_build_params;
 
 typedef struct rinnd_index rinnd_index;
@@ -189,6 +198,16 @@ RINND_EXPORT int rinnd_heap_push_batch(int32_t n, int32_t k, int64_t n_ops, cons
                           const int32_t* ids, const float* dists, const uint8_t* flags,
                           int32_t* out_idx, float* out_dist, uint8_t* out_flags,
                           int64_t* n_accepted);
+/* One NN-Descent iteration (nndescent/mod.rs:101-155: candidate sampling,
+ * candidates.rs:51-484, then the local join, mod.rs:321-491) on host arrays:
+ * idx/dist/flags (n x k, -1 = empty) hold the neighbor heap rows on entry
+ * (distances raw, of `kind`) and the sorted rows after the iteration; `changes`
+ * receives the number of successful pushes.  `precision` selects the join tiles
+ * (RINND_PRECISION_*); the candidate sample depends only on the rows' contents,
+ * `seed` and `iteration`. */
+RINND_EXPORT int rinnd_nndescent_step(const float* data, int64_t n, int32_t d, int32_t k, int32_t max_candidates,
+                                      int32_t kind, int32_t precision, uint64_t seed, int32_t iteration,
+                                      int32_t* idx, float* dist, uint8_t* flags, int64_t* changes);
 
 /* No counterpart in the reference.  The same operation as rinnd_heap_push_batch
  * for callers that may not allocate device memory (a host engine that owns the

@@ -33,6 +33,9 @@ _KNOWN_OTHER = {
 }
 _ANGULAR = {"cosine", "inner_product", "dot"}  # index.rs:606-614
 
+# Local-join tile arithmetic (an addition of the B200 engine): "bf16" filters
+# pairs with tensor-core BF16 Gram tiles and recomputes survivors in FP32.
+_PRECISIONS = {"fp32": L.PRECISION_FP32, "bf16": L.PRECISION_BF16}
 _ENCODINGS = {"int8": L.Q8_PER_VECTOR_COSINE, "sq8u": L.Q8_GLOBAL_SYMMETRIC, "sq8p": L.Q8_PER_VECTOR_SYMMETRIC}
 
 
@@ -79,8 +82,11 @@ class RINND:
                  search_tree_leaf_budget=1, leaf_size=None, max_candidates=None, n_iters=None, delta=0.001,
                  random_state=None, diversify_prob=1.0, pruning_degree_multiplier=1.5, verbose=False,
                  normalize=False, cosine_distance_mode="log", quantized_candidate_width=0,
-                 quantized_rerank_width=0, tree_quantization="none", retain_fp32_data=None, device=0):
+                 quantized_rerank_width=0, tree_quantization="none", retain_fp32_data=None, device=0,
+                 precision="fp32"):
         self._h = None
+        if precision not in _PRECISIONS:
+            raise ValueError(f"Unknown precision: {precision}; expected 'fp32' or 'bf16'")
         data = _as_f32_2d(data)
         n_points, dim = data.shape
         if quantized_candidate_width > 0 and quantized_rerank_width > quantized_candidate_width:
@@ -158,6 +164,7 @@ class RINND:
         p.normalize = int(normalize_cosine)
         p.verbose = int(bool(verbose))
         p.device = int(device)
+        p.precision = _PRECISIONS[precision]
 
         h = ctypes.c_void_p()
         L.check(L.lib.rinnd_build(L.ptr(data), n_points, dim, ctypes.byref(p), ctypes.byref(h)))

@@ -22,6 +22,7 @@ DIST_SQEUCLIDEAN, DIST_MANHATTAN, DIST_COSINE, DIST_ALT_COSINE, DIST_ALT_DOT, DI
     DIST_INNER_PRODUCT, DIST_ALT_INNER_PRODUCT = range(8)
 CORR_NONE, CORR_SQRT, CORR_ALT_COSINE, CORR_ALT_IP = range(4)
 Q8_PER_VECTOR_COSINE, Q8_GLOBAL_SYMMETRIC, Q8_PER_VECTOR_SYMMETRIC = range(3)
+PRECISION_FP32, PRECISION_BF16 = range(2)
 
 _i32, _i64, _u64, _f32, _f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_float, ctypes.c_double
 _P = ctypes.c_void_p
@@ -33,7 +34,7 @@ class BuildParams(ctypes.Structure):
         ("leaf_size", _i32), ("max_candidates", _i32), ("n_iters", _i32), ("delta", _f32),
         ("random_seed", _u64), ("diversify_prob", _f32), ("pruning_degree_multiplier", _f32),
         ("angular", _i32), ("distance_kind", _i32), ("correction", _i32), ("normalize", _i32),
-        ("verbose", _i32), ("device", _i32), ("reserved", _i32 * 7),
+        ("verbose", _i32), ("device", _i32), ("precision", _i32), ("reserved", _i32 * 6),
     ]
 
 
@@ -79,6 +80,7 @@ SIGNATURES = {
     "rinnd_distance_pairs": (ctypes.c_int, [_i32, _P, _P, _i64, _i32, _P]),
     "rinnd_search_graph_from_knn": (ctypes.c_int, [_P, _P, _P, _i32, _i32, _i32, _i32, _f32, _P, _P, _P, _P]),
     "rinnd_heap_push_batch": (ctypes.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "rinnd_nndescent_step": (ctypes.c_int, [_P, _i64, _i32, _i32, _i32, _i32, _i32, _u64, _i32, _P, _P, _P, _P]),
     "rinnd_heap_push_batch_noalloc": (ctypes.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rinnd_last_error": (ctypes.c_char_p, []),
     "rinnd_version": (ctypes.c_char_p, []),

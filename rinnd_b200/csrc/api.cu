@@ -255,6 +255,7 @@ void validate_params(const rinnd_build_params* p, int64_t n, int d) {
   require(p->correction >= 0 && p->correction <= CK_ALT_IP, "unknown correction");
   require(p->diversify_prob >= 1.0f, "diversify_prob < 1 is not implemented");
   require(p->pruning_degree_multiplier > 0.f, "pruning_degree_multiplier must be positive");
+  require(p->precision == RINND_PRECISION_FP32 || p->precision == RINND_PRECISION_BF16, "unknown precision");
 }
 
 void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
@@ -300,6 +301,7 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   load_rows(data, on_device, n, d, ld, Dp, X0, st);
   if (ix->normalize) normalize_rows(X0.p, n, D, Dp, st);
   KnnState ks;
+  ks.precision = pin->precision;
   if (kind_uses_norms(ix->kind)) {
     ks.norms.alloc((size_t)N, st);
     compute_norms(X0.p, N, D, Dp, ks.norms.p, st);
@@ -690,6 +692,65 @@ int rinnd_heap_push_batch(int32_t n, int32_t k, int64_t n_ops, const int32_t* ro
     if (out_flags) of.to_host(out_flags, (size_t)n * k);
     RINND_CUDA(cudaStreamSynchronize(st));
     if (n_accepted) *n_accepted = (int64_t)acc;
+  });
+}
+
+int rinnd_nndescent_step(const float* data, int64_t n, int32_t d, int32_t k, int32_t max_candidates, int32_t kind,
+                         int32_t precision, uint64_t seed, int32_t iteration, int32_t* idx, float* dist,
+                         uint8_t* flags, int64_t* changes) {
+  return guarded([&] {
+    require(n >= 2 && n < (int64_t)INT32_MAX - 1 && d >= 1, "invalid shape");
+    require(k >= 1 && k <= 128, "k must be in [1, 128]");
+    require(kind >= 0 && kind < DK_COUNT, "unknown distance kind");
+    require(precision == RINND_PRECISION_FP32 || precision == RINND_PRECISION_BF16, "unknown precision");
+    require(data && idx && dist && flags, "pointers must not be null");
+    const int N = (int)n, Dp = round_up(d, 4);
+    const int c = std::min(std::min(max_candidates > 0 ? max_candidates : std::min(k, 60), 60), k);  // mod.rs:89
+    std::vector<int32_t> hr, hi;
+    std::vector<float> hd;
+    std::vector<uint8_t> hf;
+    for (int64_t r = 0; r < n; ++r)
+      for (int j = 0; j < k; ++j) {
+        const int32_t id = idx[r * k + j];
+        if (id < 0) continue;
+        require(id < N, "neighbor id out of range");
+        hr.push_back((int32_t)r);
+        hi.push_back(id);
+        hd.push_back(dist[r * k + j]);
+        hf.push_back(flags[r * k + j] ? 1 : 0);
+      }
+    ensure_device(0);
+    StreamGuard sg;
+    cudaStream_t st = sg.s;
+    DVec<float> X;
+    load_rows(data, false, n, d, d, Dp, X, st);
+    KnnState ks;
+    knn_init(ks, N, k, c, st);
+    ks.precision = precision;
+    if (kind_uses_norms(kind)) {
+      ks.norms.alloc((size_t)N, st);
+      compute_norms(X.p, N, d, Dp, ks.norms.p, st);
+    }
+    const size_t m = std::max<size_t>(hr.size(), 1);
+    DVec<int32_t> dr(m, st), di(m, st);
+    DVec<float> dd(m, st);
+    DVec<uint8_t> df(m, st);
+    dr.from_host(hr.data(), hr.size());
+    di.from_host(hi.data(), hi.size());
+    dd.from_host(hd.data(), hd.size());
+    df.from_host(hf.data(), hf.size());
+    if (!hr.empty()) heap_push_batch(ks, (long long)hr.size(), dr.p, di.p, dd.p, df.p, st);
+    build_candidates(ks, seed, iteration, st);
+    JoinStats js = local_join(ks, X.p, d, Dp, kind, st);
+    DVec<int32_t> oi((size_t)N * k, st);
+    DVec<float> od((size_t)N * k, st);
+    DVec<uint8_t> of((size_t)N * k, st);
+    finalize_rows(ks.slots.p, N, k, ks.kp, oi.p, od.p, of.p, st);
+    oi.to_host(idx, (size_t)N * k);
+    od.to_host(dist, (size_t)N * k);
+    of.to_host(flags, (size_t)N * k);
+    RINND_CUDA(cudaStreamSynchronize(st));
+    if (changes) *changes = (int64_t)js.changes;
   });
 }
 

@@ -57,6 +57,7 @@ struct KnnState {
   DVec<int> err;             // device error flag of pipelined kernels
   DVec<int32_t> desc;        // per-vertex join descriptors (counts, item prefix, ids, thresholds, norms)
   bool use_tma = true;       // bulk-copy pipelined join when shared memory allows
+  int precision = 0;         // 0: FP32 join tiles; 1: BF16 tensor-core filter + FP32 recheck
   DVec<uint32_t> urow;       // update buffer: destination rows
   DVec<uint64_t> ukey;       // update buffer: slot keys
   unsigned long long ucap = 0;
@@ -79,6 +80,9 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
 bool join_tma_supported(int c, int Dp);
 void join_tma_batch(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st);
 void join_describe(KnnState& s, int kind, cudaStream_t st);
+// Tensor-core join (join_tc.cu): BF16 Gram filter + exact FP32 recheck.
+bool join_tc_supported(int kind, int c, int Dp);
+void join_tc_batch(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st);
 // Sorted output: idx (-1 empty), raw distance (+inf empty).
 void finalize_knn(const KnnState& s, int32_t* out_idx, float* out_dist, cudaStream_t st);
 void finalize_rows(const uint64_t* slots, int N, int k, int kp, int32_t* out_idx, float* out_dist,

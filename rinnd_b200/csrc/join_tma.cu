@@ -6,8 +6,8 @@
 // an endpoint's row when it beats that row's threshold.
 //
 // Work decomposition.  A prepass (k_cand_describe) writes one descriptor per
-// vertex: counts, the compacted candidate ids (new first), their thresholds and
-// norms, and a prefix table of the work items.  An item is (4 consecutive new
+// vertex: counts, the compacted candidate ids (new first), their norms, and a
+// prefix table of the work items.  An item is (4 consecutive new
 // rows) x (1 candidate row j); items entirely on or below the new x new
 // diagonal are never generated.  Persistent CTAs of 1 producer warp + 8
 // consumer warps walk a strided vertex sequence:
@@ -24,30 +24,17 @@
 // Every wait is bounded.  A wait that runs out sets the device error flag and a
 // shared abort flag; all warps leave, the producer first waiting (bounded) for
 // every copy it issued.  The host turns the flag into an error.
-#include "async_copy.cuh"
-#include "dist.cuh"
 #include "engine.h"
-#include "heap.cuh"
+#include "join_common.cuh"
 
 namespace rinnd {
 namespace {
 
-constexpr uint32_t WAIT_POLLS = 1u << 21;
+using namespace joinc;
+
 constexpr int NSTAGE = 3;   // row stages
-constexpr int NDESC = 4;    // descriptor ring
 constexpr int NCONS = 8;    // consumer warps
 constexpr int NT = 32 * (1 + NCONS);
-constexpr int NQMAX = 16;   // max item quads per vertex (na <= 64)
-
-// Descriptor (ints): [0] na, [1] nb, [2] nq, [3] items, [4..20) quad item prefix,
-// [20..) ids (2*maxc), thresholds (2*maxc; filled in the stage by the producer), norms (2*maxc).
-struct Desc {
-  static constexpr int HDR = 4 + NQMAX;
-  __host__ __device__ static int ids(int) { return HDR; }
-  __host__ __device__ static int thr(int maxc) { return HDR + 2 * maxc; }
-  __host__ __device__ static int nrm(int maxc) { return HDR + 4 * maxc; }
-  __host__ __device__ static int stride(int maxc) { return (HDR + 6 * maxc + 15) / 16 * 16; }
-};
 
 struct Layout {
   int maxc, dp, rs, dstride;  // rs: row stride (floats); dstride: descriptor stride (ints)
@@ -116,40 +103,6 @@ struct Bars {
   uint64_t* desc;   // [NDESC]
   int* abort_flag;
 };
-
-// Bounded wait that also gives up when another warp has aborted.
-__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
-  for (uint32_t i = 0; i < WAIT_POLLS; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((i & 63) == 63 && *abort_flag) return false;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-
-// Packed FP32x2 arithmetic (each half rounded as the scalar instruction).
-__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
-  unsigned long long d;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b) {
-  unsigned long long d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
-                                                     unsigned long long c) {
-  unsigned long long d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-__device__ __forceinline__ float f2_sum(unsigned long long a) {
-  return __uint_as_float((uint32_t)a) + __uint_as_float((uint32_t)(a >> 32));
-}
 
 template <int MAXC>
 __global__ void __launch_bounds__(NT)

@@ -354,8 +354,17 @@ __global__ void __launch_bounds__(NT)
 // row i, so one warp per row selects them without atomics (k_cand_forward) and
 // records the list's priority bound; reverse offers then go through the
 // lock-free push with that bound as a pre-filter (k_cand_reverse).
-__device__ __forceinline__ uint32_t cand_priority(uint64_t seed, int iter, long long e) {
-  return (uint32_t)(mix64(seed ^ mix64(0xC0DE0000ull + (uint64_t)iter) ^ (uint64_t)e) >> 33);
+// The priority of edge (row, id) is a hash of (seed, iteration, {row, id}): a
+// uniform draw per pair, used for both endpoints' lists like the reference's
+// one draw pushed to both sides (candidates.rs:171-223).  It does not depend on
+// where the entry sits in its row (slot order follows the order of concurrent
+// pushes) nor on which endpoint's row holds the edge, so a candidate offered
+// twice carries one key and the lists are a function of the rows' contents:
+// runs (and join precisions) from equal rows sample alike.
+__device__ __forceinline__ uint32_t cand_priority(uint64_t seed, int iter, int row, int32_t id) {
+  const uint32_t lo = (uint32_t)min(row, (int)id), hi = (uint32_t)max(row, (int)id);
+  const uint64_t edge = ((uint64_t)lo << 32) | hi;
+  return (uint32_t)(mix64(seed ^ mix64(0xC0DE0000ull + (uint64_t)iter) ^ edge) >> 33);
 }
 
 template <int P>
@@ -375,7 +384,7 @@ __global__ void k_cand_forward(const uint64_t* slots, int N, int k, int kp, int 
         uint64_t sl = slots[(size_t)row * kp + j];
         int32_t id = slot_id(sl);
         if (id >= 0 && slot_new(sl) == flag)
-          key = ((uint64_t)cand_priority(seed, iter, (long long)row * k + j) << 32) | (uint32_t)id;
+          key = ((uint64_t)cand_priority(seed, iter, row, id) << 32) | (uint32_t)id;
       }
       n += __popc(__ballot_sync(0xffffffffu, key != ~0ull));
       b[j] = key;
@@ -435,7 +444,7 @@ __global__ void k_cand_reverse(const uint64_t* slots, int N, int k, int kp, int 
     int32_t id = slot_id(sl);
     if (id < 0) continue;
     const bool nw = slot_new(sl);
-    uint64_t key = ((uint64_t)cand_priority(seed, iter, e) << 32) | (uint32_t)i;
+    uint64_t key = ((uint64_t)cand_priority(seed, iter, i, id) << 32) | (uint32_t)i;
     row_push((nw ? cnew : cold) + (size_t)id * cp, c, (nw ? thr_new : thr_old) + id, key, contention);
   }
 }
@@ -625,7 +634,8 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
   cudaEvent_t e0, e1;
   RINND_CUDA(cudaEventCreate(&e0));
   RINND_CUDA(cudaEventCreate(&e1));
-  const bool use_tma = s.use_tma && join_tma_supported(s.c, Dp);
+  const bool use_tc = s.precision == 1 && join_tc_supported(kind, s.c, Dp);
+  const bool use_tma = use_tc || (s.use_tma && join_tma_supported(s.c, Dp));
   if (s.err.n == 0) {
     s.err.alloc(1, st);
     s.err.fill_bytes(0);
@@ -653,7 +663,9 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
       RINND_CUDA(cudaEventCreate(&kev.back()));
     }
     RINND_CUDA(cudaEventRecord(kev[kev.size() - 2], st));
-    if (use_tma) {
+    if (use_tc) {
+      join_tc_batch(s, X, Dp, kind, (int)v0, v1, s.err.p, st);
+    } else if (use_tma) {
       join_tma_batch(s, X, Dp, kind, (int)v0, v1, s.err.p, st);
     } else if (s.c <= 32) {
       k_local_join<32, 128><<<grid, 128, 0, st>>>(s.cand_new.p, s.cand_old.p, (int)v0, v1, s.c, s.cp, X, Dp, kind,
