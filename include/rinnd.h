@@ -126,6 +126,27 @@ RINND_EXPORT int rinnd_build_on_stream(const float* data, int32_t data_on_device
                                        int64_t ld, const rinnd_build_params* p, void* stream,
                                        rinnd_index** out);
 RINND_EXPORT int rinnd_free(rinnd_index* idx);
+/* ---- batched form: many independent indices ------------------------------- */
+/* One index of a batch: n x d f32 rows (row stride ld floats) on the host or,
+ * with data_on_device, in device memory of params->device; params as for
+ * rinnd_build (metric, k, precision, ... per index). */
+typedef struct rinnd_batch_item {
+  const float* data;
+  int64_t n;
+  int32_t d;
+  int32_t data_on_device;
+  int64_t ld;
+  const rinnd_build_params* params;
+} rinnd_batch_item;
+/* Builds n_items independent indices concurrently (no counterpart in the
+ * reference, which builds one index per call): n_workers host threads (0 =
+ * min(n_items, 16)) take items longest first (estimated n * d * k) and each
+ * build runs on its own stream, so the builds' kernels overlap on the device.
+ * out[i] receives index i (NULL on failure) and status[i] (may be NULL) its
+ * status code.  Returns RINND_OK when every item built, else the first failing
+ * item's code with its message in rinnd_last_error(). */
+RINND_EXPORT int rinnd_build_many(const rinnd_batch_item* items, int32_t n_items, int32_t n_workers,
+                                  rinnd_index** out, int32_t* status);
 RINND_EXPORT int rinnd_build_info_get(const rinnd_index* idx, rinnd_build_info* info);
 RINND_EXPORT int rinnd_index_shape(const rinnd_index* idx, int64_t* n, int32_t* d, int32_t* k);
 

@@ -75,6 +75,100 @@ def _validate_quantized_widths(k: int, candidate_width: int, rerank_width: int) 
         raise ValueError(f"rerank_width {rerank_width} must be zero or at least k ({k})")
 
 
+def _prepare(data, *, metric, n_neighbors, n_trees, n_search_trees, search_tree_leaf_budget, leaf_size,
+             max_candidates, n_iters, delta, random_state, diversify_prob, pruning_degree_multiplier, verbose,
+             normalize, cosine_distance_mode, quantized_candidate_width, quantized_rerank_width, tree_quantization,
+             retain_fp32_data, device, precision):
+    """Validates the constructor arguments (lib.rs:616-755) and maps them to
+    build parameters; returns (rows, params, state for RINND._attach)."""
+    if precision not in _PRECISIONS:
+        raise ValueError(f"Unknown precision: {precision}; expected 'fp32' or 'bf16'")
+    data = _as_f32_2d(data)
+    n_points, dim = data.shape
+    if quantized_candidate_width > 0 and quantized_rerank_width > quantized_candidate_width:
+        raise ValueError("quantized_rerank_width must not exceed quantized_candidate_width when candidate "
+                         "width is explicit")
+    name = metric.lower()
+    if name not in _ALIASES:
+        if name in _KNOWN_OTHER:
+            raise ValueError(f"Metric '{metric}' is not implemented by the B200 engine")
+        raise ValueError(f"Unknown metric: {metric}")
+    name = _ALIASES[name]
+    normalize_cosine = bool(normalize) and name == "cosine"
+    modes = {"log": (False, None), "direct": (True, None)}
+    modes.update({m: (True, e) for m, e in _ENCODINGS.items()})
+    if cosine_distance_mode not in modes:
+        raise ValueError(f"Unknown cosine_distance_mode: {cosine_distance_mode}; expected 'log', 'direct', "
+                         "'int8', 'sq8u', or 'sq8p'")
+    direct_cosine, encoding = modes[cosine_distance_mode]
+    if tree_quantization not in ("none", "int8"):
+        raise ValueError(f"Unknown tree_quantization: {tree_quantization}; expected 'none' or 'int8'")
+    quantize_trees = tree_quantization == "int8"
+    if quantize_trees and encoding is None:
+        raise ValueError("tree_quantization='int8' is available only with a quantized cosine_distance_mode")
+    if quantize_trees and encoding == L.Q8_GLOBAL_SYMMETRIC:
+        raise ValueError("tree_quantization='int8' is incompatible with cosine_distance_mode='sq8u'; use "
+                         "tree_quantization='none'")
+    if direct_cosine and not normalize_cosine:
+        raise ValueError("direct and quantized cosine modes require metric='cosine' and normalize=True")
+    if quantize_trees:
+        raise ValueError("tree_quantization='int8' is not implemented by the B200 engine")
+    if retain_fp32_data is None:
+        retain_fp32_data = (not quantize_trees) or quantized_rerank_width > 0
+
+    # lib.rs:1200-1204 n_trees default: clamp(round(2 log10 N), 3, 12)
+    if n_trees is None:
+        v = 2.0 * math.log10(n_points) if n_points > 0 else float("-inf")
+        n_trees = int(min(max(math.floor(v + 0.5) if math.isfinite(v) else 0, 3), 12))
+
+    # lib.rs:1239-1294 metric -> build distance + correction
+    if name == "euclidean":
+        kind, corr = L.DIST_SQEUCLIDEAN, L.CORR_SQRT
+    elif name == "sqeuclidean":
+        kind, corr = L.DIST_SQEUCLIDEAN, L.CORR_NONE
+    elif name == "manhattan":
+        kind, corr = L.DIST_MANHATTAN, L.CORR_NONE
+    elif name == "cosine":
+        if normalize_cosine:
+            if encoding is not None or direct_cosine:
+                kind, corr = L.DIST_DIRECT_COSINE, L.CORR_NONE
+            else:
+                kind, corr = L.DIST_ALT_DOT, L.CORR_ALT_COSINE
+        else:
+            kind, corr = L.DIST_ALT_COSINE, L.CORR_ALT_COSINE
+    elif name == "dot":
+        kind, corr = L.DIST_ALT_DOT, L.CORR_ALT_COSINE
+    else:  # inner_product
+        kind, corr = L.DIST_ALT_INNER_PRODUCT, L.CORR_ALT_IP
+
+    p = L.BuildParams()
+    L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
+    p.n_neighbors = int(n_neighbors)
+    p.n_trees = int(n_trees)
+    p.n_search_trees = int(n_search_trees)
+    p.search_tree_leaf_budget = max(int(search_tree_leaf_budget), 1)
+    p.leaf_size = int(leaf_size) if leaf_size is not None else 0
+    p.max_candidates = int(max_candidates) if max_candidates is not None else 0
+    p.n_iters = int(n_iters) if n_iters is not None else 0
+    p.delta = float(delta)
+    p.random_seed = int(random_state) if random_state is not None else 42
+    p.diversify_prob = float(diversify_prob)
+    p.pruning_degree_multiplier = float(pruning_degree_multiplier)
+    p.angular = int(name in _ANGULAR)
+    p.distance_kind = kind
+    p.correction = corr
+    p.normalize = int(normalize_cosine)
+    p.verbose = int(bool(verbose))
+    p.device = int(device)
+    p.precision = _PRECISIONS[precision]
+
+    state = {"n_points": n_points, "dim": dim, "n_neighbors": int(n_neighbors), "metric": metric,
+             "encoding": encoding, "candidate_width": int(quantized_candidate_width),
+             "rerank_width": int(quantized_rerank_width), "retain_fp32": bool(retain_fp32_data)}
+    return data, p, state
+
+
+
 class RINND:
     """NNDescent index built and queried on the GPU (crates/rinnd/src/lib.rs:616-755)."""
 
@@ -85,98 +179,29 @@ class RINND:
                  quantized_rerank_width=0, tree_quantization="none", retain_fp32_data=None, device=0,
                  precision="fp32"):
         self._h = None
-        if precision not in _PRECISIONS:
-            raise ValueError(f"Unknown precision: {precision}; expected 'fp32' or 'bf16'")
-        data = _as_f32_2d(data)
-        n_points, dim = data.shape
-        if quantized_candidate_width > 0 and quantized_rerank_width > quantized_candidate_width:
-            raise ValueError("quantized_rerank_width must not exceed quantized_candidate_width when candidate "
-                             "width is explicit")
-        name = metric.lower()
-        if name not in _ALIASES:
-            if name in _KNOWN_OTHER:
-                raise ValueError(f"Metric '{metric}' is not implemented by the B200 engine")
-            raise ValueError(f"Unknown metric: {metric}")
-        name = _ALIASES[name]
-        normalize_cosine = bool(normalize) and name == "cosine"
-        modes = {"log": (False, None), "direct": (True, None)}
-        modes.update({m: (True, e) for m, e in _ENCODINGS.items()})
-        if cosine_distance_mode not in modes:
-            raise ValueError(f"Unknown cosine_distance_mode: {cosine_distance_mode}; expected 'log', 'direct', "
-                             "'int8', 'sq8u', or 'sq8p'")
-        direct_cosine, encoding = modes[cosine_distance_mode]
-        if tree_quantization not in ("none", "int8"):
-            raise ValueError(f"Unknown tree_quantization: {tree_quantization}; expected 'none' or 'int8'")
-        quantize_trees = tree_quantization == "int8"
-        if quantize_trees and encoding is None:
-            raise ValueError("tree_quantization='int8' is available only with a quantized cosine_distance_mode")
-        if quantize_trees and encoding == L.Q8_GLOBAL_SYMMETRIC:
-            raise ValueError("tree_quantization='int8' is incompatible with cosine_distance_mode='sq8u'; use "
-                             "tree_quantization='none'")
-        if direct_cosine and not normalize_cosine:
-            raise ValueError("direct and quantized cosine modes require metric='cosine' and normalize=True")
-        if quantize_trees:
-            raise ValueError("tree_quantization='int8' is not implemented by the B200 engine")
-        if retain_fp32_data is None:
-            retain_fp32_data = (not quantize_trees) or quantized_rerank_width > 0
-
-        # lib.rs:1200-1204 n_trees default: clamp(round(2 log10 N), 3, 12)
-        if n_trees is None:
-            v = 2.0 * math.log10(n_points) if n_points > 0 else float("-inf")
-            n_trees = int(min(max(math.floor(v + 0.5) if math.isfinite(v) else 0, 3), 12))
-
-        # lib.rs:1239-1294 metric -> build distance + correction
-        if name == "euclidean":
-            kind, corr = L.DIST_SQEUCLIDEAN, L.CORR_SQRT
-        elif name == "sqeuclidean":
-            kind, corr = L.DIST_SQEUCLIDEAN, L.CORR_NONE
-        elif name == "manhattan":
-            kind, corr = L.DIST_MANHATTAN, L.CORR_NONE
-        elif name == "cosine":
-            if normalize_cosine:
-                if encoding is not None or direct_cosine:
-                    kind, corr = L.DIST_DIRECT_COSINE, L.CORR_NONE
-                else:
-                    kind, corr = L.DIST_ALT_DOT, L.CORR_ALT_COSINE
-            else:
-                kind, corr = L.DIST_ALT_COSINE, L.CORR_ALT_COSINE
-        elif name == "dot":
-            kind, corr = L.DIST_ALT_DOT, L.CORR_ALT_COSINE
-        else:  # inner_product
-            kind, corr = L.DIST_ALT_INNER_PRODUCT, L.CORR_ALT_IP
-
-        p = L.BuildParams()
-        L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
-        p.n_neighbors = int(n_neighbors)
-        p.n_trees = int(n_trees)
-        p.n_search_trees = int(n_search_trees)
-        p.search_tree_leaf_budget = max(int(search_tree_leaf_budget), 1)
-        p.leaf_size = int(leaf_size) if leaf_size is not None else 0
-        p.max_candidates = int(max_candidates) if max_candidates is not None else 0
-        p.n_iters = int(n_iters) if n_iters is not None else 0
-        p.delta = float(delta)
-        p.random_seed = int(random_state) if random_state is not None else 42
-        p.diversify_prob = float(diversify_prob)
-        p.pruning_degree_multiplier = float(pruning_degree_multiplier)
-        p.angular = int(name in _ANGULAR)
-        p.distance_kind = kind
-        p.correction = corr
-        p.normalize = int(normalize_cosine)
-        p.verbose = int(bool(verbose))
-        p.device = int(device)
-        p.precision = _PRECISIONS[precision]
-
+        data, p, state = _prepare(data, metric=metric, n_neighbors=n_neighbors, n_trees=n_trees,
+                                  n_search_trees=n_search_trees, search_tree_leaf_budget=search_tree_leaf_budget,
+                                  leaf_size=leaf_size, max_candidates=max_candidates, n_iters=n_iters, delta=delta,
+                                  random_state=random_state, diversify_prob=diversify_prob,
+                                  pruning_degree_multiplier=pruning_degree_multiplier, verbose=verbose,
+                                  normalize=normalize, cosine_distance_mode=cosine_distance_mode,
+                                  quantized_candidate_width=quantized_candidate_width,
+                                  quantized_rerank_width=quantized_rerank_width, tree_quantization=tree_quantization,
+                                  retain_fp32_data=retain_fp32_data, device=device, precision=precision)
         h = ctypes.c_void_p()
-        L.check(L.lib.rinnd_build(L.ptr(data), n_points, dim, ctypes.byref(p), ctypes.byref(h)))
+        L.check(L.lib.rinnd_build(L.ptr(data), data.shape[0], data.shape[1], ctypes.byref(p), ctypes.byref(h)))
+        self._attach(h, state)
+
+    def _attach(self, h, state):
         self._h = h
-        self.n_points, self.dim, self.n_neighbors = n_points, dim, int(n_neighbors)
-        self.metric = metric
-        self._encoding = encoding
-        self._candidate_width = int(quantized_candidate_width)
-        self._rerank_width = int(quantized_rerank_width)
-        self._retain_fp32 = bool(retain_fp32_data)
-        if encoding is not None:
-            L.check(L.lib.rinnd_quantize(self._h, encoding))
+        self.n_points, self.dim, self.n_neighbors = state["n_points"], state["dim"], state["n_neighbors"]
+        self.metric = state["metric"]
+        self._encoding = state["encoding"]
+        self._candidate_width = state["candidate_width"]
+        self._rerank_width = state["rerank_width"]
+        self._retain_fp32 = state["retain_fp32"]
+        if self._encoding is not None:
+            L.check(L.lib.rinnd_quantize(self._h, self._encoding))
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -294,3 +319,51 @@ class RINND:
         info["allocated_bytes"] = info["code_bytes"] + info["metadata_bytes"] + info["retained_fp32_bytes"]
         info["bytes_per_vector"] = info["allocated_bytes"] / self.n_points
         return info
+
+
+def build_many(datasets, params=None, n_workers=0, **common):
+    """Builds many independent indices in one call (the batched form; no
+    counterpart in the reference).  `datasets` is a sequence of float32 [N, D]
+    arrays of any sizes and dimensions; `params` an optional sequence of per-index
+    keyword dicts (metric, n_neighbors, precision, ...) merged over `common`.
+    Builds run concurrently, longest first, each on its own stream
+    (rinnd_build_many).  Returns a list of RINND, one per dataset."""
+    datasets = list(datasets)
+    params = list(params) if params is not None else [{} for _ in datasets]
+    if len(params) != len(datasets):
+        raise ValueError("params must have one entry per dataset")
+    defaults = dict(metric="euclidean", n_neighbors=30, n_trees=None, n_search_trees=1, search_tree_leaf_budget=1,
+                    leaf_size=None, max_candidates=None, n_iters=None, delta=0.001, random_state=None,
+                    diversify_prob=1.0, pruning_degree_multiplier=1.5, verbose=False, normalize=False,
+                    cosine_distance_mode="log", quantized_candidate_width=0, quantized_rerank_width=0,
+                    tree_quantization="none", retain_fp32_data=None, device=0, precision="fp32")
+    prepared = []
+    for data, kw in zip(datasets, params):
+        args = dict(defaults)
+        args.update(common)
+        args.update(kw)
+        prepared.append(_prepare(data, **args))
+    n = len(prepared)
+    if n == 0:
+        return []
+    items = (L.BatchItem * n)()
+    for i, (data, p, _) in enumerate(prepared):
+        items[i].data = data.ctypes.data
+        items[i].n, items[i].d = data.shape
+        items[i].data_on_device = 0
+        items[i].ld = data.shape[1]
+        items[i].params = ctypes.addressof(p)
+    handles = (ctypes.c_void_p * n)()
+    status = (ctypes.c_int32 * n)()
+    rc = L.lib.rinnd_build_many(items, n, int(n_workers), handles, status)
+    out = []
+    for i, (_, _, state) in enumerate(prepared):
+        if handles[i]:
+            ix = RINND.__new__(RINND)
+            ix._h = None
+            ix._attach(ctypes.c_void_p(handles[i]), state)
+            out.append(ix)
+        else:
+            out.append(None)
+    L.check(rc)
+    return out

@@ -50,6 +50,10 @@ class BuildInfo(ctypes.Structure):
     ]
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [("data", _P), ("n", _i64), ("d", _i32), ("data_on_device", _i32), ("ld", _i64), ("params", _P)]
+
+
 class StorageInfo(ctypes.Structure):
     _fields_ = [
         ("encoding", ctypes.c_char * 32), ("code_bytes", _i64), ("metadata_bytes", _i64),
@@ -64,6 +68,7 @@ SIGNATURES = {
     "rinnd_build_device": (ctypes.c_int, [_P, _i64, _i32, _i64, _P, _P]),
     "rinnd_build_on_stream": (ctypes.c_int, [_P, _i32, _i64, _i32, _i64, _P, _P, _P]),
     "rinnd_free": (ctypes.c_int, [_P]),
+    "rinnd_build_many": (ctypes.c_int, [_P, _i32, _i32, _P, _P]),
     "rinnd_build_info_get": (ctypes.c_int, [_P, _P]),
     "rinnd_index_shape": (ctypes.c_int, [_P, _P, _P, _P]),
     "rinnd_query": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _P, _P]),

@@ -8,12 +8,17 @@
 // Everything stays resident on the device; host copies are made only for
 // exports.  There is no CPU fallback: without a CUDA device every entry point
 // fails with RINND_ERR_NO_DEVICE.
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <set>
+#include <thread>
+#include <utility>
 #include <new>
 #include <string>
 #include <vector>
@@ -89,7 +94,9 @@ void ensure_device(int dev) {
   // Keep freed stream-ordered allocations cached in the device pool instead of
   // returning them to the driver at every synchronization: builds allocate and
   // free large temporaries per level / per iteration.
+  static std::mutex mu;
   static bool pool_set[64] = {};
+  std::lock_guard<std::mutex> lock(mu);
   if (dev < 64 && !pool_set[dev]) {
     cudaMemPool_t pool;
     RINND_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
@@ -136,6 +143,21 @@ size_t build_working_set(int64_t n, int Dp, int k, int c, int n_trees) {
              N * (20 + 6 * maxc) * 4.0 + std::max(4194304.0, 96 * N) * 12.0 + N * k * 8.0 * 3 + 256.0 * (1 << 20);
   return (size_t)(b * 1.25);
 }
+
+}  // namespace
+
+void rinnd::set_smem_limit_once(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  RINND_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({kernel, dev})) return;
+  RINND_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.insert({kernel, dev});
+}
+
+namespace {
 
 double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -484,6 +506,53 @@ int rinnd_build_on_stream(const float* data, int32_t data_on_device, int64_t n, 
   return guarded([&] {
     build_impl(data, data_on_device != 0, n, d, ld, p, reinterpret_cast<cudaStream_t>(stream), out);
   });
+}
+
+int rinnd_build_many(const rinnd_batch_item* items, int32_t n_items, int32_t n_workers, rinnd_index** out,
+                     int32_t* status) {
+  if (n_items < 0 || (n_items > 0 && (!items || !out)))
+    return fail(RINND_ERR_INVALID, "items and out must not be null and n_items >= 0");
+  if (n_items == 0) return RINND_OK;
+  for (int32_t i = 0; i < n_items; ++i) out[i] = nullptr;
+  // longest first: estimated work n * d * k
+  std::vector<int32_t> order((size_t)n_items);
+  for (int32_t i = 0; i < n_items; ++i) order[(size_t)i] = i;
+  auto cost = [&](int32_t i) {
+    const rinnd_build_params* p = items[i].params;
+    return (double)items[i].n * (double)std::max(items[i].d, 1) * (double)(p ? std::max(p->n_neighbors, 1) : 1);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return cost(a) > cost(b); });
+  const int workers = std::max(1, std::min<int>(n_workers > 0 ? n_workers : 16, n_items));
+  std::vector<int32_t> codes((size_t)n_items, RINND_OK);
+  std::vector<std::string> msgs((size_t)n_items);
+  std::atomic<int32_t> next{0};
+  auto work = [&]() {
+    for (;;) {
+      const int32_t t = next.fetch_add(1);
+      if (t >= n_items) return;
+      const int32_t i = order[(size_t)t];
+      const rinnd_batch_item& it = items[i];
+      codes[(size_t)i] = guarded([&] {
+        require(it.data != nullptr && it.params != nullptr, "batch item data and params must not be null");
+        build_impl(it.data, it.data_on_device != 0, it.n, it.d, it.ld > 0 ? it.ld : it.d, it.params, nullptr,
+                   &out[i]);
+      });
+      if (codes[(size_t)i] != RINND_OK) msgs[(size_t)i] = g_last_error;
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int w = 1; w < workers; ++w) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+  int rc = RINND_OK;
+  for (int32_t i = 0; i < n_items; ++i) {
+    if (status) status[i] = codes[(size_t)i];
+    if (rc == RINND_OK && codes[(size_t)i] != RINND_OK) {
+      rc = codes[(size_t)i];
+      g_last_error = "batch item " + std::to_string(i) + ": " + msgs[(size_t)i];
+    }
+  }
+  return rc;
 }
 
 int rinnd_kernel_launches(uint64_t* count) {

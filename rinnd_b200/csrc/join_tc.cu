@@ -427,11 +427,7 @@ template <bool SQ>
 void launch_tc(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, cudaStream_t st, const TcLayout& L,
                int* err) {
   const size_t smem = L.bytes();
-  static bool attr_done = false;
-  if (!attr_done) {
-    RINND_CUDA(cudaFuncSetAttribute(k_join_tc<SQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    attr_done = true;
-  }
+  set_smem_limit_once(reinterpret_cast<const void*>(k_join_tc<SQ>), 227 * 1024);
   // resident CTAs per SM: shared memory, and at most 4 x 64 of the 512 TMEM columns
   const int per_sm = std::max(1, std::min(4, (int)((227 * 1024) / (smem + 1024))));
   const int grid = std::min(v1 - v0, 148 * per_sm);

@@ -334,11 +334,7 @@ template <int MAXC>
 void launch_join(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, cudaStream_t st, const Layout& L,
                  int* err) {
   const size_t smem = L.bytes();
-  static bool attr_done = false;
-  if (!attr_done) {
-    RINND_CUDA(cudaFuncSetAttribute(k_join_ws<MAXC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    attr_done = true;
-  }
+  set_smem_limit_once(reinterpret_cast<const void*>(k_join_ws<MAXC>), 227 * 1024);
   const int per_sm = std::max(1, (int)((227 * 1024) / (smem + 1024)));
   const int grid = std::min(v1 - v0, 148 * per_sm);
   if (grid <= 0) return;

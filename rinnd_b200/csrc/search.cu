@@ -390,12 +390,8 @@ WarpLayout layout_for(const SearchIndex& ix, int k) {
   L.kmax = k <= 32 ? 32 : (k <= 128 ? 128 : 256);
   L.s = L.kmax <= 32 ? 256 : 4 * L.kmax;
   L.h = 4096;
-  static bool attr_set = false;
-  if (!attr_set) {
-    RINND_CUDA(cudaFuncSetAttribute(k_search<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    RINND_CUDA(cudaFuncSetAttribute(k_search<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr_set = true;
-  }
+  set_smem_limit_once(reinterpret_cast<const void*>(k_search<false>), 200 * 1024);
+  set_smem_limit_once(reinterpret_cast<const void*>(k_search<true>), 200 * 1024);
   if (L.bytes() * WPB > 200 * 1024) throw std::invalid_argument("query dimension too large for search shared memory");
   return L;
 }
