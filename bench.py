@@ -66,6 +66,13 @@ def parse_args():
     ap.add_argument("--verbose", action="store_true", help="per-iteration build statistics")
     ap.add_argument("--parity", action="store_true",
                     help="also build the oracle (CPU restatement) at the full size and report its recall")
+    ap.add_argument("--workload", default="build", choices=["build", "batched"],
+                    help="build: the 1M-point build (default); batched: many independent indices in one call")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"],
+                    help="local-join tiles of the timed builds (the precision form is also reported beside fp32)")
+    ap.add_argument("--items", type=int, default=512, help="batched workload: number of indices")
+    ap.add_argument("--check-items", type=int, default=16,
+                    help="batched workload: indices whose recall is compared with one-at-a-time builds")
     return ap.parse_args()
 
 
@@ -203,6 +210,158 @@ def recall(found, truth):
     return hits / (truth.shape[0] * k)
 
 
+def batched_specs(n_items, seed=0):
+    """Config of the batched form: N log-uniform in [2000, 200000], D from
+    {32, 64, 128, 256}, 10-100 mixture clusters, metric 40% sqeuclidean / 40%
+    cosine / 20% inner product, k = 15; index i uses data seed 1000 + i."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_items):
+        n = int(np.exp(rng.uniform(np.log(2000), np.log(200000))))
+        d = int(rng.choice([32, 64, 128, 256]))
+        c = int(rng.integers(10, 101))
+        u = rng.random()
+        metric = "sqeuclidean" if u < 0.4 else ("cosine" if u < 0.8 else "inner_product")
+        specs.append({"n": n, "d": d, "clusters": c, "metric": metric, "seed": 1000 + i})
+    return specs
+
+
+def run_batched(args, world, rank, local_rank):
+    """The batched form: this rank's longest-first share of the indices built
+    in one rinnd_build_many call from device-resident data; timed with CUDA
+    events, max over ranks; beside it the same share built one index at a time."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from rinnd_b200 import _lib as L
+    from rinnd_b200 import shard
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    specs = batched_specs(args.items)
+    costs = [shard.build_cost(sp["n"], sp["d"], 15) for sp in specs]
+    mine = shard.my_share(costs, rank, world)
+    metric_of = {"sqeuclidean": (L.DIST_SQEUCLIDEAN, L.CORR_NONE, 0), "cosine": (L.DIST_ALT_COSINE, L.CORR_ALT_COSINE, 1),
+                 "inner_product": (L.DIST_ALT_INNER_PRODUCT, L.CORR_ALT_IP, 1)}
+    datas, params = [], []
+    for i in mine:
+        sp = specs[i]
+        g = torch.Generator(device=dev).manual_seed(sp["seed"])
+        centers = torch.randn(sp["clusters"], sp["d"], generator=g, device=dev) * 10.0
+        a = torch.randint(0, sp["clusters"], (sp["n"],), generator=g, device=dev)
+        datas.append((centers[a] + torch.randn(sp["n"], sp["d"], generator=g, device=dev)).contiguous())
+        p = L.BuildParams()
+        L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
+        kind, corr, ang = metric_of[sp["metric"]]
+        p.n_neighbors, p.distance_kind, p.correction, p.angular = 15, kind, corr, ang
+        p.random_seed, p.device = 7 + i, local_rank
+        p.n_trees = int(min(max(np.floor(2.0 * np.log10(sp["n"]) + 0.5), 3), 12))
+        p.precision = 1 if args.precision == "bf16" else 0
+        params.append(p)
+    m = len(mine)
+    items = (L.BatchItem * max(m, 1))()
+    for j in range(m):
+        items[j].data = datas[j].data_ptr()
+        items[j].n, items[j].d = datas[j].shape
+        items[j].data_on_device, items[j].ld = 1, datas[j].shape[1]
+        items[j].params = ctypes.addressof(params[j])
+    handles = (ctypes.c_void_p * max(m, 1))()
+
+    def build_batch():
+        L.check(L.lib.rinnd_build_many(items, m, 0, handles, None))
+        for j in range(m):
+            L.check(L.lib.rinnd_free(handles[j]))
+
+    def one_at_a_time():
+        for j in range(m):
+            h = ctypes.c_void_p()
+            L.check(L.lib.rinnd_build_device(ctypes.c_void_p(datas[j].data_ptr()), datas[j].shape[0],
+                                             datas[j].shape[1], datas[j].shape[1], ctypes.byref(params[j]),
+                                             ctypes.byref(h)))
+            L.check(L.lib.rinnd_free(h))
+
+    def timed(fn):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    for _ in range(max(args.warmup, 1)):
+        build_batch()
+    # builds synchronize their own streams; the host clock brackets the call
+    t_batch = max(timed(build_batch) for _ in range(max(args.steps, 1)))
+    t_one = timed(one_at_a_time)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t_batch, t_one = max_over_ranks(t_batch), max_over_ranks(t_one)
+    n_items, n_points = shard.gather_counts(m, int(sum(d.shape[0] for d in datas)))
+    # per-index recall@15 vs FP64 exact (batched vs one at a time) on the largest checked indices of rank 0
+    quality = {}
+    if rank == 0 and args.check_items > 0 and m > 0:
+        L.check(L.lib.rinnd_build_many(items, m, 0, handles, None))
+        diffs, rb_, ro_ = [], [], []
+        for j in range(min(args.check_items, m)):
+            X = datas[j]
+            rows = torch.arange(min(200, X.shape[0]), device=dev)
+            q = X[rows].double()
+            Xd = X.double()
+            sp = specs[mine[j]]
+            if sp["metric"] == "sqeuclidean":
+                dd = (q * q).sum(1)[:, None] + (Xd * Xd).sum(1)[None, :] - 2.0 * q @ Xd.T
+            elif sp["metric"] == "cosine":
+                dd = -(q / q.norm(dim=1, keepdim=True)) @ (Xd / Xd.norm(dim=1, keepdim=True)).T
+            else:
+                dd = -(q @ Xd.T)
+            dd[torch.arange(len(rows), device=dev), rows] = float("inf")
+            truth = torch.topk(dd, 15, dim=1, largest=False).indices.int().cpu().numpy()
+            kb = np.empty((X.shape[0], 15), np.int32)
+            kd = np.empty((X.shape[0], 15), np.float32)
+            L.check(L.lib.rinnd_neighbor_graph(handles[j], L.ptr(kb), L.ptr(kd)))
+            h = ctypes.c_void_p()
+            L.check(L.lib.rinnd_build_device(ctypes.c_void_p(X.data_ptr()), X.shape[0], X.shape[1], X.shape[1],
+                                             ctypes.byref(params[j]), ctypes.byref(h)))
+            ko = np.empty((X.shape[0], 15), np.int32)
+            L.check(L.lib.rinnd_neighbor_graph(h, L.ptr(ko), L.ptr(kd)))
+            L.check(L.lib.rinnd_free(h))
+            rb_.append(recall(kb[: len(rows)], truth))
+            ro_.append(recall(ko[: len(rows)], truth))
+            diffs.append(rb_[-1] - ro_[-1])
+        for j in range(m):
+            L.check(L.lib.rinnd_free(handles[j]))
+        quality = {"checked_indices": len(diffs), "recall@15_batched_mean": float(np.mean(rb_)),
+                   "recall@15_one_at_a_time_mean": float(np.mean(ro_)), "recall@15_min_diff": float(np.min(diffs))}
+    if rank == 0:
+        line = {
+            "metric": "batched build points/s (512 independent indices, k=15)", "value": n_points / t_batch,
+            "unit": "points/s", "n_gpus": world, "steps": max(args.steps, 1), "warmup": max(args.warmup, 1),
+            "ms_per_step": 1000.0 * t_batch, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched: {n_items} indices, N log-uniform [2000, 200000], D in {{32,64,128,256}}, "
+                                   "10-100 clusters, metric 40% sqeuclidean / 40% cosine / 20% inner product, k=15, "
+                                   f"precision {args.precision}; longest-first over ranks",
+                       "points": n_points, "parallelism": f"shards{world}", "timing": "host clock around the call, "
+                       "synchronized, max over ranks (each build synchronizes its streams)"},
+            "one_at_a_time": {"value": n_points / t_one, "ms": 1000.0 * t_one},
+            "speedup_vs_one_at_a_time": t_one / t_batch, "quality": quality,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -210,6 +369,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "batched":
+        run_batched(args, world, rank, local_rank)
         return
 
     import datetime
@@ -237,6 +399,7 @@ def main():
     p.n_neighbors, p.n_trees, p.leaf_size, p.n_iters, p.delta = K, N_TREES, LEAF, N_ITERS, DELTA
     p.distance_kind, p.correction, p.random_seed, p.device = L.DIST_SQEUCLIDEAN, L.CORR_NONE, 42, local_rank
     p.verbose = int(args.verbose)
+    p.precision = 1 if args.precision == "bf16" else 0
 
     def build(src_ptr, on_device):
         h = ctypes.c_void_p()
@@ -322,6 +485,40 @@ def main():
                       "flops": "2 x D per evaluated pair"},
     }
 
+    # ---- the precision form beside the timed form (BF16 tensor-core join filter + FP32 recheck) ----
+    other = "bf16" if args.precision == "fp32" else "fp32"
+    p_other = L.BuildParams()
+    ctypes.memmove(ctypes.byref(p_other), ctypes.byref(p), ctypes.sizeof(p))
+    p_other.precision = 1 - p.precision
+    p_other.verbose = 0
+
+    def build_other():
+        h2 = ctypes.c_void_p()
+        L.check(L.lib.rinnd_build_on_stream(xp, 1, n, DIM, DIM, ctypes.byref(p_other),
+                                            ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h2)))
+        return h2
+
+    L.check(L.lib.rinnd_free(build_other()))
+    barrier()
+    o_ms, o_infos, ko = [], [], None
+    for _ in range(min(args.steps, 2)):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h2 = build_other()
+        e1.record(stream)
+        o_infos.append(info_of(h2))
+        if not o_infos[:-1] and not args.no_recall:
+            ko = np.empty((n, K), np.int32)
+            kdo = np.empty((n, K), np.float32)
+            L.check(L.lib.rinnd_neighbor_graph(h2, L.ptr(ko), L.ptr(kdo)))
+        L.check(L.lib.rinnd_free(h2))
+        torch.cuda.synchronize()
+        o_ms.append(e0.elapsed_time(e1))
+    o_s = max_over_ranks(sum(o_ms) / 1000.0)
+    other_form = {"precision": other, "value": n * world * len(o_ms) / o_s, "ms_per_step": 1000.0 * o_s / len(o_ms),
+                  "join_kernel_ms": [i.ms_join_kernel for i in o_infos]}
+
     # ---- queries (resident), QPS and recall ----
     h = build(xp, 1)
     inf = info_of(h)
@@ -358,6 +555,8 @@ def main():
                                 for s in range(0, len(sample), 512)])
         del Xd, xx
         quality["graph_recall@30"] = recall(ki[sample], truth)
+        if ko is not None:
+            other_form["graph_recall@30"] = recall(ko[sample], truth)
         qtruth = exact_knn_torch(X_dev, Q_dev, QK)
         quality["query_recall@10"] = recall(qi.cpu().numpy(), qtruth)
         quality["graph_recall_sample"] = f"{len(sample)} seeded rows vs FP64 exact"
@@ -421,6 +620,7 @@ def main():
                        "iterations_per_build": [i.iterations for i in infos]},
             "clocks": clk, "e2e": e2e, "gpu_launches": int(launches1.value - launches0.value),
             "roofline": roofline, "cpu_baseline": cpu,
+            "precision": args.precision, "other_precision_form": other_form,
             "query": {"qps": qps, "k": QK, "epsilon": EPS, "n_queries": N_QUERIES, **quality},
             "timed_steps_ms": {"event": step_ms, "host_total": [i.ms_total for i in infos],
                                "join_kernels": [i.ms_join_kernel for i in infos],
