@@ -37,6 +37,7 @@ extern "C" {
 #define RINND_ERR_CUDA (-3)      /* CUDA runtime failure (RuntimeError)             */
 #define RINND_ERR_NO_DEVICE (-4) /* no CUDA device visible                         */
 #define RINND_ERR_INTERNAL (-5)
+#define RINND_ERR_BUSY (-6)      /* server queue full: collect completed requests, retry */
 
 /* ---- distance kinds: the reference's build distances and proxies -------- */
 #define RINND_DIST_SQEUCLIDEAN 0        /* core/distance/euclidean.rs:14-93    */
@@ -190,6 +191,47 @@ RINND_EXPORT int rinnd_query_quantized(rinnd_index* idx, const float* queries, i
  * multiplier 127 / max|x|. */
 RINND_EXPORT int rinnd_quantize_rows(const float* data, int64_t n, int32_t d, int32_t encoding, int8_t* codes,
                                      float* scales, float* global_multiplier);
+
+/* ---- serving form: continuous batching over one resident index ------------ */
+/* No counterpart in the reference (one query call at a time, lib.rs:775-874).
+ * A server owns a dispatcher thread that packs the queries of pending requests
+ * (any mix of sizes, k and epsilon) into device batches of up to
+ * max_batch_queries, keeps up to max_inflight batches on the device at once and
+ * admits new queries into a batch slot as soon as it frees up.  Each query runs
+ * with its own parameters and random stream (its index within its request), so
+ * a request's results equal rinnd_query (quantized = 0) or rinnd_query_quantized
+ * with the server's widths (quantized = 1, a quantized index) run alone.  The
+ * index must outlive the server; submit and poll may be called from any thread. */
+typedef struct rinnd_server_params {
+  int32_t max_batch_queries;     /* queries per device batch, default 4096             */
+  int32_t max_inflight;          /* batches on the device at once, default 4           */
+  int32_t max_k;                 /* largest k accepted, default 256 (sizes the buffers) */
+  int32_t quantized;             /* 1: int8 search (+ exact rerank) on a quantized index */
+  int32_t candidate_width;       /* quantized widths, rules of core/index.rs:55-89      */
+  int32_t rerank_width;
+  int64_t max_pending_queries;   /* queued, undispatched queries; default 4,194,304    */
+  int32_t reserved[8];
+} rinnd_server_params;
+typedef struct rinnd_server_stats {
+  uint64_t completed_requests, completed_queries, batches, pending_queries;
+  double mean_batch_queries;
+  double p50_ms, p99_ms, max_ms;     /* request latency, submission to completion */
+  int32_t peak_inflight;
+  int32_t reserved[7];
+} rinnd_server_stats;
+typedef struct rinnd_server rinnd_server;
+RINND_EXPORT int rinnd_server_params_default(rinnd_server_params* p);
+RINND_EXPORT int rinnd_server_create(rinnd_index* idx, const rinnd_server_params* p, rinnd_server** out);
+/* Copies the nq x d query rows; returns at once with the request id. */
+RINND_EXPORT int rinnd_server_submit(rinnd_server* s, const float* queries, int64_t nq, int32_t k, float epsilon,
+                                     int64_t* request_id);
+/* Waits up to wait_ms for the request; *done = 1: nq x k results copied out and
+ * the request released (its id is then unknown), 0: still running. */
+RINND_EXPORT int rinnd_server_poll(rinnd_server* s, int64_t request_id, int32_t wait_ms, int32_t* out_idx,
+                                   float* out_dist, int32_t* done);
+RINND_EXPORT int rinnd_server_stats_get(rinnd_server* s, rinnd_server_stats* out);
+/* Finishes the batches in flight and every queued request, then frees the server. */
+RINND_EXPORT int rinnd_server_destroy(rinnd_server* s);
 
 /* ---- storage info (crates/rinnd/src/lib.rs:1028-1077) ---------------------- */
 typedef struct rinnd_storage_info {

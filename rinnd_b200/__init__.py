@@ -10,6 +10,8 @@ from __future__ import annotations
 
 import ctypes
 import math
+import threading
+import time
 
 import numpy as np
 
@@ -367,3 +369,85 @@ def build_many(datasets, params=None, n_workers=0, **common):
             out.append(None)
     L.check(rc)
     return out
+
+
+class Server:
+    """Continuous-batching query server over a built index (the serving form;
+    rinnd_server_*).  Requests of any size, k and epsilon may be submitted from
+    any thread; the server packs them into device batches, keeps several batches
+    on the device at once and admits new queries as batch slots free up.  Each
+    request's result equals `index.query` (or `index.query_quantized` with the
+    index's widths, for a quantized index) run alone.  The index is kept alive
+    by the server."""
+
+    def __init__(self, index, max_batch_queries=4096, max_inflight=4, max_k=256, max_pending_queries=1 << 22,
+                 quantized=None):
+        self._s = None
+        self.index = index
+        p = L.ServerParams()
+        L.check(L.lib.rinnd_server_params_default(ctypes.byref(p)))
+        p.max_batch_queries, p.max_inflight, p.max_k = int(max_batch_queries), int(max_inflight), int(max_k)
+        p.max_pending_queries = int(max_pending_queries)
+        if quantized is None:
+            quantized = index._encoding is not None
+        p.quantized = int(bool(quantized))
+        if quantized:
+            index._ensure_rerank_available(1, index._candidate_width, index._rerank_width)
+            p.candidate_width, p.rerank_width = index._candidate_width, index._rerank_width
+        s = ctypes.c_void_p()
+        L.check(L.lib.rinnd_server_create(index._h, ctypes.byref(p), ctypes.byref(s)))
+        self._s = s
+        self._shapes = {}
+        self._lock = threading.Lock()
+
+    def submit(self, queries, k=10, epsilon=0.1) -> int:
+        q = _as_f32_2d(queries, "queries")
+        self.index._check_dim(q.shape[1])
+        rid = ctypes.c_int64(0)
+        L.check(L.lib.rinnd_server_submit(self._s, L.ptr(q), q.shape[0], int(k), float(epsilon), ctypes.byref(rid)))
+        with self._lock:
+            self._shapes[rid.value] = (q.shape[0], int(k))
+        return rid.value
+
+    def poll(self, request_id, wait_ms=0):
+        """(indices, distances) once the request completed, else None."""
+        with self._lock:
+            if request_id not in self._shapes:
+                raise ValueError("unknown or already collected request id")
+            nq, k = self._shapes[request_id]
+        idx = np.empty((nq, k), np.int32)
+        dist = np.empty((nq, k), np.float32)
+        done = ctypes.c_int32(0)
+        L.check(L.lib.rinnd_server_poll(self._s, int(request_id), int(wait_ms), L.ptr(idx), L.ptr(dist),
+                                        ctypes.byref(done)))
+        if not done.value:
+            return None
+        with self._lock:
+            del self._shapes[request_id]
+        return idx, dist
+
+    def result(self, request_id, timeout_s=60.0):
+        """Blocks until the request completes (TimeoutError after timeout_s)."""
+        deadline = time.monotonic() + timeout_s
+        while True:
+            r = self.poll(request_id, wait_ms=50)
+            if r is not None:
+                return r
+            if time.monotonic() > deadline:
+                raise TimeoutError(f"request {request_id} did not complete in {timeout_s} s")
+
+    def stats(self) -> dict:
+        st = L.ServerStats()
+        L.check(L.lib.rinnd_server_stats_get(self._s, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in L.ServerStats._fields_ if f != "reserved"}
+
+    def close(self):
+        if self._s:
+            L.check(L.lib.rinnd_server_destroy(self._s))
+            self._s = None
+
+    def __del__(self):
+        s = getattr(self, "_s", None)
+        if s:
+            L.lib.rinnd_server_destroy(s)
+            self._s = None

@@ -16,7 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "librinnd_b200.so")
 
 OK = 0
-ERR_INVALID, ERR_OOM, ERR_CUDA, ERR_NO_DEVICE, ERR_INTERNAL = -1, -2, -3, -4, -5
+ERR_INVALID, ERR_OOM, ERR_CUDA, ERR_NO_DEVICE, ERR_INTERNAL, ERR_BUSY = -1, -2, -3, -4, -5, -6
 
 DIST_SQEUCLIDEAN, DIST_MANHATTAN, DIST_COSINE, DIST_ALT_COSINE, DIST_ALT_DOT, DIST_DIRECT_COSINE, \
     DIST_INNER_PRODUCT, DIST_ALT_INNER_PRODUCT = range(8)
@@ -54,6 +54,18 @@ class BatchItem(ctypes.Structure):
     _fields_ = [("data", _P), ("n", _i64), ("d", _i32), ("data_on_device", _i32), ("ld", _i64), ("params", _P)]
 
 
+class ServerParams(ctypes.Structure):
+    _fields_ = [("max_batch_queries", _i32), ("max_inflight", _i32), ("max_k", _i32), ("quantized", _i32),
+                ("candidate_width", _i32), ("rerank_width", _i32), ("max_pending_queries", _i64),
+                ("reserved", _i32 * 8)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed_requests", _u64), ("completed_queries", _u64), ("batches", _u64),
+                ("pending_queries", _u64), ("mean_batch_queries", _f64), ("p50_ms", _f64), ("p99_ms", _f64),
+                ("max_ms", _f64), ("peak_inflight", _i32), ("reserved", _i32 * 7)]
+
+
 class StorageInfo(ctypes.Structure):
     _fields_ = [
         ("encoding", ctypes.c_char * 32), ("code_bytes", _i64), ("metadata_bytes", _i64),
@@ -81,6 +93,12 @@ SIGNATURES = {
     "rinnd_quantize": (ctypes.c_int, [_P, _i32]),
     "rinnd_query_quantized": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _i32, _i32, _P, _P]),
     "rinnd_quantize_rows": (ctypes.c_int, [_P, _i64, _i32, _i32, _P, _P, _P]),
+    "rinnd_server_params_default": (ctypes.c_int, [_P]),
+    "rinnd_server_create": (ctypes.c_int, [_P, _P, _P]),
+    "rinnd_server_submit": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _P]),
+    "rinnd_server_poll": (ctypes.c_int, [_P, _i64, _i32, _P, _P, _P]),
+    "rinnd_server_stats_get": (ctypes.c_int, [_P, _P]),
+    "rinnd_server_destroy": (ctypes.c_int, [_P]),
     "rinnd_storage_info_get": (ctypes.c_int, [_P, _P]),
     "rinnd_distance_pairs": (ctypes.c_int, [_i32, _P, _P, _i64, _i32, _P]),
     "rinnd_search_graph_from_knn": (ctypes.c_int, [_P, _P, _P, _i32, _i32, _i32, _i32, _f32, _P, _P, _P, _P]),

@@ -26,6 +26,7 @@
 #include "../../include/rinnd.h"
 #include "common.cuh"
 #include "engine.h"
+#include "server.h"
 
 using namespace rinnd;
 
@@ -65,6 +66,8 @@ int guarded(F&& f) {
     return RINND_OK;
   } catch (const std::invalid_argument& e) {
     return fail(RINND_ERR_INVALID, e.what());
+  } catch (const ServerBusy& e) {
+    return fail(RINND_ERR_BUSY, e.what());
   } catch (const NoDevice& e) {
     return fail(RINND_ERR_NO_DEVICE, e.what());
   } catch (const std::bad_alloc& e) {
@@ -553,6 +556,83 @@ int rinnd_build_many(const rinnd_batch_item* items, int32_t n_items, int32_t n_w
     }
   }
   return rc;
+}
+
+int rinnd_server_params_default(rinnd_server_params* p) {
+  if (!p) return fail(RINND_ERR_INVALID, "params must not be null");
+  std::memset(p, 0, sizeof(*p));
+  p->max_batch_queries = 4096;
+  p->max_inflight = 4;
+  p->max_k = 256;
+  p->max_pending_queries = 1ll << 22;
+  return RINND_OK;
+}
+
+int rinnd_server_create(rinnd_index* idx, const rinnd_server_params* p, rinnd_server** out) {
+  return guarded([&] {
+    check_index(idx);
+    require(p != nullptr && out != nullptr, "params and out must not be null");
+    require(p->max_batch_queries >= 1 && p->max_batch_queries <= (1 << 20), "max_batch_queries must be in [1, 2^20]");
+    require(p->max_inflight >= 1 && p->max_inflight <= 64, "max_inflight must be in [1, 64]");
+    require(p->max_k >= 1 && p->max_k <= 256, "max_k must be in [1, 256]");
+    require(p->max_pending_queries >= p->max_batch_queries, "max_pending_queries must be >= max_batch_queries");
+    if (p->quantized) {
+      require(idx->encoding >= 0, "a quantized server needs a quantized index (rinnd_quantize)");
+      require(p->candidate_width >= 0 && p->rerank_width >= 0, "quantized widths must be >= 0");
+      require(quantized_width(1, p->candidate_width, p->rerank_width) <= 256, "candidate width must be <= 256");
+    }
+    ServerIndexView v;
+    v.index = idx->search_view();
+    v.device = idx->device;
+    v.D = idx->D;
+    v.Dp = idx->Dp;
+    v.normalize = idx->normalize;
+    v.quantized = p->quantized != 0;
+    v.encoding = idx->encoding;
+    v.global_mult = idx->global_mult;
+    v.stats = idx->search_stats.p;
+    *out = reinterpret_cast<rinnd_server*>(server_create(v, *p));
+  });
+}
+
+int rinnd_server_submit(rinnd_server* s, const float* queries, int64_t nq, int32_t k, float epsilon,
+                        int64_t* request_id) {
+  return guarded([&] {
+    require(s != nullptr && request_id != nullptr, "server and request_id must not be null");
+    Server* sv = reinterpret_cast<Server*>(s);
+    require(nq >= 1 && nq <= (int64_t)INT32_MAX, "nq must be >= 1");
+    require(queries != nullptr, "queries must not be null");
+    const rinnd_server_params& p = server_params(sv);
+    require(k >= 1 && k <= p.max_k, "k must be in [1, max_k]");
+    if (p.quantized) {
+      require(quantized_width(k, p.candidate_width, p.rerank_width) >= k, "quantized candidate width must be at least k");
+      require(quantized_width(k, p.candidate_width, p.rerank_width) <= 256, "quantized candidate width must be <= 256");
+      require(p.candidate_width == 0 || p.rerank_width == 0 || p.rerank_width >= k,
+              "quantized rerank width must be zero or at least k");
+    }
+    *request_id = server_submit(sv, queries, nq, k, epsilon);
+  });
+}
+
+int rinnd_server_poll(rinnd_server* s, int64_t request_id, int32_t wait_ms, int32_t* out_idx, float* out_dist,
+                      int32_t* done) {
+  return guarded([&] {
+    require(s != nullptr && done != nullptr, "server and done must not be null");
+    *done = server_poll(reinterpret_cast<Server*>(s), request_id, wait_ms, out_idx, out_dist) ? 1 : 0;
+  });
+}
+
+int rinnd_server_stats_get(rinnd_server* s, rinnd_server_stats* out) {
+  return guarded([&] {
+    require(s != nullptr && out != nullptr, "server and out must not be null");
+    server_stats(reinterpret_cast<Server*>(s), out);
+  });
+}
+
+int rinnd_server_destroy(rinnd_server* s) {
+  return guarded([&] {
+    if (s) server_destroy(reinterpret_cast<Server*>(s));
+  });
 }
 
 int rinnd_kernel_launches(uint64_t* count) {

@@ -138,6 +138,22 @@ struct SearchStats {
 void greedy_search(const SearchIndex& ix, const float* Q, int nq, int k, float eps,
                    uint64_t qid_base, int32_t* out_idx, float* out_dist, cudaStream_t st,
                    unsigned long long* dstats);
+// Per-query parameters of a packed batch (device arrays of nq entries): result
+// list width, entries written, exact-rerank width (quantized; may be null), epsilon,
+// random stream (added to the index seed; unused by quantized queries, which all use
+// the seed alone) and output offset (entries) into out_idx / out_dist.
+struct QueryMeta {
+  const int32_t* width = nullptr;
+  const int32_t* kout = nullptr;
+  const int32_t* rerank = nullptr;
+  const float* eps = nullptr;
+  const uint64_t* stream = nullptr;
+  const int64_t* out_off = nullptr;
+};
+// Packed batch of queries with per-query parameters (Q8/qinv non-null: quantized).
+void greedy_search_packed(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq,
+                          int max_width, const QueryMeta& meta, int32_t* out_idx, float* out_dist, cudaStream_t st,
+                          unsigned long long* dstats);
 // Quantized search (index.rs:283-334): int8 query codes Q8 (nq x Dq) with scales
 // qinv; the result list holds k_search entries; with rerank > 0 the first
 // `rerank` results are re-ordered by their exact FP32 distance to Q (index.rs:103-126);

@@ -42,6 +42,10 @@ struct WarpLayout {
   __host__ __device__ size_t bytes() const { return vis_off() + (size_t)h * 4; }
 };
 
+__host__ __device__ __forceinline__ int seed_capacity(int width) {
+  return width <= 32 ? 256 : (width <= 128 ? 512 : 1024);
+}
+
 __device__ __forceinline__ uint64_t rkey(float d, int32_t id) {
   return ((uint64_t)fkey(d) << 32) | (uint32_t)id;
 }
@@ -144,15 +148,16 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
 }
 
 // Merge the sorted batch (one key per lane, ascending, ~0 = none; nb valid) into
-// the sorted seed array A[head, tail) -> C[0, min(na + nb, S)).
-__device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int S, int& cur,
+// the sorted seed array A[head, tail) -> C[0, min(na + nb, S)); the two arrays
+// are `stride` entries apart (stride >= S).
+__device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int stride, int S, int& cur,
                                             int& head, int& tail, uint64_t bkey, int nb) {
   const int lane = threadIdx.x & 31;
   if (nb == 0) return;
   bbuf[lane] = bkey;
   __syncwarp();
-  const uint64_t* A = seeds + (size_t)cur * S;
-  uint64_t* C = seeds + (size_t)(cur ^ 1) * S;
+  const uint64_t* A = seeds + (size_t)cur * stride;
+  uint64_t* C = seeds + (size_t)(cur ^ 1) * stride;
   const int na = tail - head;
   for (int i = lane; i < na; i += 32) {  // out = i + #(b < a)
     uint64_t a = A[head + i];
@@ -180,13 +185,14 @@ __device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int
   tail = min(na + nb, S);
 }
 
-// k: result-list width; k_out: entries written per query; rerank (QUANT only):
-// number of leading results re-ordered by exact FP32 distance before output.
+// k: result-list width; k_out: entries written to oi/od; rerank (QUANT only):
+// number of leading results re-ordered by exact FP32 distance before output;
+// rng_seed: the query's random stream.
 template <bool QUANT>
 __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_t* Q8row,
-                           float qinv, int qid, uint64_t seed_base, int k, int k_out, int rerank, float eps,
-                           const WarpLayout& L, unsigned char* wsm, int32_t* out_idx,
-                           float* out_dist, unsigned long long* stats) {
+                           float qinv, uint64_t rng_seed, int k, int k_out, int rerank, float eps,
+                           const WarpLayout& L, unsigned char* wsm, int32_t* oi,
+                           float* od, unsigned long long* stats) {
   const int lane = threadIdx.x & 31;
   float* q = reinterpret_cast<float*>(wsm + L.q_off());
   uint64_t* res = reinterpret_cast<uint64_t*>(wsm + L.res_off());
@@ -202,9 +208,10 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
   }
   for (int t = lane; t < L.h; t += 32) vis[t] = -1;
   __syncwarp();
-  // FP32 queries seed with seed + query index (index.rs:165); quantized queries
-  // all use the seed alone (index.rs:298).
-  QRng rng{seed_base + (QUANT ? 0ull : (uint64_t)qid), 0};
+  QRng rng{rng_seed, 0};
+  // seed-set capacity from this query's own width (not the batch's), so a
+  // query's result does not depend on the queries it is batched with
+  const int scap = seed_capacity(k);
   int rc = 0, cur = 0, head = 0, tail = 0;
   unsigned long long evals = 0, expansions = 0;
   unsigned long long* overflow = &stats[2];
@@ -231,7 +238,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
       result_push(res, rc, k, dj, ij);
     }
     uint64_t sorted = warp_sort32(bkey);
-    seeds_merge(seeds, bbuf, L.s, cur, head, tail, sorted, __popc(m));
+    seeds_merge(seeds, bbuf, L.s, scap, cur, head, tail, sorted, __popc(m));
   };
 
   // ---- tree seeding (greedy.rs:70-99, leaf budget 1) ----
@@ -283,7 +290,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
         result_push(res, rc, k, __shfl_sync(0xffffffffu, d, j), __shfl_sync(0xffffffffu, id, j));
       }
       uint64_t sorted = warp_sort32(fresh ? rkey(d, id) : ~0ull);
-      seeds_merge(seeds, bbuf, L.s, cur, head, tail, sorted, __popc(m));
+      seeds_merge(seeds, bbuf, L.s, scap, cur, head, tail, sorted, __popc(m));
     }
   }
   // ---- traverse (greedy.rs:165-201) ----
@@ -324,7 +331,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
       }
       bool acc = (acc_mask >> lane) & 1u;
       uint64_t sorted = warp_sort32(acc ? rkey(d, nb) : ~0ull);
-      seeds_merge(seeds, bbuf, L.s, cur, head, tail, sorted, __popc(acc_mask));
+      seeds_merge(seeds, bbuf, L.s, scap, cur, head, tail, sorted, __popc(acc_mask));
     }
   }
   // ---- exact rerank of the first `rerank` results (index.rs:103-126): exact
@@ -353,11 +360,11 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
       uint64_t key = res[j];
       int32_t id = (int32_t)(uint32_t)key;
       float d = fkey_inv((uint32_t)(key >> 32));
-      out_idx[(size_t)qid * k_out + j] = ix.vertex_order ? ix.vertex_order[id] : id;
-      out_dist[(size_t)qid * k_out + j] = QUANT ? d : apply_correction(ix.corr, d);
+      oi[j] = ix.vertex_order ? ix.vertex_order[id] : id;
+      od[j] = QUANT ? d : apply_correction(ix.corr, d);
     } else {
-      out_idx[(size_t)qid * k_out + j] = -1;
-      out_dist[(size_t)qid * k_out + j] = __int_as_float(0x7f800000);
+      oi[j] = -1;
+      od[j] = __int_as_float(0x7f800000);
     }
   }
   if (lane == 0) {
@@ -370,16 +377,30 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
 template <bool QUANT>
 __global__ void __launch_bounds__(WPB * 32)
     k_search(SearchIndex ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k, int k_out,
-             int rerank, float eps, uint64_t qid_base, WarpLayout L, int32_t* out_idx, float* out_dist,
-             unsigned long long* stats) {
+             int rerank, float eps, uint64_t qid_base, QueryMeta meta, WarpLayout L, int32_t* out_idx,
+             float* out_dist, unsigned long long* stats) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = threadIdx.x >> 5;
   unsigned char* wsm = smem + (size_t)w * L.bytes();
   const int total_warps = gridDim.x * WPB;
   for (int qi = blockIdx.x * WPB + w; qi < nq; qi += total_warps) {
+    int qk = k, qko = k_out, qr = rerank;
+    float qe = eps;
+    // FP32 queries seed with seed + query index (index.rs:165); quantized
+    // queries all use the seed alone (index.rs:298)
+    uint64_t stream = QUANT ? 0ull : qid_base + (uint64_t)qi;
+    int64_t off = (int64_t)qi * k_out;
+    if (meta.width) {  // per-query parameters of a packed batch
+      qk = meta.width[qi];
+      qko = meta.kout[qi];
+      qr = meta.rerank ? meta.rerank[qi] : 0;
+      qe = meta.eps[qi];
+      stream = QUANT ? 0ull : meta.stream[qi];
+      off = meta.out_off[qi];
+    }
     search_one<QUANT>(ix, Q + (size_t)qi * ix.Dp, QUANT ? Q8 + (size_t)qi * ix.Dq : nullptr,
-                      QUANT ? qinv[qi] : 0.f, qi, ix.seed + qid_base, k, k_out, rerank, eps, L, wsm, out_idx,
-                      out_dist, stats);
+                      QUANT ? qinv[qi] : 0.f, ix.seed + stream, qk, qko, qr, qe, L, wsm, out_idx + off,
+                      out_dist + off, stats);
   }
 }
 
@@ -388,7 +409,7 @@ WarpLayout layout_for(const SearchIndex& ix, int k) {
   WarpLayout L;
   L.dp = std::max(ix.Dp, ix.Dq / 4);
   L.kmax = k <= 32 ? 32 : (k <= 128 ? 128 : 256);
-  L.s = L.kmax <= 32 ? 256 : 4 * L.kmax;
+  L.s = seed_capacity(L.kmax);
   L.h = 4096;
   set_smem_limit_once(reinterpret_cast<const void*>(k_search<false>), 200 * 1024);
   set_smem_limit_once(reinterpret_cast<const void*>(k_search<true>), 200 * 1024);
@@ -405,7 +426,26 @@ void greedy_search(const SearchIndex& ix, const float* Q, int nq, int k, float e
   const WarpLayout L = layout_for(ix, k);
   int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
   k_search<false><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, nullptr, nullptr, nq, k, k, 0, eps, qid_base,
-                                                             L, out_idx, out_dist, dstats);
+                                                             QueryMeta{}, L, out_idx, out_dist, dstats);
+  RINND_LAUNCH_CHECK();
+}
+
+void greedy_search_packed(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq,
+                          int max_width, const QueryMeta& meta, int32_t* out_idx, float* out_dist, cudaStream_t st,
+                          unsigned long long* dstats) {
+  if (nq <= 0) return;
+  if (!meta.width || !meta.kout || !meta.eps || !meta.stream || !meta.out_off)
+    throw std::invalid_argument("packed search needs every per-query array");
+  const bool quant = Q8 != nullptr;
+  if (quant && (!ix.codes || ix.Dq % 16 != 0)) throw std::invalid_argument("index has no int8 codes");
+  const WarpLayout L = layout_for(ix, max_width);
+  int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
+  if (quant)
+    k_search<true><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, 0, 0, 0, 0.f, 0, meta, L,
+                                                              out_idx, out_dist, dstats);
+  else
+    k_search<false><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, nullptr, nullptr, nq, 0, 0, 0, 0.f, 0, meta, L,
+                                                               out_idx, out_dist, dstats);
   RINND_LAUNCH_CHECK();
 }
 
@@ -418,7 +458,7 @@ void greedy_search_quantized(const SearchIndex& ix, const float* Q, const int8_t
   const WarpLayout L = layout_for(ix, width);
   int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
   k_search<true><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, width, k_out, rerank, eps, 0,
-                                                            L, out_idx, out_dist, dstats);
+                                                            QueryMeta{}, L, out_idx, out_dist, dstats);
   RINND_LAUNCH_CHECK();
 }
 
