@@ -66,8 +66,11 @@ def parse_args():
     ap.add_argument("--verbose", action="store_true", help="per-iteration build statistics")
     ap.add_argument("--parity", action="store_true",
                     help="also build the oracle (CPU restatement) at the full size and report its recall")
-    ap.add_argument("--workload", default="build", choices=["build", "batched"],
-                    help="build: the 1M-point build (default); batched: many independent indices in one call")
+    ap.add_argument("--workload", default="build", choices=["build", "batched", "serving"],
+                    help="build: the 1M-point build (default); batched: many independent indices in one call; "
+                         "serving: continuous-batching queries against a 10M x 96 index")
+    ap.add_argument("--serve-n", type=int, default=10_000_000, help="serving workload: index size")
+    ap.add_argument("--serve-seconds", type=float, default=4.0, help="serving workload: seconds per offered load")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"],
                     help="local-join tiles of the timed builds (the precision form is also reported beside fp32)")
     ap.add_argument("--items", type=int, default=512, help="batched workload: number of indices")
@@ -362,6 +365,161 @@ def run_batched(args, world, rank, local_rank):
         dist.destroy_process_group()
 
 
+def run_serving(args, world, rank, local_rank):
+    """The serving form on one GPU (replicas per rank otherwise): a 10M x 96
+    index of L2-normalised Gaussian-mixture rows (1000 clusters), cosine, k=30,
+    built with the BF16 join (FP32 recheck); int8 per-vector search codes with
+    an exact FP32 rerank behind the continuous-batching server.  Request sizes
+    are log-uniform in [1, 4096], k in {10, 100}, epsilon 0.1, arrivals Poisson
+    at 0.5 / 0.8 / 0.95 of the measured saturated QPS."""
+    import torch
+
+    import rinnd_b200
+    from rinnd_b200 import _lib as L
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n, d = args.serve_n, 96
+    g = torch.Generator(device=dev).manual_seed(5 + rank)
+    centers = torch.randn(1000, d, generator=g, device=dev) * 10.0
+
+    def sample(m):
+        out = torch.empty(m, d, device=dev)
+        for s0 in range(0, m, 1 << 21):
+            s1 = min(m, s0 + (1 << 21))
+            a = torch.randint(0, 1000, (s1 - s0,), generator=g, device=dev)
+            x = centers[a] + torch.randn(s1 - s0, d, generator=g, device=dev)
+            out[s0:s1] = x / x.norm(dim=1, keepdim=True)
+        return out
+
+    X = sample(n)
+    Qd = sample(60000)
+    Q = Qd.cpu().numpy()
+    p = L.BuildParams()
+    L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
+    p.n_neighbors, p.distance_kind, p.correction, p.angular, p.normalize = 30, L.DIST_DIRECT_COSINE, L.CORR_NONE, 1, 1
+    p.n_trees, p.precision, p.device, p.random_seed = 12, 1, local_rank, 42
+    h = ctypes.c_void_p()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L.check(L.lib.rinnd_build_device(ctypes.c_void_p(X.data_ptr()), n, d, d, ctypes.byref(p), ctypes.byref(h)))
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    L.check(L.lib.rinnd_quantize(h, L.Q8_PER_VECTOR_COSINE))
+    t_encode = time.perf_counter() - t0
+    # a RINND view of the built index for the server and the plain FP32 search
+    ix = rinnd_b200.RINND.__new__(rinnd_b200.RINND)
+    ix._h = None
+    ix._attach(h, {"n_points": n, "dim": d, "n_neighbors": 30, "metric": "cosine", "encoding": None,
+                   "candidate_width": 0, "rerank_width": 100, "retain_fp32": True})
+    ix._encoding = L.Q8_PER_VECTOR_COSINE  # codes made above
+    # exact cosine top-10 of 1000 sampled queries (FP64, the recall checker)
+    ns = 1000
+    qs = Qd[:ns].double()
+    best_v = torch.full((ns, 10), -2.0, dtype=torch.float64, device=dev)
+    best_i = torch.zeros((ns, 10), dtype=torch.int64, device=dev)
+    for s0 in range(0, n, 1 << 20):
+        sims = qs @ X[s0:s0 + (1 << 20)].double().T
+        v, i = torch.topk(sims, 10, dim=1)
+        cv = torch.cat([best_v, v], 1)
+        ci = torch.cat([best_i, i + s0], 1)
+        best_v, o = torch.topk(cv, 10, dim=1)
+        best_i = torch.gather(ci, 1, o)
+    truth = best_i.int().cpu().numpy()
+    rng = np.random.default_rng(11)
+
+    def make_requests(m):
+        out = []
+        for _ in range(m):
+            sz = int(np.exp(rng.uniform(0, np.log(4096))))
+            lo = int(rng.integers(0, len(Q) - sz))
+            out.append((lo, sz, int(rng.choice([10, 100]))))
+        return out
+
+    def serve(reqs, rate_qps=None):
+        """Submits the requests (all at once, or Poisson at rate_qps queries/s) and collects
+        them; returns (wall seconds, server stats)."""
+        srv = rinnd_b200.Server(ix, max_batch_queries=4096, max_inflight=4, quantized=True)
+        ids = []
+        done = []
+
+        def collector():
+            i = 0
+            while i < len(reqs):
+                while i >= len(ids):
+                    time.sleep(0.0002)
+                srv.result(ids[i], timeout_s=120.0)
+                i += 1
+            done.append(time.perf_counter())
+
+        th = threading.Thread(target=collector)
+        th.start()
+        mean_sz = float(np.mean([r[1] for r in reqs]))
+        t_start = time.perf_counter()
+        t_next = t_start
+        for lo, sz, k in reqs:
+            if rate_qps:
+                t_next += rng.exponential(mean_sz / rate_qps)
+                delay = t_next - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+            ids.append(srv.submit(Q[lo:lo + sz], k=k, epsilon=0.1))
+        th.join()
+        st = srv.stats()
+        srv.close()
+        return done[0] - t_start, st
+
+    # saturated throughput: a backlog submitted at once
+    sat_reqs = make_requests(1000)
+    sat_q = sum(r[1] for r in sat_reqs)
+    serve(make_requests(20))  # warm-up
+    t_sat, st_sat = serve(sat_reqs)
+    qps_sat = sat_q / t_sat
+    loads = []
+    for f in (0.5, 0.8, 0.95):
+        rate = f * qps_sat
+        mean_sz = 4095.0 / np.log(4096.0)
+        m = max(20, int(args.serve_seconds * rate / mean_sz))
+        reqs = make_requests(m)
+        t, st = serve(reqs, rate_qps=rate)
+        loads.append({"offered_fraction": f, "offered_qps": rate, "achieved_qps": sum(r[1] for r in reqs) / t,
+                      "requests": m, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+                      "mean_batch_queries": st["mean_batch_queries"], "peak_inflight": st["peak_inflight"]})
+    # recall@10: int8 search + FP32 rerank through the server, and the plain FP32 search
+    srv = rinnd_b200.Server(ix, quantized=True)
+    rid = srv.submit(Q[:ns], k=10, epsilon=0.1)
+    qi, _ = srv.result(rid)
+    srv.close()
+    fi = torch.empty((10000, 10), dtype=torch.int32, device=dev)
+    fd = torch.empty((10000, 10), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L.check(L.lib.rinnd_query_device(h, ctypes.c_void_p(Qd.data_ptr()), 10000, d, 10, 0.1, 0,
+                                     ctypes.c_void_p(fi.data_ptr()), ctypes.c_void_p(fd.data_ptr()), None))
+    torch.cuda.synchronize()
+    t_fp32 = time.perf_counter() - t0
+    fp32_ids = fi[:ns].cpu().numpy()
+    if rank == 0:
+        line = {
+            "metric": "serving QPS and p50/p99 latency at recall@10 (10M x 96, int8 + FP32 rerank)",
+            "value": qps_sat, "unit": "queries/s", "n_gpus": world, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int8 search / f32 rerank", "data": "synthetic",
+            "config": {"workload": f"serving: {n} x {d} L2-normalised GMM (1000 clusters), cosine, k=30, BF16 join + "
+                                   "FP32 recheck build; int8 per-vector codes, candidate width max(k, 100), rerank 100; "
+                                   "requests log-uniform 1-4096 queries, k in {10, 100}, eps 0.1, Poisson arrivals",
+                       "parallelism": f"replicas{world}"},
+            "build_s": t_build, "encode_s": t_encode, "saturated": {"qps": qps_sat, "p50_ms": st_sat["p50_ms"],
+                                                                     "p99_ms": st_sat["p99_ms"]},
+            "loads": loads,
+            "recall@10": {"server_int8_rerank": recall(qi, truth), "plain_fp32_search": recall(fp32_ids, truth),
+                          "sample_queries": ns},
+            "plain_fp32_search_qps": 10000 / t_fp32,
+        }
+        print(json.dumps(line), flush=True)
+    L.check(L.lib.rinnd_free(h))
+    ix._h = None
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -372,6 +530,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args, world, rank, local_rank)
+        return
+    if args.workload == "serving":
+        run_serving(args, world, rank, local_rank)
         return
 
     import datetime

@@ -233,6 +233,12 @@ RINND_EXPORT int rinnd_server_stats_get(rinnd_server* s, rinnd_server_stats* out
 /* Finishes the batches in flight and every queued request, then frees the server. */
 RINND_EXPORT int rinnd_server_destroy(rinnd_server* s);
 
+/* Search counters of an index since it was built (or last reset): distance
+ * evaluations, node expansions and visited-table overflows (ids skipped because
+ * their table had no free slot within the probe limit).  reset != 0 zeroes them. */
+RINND_EXPORT int rinnd_search_stats_get(rinnd_index* idx, uint64_t* evaluations, uint64_t* expansions,
+                                        uint64_t* visited_overflows, int32_t reset);
+
 /* ---- storage info (crates/rinnd/src/lib.rs:1028-1077) ---------------------- */
 typedef struct rinnd_storage_info {
   char encoding[32];

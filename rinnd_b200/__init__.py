@@ -303,6 +303,13 @@ class RINND:
         L.check(L.lib.rinnd_vertex_order(self._h, L.ptr(out)))
         return out
 
+    def search_stats(self, reset=False) -> dict:
+        """Distance evaluations, node expansions and visited-table overflows of
+        the searches since the build (or the last reset)."""
+        v = [ctypes.c_uint64(0) for _ in range(3)]
+        L.check(L.lib.rinnd_search_stats_get(self._h, *(ctypes.byref(x) for x in v), int(bool(reset))))
+        return {"evaluations": v[0].value, "expansions": v[1].value, "visited_overflows": v[2].value}
+
     @property
     def build_info(self) -> dict:
         info = L.BuildInfo()

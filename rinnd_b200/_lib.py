@@ -93,6 +93,7 @@ SIGNATURES = {
     "rinnd_quantize": (ctypes.c_int, [_P, _i32]),
     "rinnd_query_quantized": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _i32, _i32, _P, _P]),
     "rinnd_quantize_rows": (ctypes.c_int, [_P, _i64, _i32, _i32, _P, _P, _P]),
+    "rinnd_search_stats_get": (ctypes.c_int, [_P, _P, _P, _P, _i32]),
     "rinnd_server_params_default": (ctypes.c_int, [_P]),
     "rinnd_server_create": (ctypes.c_int, [_P, _P, _P]),
     "rinnd_server_submit": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _P]),

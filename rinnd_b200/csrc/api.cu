@@ -558,6 +558,21 @@ int rinnd_build_many(const rinnd_batch_item* items, int32_t n_items, int32_t n_w
   return rc;
 }
 
+int rinnd_search_stats_get(rinnd_index* idx, uint64_t* evaluations, uint64_t* expansions,
+                           uint64_t* visited_overflows, int32_t reset) {
+  return guarded([&] {
+    check_index(idx);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    unsigned long long h[4] = {0, 0, 0, 0};
+    RINND_CUDA(cudaDeviceSynchronize());
+    RINND_CUDA(cudaMemcpy(h, idx->search_stats.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (evaluations) *evaluations = h[0];
+    if (expansions) *expansions = h[1];
+    if (visited_overflows) *visited_overflows = h[2];
+    if (reset) RINND_CUDA(cudaMemset(idx->search_stats.p, 0, sizeof(h)));
+  });
+}
+
 int rinnd_server_params_default(rinnd_server_params* p) {
   if (!p) return fail(RINND_ERR_INVALID, "params must not be null");
   std::memset(p, 0, sizeof(*p));

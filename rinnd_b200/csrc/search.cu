@@ -58,6 +58,8 @@ struct QRng {  // counter-based per-query stream (seed + query id, as index.rs:1
 };
 
 // Visited table: returns true if id was already present (VisitedSet::check_and_mark).
+// An id that finds no free slot within HASH_PROBES probes is counted and treated
+// as visited: it is skipped, which keeps the work of a search bounded.
 __device__ __forceinline__ bool visited_check_and_mark(int32_t* tab, int h, int32_t id,
                                                        unsigned long long* overflow) {
   uint32_t pos = ((uint32_t)id * 2654435761u) & (uint32_t)(h - 1);
@@ -68,7 +70,18 @@ __device__ __forceinline__ bool visited_check_and_mark(int32_t* tab, int h, int3
     pos = (pos + 1) & (uint32_t)(h - 1);
   }
   atomicAdd(overflow, 1ull);
-  return false;
+  return true;
+}
+
+// Visited-table entries of a query of result width w: shared memory up to w = 32,
+// beyond that a per-warp region of global memory (a search of width w
+// evaluates on the order of 100 w nodes).  A query's capacity depends on its
+// own width only, so its result does not depend on the queries batched with it.
+__host__ __device__ __forceinline__ int visited_capacity(int width) {
+  if (width <= 32) return 4096;
+  int h = 8192;
+  while (h < 128 * width) h <<= 1;
+  return h;
 }
 
 template <bool QUANT>
@@ -191,7 +204,7 @@ __device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int
 template <bool QUANT>
 __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_t* Q8row,
                            float qinv, uint64_t rng_seed, int k, int k_out, int rerank, float eps,
-                           const WarpLayout& L, unsigned char* wsm, int32_t* oi,
+                           const WarpLayout& L, unsigned char* wsm, int32_t* gvis, int32_t* oi,
                            float* od, unsigned long long* stats) {
   const int lane = threadIdx.x & 31;
   float* q = reinterpret_cast<float*>(wsm + L.q_off());
@@ -206,7 +219,9 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
   } else {
     for (int t = lane; t < ix.Dp; t += 32) q[t] = t < ix.D ? Qrow[t] : 0.f;
   }
-  for (int t = lane; t < L.h; t += 32) vis[t] = -1;
+  const int vcap = visited_capacity(k);
+  if (gvis) vis = gvis;  // global-memory table of this warp
+  for (int t = lane; t < vcap; t += 32) vis[t] = -1;
   __syncwarp();
   QRng rng{rng_seed, 0};
   // seed-set capacity from this query's own width (not the batch's), so a
@@ -223,7 +238,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
     bool fresh = false;
     float d = 0.f;
     if (have) {
-      fresh = !visited_check_and_mark(vis, L.h, my_id, overflow);
+      fresh = !visited_check_and_mark(vis, vcap, my_id, overflow);
       if (fresh) d = dist_to<QUANT>(ix, q, q8, qinv, my_id);
     }
     unsigned m = __ballot_sync(0xffffffffu, fresh);
@@ -275,7 +290,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
       for (int r = 0; r < 32 && r0 + r < need; ++r) {
         int32_t x = __shfl_sync(0xffffffffu, id, r);
         bool f = false;
-        if (lane == 0) f = !visited_check_and_mark(vis, L.h, x, overflow);
+        if (lane == 0) f = !visited_check_and_mark(vis, vcap, x, overflow);
         f = __shfl_sync(0xffffffffu, f, 0);
         if (lane == r) fresh = f;
       }
@@ -310,7 +325,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
     for (int c0 = s; c0 < e; c0 += 32) {
       int c = c0 + lane;
       int32_t nb = c < e ? ix.indices[c] : -1;
-      bool fresh = nb >= 0 && !visited_check_and_mark(vis, L.h, nb, overflow);
+      bool fresh = nb >= 0 && !visited_check_and_mark(vis, vcap, nb, overflow);
       float d = fresh ? dist_to<QUANT>(ix, q, q8, qinv, nb) : 0.f;
       unsigned m = __ballot_sync(0xffffffffu, fresh);
       evals += __popc(m);
@@ -377,11 +392,12 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
 template <bool QUANT>
 __global__ void __launch_bounds__(WPB * 32)
     k_search(SearchIndex ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k, int k_out,
-             int rerank, float eps, uint64_t qid_base, QueryMeta meta, WarpLayout L, int32_t* out_idx,
-             float* out_dist, unsigned long long* stats) {
+             int rerank, float eps, uint64_t qid_base, QueryMeta meta, WarpLayout L, int32_t* gvis, int gcap,
+             int32_t* out_idx, float* out_dist, unsigned long long* stats) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = threadIdx.x >> 5;
   unsigned char* wsm = smem + (size_t)w * L.bytes();
+  int32_t* my_gvis = gvis ? gvis + (size_t)(blockIdx.x * WPB + w) * gcap : nullptr;
   const int total_warps = gridDim.x * WPB;
   for (int qi = blockIdx.x * WPB + w; qi < nq; qi += total_warps) {
     int qk = k, qko = k_out, qr = rerank;
@@ -399,7 +415,7 @@ __global__ void __launch_bounds__(WPB * 32)
       off = meta.out_off[qi];
     }
     search_one<QUANT>(ix, Q + (size_t)qi * ix.Dp, QUANT ? Q8 + (size_t)qi * ix.Dq : nullptr,
-                      QUANT ? qinv[qi] : 0.f, ix.seed + stream, qk, qko, qr, qe, L, wsm, out_idx + off,
+                      QUANT ? qinv[qi] : 0.f, ix.seed + stream, qk, qko, qr, qe, L, wsm, my_gvis, out_idx + off,
                       out_dist + off, stats);
   }
 }
@@ -410,12 +426,25 @@ WarpLayout layout_for(const SearchIndex& ix, int k) {
   L.dp = std::max(ix.Dp, ix.Dq / 4);
   L.kmax = k <= 32 ? 32 : (k <= 128 ? 128 : 256);
   L.s = seed_capacity(L.kmax);
-  L.h = 4096;
+  L.h = L.kmax <= 32 ? visited_capacity(L.kmax) : 0;  // wider searches use a global-memory table
   set_smem_limit_once(reinterpret_cast<const void*>(k_search<false>), 200 * 1024);
   set_smem_limit_once(reinterpret_cast<const void*>(k_search<true>), 200 * 1024);
   if (L.bytes() * WPB > 200 * 1024) throw std::invalid_argument("query dimension too large for search shared memory");
   return L;
 }
+
+// Per-warp global-memory visited tables of a launch whose widest query does
+// not fit the shared-memory table (freed stream-ordered after the launch).
+struct GlobalVisited {
+  DVec<int32_t> buf;
+  int cap = 0;
+  GlobalVisited(const WarpLayout& L, int blocks, cudaStream_t st) {
+    if (L.h > 0) return;
+    cap = visited_capacity(L.kmax);
+    buf.alloc((size_t)blocks * WPB * cap, st);
+  }
+  int32_t* p() const { return buf.p; }
+};
 
 }  // namespace
 
@@ -425,8 +454,9 @@ void greedy_search(const SearchIndex& ix, const float* Q, int nq, int k, float e
   if (nq <= 0) return;
   const WarpLayout L = layout_for(ix, k);
   int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
+  GlobalVisited gv(L, blocks, st);
   k_search<false><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, nullptr, nullptr, nq, k, k, 0, eps, qid_base,
-                                                             QueryMeta{}, L, out_idx, out_dist, dstats);
+                                                             QueryMeta{}, L, gv.p(), gv.cap, out_idx, out_dist, dstats);
   RINND_LAUNCH_CHECK();
 }
 
@@ -440,12 +470,13 @@ void greedy_search_packed(const SearchIndex& ix, const float* Q, const int8_t* Q
   if (quant && (!ix.codes || ix.Dq % 16 != 0)) throw std::invalid_argument("index has no int8 codes");
   const WarpLayout L = layout_for(ix, max_width);
   int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
+  GlobalVisited gv(L, blocks, st);
   if (quant)
-    k_search<true><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, 0, 0, 0, 0.f, 0, meta, L,
-                                                              out_idx, out_dist, dstats);
+    k_search<true><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, 0, 0, 0, 0.f, 0, meta, L, gv.p(),
+                                                              gv.cap, out_idx, out_dist, dstats);
   else
     k_search<false><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, nullptr, nullptr, nq, 0, 0, 0, 0.f, 0, meta, L,
-                                                               out_idx, out_dist, dstats);
+                                                               gv.p(), gv.cap, out_idx, out_dist, dstats);
   RINND_LAUNCH_CHECK();
 }
 
@@ -457,8 +488,10 @@ void greedy_search_quantized(const SearchIndex& ix, const float* Q, const int8_t
   if (k_out > width || rerank > width) throw std::invalid_argument("invalid quantized widths");
   const WarpLayout L = layout_for(ix, width);
   int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
+  GlobalVisited gv(L, blocks, st);
   k_search<true><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, width, k_out, rerank, eps, 0,
-                                                            QueryMeta{}, L, out_idx, out_dist, dstats);
+                                                            QueryMeta{}, L, gv.p(), gv.cap, out_idx, out_dist,
+                                                            dstats);
   RINND_LAUNCH_CHECK();
 }
 
