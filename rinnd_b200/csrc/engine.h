@@ -33,7 +33,8 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
                   int max_depth, uint64_t seed, cudaStream_t st, TempStorage& tmp, Forest& out);
 
 // Raises `kernel`'s dynamic shared-memory limit to `bytes` once per (kernel,
-// current device); safe to call from concurrent host threads (api.cu).
+// current device); safe to call from concurrent host threads (api.cu).  Later
+// calls for the same kernel are ignored, so pass the largest size any launch uses.
 void set_smem_limit_once(const void* kernel, int bytes);
 
 // ---- NN-Descent (nndescent.cu) ---------------------------------------------

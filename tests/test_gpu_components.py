@@ -95,13 +95,16 @@ def gpu_search_graph(knn_idx, knn_dist, data, kind, mult=1.5):
     return indptr, indices[: nnz.value], md.value
 
 
-@pytest.mark.parametrize("kind,gen", [(0, "gmm"), (0, "uniform"), (3, "gmm"), (7, "uniform"), (1, "gmm")])
-def test_search_graph_identical_on_shared_input(rb, orc, kind, gen):
-    """from_dense_diversified on the same sorted kNN graph gives the same CSR."""
-    data = gmm(3000, 24, 30, seed=5) if gen == "gmm" else uniform(3000, 24, seed=5)
+@pytest.mark.parametrize("kind,gen,k,d", [(0, "gmm", 15, 24), (0, "uniform", 15, 24), (3, "gmm", 15, 24),
+                                         (7, "uniform", 15, 24), (1, "gmm", 15, 24), (0, "gmm", 30, 128),
+                                         (3, "gmm", 30, 300), (0, "gmm", 40, 64)])
+def test_search_graph_identical_on_shared_input(rb, orc, kind, gen, k, d):
+    """from_dense_diversified on the same sorted kNN graph gives the same CSR
+    (the staged and the sequential forward-diversify kernels both covered)."""
+    data = gmm(3000, d, 30, seed=5) if gen == "gmm" else uniform(3000, d, seed=5)
     if kind == 7:
         data = np.abs(data) + np.float32(0.01)
-    ix = orc.OracleIndex(data, n_neighbors=15, n_trees=4, distance_kind=kind, correction=0,
+    ix = orc.OracleIndex(data, n_neighbors=k, n_trees=4, distance_kind=kind, correction=0,
                          angular=kind in (3, 7))
     ki, kd = ix.neighbor_graph
     op, oi, omd = orc.search_graph_from_knn(ki, kd, data, kind)
