@@ -84,20 +84,77 @@ __global__ void k_diversify_fwd(const int32_t* knn_idx, const float* knn_dist, i
   }
 }
 
-// Forward diversify with the row's candidates staged in shared memory (k <= 32,
-// Dp <= 256): the warp first evaluates d(a, b) for every candidate pair a < b
+// Forward diversify with a row's candidates staged in shared memory (<= 32
+// candidates, Dp <= 256): the warp first evaluates d(a, b) for every candidate pair a < b
 // from shared memory, in parallel and in the reference's exact order (the same
 // exact_distance call as the sequential form, argument order (earlier, later)),
-// then runs diversify_row's sequential keep/prune pass on that table.  Same
-// output as k_diversify_fwd; the pairs of pruned candidates are evaluated too,
-// trading a little arithmetic for all the latency of the sequential form.
+// then runs the sequential keep/prune pass (diversify_row / diversify_sorted_csr)
+// on that table.  Same output as the sequential kernels; the pairs of pruned
+// candidates are evaluated too, trading a little arithmetic for the latency of
+// evaluating one candidate at a time against rows in global memory.
 constexpr int SK = 32;
-struct FwdSmem {
+struct StagedSmem {
   // rows padded to Dp + 4 floats: lanes reading the same offset of different rows hit different banks
   __host__ __device__ static size_t per_warp(int Dp) {
     return (size_t)SK * (Dp + 4) * 4 + (size_t)SK * SK * 4 + SK * 12;
   }
 };
+
+struct StagedWarp {
+  float* rows;   // SK x (Dp + 4)
+  float* M;      // SK x SK, M[a * SK + b] = d(a, b), a < b
+  int32_t* ret;  // retained candidate positions
+  float* dpos;   // d(row, candidate)
+  int32_t* cid;  // candidate ids
+};
+
+__device__ __forceinline__ StagedWarp staged_warp(unsigned char* smem, int w, int Dp) {
+  unsigned char* base = smem + (size_t)w * StagedSmem::per_warp(Dp);
+  StagedWarp sw;
+  sw.rows = reinterpret_cast<float*>(base);
+  sw.M = sw.rows + (size_t)SK * (Dp + 4);
+  sw.ret = reinterpret_cast<int32_t*>(sw.M + SK * SK);
+  sw.dpos = reinterpret_cast<float*>(sw.ret + SK);
+  sw.cid = reinterpret_cast<int32_t*>(sw.dpos + SK);
+  return sw;
+}
+
+// The n candidates (cid/dpos filled, synchronized) -> sw.ret[0, nret); returns nret.
+__device__ __forceinline__ int staged_prune(const StagedWarp& sw, int n, const float* X, int D, int Dp, int kind,
+                                            int max_degree) {
+  const int lane = threadIdx.x & 31, rs = Dp + 4, q4 = Dp / 4;
+  // every 16-byte piece of every candidate row in flight at once (cp.async, L2 only)
+  for (int e = lane; e < n * q4; e += 32) {
+    const int r = e / q4, t = e - r * q4;
+    const float* src = X + (size_t)sw.cid[r] * Dp + 4 * t;
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(sw.rows + (size_t)r * rs + 4 * t);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncwarp();
+  for (int e = lane; e < n * n; e += 32) {
+    const int a = e / n, b = e % n;
+    if (a < b) sw.M[a * SK + b] = exact_distance(kind, sw.rows + (size_t)a * rs, sw.rows + (size_t)b * rs, D);
+  }
+  __syncwarp();
+  int nret = 0;
+  for (int pos = 0; pos < n; ++pos) {
+    const float dij = sw.dpos[pos];
+    bool pr = false;
+    if (lane < nret) {
+      const int c = sw.ret[lane];
+      pr = sw.dpos[c] > FLT_MIN && sw.M[c * SK + pos] < dij;
+    }
+    if (!__any_sync(0xffffffffu, pr)) {
+      if (lane == 0) sw.ret[nret] = pos;
+      __syncwarp();
+      ++nret;
+      if (nret >= max_degree) break;
+    }
+  }
+  __syncwarp();
+  return nret;
+}
 
 __global__ void __launch_bounds__(32 * WARPS)
     k_diversify_fwd_staged(const int32_t* knn_idx, const float* knn_dist, int N, int k, const float* X, int D,
@@ -107,13 +164,7 @@ __global__ void __launch_bounds__(32 * WARPS)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * WARPS + w;
   if (row >= N) return;
-  unsigned char* base = smem + (size_t)w * FwdSmem::per_warp(Dp);
-  const int rs = Dp + 4;
-  float* rows = reinterpret_cast<float*>(base);                 // SK x rs
-  float* M = rows + (size_t)SK * rs;                             // SK x SK, M[a * SK + b] = d(a, b), a < b
-  int32_t* ret = reinterpret_cast<int32_t*>(M + SK * SK);        // retained candidate positions
-  float* dpos = reinterpret_cast<float*>(ret + SK);              // d(row, candidate)
-  int32_t* cid = reinterpret_cast<int32_t*>(dpos + SK);          // candidate ids
+  const StagedWarp sw = staged_warp(smem, w, Dp);
   int32_t my_id = -1;
   float my_d = 0.f;
   if (lane < k) {
@@ -123,48 +174,20 @@ __global__ void __launch_bounds__(32 * WARPS)
   // candidates end at the first -1
   const unsigned valid = __ballot_sync(0xffffffffu, lane < k && my_id >= 0);
   const int n = (~valid) ? __ffs(~valid) - 1 : 32;
-  dpos[lane] = my_d;
-  cid[lane] = my_id;
+  sw.dpos[lane] = my_d;
+  sw.cid[lane] = my_id;
   __syncwarp();
-  // every 16-byte piece of every candidate row in flight at once (cp.async, L2 only)
-  const int q4 = Dp / 4;
-  for (int e = lane; e < n * q4; e += 32) {
-    const int r = e / q4, t = e - r * q4;
-    const float* src = X + (size_t)cid[r] * Dp + 4 * t;
-    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(rows + (size_t)r * rs + 4 * t);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-  }
-  asm volatile("cp.async.wait_all;" ::: "memory");
-  __syncwarp();
-  for (int e = lane; e < n * n; e += 32) {
-    const int a = e / n, b = e % n;
-    if (a < b) M[a * SK + b] = exact_distance(kind, rows + (size_t)a * rs, rows + (size_t)b * rs, D);
-  }
-  __syncwarp();
-  int nret = 0;
+  const int nret = staged_prune(sw, n, X, D, Dp, kind, max_degree);
   uint32_t local_min = KEY_INF;
-  for (int pos = 0; pos < n; ++pos) {
-    const float dij = dpos[pos];
-    bool pr = false;
-    if (lane < nret) {
-      const int c = ret[lane];
-      pr = dpos[c] > FLT_MIN && M[c * SK + pos] < dij;
-    }
-    if (!__any_sync(0xffffffffu, pr)) {
-      if (lane == 0) ret[nret] = pos;
-      __syncwarp();
-      ++nret;
-      const float v = dij == 0.f ? FLT_EPSILON : dij;
-      if (isfinite(v)) local_min = min(local_min, fkey(v));
-      if (nret >= max_degree) break;
-    }
-  }
-  __syncwarp();
   for (int r = lane; r < nret; r += 32) {
-    const int pos = ret[r];
-    fwd_idx[(size_t)row * k + r] = cid[pos];
-    fwd_dist[(size_t)row * k + r] = dpos[pos];
+    const int pos = sw.ret[r];
+    const float dij = sw.dpos[pos];
+    fwd_idx[(size_t)row * k + r] = sw.cid[pos];
+    fwd_dist[(size_t)row * k + r] = dij;
+    const float v = dij == 0.f ? FLT_EPSILON : dij;
+    if (isfinite(v)) local_min = min(local_min, fkey(v));
   }
+  for (int o = 16; o; o >>= 1) local_min = min(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
   if (lane == 0) {
     fwd_cnt[row] = nret;
     if (local_min != KEY_INF) atomicMin(min_key, local_min);
@@ -362,7 +385,7 @@ void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const flo
   DVec<float> fwd_dist((size_t)N * k, st);
   DVec<uint32_t> min_key(1, st);
   RINND_CUDA(cudaMemcpyAsync(min_key.p, &KEY_INF, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-  const size_t staged_bytes = FwdSmem::per_warp(Dp) * WARPS;
+  const size_t staged_bytes = StagedSmem::per_warp(Dp) * WARPS;
   if (k <= SK && Dp <= 256) {
     set_smem_limit_once(reinterpret_cast<const void*>(k_diversify_fwd_staged), 227 * 1024);
     k_diversify_fwd_staged<<<blocks, 32 * WARPS, staged_bytes, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind,
@@ -402,6 +425,8 @@ void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const flo
   }
   DVec<int32_t> rret_idx((size_t)N * max_degree, st), rret_cnt((size_t)N, st);
   DVec<float> rret_dist((size_t)N * max_degree, st);
+  // (reverse rows stay sequential: they are short, and the early exits of the
+  // sequential form beat the staged pair table there)
   if (max_degree <= 32)
     k_diversify_rev<32><<<blocks, 32 * WARPS, 0, st>>>(rev_ptr.p, rev_sorted.p, N, X, D, Dp, kind,
                                                       max_degree, rret_idx.p, rret_dist.p, rret_cnt.p);
