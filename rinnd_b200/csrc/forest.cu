@@ -98,33 +98,61 @@ __global__ void k_fill_segmap(const long long* seg_gstart, const long long* seg_
       seg_of[g] = s;
 }
 
-// builder.rs:312-348 partition_inplace side decision, one thread per position:
-// margin = dot(point, hyperplane) + offset in the reference's dot order
-// (builder.rs:11-60); |margin| < 1e-8 -> random side; else margin < 0 -> left.
-__global__ void k_margins(const int32_t* seg_of, const int32_t* perm, int N, const float* X, int D,
-                          int Dp, const float* hp, const float* off, uint64_t seed, int depth,
-                          long long total, int32_t* is_left) {
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
-       g += (long long)gridDim.x * blockDim.x) {
-    int s = seg_of[g];
-    int left = 0;
-    if (s >= 0) {
-      int32_t pid = perm[g];
-      float margin = __fadd_rn(exact_dot_a(X + (size_t)pid * Dp, hp + (size_t)s * Dp, D), off[s]);
-      if (fabsf(margin) < 1e-8f) {
-        uint64_t tree = (uint64_t)(g / N);
-        left = (int)(hash3(seed ^ 0x7a11u, (tree << 32) | (uint32_t)depth, (uint64_t)pid) >> 63);
-      } else {
-        left = margin < 0.f;
+// builder.rs:312-348 partition_inplace side decision for every tree's position
+// of a point: margin = dot(point, hyperplane) + offset in the reference's dot
+// order (builder.rs:11-60, exact_dot_a); |margin| < 1e-8 -> random side; else
+// margin < 0 -> left.  One warp per point reads the point's row once per level
+// for all trees: 4 trees at a time, 8 lanes per dot, lane t carrying the
+// reference's accumulator chain t (elements 8c + t, c in order), the same
+// horizontal-sum tree over shuffles and the remainder added by lane 0 -- the
+// margins are bit-identical to exact_dot_a's.  inv[t N + p] is point p's
+// position in tree t; positions of finished leaves (segment -1) get side 0.
+__global__ void k_margins(const int32_t* seg_of, const int32_t* inv, int N, int T, const float* X, int D, int Dp,
+                          const float* hp, const float* off, uint64_t seed, int depth, int32_t* is_left) {
+  const int lane = threadIdx.x & 31, grp = lane >> 3, t8 = lane & 7;
+  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int chunks = D >> 3;
+  for (long long pid = warp; pid < N; pid += nwarps) {
+    const float* x = X + (size_t)pid * Dp;
+    for (int t0 = 0; t0 < T; t0 += 4) {
+      const int t = t0 + grp;
+      long long g = -1;
+      int sg = -1;
+      if (t < T) {
+        g = (long long)t * N + inv[(size_t)t * N + pid];
+        sg = seg_of[g];
+      }
+      const float* h = hp + (size_t)(sg >= 0 ? sg : 0) * Dp;
+      float acc = 0.f;
+      if (sg >= 0)
+        for (int c = 0; c < chunks; ++c) acc = __fmaf_rn(x[8 * c + t8], h[8 * c + t8], acc);
+      // hsum_a: ((s4 + s0) + (s5 + s1)) + ((s6 + s2) + (s7 + s3))
+      const float up4 = __shfl_down_sync(0xffffffffu, acc, 4, 8);
+      const float a = __fadd_rn(up4, acc);
+      const float up1 = __shfl_down_sync(0xffffffffu, a, 1, 8);
+      const float b = __fadd_rn(a, up1);
+      const float up2 = __shfl_down_sync(0xffffffffu, b, 2, 8);
+      if (t8 == 0 && g >= 0) {
+        int left = 0;
+        if (sg >= 0) {
+          float r = __fadd_rn(b, up2);
+          for (int i = chunks * 8; i < D; ++i) r = __fadd_rn(r, __fmul_rn(x[i], h[i]));
+          const float margin = __fadd_rn(r, off[sg]);
+          if (fabsf(margin) < 1e-8f)
+            left = (int)(hash3(seed ^ 0x7a11u, ((uint64_t)t << 32) | (uint32_t)depth, (uint64_t)pid) >> 63);
+          else
+            left = margin < 0.f;
+        }
+        is_left[g] = left;
       }
     }
-    is_left[g] = left;
   }
 }
 
 __global__ void k_scatter(const int32_t* seg_of, const long long* seg_gstart,
                           const long long* seg_gend, const int32_t* scan, const int32_t* is_left,
-                          const int32_t* perm, int32_t* perm_next, long long total) {
+                          const int32_t* perm, int32_t* perm_next, int32_t* inv, int N, long long total) {
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
        g += (long long)gridDim.x * blockDim.x) {
     int s = seg_of[g];
@@ -133,7 +161,10 @@ __global__ void k_scatter(const int32_t* seg_of, const long long* seg_gstart,
     int lrank = scan[g] - scan[gs];
     int nl = scan[ge] - scan[gs];
     long long dst = is_left[g] ? gs + lrank : gs + nl + ((g - gs) - lrank);
-    perm_next[dst] = perm[g];
+    const int32_t pid = perm[g];
+    perm_next[dst] = pid;
+    const long long base = (g / N) * N;  // the tree's first position
+    inv[base + pid] = (int32_t)(dst - base);
   }
 }
 
@@ -231,7 +262,10 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
   long long total = (long long)N * T;
   f.perm.alloc((size_t)total, st);
   DVec<int32_t> perm_next((size_t)total, st);
+  DVec<int32_t> inv((size_t)total, st);  // inv[t N + p]: position of point p in tree t
   k_init_perm<<<grid_for(total, 256, 148 * 64), 256, 0, st>>>(f.perm.p, N, T);
+  RINND_LAUNCH_CHECK();
+  k_init_perm<<<grid_for(total, 256, 148 * 64), 256, 0, st>>>(inv.p, N, T);  // identity is its own inverse
   RINND_LAUNCH_CHECK();
 
   size_t node_cap = (size_t)T * 64;
@@ -270,15 +304,14 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
     RINND_CUDA(cudaMemsetAsync(seg_of.p, 0xFF, sizeof(int32_t) * (size_t)total, st));
     k_fill_segmap<<<std::min(S, 148 * 16), 256, 0, st>>>(gs.p, ge.p, S, seg_of.p);
     RINND_LAUNCH_CHECK();
-    k_margins<<<grid_for(total, 256, 148 * 32), 256, 0, st>>>(seg_of.p, f.perm.p, N, X, D, Dp,
-                                                             hp.p, off.p, seed, depth, total,
-                                                             is_left.p);
+    k_margins<<<grid_for((long long)N * 32, 256, 148 * 32), 256, 0, st>>>(seg_of.p, inv.p, N, T, X, D, Dp, hp.p,
+                                                                         off.p, seed, depth, is_left.p);
     RINND_LAUNCH_CHECK();
     exclusive_scan(is_left.p, scan.p, total + 1, tmp, st);
     RINND_CUDA(cudaMemcpyAsync(perm_next.p, f.perm.p, sizeof(int32_t) * (size_t)total,
                                cudaMemcpyDeviceToDevice, st));
     k_scatter<<<grid_for(total, 256, 148 * 32), 256, 0, st>>>(seg_of.p, gs.p, ge.p, scan.p,
-                                                             is_left.p, f.perm.p, perm_next.p,
+                                                             is_left.p, f.perm.p, perm_next.p, inv.p, N,
                                                              total);
     RINND_LAUNCH_CHECK();
     std::swap(f.perm.p, perm_next.p);
