@@ -66,8 +66,64 @@ __device__ __forceinline__ RowScan scan_row(const uint64_t* row, int k, uint32_t
   return r;
 }
 
+// row_push for rows of at most KP (16 or 32) slots: the whole snapshot is held
+// in registers, the scan tracks only the duplicate flag and the max slot, and
+// the runner-up (for the bound update) is computed only after a successful CAS.
+// Same decisions as the general form below.
+template <int KP>
+__device__ __forceinline__ int row_push_small(uint64_t* row, int k, uint32_t* thr, uint64_t key,
+                                              unsigned long long* contention) {
+  const uint32_t vk = (uint32_t)(key >> 32);
+  const uint32_t id = ((uint32_t)key) & 0x7FFFFFFFu;
+  const ulonglong2* r2 = reinterpret_cast<const ulonglong2*>(row);
+  for (int attempt = 0; attempt < PUSH_MAX_RETRY; ++attempt) {
+    uint64_t v[KP];
+#pragma unroll
+    for (int t = 0; t < KP / 2; ++t) {
+      const ulonglong2 q = __ldcg(r2 + t);
+      v[2 * t] = q.x;
+      v[2 * t + 1] = q.y;
+    }
+    bool dup = false;
+    uint64_t vmax = v[0];
+    int m = 0;
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+      if (j < k) {
+        dup |= (((uint32_t)v[j]) & 0x7FFFFFFFu) == id;
+        if (j > 0 && v[j] > vmax) {
+          vmax = v[j];
+          m = j;
+        }
+      }
+    }
+    if (dup) return 0;
+    if (vk >= (uint32_t)(vmax >> 32)) {
+      if (thr != nullptr) atomicMin(thr, (uint32_t)(vmax >> 32));
+      return 0;
+    }
+    unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long*>(row + m), (unsigned long long)vmax,
+                                       (unsigned long long)key);
+    if (old == vmax) {
+      if (thr != nullptr) {
+        uint64_t v2 = 0;
+#pragma unroll
+        for (int j = 0; j < KP; ++j)
+          if (j < k && j != m && v[j] > v2) v2 = v[j];
+        const uint64_t nm = v2 > key ? v2 : key;
+        atomicMin(thr, (uint32_t)(nm >> 32));
+      }
+      return 1;
+    }
+  }
+  if (contention) atomicAdd(contention, 1ull);
+  return 0;
+}
+
 // Returns 1 if inserted.  `key` = (fkey(v) << 32) | lo, lo's low 31 bits = id.
-// `thr` (may be null) holds an upper bound of fkey(row max value).
+// `thr` (may be null) holds an upper bound of fkey(row max value).  This form
+// scans the row in 16-slot chunks and keeps few registers: kernels whose push
+// is a rare fallback (the join kernels' update-buffer overflow) use it.
 __device__ __forceinline__ int row_push(uint64_t* row, int k, uint32_t* thr, uint64_t key,
                                         unsigned long long* contention) {
   const uint32_t vk = (uint32_t)(key >> 32);
@@ -94,6 +150,17 @@ __device__ __forceinline__ int row_push(uint64_t* row, int k, uint32_t* thr, uin
   }
   if (contention) atomicAdd(contention, 1ull);
   return 0;
+}
+
+// The push of the reverse candidate offers: rows of up to 32 slots take the
+// register-snapshot form (faster there; in the update-application kernel its
+// registers cost more occupancy than the shorter scan saves).
+__device__ __forceinline__ int row_push_fast(uint64_t* row, int k, uint32_t* thr, uint64_t key,
+                                             unsigned long long* contention) {
+  if (thr != nullptr && (uint32_t)(key >> 32) >= __ldcg(thr)) return 0;
+  if (k <= 16) return row_push_small<16>(row, k, thr, key, contention);
+  if (k <= 32) return row_push_small<32>(row, k, thr, key, contention);
+  return row_push(row, k, thr, key, contention);
 }
 
 }  // namespace rinnd

@@ -445,7 +445,7 @@ __global__ void k_cand_reverse(const uint64_t* slots, int N, int k, int kp, int 
     if (id < 0) continue;
     const bool nw = slot_new(sl);
     uint64_t key = ((uint64_t)cand_priority(seed, iter, i, id) << 32) | (uint32_t)i;
-    row_push((nw ? cnew : cold) + (size_t)id * cp, c, (nw ? thr_new : thr_old) + id, key, contention);
+    row_push_fast((nw ? cnew : cold) + (size_t)id * cp, c, (nw ? thr_new : thr_old) + id, key, contention);
   }
 }
 
