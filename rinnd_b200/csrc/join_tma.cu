@@ -32,7 +32,7 @@ namespace {
 
 using namespace joinc;
 
-constexpr int NSTAGE = 2;   // row stages
+constexpr int NSTAGE = 2;   // row stages (72 KB: three CTAs per SM beat a deeper prefetch)
 constexpr int NCONS = 8;    // consumer warps
 constexpr int NT = 32 * (1 + NCONS);
 
