@@ -142,34 +142,72 @@ __global__ void __launch_bounds__(NT)
         mbar_arrive_expect_tx(&B.desc[i], dbytes);
         bulk_g2s(dring + (size_t)i * dstride, desc + (size_t)(first + i * stride) * dstride, dbytes, &B.desc[i]);
       }
+    constexpr int TPL = (2 * MAXC + 31) / 32;  // candidate rows per lane
     bool ok = true;
-    int i = 0;
+    int i = 0, jobs = 0;                        // vertices walked, stages filled
     int desc_issued = nv < NDESC ? nv : NDESC;  // descriptors issued for vertices [0, desc_issued)
-    for (; i < nv; ++i) {
-      const int ds = i % NDESC, s = i % NSTAGE;
-      ok = wait_or_abort(&B.desc[ds], (uint32_t)(i / NDESC) & 1u, abort_flag);
-      if (!ok) break;
-      if (i >= NSTAGE) {
-        ok = wait_or_abort(&B.empty[s], (uint32_t)((i / NSTAGE) - 1) & 1u, abort_flag);
+    // Candidate ids and current row thresholds of the next vertex, loaded one
+    // vertex ahead so the threshold loads overlap the previous vertex's copies.
+    int32_t nx_ids[TPL];
+    uint32_t nx_thr[TPL];
+    auto prefetch = [&](int v) {
+      const bool got = wait_or_abort(&B.desc[v % NDESC], (uint32_t)(v / NDESC) & 1u, abort_flag);
+      const int32_t* dn = dring + (size_t)(v % NDESC) * dstride;
+      const int nbn = got ? dn[1] : 0;
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        const int r = lane + 32 * t;
+        nx_ids[t] = r < nbn ? dn[Desc::ids(MAXC) + r] : 0;
+        nx_thr[t] = r < nbn ? __ldcg(thr + nx_ids[t]) : 0u;
+      }
+      return got;
+    };
+    if (nv > 0) ok = prefetch(0);
+    for (; ok && i < nv; ++i) {
+      const int ds = i % NDESC;
+      int32_t my_ids[TPL];
+      uint32_t my_thr[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        my_ids[t] = nx_ids[t];
+        my_thr[t] = nx_thr[t];
+      }
+      if (i + 1 < nv) {
+        ok = prefetch(i + 1);
         if (!ok) break;
       }
       const int32_t* dsc = dring + (size_t)ds * dstride;
-      unsigned char* st = stage0 + (size_t)s * sbytes;
-      int32_t* sd = reinterpret_cast<int32_t*>(st);
-      const int nb = dsc[1];
-      for (int t = lane; t < dstride; t += 32) sd[t] = dsc[t];  // descriptor -> stage header
-      // row thresholds as of now (pushes applied by earlier batches tighten them)
-      int32_t my_ids[(2 * MAXC + 31) / 32];
-      uint32_t* sthr = reinterpret_cast<uint32_t*>(sd + Desc::thr(MAXC));
+      const int nb = dsc[1], items = dsc[3];
+      if (items > 0) {  // vertices without pairs take no stage
+        const int s = jobs % NSTAGE;
+        if (jobs >= NSTAGE) {
+          ok = wait_or_abort(&B.empty[s], (uint32_t)((jobs / NSTAGE) - 1) & 1u, abort_flag);
+          if (!ok) break;
+        }
+        unsigned char* st = stage0 + (size_t)s * sbytes;
+        int32_t* sd = reinterpret_cast<int32_t*>(st);
+        for (int t = lane; t < dstride; t += 32)  // descriptor -> stage header (thresholds below)
+          if (t < Desc::thr(MAXC) || t >= Desc::nrm(MAXC)) sd[t] = dsc[t];
+        uint32_t* sthr = reinterpret_cast<uint32_t*>(sd + Desc::thr(MAXC));
 #pragma unroll
-      for (int t = 0; t < (2 * MAXC + 31) / 32; ++t) {
-        const int r = lane + 32 * t;
-        my_ids[t] = r < nb ? dsc[Desc::ids(MAXC) + r] : 0;
-        if (r < nb) sthr[r] = __ldcg(thr + my_ids[t]);
+        for (int t = 0; t < TPL; ++t) {
+          const int r = lane + 32 * t;
+          if (r < nb) sthr[r] = my_thr[t];
+        }
+        float* rows = reinterpret_cast<float*>(st + L.rows_off());
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect_tx(&B.full[s], (uint32_t)nb * (uint32_t)Dp * 4u);
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < TPL; ++t) {
+          const int r = lane + 32 * t;
+          if (r < nb) bulk_g2s(rows + (size_t)r * L.rs, X + (size_t)my_ids[t] * Dp, (uint32_t)Dp * 4u, &B.full[s]);
+        }
+        ++jobs;
       }
+      // descriptor slot consumed: refill it NDESC vertices ahead
       fence_proxy_async_smem();
       __syncwarp();
-      // descriptor slot consumed: refill it NDESC vertices ahead
       if (i + NDESC < nv) {
         desc_issued = i + NDESC + 1;
         if (lane == 0) {
@@ -178,13 +216,13 @@ __global__ void __launch_bounds__(NT)
                    &B.desc[ds]);
         }
       }
-      float* rows = reinterpret_cast<float*>(st + L.rows_off());
-      if (lane == 0) mbar_arrive_expect_tx(&B.full[s], (uint32_t)nb * (uint32_t)Dp * 4u);
-      __syncwarp();
-#pragma unroll
-      for (int t = 0; t < (2 * MAXC + 31) / 32; ++t) {
-        const int r = lane + 32 * t;
-        if (r < nb) bulk_g2s(rows + (size_t)r * L.rs, X + (size_t)my_ids[t] * Dp, (uint32_t)Dp * 4u, &B.full[s]);
+    }
+    if (ok) {  // end-of-work stage (nb = -1)
+      const int s = jobs % NSTAGE;
+      if (jobs >= NSTAGE) ok = wait_or_abort(&B.empty[s], (uint32_t)((jobs / NSTAGE) - 1) & 1u, abort_flag);
+      if (ok && lane == 0) {
+        reinterpret_cast<int32_t*>(stage0 + (size_t)s * sbytes)[1] = -1;
+        mbar_arrive(&B.full[s]);
       }
     }
     if (!ok && lane == 0) {
@@ -193,7 +231,7 @@ __global__ void __launch_bounds__(NT)
       // drain: wait (bounded) for every descriptor and row copy this warp issued
       for (int j = i; j < desc_issued; ++j)
         mbar_wait_bounded(&B.desc[j % NDESC], (uint32_t)(j / NDESC) & 1u, WAIT_POLLS);
-      for (int j = (i > NSTAGE ? i - NSTAGE : 0); j < i; ++j)
+      for (int j = (jobs > NSTAGE ? jobs - NSTAGE : 0); j < jobs; ++j)
         mbar_wait_bounded(&B.full[j % NSTAGE], (uint32_t)(j / NSTAGE) & 1u, WAIT_POLLS);
     }
     return;
@@ -204,9 +242,9 @@ __global__ void __launch_bounds__(NT)
   const bool is_dot = kind_is_dot(kind);
   unsigned int pairs_total = 0;
   unsigned long long rows_total = 0;
-  for (int i = 0; i < nv; ++i) {
+  for (int i = 0;; ++i) {  // stages in fill order, up to the end-of-work stage
     const int s = i % NSTAGE;
-    if (!wait_or_abort(&B.full[s], (uint32_t)(i / NSTAGE) & 1u, abort_flag)) {
+    if (!__all_sync(0xffffffffu, wait_or_abort(&B.full[s], (uint32_t)(i / NSTAGE) & 1u, abort_flag))) {
       if (lane == 0) {
         *abort_flag = 1;
         atomicExch(err, 1);
@@ -216,6 +254,7 @@ __global__ void __launch_bounds__(NT)
     const unsigned char* st = stage0 + (size_t)s * sbytes;
     const int32_t* sd = reinterpret_cast<const int32_t*>(st);
     const int na = sd[0], nb = sd[1], nq = sd[2], items = sd[3];
+    if (nb < 0) break;
     const int32_t* ids = sd + Desc::ids(MAXC);
     const uint32_t* sthr = reinterpret_cast<const uint32_t*>(sd + Desc::thr(MAXC));
     const float* snrm = reinterpret_cast<const float*>(sd + Desc::nrm(MAXC));
