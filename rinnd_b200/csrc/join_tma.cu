@@ -12,11 +12,13 @@
 // diagonal are never generated.  Persistent CTAs of 1 producer warp + 8
 // consumer warps walk a strided vertex sequence:
 //   producer: keeps NDESC descriptors in flight (one cp.async.bulk each into a
-//     ring, completing on per-slot mbarriers); per vertex it waits for a free
-//     row stage (empty mbarrier, armed by the consumer warps), copies the
-//     descriptor and the candidates' current row thresholds into the stage and
-//     issues one cp.async.bulk per candidate row
-//     (Dp floats) into a padded slot, completing on the stage's full mbarrier;
+//     ring, completing on per-slot mbarriers) and loads the next vertex's
+//     candidate ids and current row thresholds one vertex ahead; a vertex with
+//     pairs takes the next free row stage (empty mbarrier, armed by the
+//     consumer warps): the producer copies the descriptor and the thresholds
+//     into the stage and issues one cp.async.bulk per candidate row (Dp floats)
+//     into a padded slot, completing on the stage's full mbarrier.  Vertices
+//     without pairs take no stage; a stage with nb = -1 ends the work;
 //   consumers: wait for the stage; each thread computes one item per round --
 //     4 distances with packed FP32x2 arithmetic from 5 conflict-free 16-byte
 //     shared loads per 4 dimensions -- and appends threshold-passing updates to
