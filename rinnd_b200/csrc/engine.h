@@ -66,6 +66,11 @@ struct KnnState {
   DVec<uint32_t> urow;       // update buffer: destination rows
   DVec<uint64_t> ukey;       // update buffer: slot keys
   unsigned long long ucap = 0;
+  // Region form of the update buffer (FP32 pipelined join): nreg regions of
+  // rsize entries, region r holding rcnt[r] updates; nreg = 0 after they are applied.
+  DVec<uint32_t> rcnt;
+  int nreg = 0;
+  unsigned int rsize = 0;
   double upv_prev = -1.0;    // updates appended per vertex by the previous join (-1: none yet)
 };
 

@@ -22,7 +22,9 @@
 //   consumers: wait for the stage; each thread computes one item per round --
 //     4 distances with packed FP32x2 arithmetic from 5 conflict-free 16-byte
 //     shared loads per 4 dimensions -- and appends threshold-passing updates to
-//     the device update buffer (one atomic per warp) for k_apply_updates.
+//     its CTA's region of the device update buffer (one shared-memory atomic
+//     per warp and round; an update beyond the region is pushed directly) for
+//     k_apply_regions.
 // Every wait is bounded.  A wait that runs out sets the device error flag and a
 // shared abort flag; all warps leave, the producer first waiting (bounded) for
 // every copy it issued.  The host turns the flag into an error.
@@ -110,11 +112,17 @@ template <int MAXC>
 __global__ void __launch_bounds__(NT)
     k_join_ws(const int32_t* __restrict__ desc, int v0, int v1, const float* __restrict__ X, int Dp, int kind,
               uint64_t* slots, uint32_t* thr, int k, int kp, Layout L, uint32_t* urow_buf, uint64_t* ukey_buf,
-              unsigned long long* ucount, unsigned long long ucap, unsigned long long* counters, int* err) {
+              unsigned long long* ucount, uint32_t* rcnt, unsigned int rsize, unsigned long long* counters,
+              int* err) {
   extern __shared__ __align__(16) unsigned char smem[];
   Bars B{reinterpret_cast<uint64_t*>(smem), reinterpret_cast<uint64_t*>(smem) + NSTAGE,
          reinterpret_cast<uint64_t*>(smem) + 2 * NSTAGE,
          reinterpret_cast<int*>(smem + 8 * (2 * NSTAGE + NDESC))};
+  // this CTA's region of the update buffer and its fill count (shared memory)
+  unsigned int* s_ucnt = reinterpret_cast<unsigned int*>(B.abort_flag + 1);
+  unsigned int* s_done = s_ucnt + 1;  // consumer warps finished
+  uint32_t* urow_reg = urow_buf + (size_t)blockIdx.x * rsize;
+  uint64_t* ukey_reg = ukey_buf + (size_t)blockIdx.x * rsize;
   int32_t* dring = reinterpret_cast<int32_t*>(smem + L.desc_off());
   unsigned char* stage0 = smem + L.stage_off();
   const size_t sbytes = L.stage_bytes();
@@ -126,6 +134,8 @@ __global__ void __launch_bounds__(NT)
     }
     for (int s = 0; s < NDESC; ++s) mbar_init(&B.desc[s], 1);
     *B.abort_flag = 0;
+    *s_ucnt = 0;
+    *s_done = 0;
     fence_mbar_init();
   }
   __syncthreads();
@@ -339,9 +349,9 @@ __global__ void __launch_bounds__(NT)
         if (lane >= o) incl += y;
       }
       const int warp_total = __shfl_sync(0xffffffffu, incl, 31);
-      unsigned long long base = 0;
-      if (lane == 0 && warp_total) base = atomicAdd(ucount, (unsigned long long)warp_total);
-      base = __shfl_sync(0xffffffffu, base, 0) + (unsigned long long)(incl - n_emit);
+      unsigned int base = 0;
+      if (lane == 0 && warp_total) base = atomicAdd(s_ucnt, (unsigned int)warp_total);
+      base = __shfl_sync(0xffffffffu, base, 0) + (unsigned int)(incl - n_emit);
       if (emit) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -352,9 +362,9 @@ __global__ void __launch_bounds__(NT)
             const int32_t row = side ? bid : aid;
             const int32_t other = side ? aid : bid;
             const uint64_t key = ((uint64_t)kd[u] << 32) | (uint32_t)other | 0x80000000u;
-            if (base < ucap) {
-              urow_buf[base] = (uint32_t)row;
-              ukey_buf[base] = key;
+            if (base < rsize) {
+              urow_reg[base] = (uint32_t)row;
+              ukey_reg[base] = key;
             } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
               atomicAdd(&counters[0], 1ull);
             }
@@ -365,6 +375,19 @@ __global__ void __launch_bounds__(NT)
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&B.empty[s]);  // this warp is done with stage s
+  }
+  // The last consumer warp to finish publishes the region's fill count (capped
+  // at the region size; the rest were pushed directly) and adds the CTA's
+  // appended updates to the launch total.  An aborted CTA publishes nothing:
+  // its region count stays 0.
+  __syncwarp();
+  if (lane == 0) {
+    __threadfence_block();
+    if (atomicAdd(s_done, 1u) == NCONS - 1) {
+      const unsigned int total = atomicAdd(s_ucnt, 0u);
+      rcnt[blockIdx.x] = total < rsize ? total : rsize;
+      atomicAdd(ucount, (unsigned long long)total);
+    }
   }
   for (int o = 16; o; o >>= 1) pairs_total += __shfl_xor_sync(0xffffffffu, pairs_total, o);
   if (lane == 0 && pairs_total) atomicAdd(&counters[2], (unsigned long long)pairs_total);
@@ -379,8 +402,14 @@ void launch_join(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, 
   const int per_sm = std::max(1, (int)((227 * 1024) / (smem + 1024)));
   const int grid = std::min(v1 - v0, 148 * per_sm);
   if (grid <= 0) return;
+  // one region of the update buffer per CTA (k_apply_regions reads them back)
+  if (s.rcnt.n < (size_t)grid) s.rcnt.alloc((size_t)grid, st);
+  RINND_CUDA(cudaMemsetAsync(s.rcnt.p, 0, sizeof(uint32_t) * grid, st));
+  s.nreg = grid;
+  s.rsize = (unsigned int)std::min<unsigned long long>(s.ucap / (unsigned long long)grid, 0xFFFFFFFFull);
   k_join_ws<MAXC><<<grid, NT, smem, st>>>(s.desc.p, v0, v1, X, Dp, kind, s.slots.p, s.thr.p, s.k, s.kp, L,
-                                          s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap, s.counters.p, err);
+                                          s.urow.p, s.ukey.p, s.counters.p + 4, s.rcnt.p, s.rsize, s.counters.p,
+                                          err);
   RINND_LAUNCH_CHECK();
 }
 

@@ -299,6 +299,28 @@ __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, cons
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&counters[0], (unsigned long long)mine);
 }
 
+// k_apply_updates for the region form: region r of the buffer holds rcnt[r]
+// updates from entry r * rsize; `sub` blocks share a region.
+__global__ void k_apply_regions(const uint32_t* urow, const uint64_t* ukey, const uint32_t* rcnt, int nreg,
+                                unsigned int rsize, int sub, const unsigned long long* count, uint64_t* slots,
+                                uint32_t* thr, int k, int kp, unsigned long long* counters) {
+  const int r = blockIdx.x / sub, part = blockIdx.x - r * sub;
+  if (r >= nreg) return;
+  const unsigned int cnt = rcnt[r];
+  if (threadIdx.x == 0) {
+    if (part == 0) atomicAdd(&counters[5], (unsigned long long)cnt);
+    if (blockIdx.x == 0) atomicAdd(&counters[6], *count);  // appended, including overflow pushed directly
+  }
+  const size_t base = (size_t)r * rsize;
+  unsigned int mine = 0;
+  for (unsigned int e = part * blockDim.x + threadIdx.x; e < cnt; e += sub * blockDim.x) {
+    const uint32_t row = urow[base + e];
+    mine += row_push(slots + (size_t)row * kp, k, thr + row, ukey[base + e], &counters[1]);
+  }
+  for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&counters[0], (unsigned long long)mine);
+}
+
 // Leaf jobs: blocks of BS points of one leaf, (a, b) with a <= b.
 __global__ void k_leaf_job_count(const int4* leaves, long long nl, int BS, int32_t* cnt) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nl;
@@ -556,6 +578,14 @@ void ensure_update_buffer(KnnState& s, cudaStream_t st) {
 
 namespace {
 void apply_pending(KnnState& s, cudaStream_t st) {
+  if (s.nreg > 0) {
+    const int sub = std::max(1, (148 * 16) / s.nreg);
+    k_apply_regions<<<s.nreg * sub, 256, 0, st>>>(s.urow.p, s.ukey.p, s.rcnt.p, s.nreg, s.rsize, sub,
+                                                  s.counters.p + 4, s.slots.p, s.thr.p, s.k, s.kp, s.counters.p);
+    RINND_LAUNCH_CHECK();
+    s.nreg = 0;
+    return;
+  }
   k_apply_updates<<<148 * 16, 256, 0, st>>>(s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap, s.slots.p, s.thr.p,
                                             s.k, s.kp, s.counters.p);
   RINND_LAUNCH_CHECK();
