@@ -72,6 +72,7 @@ struct KnnState {
   int nreg = 0;
   unsigned int rsize = 0;
   double upv_prev = -1.0;    // updates appended per vertex by the previous join (-1: none yet)
+  bool seeded = false;       // rows initialized from tree leaves (their thresholds already filter)
 };
 
 void knn_init(KnnState& s, int N, int k, int c, cudaStream_t st);
