@@ -66,9 +66,10 @@ def parse_args():
     ap.add_argument("--verbose", action="store_true", help="per-iteration build statistics")
     ap.add_argument("--parity", action="store_true",
                     help="also build the oracle (CPU restatement) at the full size and report its recall")
-    ap.add_argument("--workload", default="build", choices=["build", "batched", "serving"],
+    ap.add_argument("--workload", default="build", choices=["build", "batched", "serving", "precision"],
                     help="build: the 1M-point build (default); batched: many independent indices in one call; "
-                         "serving: continuous-batching queries against a 10M x 96 index")
+                         "serving: continuous-batching queries against a 10M x 96 index; precision: FP32 and "
+                         "BF16 join forms at 1M x 960 cosine with distance error vs FP64")
     ap.add_argument("--serve-n", type=int, default=10_000_000, help="serving workload: index size")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="serving workload: seconds per offered load")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"],
@@ -365,6 +366,125 @@ def run_batched(args, world, rank, local_rank):
         dist.destroy_process_group()
 
 
+PREC_D, PREC_K, PREC_SAMPLE = 960, 15, 4000
+
+
+def run_precision(args, world, rank, local_rank):
+    """The precision workload: N x 960 rows with entries |N(0,1)|^1.5,
+    L2-normalised, cosine, k=15, built with FP32 join tiles and with the BF16
+    precision form (which falls back to FP32 tiles where its tensor-core join
+    does not apply; `join_form` says which kernel ran).  Reports each form's
+    build points/s, recall@15 against FP64 exact kNN on a seeded sample of rows,
+    and the error of the reported neighbor distances against the same pairs'
+    cosine distances recomputed in FP64.  Replicas on N > 1 ranks."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from rinnd_b200 import _lib as L
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    n = args.n
+    g = torch.Generator(device=dev).manual_seed(0)
+    X = torch.randn(n, PREC_D, generator=g, device=dev).abs_().pow_(1.5)
+    X /= X.norm(dim=1, keepdim=True)
+    X = X.contiguous()
+    forms_names = {L.JOIN_CHUNKED_FP32: "chunked FP32", L.JOIN_PIPELINED_FP32: "pipelined FP32",
+                   L.JOIN_TENSOR_BF16: "tensor-core BF16 filter + FP32 recheck"}
+
+    def build(prec):
+        p = L.BuildParams()
+        L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
+        p.n_neighbors, p.distance_kind, p.correction, p.angular = PREC_K, L.DIST_ALT_COSINE, L.CORR_ALT_COSINE, 1
+        p.n_trees = int(min(max(np.floor(2.0 * np.log10(n) + 0.5), 3), 12))  # lib.rs:1200-1204
+        p.random_seed, p.device, p.precision = 42, local_rank, prec
+        h = ctypes.c_void_p()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.check(L.lib.rinnd_build_device(ctypes.c_void_p(X.data_ptr()), n, PREC_D, PREC_D, ctypes.byref(p),
+                                         ctypes.byref(h)))
+        torch.cuda.synchronize()
+        return h, time.perf_counter() - t0
+
+    rows = np.sort(np.random.default_rng(7).choice(n, min(PREC_SAMPLE, n), replace=False))
+    truth = None
+    if rank == 0 and not args.no_recall:
+        Xd = X.double()
+        parts = []
+        for s in range(0, len(rows), 250):
+            r = torch.from_numpy(rows[s:s + 250]).to(dev).long()
+            dd = -(Xd[r] @ Xd.T)  # rows are unit vectors: order of 1 - cos
+            dd[torch.arange(len(r), device=dev), r] = float("inf")
+            parts.append(torch.topk(dd, PREC_K, dim=1, largest=False).indices.int().cpu().numpy())
+        truth = np.concatenate(parts)
+        del Xd
+
+    forms = {}
+    for name, prec in (("fp32", L.PRECISION_FP32), ("bf16", L.PRECISION_BF16)):
+        for _ in range(max(args.warmup, 1) if name == "fp32" else 1):
+            h, _t = build(prec)
+            L.check(L.lib.rinnd_free(h))
+        times = []
+        for _ in range(max(min(args.steps, 2), 1)):
+            h, t = build(prec)
+            times.append(t)
+            if len(times) < max(min(args.steps, 2), 1):
+                L.check(L.lib.rinnd_free(h))
+        t = max(times)
+        if world > 1:
+            tt = torch.tensor([t], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        inf = L.BuildInfo()
+        L.check(L.lib.rinnd_build_info_get(h, ctypes.byref(inf)))
+        entry = {"value": n * world / t, "ms_per_build": 1000.0 * t, "iterations": int(inf.iterations),
+                 "join_form": forms_names.get(int(inf.join_form), str(int(inf.join_form))),
+                 "ms_join_kernel": float(inf.ms_join_kernel)}
+        if truth is not None:
+            ki = np.empty((n, PREC_K), np.int32)
+            kd = np.empty((n, PREC_K), np.float32)
+            L.check(L.lib.rinnd_neighbor_graph(h, L.ptr(ki), L.ptr(kd)))
+            entry["recall@15"] = recall(ki[rows], truth)
+            # reported distance vs the pair's cosine distance in FP64
+            ids = torch.from_numpy(ki[rows]).to(dev).long()
+            ok = ids >= 0
+            q = X[torch.from_numpy(rows).to(dev).long()].double()
+            nb = X[ids.clamp(min=0)].double()
+            exact = 1.0 - (nb * q[:, None, :]).sum(-1) / (nb.norm(dim=-1) * q.norm(dim=-1)[:, None])
+            got = torch.from_numpy(kd[rows]).to(dev).double()
+            err = (got - exact).abs()[ok]
+            rel = err / exact.abs()[ok].clamp(min=1e-30)
+            entry["distance_error_vs_fp64"] = {
+                "pairs": int(err.numel()), "max_abs": float(err.max()), "p99_abs": float(torch.quantile(err, 0.99)),
+                "max_rel": float(rel.max()), "p99_rel": float(torch.quantile(rel, 0.99))}
+        L.check(L.lib.rinnd_free(h))
+        forms[name] = entry
+    if rank == 0:
+        line = {
+            "metric": "precision form: build points/s, recall@15 and distance error vs FP64 (1M x 960 cosine, k=15)",
+            "value": forms["fp32"]["value"], "unit": "points/s", "n_gpus": world, "steps": max(min(args.steps, 2), 1),
+            "warmup": max(args.warmup, 1), "ms_per_step": forms["fp32"]["ms_per_build"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"precision: {n} x {PREC_D}, x = |N(0,1)|^1.5 (torch generator seed 0) "
+                                   "L2-normalised rows, cosine (alternative-cosine proxy + correction), k=15, "
+                                   "default trees/leaf/candidates/iterations",
+                       "points_per_rank": n, "parallelism": f"replicas{world}",
+                       "recall_sample": f"{len(rows)} seeded rows vs FP64 exact",
+                       "timing": "host clock around the synchronized build call, max over ranks"},
+            "forms": forms,
+            "bf16_speedup_vs_fp32": forms["fp32"]["ms_per_build"] / forms["bf16"]["ms_per_build"],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def run_serving(args, world, rank, local_rank):
     """The serving form on one GPU (replicas per rank otherwise): a 10M x 96
     index of L2-normalised Gaussian-mixture rows (1000 clusters), cosine, k=30,
@@ -533,6 +653,9 @@ def main():
         return
     if args.workload == "serving":
         run_serving(args, world, rank, local_rank)
+        return
+    if args.workload == "precision":
+        run_precision(args, world, rank, local_rank)
         return
 
     import datetime

@@ -110,7 +110,16 @@ typedef struct rinnd_build_info {
   uint64_t kernel_launches;      /* kernels this library launched during the build  */
   uint64_t join_kernel_launches; /* local-join kernel launches (ms_join_kernel covers these) */
   uint64_t join_updates;         /* updates the join kernels appended for the heap pushes */
+  int32_t join_form;             /* RINND_JOIN_* of the last iteration's local join      */
 } rinnd_build_info;
+
+/* Local-join kernels (rinnd_build_info.join_form).  The pipelined FP32 join
+ * holds a vertex's candidate rows in shared memory (D up to ~400 at k <= 32);
+ * the tensor-core form (precision BF16) needs k <= 32, a non-Manhattan metric
+ * and D up to ~190; other builds use the chunked FP32 join. */
+#define RINND_JOIN_CHUNKED_FP32 0
+#define RINND_JOIN_PIPELINED_FP32 1
+#define RINND_JOIN_TENSOR_BF16 2
 
 /* ---- lifecycle ------------------------------------------------------------ */
 RINND_EXPORT int rinnd_params_default(rinnd_build_params* p);

@@ -23,6 +23,7 @@ DIST_SQEUCLIDEAN, DIST_MANHATTAN, DIST_COSINE, DIST_ALT_COSINE, DIST_ALT_DOT, DI
 CORR_NONE, CORR_SQRT, CORR_ALT_COSINE, CORR_ALT_IP = range(4)
 Q8_PER_VECTOR_COSINE, Q8_GLOBAL_SYMMETRIC, Q8_PER_VECTOR_SYMMETRIC = range(3)
 PRECISION_FP32, PRECISION_BF16 = range(2)
+JOIN_CHUNKED_FP32, JOIN_PIPELINED_FP32, JOIN_TENSOR_BF16 = range(3)  # rinnd_build_info.join_form
 
 _i32, _i64, _u64, _f32, _f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_float, ctypes.c_double
 _P = ctypes.c_void_p
@@ -46,7 +47,7 @@ class BuildInfo(ctypes.Structure):
         ("pairs_evaluated", _u64), ("pushes_accepted", _u64), ("push_contention", _u64),
         ("search_graph_nnz", _i64), ("min_distance", _f32), ("join_rows_gathered", _u64),
         ("ms_join_kernel", _f64), ("kernel_launches", _u64), ("join_kernel_launches", _u64),
-        ("join_updates", _u64),
+        ("join_updates", _u64), ("join_form", _i32),
     ]
 
 

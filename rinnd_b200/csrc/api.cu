@@ -345,6 +345,7 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   uint64_t pairs_total = 0, pushes_total = 0, rows_total = 0;
   double ms_cand = 0, ms_join = 0, ms_join_kernel = 0;
   uint64_t join_launches = 0, join_updates = 0;
+  int join_form = RINND_JOIN_CHUNKED_FP32;
   int iters = 0;
   for (int it = 0; it < n_iters; ++it) {
     iters = it + 1;
@@ -359,6 +360,7 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
     ms_join_kernel += js.kernel_ms;
     join_launches += (uint64_t)js.launches;
     join_updates += js.appended;
+    join_form = js.form;
     pairs_total += js.pairs;
     pushes_total += js.changes;
     rows_total += js.rows;
@@ -438,6 +440,7 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   inf.ms_join_kernel = ms_join_kernel;
   inf.join_kernel_launches = join_launches;
   inf.join_updates = join_updates;
+  inf.join_form = join_form;
   inf.kernel_launches = launch_counter() - launches0;
   inf.pushes_accepted = pushes_total;
   inf.push_contention = hc[1];

@@ -86,6 +86,7 @@ struct JoinStats {
   float kernel_ms = 0.f;   // CUDA-event duration of the join kernel launches on their stream
   float total_ms = 0.f;    // CUDA-event duration of the whole join step (describe, joins, applies)
   int launches = 0;        // join kernel launches
+  int form = 0;            // RINND_JOIN_* of the kernel that ran
 };
 JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st);
 bool join_tma_supported(int c, int Dp);

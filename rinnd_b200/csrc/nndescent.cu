@@ -26,6 +26,7 @@
 
 #include "dist.cuh"
 #include "engine.h"
+#include "../../include/rinnd.h"
 #include "heap.cuh"
 
 namespace rinnd {
@@ -731,6 +732,7 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
     js.kernel_ms += ms;
   }
   js.launches = (int)(kev.size() / 2);
+  js.form = use_tc ? RINND_JOIN_TENSOR_BF16 : use_tma ? RINND_JOIN_PIPELINED_FP32 : RINND_JOIN_CHUNKED_FP32;
   for (cudaEvent_t ev : kev) cudaEventDestroy(ev);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

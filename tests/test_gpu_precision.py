@@ -82,7 +82,8 @@ def test_bf16_iteration_matches_fp32_bit_for_bit(rb, orc, kind, d):
         tied_max = fp[1] == fp[1][:, -1:]
         differ = (bf[0] != fp[0]) | (bf[2] != fp[2])
         assert not np.any(differ & ~tied_max)
-        assert differ.sum() <= 2
+        # such ties are rare: at most 0.05 % of the entries
+        assert differ.sum() <= 5e-4 * differ.size
         heap = fp
 
 
