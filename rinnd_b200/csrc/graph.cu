@@ -132,9 +132,14 @@ __device__ __forceinline__ int staged_prune(const StagedWarp& sw, int n, const f
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
   __syncwarp();
-  for (int e = lane; e < n * n; e += 32) {
-    const int a = e / n, b = e % n;
-    if (a < b) sw.M[a * SK + b] = exact_distance(kind, sw.rows + (size_t)a * rs, sw.rows + (size_t)b * rs, D);
+  // pairs a < b < n in the order (b, then a): pair e is (e - b(b-1)/2, b) with
+  // b = floor((1 + sqrt(1 + 8e)) / 2), so no lane idles on a >= b
+  for (int e = lane; e < n * (n - 1) / 2; e += 32) {
+    int b = (int)((1.0f + sqrtf((float)(8 * e + 1))) * 0.5f);
+    if (b * (b - 1) / 2 > e) --b;
+    else if ((b + 1) * b / 2 <= e) ++b;
+    const int a = e - b * (b - 1) / 2;
+    sw.M[a * SK + b] = exact_distance(kind, sw.rows + (size_t)a * rs, sw.rows + (size_t)b * rs, D);
   }
   __syncwarp();
   int nret = 0;
