@@ -282,6 +282,15 @@ __global__ void __launch_bounds__(NT)
 }
 
 // Lock-free pushes of buffered updates (heap.cuh protocol).
+// Entry handled in place e of n: consecutive entries of the leaf initialization
+// come from one leaf block and target the same few rows (all racing for an
+// empty row's max slot in the first trees), so they are spread over the launch
+// (e * P mod n, a bijection when the prime P does not divide n).
+__device__ __forceinline__ unsigned long long spread_entry(unsigned long long e, unsigned long long n) {
+  constexpr unsigned long long P = 1000003ull;
+  return n % P ? (e * P) % n : e;
+}
+
 __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, const unsigned long long* count,
                                 unsigned long long cap, uint64_t* slots, uint32_t* thr, int k, int kp,
                                 unsigned long long* counters) {
@@ -293,8 +302,9 @@ __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, cons
   unsigned int mine = 0;
   for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
        e += (unsigned long long)gridDim.x * blockDim.x) {
-    uint32_t r = urow[e];
-    mine += row_push(slots + (size_t)r * kp, k, thr + r, ukey[e], &counters[1]);
+    const unsigned long long x = spread_entry(e, n);
+    uint32_t r = urow[x];
+    mine += row_push(slots + (size_t)r * kp, k, thr + r, ukey[x], &counters[1]);
   }
   for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&counters[0], (unsigned long long)mine);
@@ -314,6 +324,8 @@ __global__ void k_apply_regions(const uint32_t* urow, const uint64_t* ukey, cons
   }
   const size_t base = (size_t)r * rsize;
   unsigned int mine = 0;
+  // (in order: the join's updates rarely share rows within a warp, and reads
+  // in order are cheaper than spread ones)
   for (unsigned int e = part * blockDim.x + threadIdx.x; e < cnt; e += sub * blockDim.x) {
     const uint32_t row = urow[base + e];
     mine += row_push(slots + (size_t)row * kp, k, thr + row, ukey[base + e], &counters[1]);
