@@ -293,7 +293,7 @@ __device__ __forceinline__ unsigned long long spread_entry(unsigned long long e,
 
 __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, const unsigned long long* count,
                                 unsigned long long cap, uint64_t* slots, uint32_t* thr, int k, int kp,
-                                unsigned long long* counters) {
+                                unsigned long long* counters, bool spread) {
   const unsigned long long n = min(*count, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     atomicAdd(&counters[5], n);
@@ -302,7 +302,7 @@ __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, cons
   unsigned int mine = 0;
   for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
        e += (unsigned long long)gridDim.x * blockDim.x) {
-    const unsigned long long x = spread_entry(e, n);
+    const unsigned long long x = spread ? spread_entry(e, n) : e;
     uint32_t r = urow[x];
     mine += row_push(slots + (size_t)r * kp, k, thr + r, ukey[x], &counters[1]);
   }
@@ -590,7 +590,8 @@ void ensure_update_buffer(KnnState& s, cudaStream_t st) {
 }
 
 namespace {
-void apply_pending(KnnState& s, cudaStream_t st) {
+// `spread`: apply in the spread order (leaf-initialization updates).
+void apply_pending(KnnState& s, cudaStream_t st, bool spread = false) {
   if (s.nreg > 0) {
     const int sub = std::max(1, (148 * 16) / s.nreg);
     k_apply_regions<<<s.nreg * sub, 256, 0, st>>>(s.urow.p, s.ukey.p, s.rcnt.p, s.nreg, s.rsize, sub,
@@ -600,7 +601,7 @@ void apply_pending(KnnState& s, cudaStream_t st) {
     return;
   }
   k_apply_updates<<<148 * 16, 256, 0, st>>>(s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap, s.slots.p, s.thr.p,
-                                            s.k, s.kp, s.counters.p);
+                                            s.k, s.kp, s.counters.p, spread);
   RINND_LAUNCH_CHECK();
 }
 UpdateBuf update_buf(KnnState& s) { return UpdateBuf{s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap}; }
@@ -640,7 +641,7 @@ void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int 
       k_leaf_join<64, 256><<<grid, 256, 0, st>>>(jobs.p, j0, j1, f.leaves.p, f.perm.p, f.N, X, Dp, kind, norms,
                                                  s.slots.p, s.thr.p, s.k, s.kp, update_buf(s), s.counters.p);
     RINND_LAUNCH_CHECK();
-    apply_pending(s, st);
+    apply_pending(s, st, true);
   }
 }
 
