@@ -33,6 +33,41 @@ __device__ __forceinline__ float hsum_b(const float* s) {
   return __fadd_rn(__fadd_rn(a0, a2), __fadd_rn(a1, a3));
 }
 
+// Packed FP32x2 arithmetic: each 32-bit half is computed and rounded exactly
+// as the scalar instruction (sub.rn / add.rn / fma.rn), so a pair of
+// independent accumulator chains advances in one instruction with the same
+// results.  Element 2t of a chunk is the low half of 64-bit word t.
+__device__ __forceinline__ unsigned long long pk_sub(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long pk_add(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long pk_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+// A chunk of 8 as four packed pairs (two 16-byte loads).
+__device__ __forceinline__ void load8p(const float* p, unsigned long long* v) {
+  const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(p);
+  const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(p + 4);
+  v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+}
+// Packed accumulators back to the eight chains s[0..7].
+__device__ __forceinline__ void unpack8(const unsigned long long* p, float* s) {
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    s[2 * t] = __uint_as_float((uint32_t)p[t]);
+    s[2 * t + 1] = __uint_as_float((uint32_t)(p[t] >> 32));
+  }
+}
+
 // Rows are 16-byte aligned (row stride is a multiple of 4 floats), so each
 // chunk of 8 is read as two float4 loads.
 __device__ __forceinline__ void load8(const float* p, float* v) {
@@ -43,18 +78,20 @@ __device__ __forceinline__ void load8(const float* p, float* v) {
 }
 
 __device__ __forceinline__ float exact_sqeuclid(const float* a, const float* b, int n) {
-  float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long p[4] = {0ull, 0ull, 0ull, 0ull};  // chains (0,1) (2,3) (4,5) (6,7)
   int chunks = n >> 3;
   for (int c = 0; c < chunks; ++c) {
-    float x[8], y[8];
-    load8(a + 8 * c, x);
-    load8(b + 8 * c, y);
+    unsigned long long x[4], y[4];
+    load8p(a + 8 * c, x);
+    load8p(b + 8 * c, y);
 #pragma unroll
-    for (int l = 0; l < 8; ++l) {
-      float d = __fsub_rn(x[l], y[l]);
-      s[l] = __fmaf_rn(d, d, s[l]);
+    for (int t = 0; t < 4; ++t) {
+      const unsigned long long d = pk_sub(x[t], y[t]);
+      p[t] = pk_fma(d, d, p[t]);
     }
   }
+  float s[8];
+  unpack8(p, s);
   float r = hsum_a(s);
   for (int i = chunks * 8; i < n; ++i) {
     float d = __fsub_rn(a[i], b[i]);
@@ -64,30 +101,34 @@ __device__ __forceinline__ float exact_sqeuclid(const float* a, const float* b, 
 }
 
 __device__ __forceinline__ float exact_manhattan(const float* a, const float* b, int n) {
-  float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long p[4] = {0ull, 0ull, 0ull, 0ull};
   int chunks = n >> 3;
   for (int c = 0; c < chunks; ++c) {
-    float x[8], y[8];
-    load8(a + 8 * c, x);
-    load8(b + 8 * c, y);
+    unsigned long long x[4], y[4];
+    load8p(a + 8 * c, x);
+    load8p(b + 8 * c, y);
 #pragma unroll
-    for (int l = 0; l < 8; ++l) s[l] = __fadd_rn(s[l], fabsf(__fsub_rn(x[l], y[l])));
+    for (int t = 0; t < 4; ++t) p[t] = pk_add(p[t], pk_sub(x[t], y[t]) & 0x7FFFFFFF7FFFFFFFull);
   }
+  float s[8];
+  unpack8(p, s);
   float r = hsum_a(s);
   for (int i = chunks * 8; i < n; ++i) r = __fadd_rn(r, fabsf(__fsub_rn(a[i], b[i])));
   return r;
 }
 
 __device__ __forceinline__ float exact_dot_a(const float* a, const float* b, int n) {
-  float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long p[4] = {0ull, 0ull, 0ull, 0ull};
   int chunks = n >> 3;
   for (int c = 0; c < chunks; ++c) {
-    float x[8], y[8];
-    load8(a + 8 * c, x);
-    load8(b + 8 * c, y);
+    unsigned long long x[4], y[4];
+    load8p(a + 8 * c, x);
+    load8p(b + 8 * c, y);
 #pragma unroll
-    for (int l = 0; l < 8; ++l) s[l] = __fmaf_rn(x[l], y[l], s[l]);
+    for (int t = 0; t < 4; ++t) p[t] = pk_fma(x[t], y[t], p[t]);
   }
+  float s[8];
+  unpack8(p, s);
   float r = hsum_a(s);
   for (int i = chunks * 8; i < n; ++i) r = __fadd_rn(r, __fmul_rn(a[i], b[i]));
   return r;
