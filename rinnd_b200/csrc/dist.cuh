@@ -53,7 +53,8 @@ __device__ __forceinline__ unsigned long long pk_fma(unsigned long long a, unsig
   asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
   return d;
 }
-// A chunk of 8 as four packed pairs (two 16-byte loads).
+// A chunk of 8 as four packed pairs: rows are 16-byte aligned (the row stride
+// is a multiple of 4 floats), so a chunk is two 16-byte loads.
 __device__ __forceinline__ void load8p(const float* p, unsigned long long* v) {
   const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(p);
   const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(p + 4);
@@ -68,14 +69,6 @@ __device__ __forceinline__ void unpack8(const unsigned long long* p, float* s) {
   }
 }
 
-// Rows are 16-byte aligned (row stride is a multiple of 4 floats), so each
-// chunk of 8 is read as two float4 loads.
-__device__ __forceinline__ void load8(const float* p, float* v) {
-  float4 x = *reinterpret_cast<const float4*>(p);
-  float4 y = *reinterpret_cast<const float4*>(p + 4);
-  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
-  v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
-}
 
 __device__ __forceinline__ float exact_sqeuclid(const float* a, const float* b, int n) {
   unsigned long long p[4] = {0ull, 0ull, 0ull, 0ull};  // chains (0,1) (2,3) (4,5) (6,7)
@@ -135,26 +128,27 @@ __device__ __forceinline__ float exact_dot_a(const float* a, const float* b, int
 }
 
 __device__ __forceinline__ float exact_dot_b(const float* a, const float* b, int n) {
-  float t0[8] = {0, 0, 0, 0, 0, 0, 0, 0}, t1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  float t2[8] = {0, 0, 0, 0, 0, 0, 0, 0}, t3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // four sets of eight chains, advanced in packed pairs
+  unsigned long long q[4][4] = {{0ull, 0ull, 0ull, 0ull}, {0ull, 0ull, 0ull, 0ull},
+                                {0ull, 0ull, 0ull, 0ull}, {0ull, 0ull, 0ull, 0ull}};
   int chunks = n >> 5;
   for (int c = 0; c < chunks; ++c) {
     const float* pa = a + 32 * c;
     const float* pb = b + 32 * c;
-    float x[8], y[8];
-    load8(pa, x); load8(pb, y);
 #pragma unroll
-    for (int l = 0; l < 8; ++l) t0[l] = __fmaf_rn(x[l], y[l], t0[l]);
-    load8(pa + 8, x); load8(pb + 8, y);
+    for (int g = 0; g < 4; ++g) {
+      unsigned long long x[4], y[4];
+      load8p(pa + 8 * g, x);
+      load8p(pb + 8 * g, y);
 #pragma unroll
-    for (int l = 0; l < 8; ++l) t1[l] = __fmaf_rn(x[l], y[l], t1[l]);
-    load8(pa + 16, x); load8(pb + 16, y);
-#pragma unroll
-    for (int l = 0; l < 8; ++l) t2[l] = __fmaf_rn(x[l], y[l], t2[l]);
-    load8(pa + 24, x); load8(pb + 24, y);
-#pragma unroll
-    for (int l = 0; l < 8; ++l) t3[l] = __fmaf_rn(x[l], y[l], t3[l]);
+      for (int t = 0; t < 4; ++t) q[g][t] = pk_fma(x[t], y[t], q[g][t]);
+    }
   }
+  float t0[8], t1[8], t2[8], t3[8];
+  unpack8(q[0], t0);
+  unpack8(q[1], t1);
+  unpack8(q[2], t2);
+  unpack8(q[3], t3);
   float s[8];
 #pragma unroll
   for (int l = 0; l < 8; ++l) s[l] = __fadd_rn(__fadd_rn(t0[l], t1[l]), __fadd_rn(t2[l], t3[l]));
@@ -180,20 +174,24 @@ __device__ __forceinline__ float exact_dot_c(const float* a, const float* b, int
 }
 
 __device__ __forceinline__ float exact_cosine(const float* a, const float* b, int n) {
-  float sd[8] = {0, 0, 0, 0, 0, 0, 0, 0}, sa[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  float sb[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long pd[4] = {0ull, 0ull, 0ull, 0ull}, pa[4] = {0ull, 0ull, 0ull, 0ull};
+  unsigned long long pb[4] = {0ull, 0ull, 0ull, 0ull};
   int chunks = n >> 3;
   for (int c = 0; c < chunks; ++c) {
-    float x[8], y[8];
-    load8(a + 8 * c, x);
-    load8(b + 8 * c, y);
+    unsigned long long x[4], y[4];
+    load8p(a + 8 * c, x);
+    load8p(b + 8 * c, y);
 #pragma unroll
-    for (int l = 0; l < 8; ++l) {
-      sd[l] = __fmaf_rn(x[l], y[l], sd[l]);
-      sa[l] = __fmaf_rn(x[l], x[l], sa[l]);
-      sb[l] = __fmaf_rn(y[l], y[l], sb[l]);
+    for (int t = 0; t < 4; ++t) {
+      pd[t] = pk_fma(x[t], y[t], pd[t]);
+      pa[t] = pk_fma(x[t], x[t], pa[t]);
+      pb[t] = pk_fma(y[t], y[t], pb[t]);
     }
   }
+  float sd[8], sa[8], sb[8];
+  unpack8(pd, sd);
+  unpack8(pa, sa);
+  unpack8(pb, sb);
   float dot = hsum_a(sd), na = hsum_a(sa), nb = hsum_a(sb);
   for (int i = chunks * 8; i < n; ++i) {
     dot = __fadd_rn(dot, __fmul_rn(a[i], b[i]));
