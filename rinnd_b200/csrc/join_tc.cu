@@ -142,31 +142,49 @@ __global__ void __launch_bounds__(NT)
         bulk_g2s(dring + (size_t)i * dstride, desc + (size_t)(first + i * stride) * dstride, dbytes, &dbar[i]);
       }
     bool ok = true;
-    int i = 0;
+    int i = 0, jobs = 0;  // vertices walked, stages filled
     int desc_issued = nv < NDESC ? nv : NDESC;
     for (; i < nv; ++i) {
-      const int ds = i % NDESC, s = i % NSTAGE;
+      const int ds = i % NDESC;
       const int v = first + i * stride;
       ok = wait_or_abort(&dbar[ds], (uint32_t)(i / NDESC) & 1u, abort_flag);
       if (!ok) break;
-      if (i >= NSTAGE) {
-        ok = wait_or_abort(&empty[s], (uint32_t)((i / NSTAGE) - 1) & 1u, abort_flag);
-        if (!ok) break;
-      }
       const int32_t* dsc = dring + (size_t)ds * dstride;
-      unsigned char* st = stage0 + (size_t)s * sbytes;
-      int32_t* sd = reinterpret_cast<int32_t*>(st);
-      const int nb = dsc[1];
-      for (int t = lane; t < dstride; t += 32) sd[t] = dsc[t];
-      // row thresholds as of now (pushes applied by earlier batches tighten them)
-      int32_t my_ids[2];
-      uint32_t* sthr = reinterpret_cast<uint32_t*>(sd + Desc::thr(MAXC));
+      const int nb = dsc[1], items = dsc[3];
+      if (items > 0) {  // vertices without pairs take no stage
+        const int s = jobs % NSTAGE;
+        if (jobs >= NSTAGE) {
+          ok = wait_or_abort(&empty[s], (uint32_t)((jobs / NSTAGE) - 1) & 1u, abort_flag);
+          if (!ok) break;
+        }
+        unsigned char* st = stage0 + (size_t)s * sbytes;
+        int32_t* sd = reinterpret_cast<int32_t*>(st);
+        for (int t = lane; t < dstride; t += 32)  // descriptor -> stage header (thresholds below)
+          if (t < Desc::thr(MAXC) || t >= Desc::nrm(MAXC)) sd[t] = dsc[t];
+        // row thresholds as of now (pushes applied by earlier batches tighten them)
+        int32_t my_ids[2];
+        uint32_t* sthr = reinterpret_cast<uint32_t*>(sd + Desc::thr(MAXC));
 #pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        const int r = lane + 32 * t;
-        my_ids[t] = r < nb ? dsc[Desc::ids(MAXC) + r] : 0;
-        if (r < nb) sthr[r] = __ldcg(thr + my_ids[t]);
+        for (int t = 0; t < 2; ++t) {
+          const int r = lane + 32 * t;
+          my_ids[t] = r < nb ? dsc[Desc::ids(MAXC) + r] : 0;
+          if (r < nb) sthr[r] = __ldcg(thr + my_ids[t]);
+        }
+        float* rows = reinterpret_cast<float*>(st + L.rows_off());
+        const int ncopy = nb + (SQ ? 1 : 0);
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect_tx(&full[s], (uint32_t)ncopy * (uint32_t)Dp * 4u);
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const int r = lane + 32 * t;
+          if (r < nb) bulk_g2s(rows + (size_t)r * L.rs, X + (size_t)my_ids[t] * Dp, (uint32_t)Dp * 4u, &full[s]);
+        }
+        if (SQ && lane == 0)
+          bulk_g2s(rows + (size_t)TROWS * L.rs, X + (size_t)v * Dp, (uint32_t)Dp * 4u, &full[s]);
+        ++jobs;
       }
+      // descriptor slot consumed: refill it NDESC vertices ahead
       fence_proxy_async_smem();
       __syncwarp();
       if (i + NDESC < nv) {
@@ -177,17 +195,14 @@ __global__ void __launch_bounds__(NT)
                    &dbar[ds]);
         }
       }
-      float* rows = reinterpret_cast<float*>(st + L.rows_off());
-      const int ncopy = nb + ((SQ && nb > 0) ? 1 : 0);
-      if (lane == 0) mbar_arrive_expect_tx(&full[s], (uint32_t)ncopy * (uint32_t)Dp * 4u);
-      __syncwarp();
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        const int r = lane + 32 * t;
-        if (r < nb) bulk_g2s(rows + (size_t)r * L.rs, X + (size_t)my_ids[t] * Dp, (uint32_t)Dp * 4u, &full[s]);
+    }
+    if (ok) {  // end-of-work stage (nb = -1)
+      const int s = jobs % NSTAGE;
+      if (jobs >= NSTAGE) ok = wait_or_abort(&empty[s], (uint32_t)((jobs / NSTAGE) - 1) & 1u, abort_flag);
+      if (ok && lane == 0) {
+        reinterpret_cast<int32_t*>(stage0 + (size_t)s * sbytes)[1] = -1;
+        mbar_arrive(&full[s]);
       }
-      if (SQ && nb > 0 && lane == 0)
-        bulk_g2s(rows + (size_t)TROWS * L.rs, X + (size_t)v * Dp, (uint32_t)Dp * 4u, &full[s]);
     }
     if (!ok && lane == 0) {
       *abort_flag = 1;
@@ -195,7 +210,7 @@ __global__ void __launch_bounds__(NT)
       // drain: wait (bounded) for every descriptor and row copy this warp issued
       for (int j = i; j < desc_issued; ++j)
         mbar_wait_bounded(&dbar[j % NDESC], (uint32_t)(j / NDESC) & 1u, WAIT_POLLS);
-      for (int j = (i > NSTAGE ? i - NSTAGE : 0); j < i; ++j)
+      for (int j = (jobs > NSTAGE ? jobs - NSTAGE : 0); j < jobs; ++j)
         mbar_wait_bounded(&full[j % NSTAGE], (uint32_t)(j / NSTAGE) & 1u, WAIT_POLLS);
     }
     return;
@@ -213,7 +228,7 @@ __global__ void __launch_bounds__(NT)
   unsigned int pairs_total = 0;
   unsigned long long rows_total = 0;
   int nmma = 0;
-  for (int i = 0; i < nv; ++i) {
+  for (int i = 0;; ++i) {  // stages in fill order, up to the end-of-work stage
     const int s = i % NSTAGE;
     if (ct == 0) {
       const bool ok = wait_or_abort(&full[s], (uint32_t)(i / NSTAGE) & 1u, abort_flag);
@@ -230,6 +245,7 @@ __global__ void __launch_bounds__(NT)
     const unsigned char* st = stage0 + (size_t)s * sbytes;
     const int32_t* sd = reinterpret_cast<const int32_t*>(st);
     const int na = sd[0], nb = sd[1];
+    if (nb < 0) break;  // read by every compute thread after the same barrier
     const int32_t* ids = sd + Desc::ids(MAXC);
     const uint32_t* sthr = reinterpret_cast<const uint32_t*>(sd + Desc::thr(MAXC));
     const float* snrm = reinterpret_cast<const float*>(sd + Desc::nrm(MAXC));
