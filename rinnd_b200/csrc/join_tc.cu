@@ -11,7 +11,8 @@
 // Per vertex (candidate lists of <= 32 new + 32 old ids, so nb <= 64 rows):
 //   producer warp: one cp.async.bulk per candidate row (FP32, Dp floats) plus,
 //     for squared Euclidean, the vertex's own row, into a shared-memory stage
-//     (the FP32 join's descriptor/stage pipeline, two stages);
+//     (the FP32 join's descriptor/stage pipeline, two stages; vertices without
+//     pairs take no stage, and a stage with nb = -1 ends the work);
 //   4 compute warps (one per tensor-memory lane quadrant):
 //     1. convert the rows to BF16 into a K-major tile; squared Euclidean rows
 //        are centered on the vertex's own row first (distances are translation
