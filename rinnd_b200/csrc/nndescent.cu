@@ -121,7 +121,7 @@ template <int MAXA, int MAXB, int AROWS, int NT>
 __device__ __forceinline__ void join_pairs(PairSmem<MAXA, MAXB, AROWS>& sm, int na, int nb, int mode,
                                            const float* __restrict__ X, int Dp, int kind, uint64_t* slots,
                                            uint32_t* thr, int k, int kp, UpdateBuf ub,
-                                           unsigned long long* counters) {
+                                           unsigned long long* counters, bool direct = false) {
   constexpr int PPT = (MAXA * MAXB + NT - 1) / NT;
   const bool a_prefix = mode != MODE_RECT;
   const float* rowsB = sm.rows;
@@ -199,6 +199,25 @@ __device__ __forceinline__ void join_pairs(PairSmem<MAXA, MAXB, AROWS>& sm, int 
       if (kd[s] < tp) { emit_p |= 1u << s; ++n_emit; }
       if (kd[s] < sm.bthr[j]) { emit_q |= 1u << s; ++n_emit; }
     }
+  }
+  if (direct) {
+    // MODE_TRI job over rows nothing else writes, all empty (first tree's leaf
+    // of at most k + 1 points): every passing (row, id) has its own slot --
+    // row of point i holds point j at slot j - 1 (j > i), row of j holds i at
+    // slot i -- the keys the updates would carry, in place of the updates.
+#pragma unroll
+    for (int s = 0; s < PPT; ++s) {
+      if ((emit_p | emit_q) & (1u << s)) {
+        const int t = tid + s * NT;
+        const int i = t / nb, j = t % nb;
+        const int32_t p = sm.bid[i], q = sm.bid[j];
+        if (emit_p & (1u << s)) slots[(size_t)p * kp + (j - 1)] = ((uint64_t)kd[s] << 32) | (uint32_t)q | 0x80000000u;
+        if (emit_q & (1u << s)) slots[(size_t)q * kp + i] = ((uint64_t)kd[s] << 32) | (uint32_t)p | 0x80000000u;
+      }
+    }
+    const unsigned int my_pairs = __popc(valid_mask);
+    if (my_pairs) atomicAdd(&sm.pairs, my_pairs);
+    return;
   }
   const int lane = tid & 31;
   int incl = n_emit;
@@ -357,17 +376,23 @@ __global__ void k_leaf_job_emit(const int4* leaves, long long nl, int BS, const 
 }
 
 // nndescent/mod.rs:203-300 initialize_from_leaves, one CTA per (leaf, block pair).
+// Pass 1 (first, on empty rows) takes only the first tree's leaves of at most
+// min(BS, k + 1) points: each is one job, its rows belong to no other leaf of
+// that tree, and all its passing pairs fit the rows, so it writes its slots
+// directly.  Pass 0 takes every other job and appends updates.
 template <int BS, int NT>
 __global__ void __launch_bounds__(NT)
     k_leaf_join(const int4* jobs, long long j0, long long j1, const int4* leaves, const int32_t* perm, int N,
                 const float* __restrict__ X, int Dp, int kind, const float* norms, uint64_t* slots,
-                uint32_t* thr, int k, int kp, UpdateBuf ub, unsigned long long* counters) {
+                uint32_t* thr, int k, int kp, UpdateBuf ub, unsigned long long* counters, int pass) {
   __shared__ PairSmem<BS, BS, BS> sm;
   for (long long jb = j0 + blockIdx.x; jb < j1; jb += gridDim.x) {
     int4 job = jobs[jb];
     int4 leaf = leaves[job.x];
     const int32_t* P = perm + (size_t)leaf.x * N + leaf.y;
     int L = leaf.z - leaf.y;
+    const bool direct = leaf.x == 0 && L <= BS && L <= k + 1;
+    if (direct != (pass == 1)) continue;  // uniform over the CTA
     int a0 = job.y * BS, b0 = job.z * BS;
     int na = min(BS, L - a0), nb = min(BS, L - b0);
     int mode = job.y == job.z ? MODE_TRI : MODE_RECT;
@@ -377,7 +402,7 @@ __global__ void __launch_bounds__(NT)
     for (int t = threadIdx.x; t < na; t += blockDim.x) sm.aid[t] = P[a0 + t];
     __syncthreads();
     load_meta(sm, na, nb, mode != MODE_RECT, thr, kind_is_dot(kind) ? norms : nullptr);
-    join_pairs<BS, BS, BS, NT>(sm, na, nb, mode, X, Dp, kind, slots, thr, k, kp, ub, counters);
+    join_pairs<BS, BS, BS, NT>(sm, na, nb, mode, X, Dp, kind, slots, thr, k, kp, ub, counters, direct);
     __syncthreads();
     if (threadIdx.x == 0) atomicAdd(&counters[2], (unsigned long long)sm.pairs);
   }
@@ -628,19 +653,24 @@ void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int 
   k_leaf_job_emit<<<grid_for(f.n_leaves, 256, 148 * 32), 256, 0, st>>>(f.leaves.p, f.n_leaves, BS, off.p, jobs.p);
   RINND_LAUNCH_CHECK();
   const float* norms = s.norms.p;
+  auto launch = [&](long long j0, long long j1, int pass) {
+    const int grid = (int)std::min<long long>(j1 - j0, 148LL * 16);
+    if (BS == 32)
+      k_leaf_join<32, 128><<<grid, 128, 0, st>>>(jobs.p, j0, j1, f.leaves.p, f.perm.p, f.N, X, Dp, kind, norms,
+                                                 s.slots.p, s.thr.p, s.k, s.kp, update_buf(s), s.counters.p, pass);
+    else
+      k_leaf_join<64, 256><<<grid, 256, 0, st>>>(jobs.p, j0, j1, f.leaves.p, f.perm.p, f.N, X, Dp, kind, norms,
+                                                 s.slots.p, s.thr.p, s.k, s.kp, update_buf(s), s.counters.p, pass);
+    RINND_LAUNCH_CHECK();
+  };
+  // the first tree's small leaves write their (still empty) rows directly
+  launch(0, njobs, 1);
   // Worst case 2 * BS^2 updates per job: batches never overflow the buffer.
   const long long per_batch = std::max<long long>(1, (long long)(s.ucap / (2ull * BS * BS)));
   for (long long j0 = 0; j0 < njobs; j0 += per_batch) {
     long long j1 = std::min<long long>(njobs, j0 + per_batch);
     RINND_CUDA(cudaMemsetAsync(s.counters.p + 4, 0, sizeof(unsigned long long), st));
-    int grid = (int)std::min<long long>(j1 - j0, 148LL * 16);
-    if (BS == 32)
-      k_leaf_join<32, 128><<<grid, 128, 0, st>>>(jobs.p, j0, j1, f.leaves.p, f.perm.p, f.N, X, Dp, kind, norms,
-                                                 s.slots.p, s.thr.p, s.k, s.kp, update_buf(s), s.counters.p);
-    else
-      k_leaf_join<64, 256><<<grid, 256, 0, st>>>(jobs.p, j0, j1, f.leaves.p, f.perm.p, f.N, X, Dp, kind, norms,
-                                                 s.slots.p, s.thr.p, s.k, s.kp, update_buf(s), s.counters.p);
-    RINND_LAUNCH_CHECK();
+    launch(j0, j1, 0);
     apply_pending(s, st, true);
   }
 }
