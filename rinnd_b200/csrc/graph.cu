@@ -254,12 +254,13 @@ __global__ void k_diversify_rev(const int32_t* rev_ptr, const uint64_t* rev_key,
   if (lane == 0) rret_cnt[row] = nret;
 }
 
-template <int P>
-__device__ __forceinline__ void warp_bitonic(uint64_t* b) {
+// Bitonic sort of b[0, n), n a power of two; entries from n on are ~0 (no
+// smaller than any sorted key), so the whole array ends sorted.
+__device__ __forceinline__ void warp_bitonic_n(uint64_t* b, int n) {
   const int lane = threadIdx.x & 31;
-  for (int size = 2; size <= P; size <<= 1)
+  for (int size = 2; size <= n; size <<= 1)
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int j = lane; j < P; j += 32) {
+      for (int j = lane; j < n; j += 32) {
         int partner = j ^ stride;
         if (partner > j) {
           bool up = (j & size) == 0;
@@ -285,6 +286,8 @@ __global__ void k_union(const int32_t* fwd_idx, const float* fwd_dist, const int
   if (v >= N) return;
   uint64_t* b = buf[w];
   const int nf = fwd_cnt[v], nr = rret_cnt[v];
+  int span = 32;  // sorts cover the live entries only (nf + nr <= P)
+  while (span < nf + nr) span <<= 1;
   // (id, distance) keys; dropped entries become ~0.
   for (int e = lane; e < P; e += 32) {
     uint64_t key = ~0ull;
@@ -301,7 +304,7 @@ __global__ void k_union(const int32_t* fwd_idx, const float* fwd_dist, const int
     b[e] = key;
   }
   __syncwarp();
-  warp_bitonic<P>(b);
+  warp_bitonic_n(b, span);
   // keep the last (max distance) entry of each id run; re-key by (distance, id)
   uint64_t nk[P / 32];
 #pragma unroll
@@ -320,7 +323,7 @@ __global__ void k_union(const int32_t* fwd_idx, const float* fwd_dist, const int
 #pragma unroll
   for (int t = 0; t < P / 32; ++t) b[t * 32 + lane] = nk[t];
   __syncwarp();
-  warp_bitonic<P>(b);
+  warp_bitonic_n(b, span);
   // first max_degree valid entries, re-keyed by id
 #pragma unroll
   for (int t = 0; t < P / 32; ++t) {
@@ -332,7 +335,7 @@ __global__ void k_union(const int32_t* fwd_idx, const float* fwd_dist, const int
 #pragma unroll
   for (int t = 0; t < P / 32; ++t) b[t * 32 + lane] = nk[t];
   __syncwarp();
-  warp_bitonic<P>(b);
+  warp_bitonic_n(b, span);
   int cnt = 0;
 #pragma unroll
   for (int t = 0; t < P / 32; ++t) {
