@@ -124,3 +124,40 @@ def test_quantized_width_validation():
         with pytest.raises(ValueError):
             v(*args)
     v(10, 20, 10)
+
+
+STRUCTS = {"rinnd_build_params": "BuildParams", "rinnd_build_info": "BuildInfo", "rinnd_batch_item": "BatchItem",
+           "rinnd_server_params": "ServerParams", "rinnd_server_stats": "ServerStats",
+           "rinnd_storage_info": "StorageInfo"}
+
+
+def test_ctypes_mirrors_match_the_header_layout(tmp_path):
+    """Every ctypes structure in rinnd_b200/_lib.py has the size and field
+    offsets the C compiler gives the struct in include/rinnd.h (a field added on
+    one side only would shift every later field)."""
+    import shutil
+
+    from rinnd_b200 import _lib as L
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "rinnd.h"', "int main(void) {"]
+    for cname, pyname in STRUCTS.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in getattr(L, pyname)._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, field, value = line.split()
+        got[(cname, field)] = int(value)
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(L, pyname)
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)
