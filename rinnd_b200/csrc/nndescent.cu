@@ -510,20 +510,26 @@ __global__ void k_cand_reverse(const uint64_t* slots, int N, int k, int kp, int 
 }
 
 // candidates.rs:354-417 mark_old_flags, one warp per row.
+// The new list is read once per warp (list entry t in lane t % 32) and each
+// slot's id is tested against it by shuffles.
 __global__ void k_mark_old(uint64_t* slots, int N, int k, int kp, const uint64_t* cnew, int c, int cp) {
   int row = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
   int lane = threadIdx.x & 31;
   if (row >= N) return;
   const uint64_t* nl = cnew + (size_t)row * cp;
+  const int32_t l0 = lane < c ? slot_id(nl[lane]) : -1;
+  const int32_t l1 = lane + 32 < c ? slot_id(nl[lane + 32]) : -1;  // c <= 64
   for (int j0 = 0; j0 < k; j0 += 32) {
     int j = j0 + lane;
     uint64_t s = j < k ? slots[(size_t)row * kp + j] : SLOT_EMPTY;
     int32_t id = slot_id(s);
+    const bool want = id >= 0 && slot_new(s);
     bool hit = false;
-    if (id >= 0 && slot_new(s))
-      for (int t = 0; t < c; ++t)
-        if (slot_id(nl[t]) == id) { hit = true; break; }
-    if (hit) slots[(size_t)row * kp + j] = s & ~(1ull << 31);
+    if (__any_sync(0xffffffffu, want)) {
+      for (int t = 0; t < 32 && t < c; ++t) hit |= __shfl_sync(0xffffffffu, l0, t) == id;
+      for (int t = 0; t + 32 < c; ++t) hit |= __shfl_sync(0xffffffffu, l1, t) == id;
+    }
+    if (want && hit) slots[(size_t)row * kp + j] = s & ~(1ull << 31);
   }
 }
 
