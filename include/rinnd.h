@@ -114,9 +114,10 @@ typedef struct rinnd_build_info {
 } rinnd_build_info;
 
 /* Local-join kernels (rinnd_build_info.join_form).  The pipelined FP32 join
- * holds a vertex's candidate rows in shared memory (D up to ~400 at k <= 32);
- * the tensor-core form (precision BF16) needs k <= 32, a non-Manhattan metric
- * and D up to ~190; other builds use the chunked FP32 join. */
+ * holds a vertex's candidate rows in shared memory (rows padded to Dp =
+ * round_up(D, 4) floats: Dp <= 424 with candidate lists of <= 32, Dp <= 204 with
+ * longer lists); the tensor-core form (precision BF16) needs lists of <= 32, a
+ * non-Manhattan metric and Dp <= 304; other builds use the chunked FP32 join. */
 #define RINND_JOIN_CHUNKED_FP32 0
 #define RINND_JOIN_PIPELINED_FP32 1
 #define RINND_JOIN_TENSOR_BF16 2
@@ -282,10 +283,12 @@ RINND_EXPORT int rinnd_heap_push_batch(int32_t n, int32_t k, int64_t n_ops, cons
  * (distances raw, of `kind`) and the sorted rows after the iteration; `changes`
  * receives the number of successful pushes.  `precision` selects the join tiles
  * (RINND_PRECISION_*); the candidate sample depends only on the rows' contents,
- * `seed` and `iteration`. */
+ * `seed` and `iteration`.  `join_form` (may be NULL) receives the RINND_JOIN_*
+ * of the join kernel that ran. */
 RINND_EXPORT int rinnd_nndescent_step(const float* data, int64_t n, int32_t d, int32_t k, int32_t max_candidates,
                                       int32_t kind, int32_t precision, uint64_t seed, int32_t iteration,
-                                      int32_t* idx, float* dist, uint8_t* flags, int64_t* changes);
+                                      int32_t* idx, float* dist, uint8_t* flags, int64_t* changes,
+                                      int32_t* join_form);
 
 /* No counterpart in the reference.  The same operation as rinnd_heap_push_batch
  * for callers that may not allocate device memory (a host engine that owns the
@@ -296,8 +299,12 @@ RINND_EXPORT int rinnd_nndescent_step(const float* data, int64_t n, int32_t d, i
  * the library holds until exit.  Limits: n <= 65536 and n * round_up(k, 16) <=
  * 1,048,576; larger requests fail with RINND_ERR_INVALID.  The first call on a
  * device resolves the scratch address and should come before any stream
- * capture.  Calls that overlap on the GPU race on the shared scratch.  Returns
- * after the stream has finished the work (*n_accepted is read back). */
+ * capture.  Calls that overlap on the GPU race on the shared scratch.  Every
+ * call synchronizes `stream` before it returns, to read back *n_accepted and
+ * its validity count.  Pushes are validated on the device with the bounds of
+ * rinnd_heap_push_batch (row in [0, n), id in [0, 2^31 - 2)); when any push is
+ * invalid the call returns RINND_ERR_INVALID, and the outputs have already been
+ * overwritten with the rows built from the valid pushes. */
 RINND_EXPORT int rinnd_heap_push_batch_noalloc(int32_t n, int32_t k, int64_t n_ops, const int32_t* d_rows,
                                                const int32_t* d_ids, const float* d_dists,
                                                const uint8_t* d_flags, int32_t* d_out_idx,
@@ -308,6 +315,11 @@ RINND_EXPORT int rinnd_heap_push_batch_noalloc(int32_t n, int32_t k, int64_t n_o
 RINND_EXPORT const char* rinnd_last_error(void);
 RINND_EXPORT const char* rinnd_version(void);
 RINND_EXPORT int rinnd_device_count(int32_t* count);
+/* Compiled target of this library's kernels on the current device, from
+ * cudaFuncGetAttributes: binaryVersion (100 for sm_100a code) and, when
+ * ptx_version is not NULL, ptxVersion (the virtual architecture the code was
+ * compiled from, 100 for compute_100a). */
+RINND_EXPORT int rinnd_kernel_target(int32_t* binary_version, int32_t* ptx_version);
 /* Number of kernels this library has launched in the process so far. */
 RINND_EXPORT int rinnd_kernel_launches(uint64_t* count);
 

@@ -105,12 +105,13 @@ SIGNATURES = {
     "rinnd_distance_pairs": (ctypes.c_int, [_i32, _P, _P, _i64, _i32, _P]),
     "rinnd_search_graph_from_knn": (ctypes.c_int, [_P, _P, _P, _i32, _i32, _i32, _i32, _f32, _P, _P, _P, _P]),
     "rinnd_heap_push_batch": (ctypes.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P, _P]),
-    "rinnd_nndescent_step": (ctypes.c_int, [_P, _i64, _i32, _i32, _i32, _i32, _i32, _u64, _i32, _P, _P, _P, _P]),
+    "rinnd_nndescent_step": (ctypes.c_int, [_P, _i64, _i32, _i32, _i32, _i32, _i32, _u64, _i32, _P, _P, _P, _P, _P]),
     "rinnd_heap_push_batch_noalloc": (ctypes.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rinnd_last_error": (ctypes.c_char_p, []),
     "rinnd_version": (ctypes.c_char_p, []),
     "rinnd_device_count": (ctypes.c_int, [_P]),
     "rinnd_kernel_launches": (ctypes.c_int, [_P]),
+    "rinnd_kernel_target": (ctypes.c_int, [_P, _P]),
 }
 
 if not os.path.exists(LIB_PATH):

@@ -653,6 +653,26 @@ int rinnd_server_destroy(rinnd_server* s) {
   });
 }
 
+int rinnd_kernel_target(int32_t* binary_version, int32_t* ptx_version) {
+  return guarded([&] {
+    require(binary_version != nullptr, "binary_version must not be null");
+    int dev = 0;
+    {
+      int n = 0;
+      cudaError_t e = cudaGetDeviceCount(&n);
+      if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        throw NoDevice("no CUDA device is available: the B200 engine has no CPU fallback");
+      }
+      RINND_CUDA(cudaGetDevice(&dev));
+    }
+    cudaFuncAttributes a{};
+    RINND_CUDA(cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(k_iota)));
+    *binary_version = a.binaryVersion;
+    if (ptx_version) *ptx_version = a.ptxVersion;
+  });
+}
+
 int rinnd_kernel_launches(uint64_t* count) {
   return guarded([&] {
     require(count != nullptr, "count must not be null");
@@ -864,7 +884,7 @@ int rinnd_heap_push_batch(int32_t n, int32_t k, int64_t n_ops, const int32_t* ro
 
 int rinnd_nndescent_step(const float* data, int64_t n, int32_t d, int32_t k, int32_t max_candidates, int32_t kind,
                          int32_t precision, uint64_t seed, int32_t iteration, int32_t* idx, float* dist,
-                         uint8_t* flags, int64_t* changes) {
+                         uint8_t* flags, int64_t* changes, int32_t* join_form) {
   return guarded([&] {
     require(n >= 2 && n < (int64_t)INT32_MAX - 1 && d >= 1, "invalid shape");
     require(k >= 1 && k <= 128, "k must be in [1, 128]");
@@ -918,6 +938,7 @@ int rinnd_nndescent_step(const float* data, int64_t n, int32_t d, int32_t k, int
     of.to_host(flags, (size_t)N * k);
     RINND_CUDA(cudaStreamSynchronize(st));
     if (changes) *changes = (int64_t)js.changes;
+    if (join_form) *join_form = js.form;
   });
 }
 

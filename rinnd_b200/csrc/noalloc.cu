@@ -13,8 +13,12 @@
 // device addresses, so once per device, with that device current, the first
 // call looks them up with cudaGetSymbolAddress and caches them; that first call
 // on a device should therefore happen before any stream capture.  Every call
-// shares the arrays and clears the rows, bounds and counters it uses; calls that
-// overlap on the GPU (other streams, other host threads) race on them.
+// also waits for its stream to finish before it returns, to read its counters
+// back.  Every call shares the arrays and clears the rows, bounds and counters it
+// uses; calls that overlap on the GPU (other streams, other host threads) race on
+// them.  Pushes are validated like rinnd_heap_push_batch's (row in [0, n), id in
+// [0, 2^31 - 2)), but on the device: an invalid push makes the call fail after the
+// outputs were written from the valid pushes.
 #include <mutex>
 #include <string>
 
@@ -67,14 +71,16 @@ __global__ void k_noalloc_clear(uint64_t* slots, long long n_slots, uint32_t* th
   }
 }
 
-// Pushes with device-side range checks (inputs are device memory the host cannot inspect).
+// Pushes with device-side range checks (inputs are device memory the host cannot
+// inspect); the bounds are rinnd_heap_push_batch's: rows in [0, n), ids in
+// [0, INT32_MAX - 1).
 __global__ void k_noalloc_push(uint64_t* slots, uint32_t* thr, int n, int k, int kp, long long n_ops,
                                const int32_t* rows, const int32_t* ids, const float* dists,
                                const uint8_t* flags, unsigned long long* counters) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_ops;
        i += (long long)gridDim.x * blockDim.x) {
     int32_t r = rows[i], id = ids[i];
-    if (r < 0 || r >= n || id < 0 || id >= 0x7FFFFFFF) {
+    if (r < 0 || r >= n || id < 0 || id >= 0x7FFFFFFE) {
       atomicAdd(&counters[2], 1ull);
       continue;
     }

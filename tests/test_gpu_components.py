@@ -25,6 +25,18 @@ def gpu_pairs(kind, a, b):
     return out
 
 
+def test_kernels_are_sm100a_code(rb):
+    """The library's kernels run as sm_100a binaries (cudaFuncGetAttributes
+    binaryVersion 100).  ptxVersion is the virtual architecture the code was
+    compiled from (compute_100a)."""
+    from rinnd_b200 import _lib as L
+
+    b, p = ctypes.c_int32(-1), ctypes.c_int32(-1)
+    L.check(L.lib.rinnd_kernel_target(ctypes.byref(b), ctypes.byref(p)))
+    assert b.value == 100, b.value
+    assert p.value == 100, p.value
+
+
 def test_distance_kats(rb, kats):
     for c in kats["distances"]:
         d = gpu_pairs(KIND[c["kind"]], np.array([c["a"]]), np.array([c["b"]]))[0]

@@ -37,12 +37,16 @@ def random_rows(orc, X, k, kind, seed):
 
 
 def step(X, heap, k, kind, precision, seed, it):
+    """One iteration; the join kernel that ran must be the one the precision asks for."""
     from rinnd_b200 import _lib as L
 
     idx, dist, flags = (np.ascontiguousarray(a).copy() for a in heap)
     ch = ctypes.c_int64(0)
+    form = ctypes.c_int32(-1)
     L.check(L.lib.rinnd_nndescent_step(L.ptr(X), X.shape[0], X.shape[1], k, 0, kind, precision, seed, it,
-                                       L.ptr(idx), L.ptr(dist), L.ptr(flags), ctypes.byref(ch)))
+                                       L.ptr(idx), L.ptr(dist), L.ptr(flags), ctypes.byref(ch), ctypes.byref(form)))
+    want = L.JOIN_TENSOR_BF16 if precision == L.PRECISION_BF16 else L.JOIN_PIPELINED_FP32
+    assert form.value == want, (precision, form.value)
     return (idx, dist, flags), ch.value
 
 
@@ -99,6 +103,8 @@ def test_bf16_build_recall_equals_fp32(rb, orc, metric, kind, k, d):
         ix = rb.RINND(X, metric=metric, n_neighbors=k, random_state=5, precision=prec)
         gi, gd = ix.neighbor_graph
         rec[prec] = recall(gi[:3000], truth)
+        want = rb._lib.JOIN_TENSOR_BF16 if prec == "bf16" else rb._lib.JOIN_PIPELINED_FP32
+        assert ix.build_info["join_form"] == want, (prec, ix.build_info["join_form"])
         assert np.all(np.diff(gd, axis=1) >= 0)
         assert ix.build_info["push_contention"] == 0
     assert rec["bf16"] >= rec["fp32"] - 0.005, rec

@@ -79,3 +79,49 @@ def test_noalloc_rejects_oversized_requests():
                                                  ctypes.c_void_p(8), None, None, None)
         assert rc == L.ERR_INVALID
         assert "allocation-free" in L.last_error()
+
+
+def test_noalloc_invalid_pushes_fail_like_the_allocating_entry_point():
+    """Row n and id -1 are out of range for both entry points; id 2^31 - 3 is the
+    largest id both accept and 2^31 - 2 the smallest both reject.  The allocation-
+    free call checks on the device, so it reports the failure after writing the
+    rows built from the valid pushes."""
+    torch = pytest.importorskip("torch")
+    from rinnd_b200 import _lib as L
+
+    n, k = 64, 8
+    rows, ids, dists, flags = make_pushes(21, n, k, 2000, 200)
+    ok_ids = ids.copy()
+    ok_ids[5] = 0x7FFFFFFD
+    ai, ad, af, _ = allocating(L, n, k, rows, ok_ids, dists, flags)
+    ni, nd, nf, _ = noalloc(L, torch, n, k, rows, ok_ids, dists, flags)
+    np.testing.assert_array_equal(ni, ai)
+    np.testing.assert_array_equal(nd.view(np.uint32), ad.view(np.uint32))
+    cases = []
+    r1, i1 = rows.copy(), ids.copy()
+    r1[3] = n
+    cases.append((r1, i1))
+    r2, i2 = rows.copy(), ids.copy()
+    i2[7] = -1
+    cases.append((r2, i2))
+    r3, i3 = rows.copy(), ids.copy()
+    i3[9] = 0x7FFFFFFE
+    cases.append((r3, i3))
+    dev = torch.device("cuda", 0)
+    for br, bi in cases:
+        oi = np.empty((n, k), np.int32)
+        od = np.empty((n, k), np.float32)
+        rc = L.lib.rinnd_heap_push_batch(n, k, br.size, L.ptr(br), L.ptr(bi), L.ptr(dists), L.ptr(flags), L.ptr(oi),
+                                         L.ptr(od), None, None)
+        assert rc == L.ERR_INVALID and "out of range" in L.last_error()
+        t = [torch.from_numpy(a).to(dev) for a in (br, bi, dists, flags)]
+        toi = torch.empty((n, k), dtype=torch.int32, device=dev)
+        tod = torch.empty((n, k), dtype=torch.float32, device=dev)
+        p = lambda x: ctypes.c_void_p(x.data_ptr())
+        rc = L.lib.rinnd_heap_push_batch_noalloc(n, k, br.size, *(p(x) for x in t), p(toi), p(tod), None, None,
+                                                 ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+        assert rc == L.ERR_INVALID and "out of range" in L.last_error()
+    # the scratch is usable again after a failed call
+    ni2, nd2, _, _ = noalloc(L, torch, n, k, rows, ok_ids, dists, flags)
+    np.testing.assert_array_equal(ni2, ai)
+    np.testing.assert_array_equal(nd2.view(np.uint32), ad.view(np.uint32))
