@@ -15,7 +15,9 @@ Multi-GPU: one independent index per rank (weak scaling, no collective on the
 data path); the max over ranks of the device-timed region is reported.
 
 --impl reference: the reference's CPU algorithm (the C++ restatement under
-oracle/, all host threads) on a bounded sample of the same workload.
+oracle/, all host threads) on the same full workload, one build per step.
+The default run also builds that oracle index once (the `cpu_baseline` leg)
+and reports its recall beside the GPU's, on the same sample and queries.
 """
 from __future__ import annotations
 
@@ -38,7 +40,6 @@ METRIC = "k-NN graph build pts/sec & QPS at fixed recall@k; vs plain FP32 GPU, %
 N_FULL, DIM, N_CLUSTERS, K = 1_000_000, 128, 100, 30
 N_TREES, LEAF, N_ITERS, DELTA = 8, 30, 10, 0.001
 N_QUERIES, QK, EPS = 10_000, 10, 0.1
-CPU_SAMPLE = 250_000
 # FP32 SIMT peak for context: 148 SMs x 128 FP32 lanes x 2 flops (FMA) x 1.965 GHz.
 FP32_SIMT_NOMINAL_TFLOPS = 74.4
 WORKLOAD = ("nndescent-build 1M x 128 f32 GMM(100 clusters, center std 10, unit std), sqeuclidean, "
@@ -64,8 +65,6 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--verbose", action="store_true", help="per-iteration build statistics")
-    ap.add_argument("--parity", action="store_true",
-                    help="also build the oracle (CPU restatement) at the full size and report its recall")
     ap.add_argument("--workload", default="build", choices=["build", "batched", "serving", "precision"],
                     help="build: the 1M-point build (default); batched: many independent indices in one call; "
                          "serving: continuous-batching queries against a 10M x 96 index; precision: FP32 and "
@@ -167,13 +166,20 @@ def cpu_build(X, n_threads=0):
     return ix, dt
 
 
+def bench_config(n, world):
+    """The `config` object of both arms (identical for the same workload)."""
+    return {"workload": WORKLOAD, "points_per_rank": n, "parallelism": f"replicas{world}",
+            "l2": "inputs (512 MB/rank) exceed L2 (126 MB); no flush"}
+
+
 def run_reference(args, rank):
-    """The reference's CPU build (restated in oracle/) on bounded samples."""
+    """The reference's CPU build (restated in oracle/) on the full workload:
+    every step builds the whole N-point index with all host threads."""
     if rank != 0:
         return
     import oracle
 
-    n = min(args.n, CPU_SAMPLE)
+    n = args.n
     X = gen_mixture(n, DIM, seed=0)
     cores = oracle.max_threads()
     for _ in range(args.warmup):
@@ -181,12 +187,12 @@ def run_reference(args, rank):
     times = [cpu_build(X)[1] for _ in range(args.steps)]
     total = sum(times)
     value = n * args.steps / total
-    sample = f"N={n} rows of the same 100-cluster mixture per step (bounded sample of the 1M workload)"
+    sample = f"the full workload: N={n} rows of the 100-cluster mixture per step"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_points": n, "threads": cores},
+        "config": bench_config(n, args.gpus),
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -366,7 +372,8 @@ def run_batched(args, world, rank, local_rank):
         dist.destroy_process_group()
 
 
-PREC_D, PREC_K, PREC_SAMPLE, PREC_PARITY_N = 960, 15, 4000, 20_000
+PREC_D, PREC_K, PREC_SAMPLE = 960, 15, 4000
+PREC_PARITY_SIZES = (20_000, 100_000)
 
 
 def run_precision(args, world, rank, local_rank):
@@ -466,38 +473,52 @@ def run_precision(args, world, rank, local_rank):
         L.check(L.lib.rinnd_free(h))
         forms[name] = entry
     # Recall on this distribution is low for any NN-Descent build (i.i.d. rows in
-    # 960 dimensions have little neighborhood structure); the restatement of the
-    # reference's CPU build on the first PREC_PARITY_N rows is the yardstick.
-    parity = None
-    if rank == 0 and not args.no_recall and n >= PREC_PARITY_N:
+    # 960 dimensions have little neighborhood structure, and less the more rows
+    # there are); the restatement of the reference's CPU build on the first
+    # n_s rows, for each n_s in PREC_PARITY_SIZES, is the yardstick: both builds
+    # see the same rows and are scored on the same seeded sample of them.
+    parity = []
+    if rank == 0 and not args.no_recall:
         import oracle
 
-        Xs_d = X[:PREC_PARITY_N].contiguous()
-        Xs = Xs_d.cpu().numpy()
-        Xsd = Xs_d.double()
-        dd = -(Xsd @ Xsd.T)
-        dd.fill_diagonal_(float("inf"))
-        truth_s = torch.topk(dd, PREC_K, dim=1, largest=False).indices.int().cpu().numpy()
-        del dd, Xsd
-        n_trees_s = int(min(max(np.floor(2.0 * np.log10(PREC_PARITY_N) + 0.5), 3), 12))
-        p = L.BuildParams()
-        L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
-        p.n_neighbors, p.distance_kind, p.correction, p.angular = PREC_K, L.DIST_ALT_COSINE, L.CORR_ALT_COSINE, 1
-        p.n_trees, p.random_seed, p.device = n_trees_s, 42, local_rank
-        h = ctypes.c_void_p()
-        L.check(L.lib.rinnd_build_device(ctypes.c_void_p(Xs_d.data_ptr()), PREC_PARITY_N, PREC_D, PREC_D,
-                                         ctypes.byref(p), ctypes.byref(h)))
-        ks = np.empty((PREC_PARITY_N, PREC_K), np.int32)
-        kds = np.empty((PREC_PARITY_N, PREC_K), np.float32)
-        L.check(L.lib.rinnd_neighbor_graph(h, L.ptr(ks), L.ptr(kds)))
-        L.check(L.lib.rinnd_free(h))
-        t0 = time.perf_counter()
-        ox = oracle.OracleIndex(Xs, n_neighbors=PREC_K, n_trees=n_trees_s, angular=True,
-                                distance_kind=oracle.ALT_COSINE, correction=oracle.CORR_ALT_COSINE)
-        t_oracle = time.perf_counter() - t0
-        ko = ox.neighbor_graph[0]
-        parity = {"n": PREC_PARITY_N, "gpu_recall@15": recall(ks, truth_s), "oracle_recall@15": recall(ko, truth_s),
-                  "oracle_build_s": t_oracle, "checker": "oracle/ C++ restatement of the reference's CPU build"}
+        for n_s in [m for m in PREC_PARITY_SIZES if m <= n]:
+            Xs_d = X[:n_s].contiguous()
+            Xs = Xs_d.cpu().numpy()
+            rows_s = np.sort(np.random.default_rng(11).choice(n_s, min(PREC_SAMPLE // 2, n_s), replace=False))
+            Xsd = Xs_d.double()
+            parts = []
+            for s0 in range(0, len(rows_s), 250):
+                r = torch.from_numpy(rows_s[s0:s0 + 250]).to(dev).long()
+                dd = -(Xsd[r] @ Xsd.T)
+                dd[torch.arange(len(r), device=dev), r] = float("inf")
+                parts.append(torch.topk(dd, PREC_K, dim=1, largest=False).indices.int().cpu().numpy())
+            truth_s = np.concatenate(parts)
+            del Xsd
+            n_trees_s = int(min(max(np.floor(2.0 * np.log10(n_s) + 0.5), 3), 12))
+            p = L.BuildParams()
+            L.check(L.lib.rinnd_params_default(ctypes.byref(p)))
+            p.n_neighbors, p.distance_kind, p.correction, p.angular = PREC_K, L.DIST_ALT_COSINE, L.CORR_ALT_COSINE, 1
+            p.n_trees, p.random_seed, p.device = n_trees_s, 42, local_rank
+            h = ctypes.c_void_p()
+            L.check(L.lib.rinnd_build_device(ctypes.c_void_p(Xs_d.data_ptr()), n_s, PREC_D, PREC_D,
+                                             ctypes.byref(p), ctypes.byref(h)))
+            ks = np.empty((n_s, PREC_K), np.int32)
+            kds = np.empty((n_s, PREC_K), np.float32)
+            L.check(L.lib.rinnd_neighbor_graph(h, L.ptr(ks), L.ptr(kds)))
+            inf_s = L.BuildInfo()
+            L.check(L.lib.rinnd_build_info_get(h, ctypes.byref(inf_s)))
+            L.check(L.lib.rinnd_free(h))
+            t0 = time.perf_counter()
+            ox = oracle.OracleIndex(Xs, n_neighbors=PREC_K, n_trees=n_trees_s, angular=True,
+                                    distance_kind=oracle.ALT_COSINE, correction=oracle.CORR_ALT_COSINE)
+            t_oracle = time.perf_counter() - t0
+            ko = ox.neighbor_graph[0]
+            parity.append({"n": n_s, "gpu_recall@15": recall(ks[rows_s], truth_s),
+                           "oracle_recall@15": recall(ko[rows_s], truth_s),
+                           "gpu_iterations": int(inf_s.iterations), "oracle_iterations": int(ox.iterations),
+                           "recall_sample": f"{len(rows_s)} seeded rows vs FP64 exact",
+                           "oracle_build_s": t_oracle, "checker": "oracle/ C++ restatement of the reference's CPU build"})
+            del ox
     if rank == 0:
         line = {
             "metric": "precision form: build points/s, recall@15 and distance error vs FP64 (1M x 960 cosine, k=15)",
@@ -512,7 +533,7 @@ def run_precision(args, world, rank, local_rank):
                        "timing": "host clock around the synchronized build call, max over ranks"},
             "forms": forms,
             "bf16_speedup_vs_fp32": forms["fp32"]["ms_per_build"] / forms["bf16"]["ms_per_build"],
-            "parity_small": parity,
+            "parity_by_size": parity,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -878,14 +899,6 @@ def main():
         qtruth = exact_knn_torch(X_dev, Q_dev, QK)
         quality["query_recall@10"] = recall(qi.cpu().numpy(), qtruth)
         quality["graph_recall_sample"] = f"{len(sample)} seeded rows vs FP64 exact"
-        if args.parity and rank == 0:
-            oix, odt = cpu_build(X)
-            oki, _ = oix.neighbor_graph
-            quality["oracle_graph_recall@30"] = recall(oki[sample], truth)
-            oqi, _ = oix.query(Q, k=QK, epsilon=EPS)
-            quality["oracle_query_recall@10"] = recall(oqi, qtruth)
-            quality["oracle_build_s"] = odt
-            quality["oracle_iterations"] = oix.iterations
     L.check(L.lib.rinnd_free(h))
 
     # ---- e2e: pinned host data -> build -> neighbor graph back to host ----
@@ -918,24 +931,33 @@ def main():
         e2e = {"value": n * world * args.steps / e_s, "unit": "points/s", "h2d_bytes_per_step": n * DIM * 4,
                "d2h_bytes_per_step": n * K * 8}
 
-    # ---- CPU baseline (rank 0, single GPU only) ----
+    # ---- CPU baseline (rank 0, single GPU only): the oracle builds the same
+    # full workload; its recall beside the GPU's is the parity check at scale ----
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         import oracle
 
-        m = min(n, CPU_SAMPLE)
-        _, dt = cpu_build(X[:m])
-        cpu = {"value": m / dt, "unit": "points/s", "cores": oracle.max_threads(), "kind": "port",
-               "sample": f"first {m} rows of this run's mixture, same k/trees/leaf/iters (oracle/ C++ restatement, OpenMP)"}
+        oix, dt = cpu_build(X)
+        cpu = {"value": n / dt, "unit": "points/s", "cores": oracle.max_threads(), "kind": "port",
+               "sample": f"the full workload: all {n} rows of this run's mixture, same k/trees/leaf/iters "
+                         "(oracle/ C++ restatement, OpenMP), one build"}
+        if not args.no_recall:
+            oki, _ = oix.neighbor_graph
+            quality["oracle_graph_recall@30"] = recall(oki[sample], truth)
+            oqi, _ = oix.query(Q, k=QK, epsilon=EPS)
+            quality["oracle_query_recall@10"] = recall(oqi, qtruth)
+            quality["oracle_iterations"] = oix.iterations
+            quality["parity_graph_recall_gap"] = quality["graph_recall@30"] - quality["oracle_graph_recall@30"]
+            quality["parity_query_recall_gap"] = quality["query_recall@10"] - quality["oracle_query_recall@10"]
+        del oix
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "points_per_rank": n, "parallelism": f"replicas{world}",
-                       "l2": "inputs (512 MB/rank) exceed L2 (126 MB); no flush",
-                       "iterations_per_build": [i.iterations for i in infos]},
+            "config": bench_config(n, world),
+            "iterations_per_build": [i.iterations for i in infos],
             "clocks": clk, "e2e": e2e, "gpu_launches": int(launches1.value - launches0.value),
             "roofline": roofline, "cpu_baseline": cpu,
             "precision": args.precision, "other_precision_form": other_form,

@@ -186,6 +186,18 @@ RINND_EXPORT int rinnd_search_graph(const rinnd_index* idx, int32_t* indptr, int
                        float* min_distance);
 /* Internal (search-layout) vertex order: vertex_order[internal] = original id (index.rs:679-715). */
 RINND_EXPORT int rinnd_vertex_order(const rinnd_index* idx, int32_t* out);
+/* export_search_tree (crates/rinnd/src/lib.rs:1105-1128, core/index.rs:145-154):
+ * the first retained RP tree in the reference's FlatTree layout, nodes numbered
+ * in depth-first preorder from the root (node 0): hyperplanes n_nodes x d
+ * (zeros for leaves), offsets n_nodes, children n_nodes x 2 (child node ids for
+ * an internal node, (-start, -end) into `indices` for a leaf), indices n leaf
+ * order in original ids.  `pivots` (n_nodes x 2, no counterpart in the
+ * reference) receives the two original points whose split gave each internal
+ * node its hyperplane (-1 for leaves).  Call with every array NULL to get
+ * *n_nodes first; any array may be NULL.  Fails with RINND_ERR_INVALID when the
+ * index retains no search tree (n_search_trees = 0). */
+RINND_EXPORT int rinnd_export_search_tree(rinnd_index* idx, int64_t* n_nodes, float* hyperplanes, float* offsets,
+                                          int32_t* children, int32_t* indices, int32_t* pivots);
 
 /* ---- int8 serving (crates/rinnd/src/lib.rs:159-416, core/index.rs:283-334) -- */
 /* Encodes the index rows (must be built with RINND_DIST_DIRECT_COSINE on

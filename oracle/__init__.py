@@ -83,6 +83,8 @@ def lib():
             "orc_normalize_rows": (None, [_P, _i64, _i32]),
             "orc_exact_knn_f64": (None, [ctypes.c_int, _P, _i64, _P, _i64, _i32, _i32, _i32, _P, _P]),
             "orc_max_threads": (_i32, []),
+            "orc_tree_hyperplane": (_f32, [_P, _P, _i32, _i32, _P]),
+            "orc_tree_route_points": (None, [_i32, _i32, _P, _P, _P, _P, _i64, _P]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -204,6 +206,26 @@ def tree_search_leaves(hyperplanes, offsets, children, point, seed, leaf_budget)
     nl = ctypes.c_int32(0)
     ev = lib().orc_tree_search_leaves(n_nodes, dim, _p(hp), _p(off), _p(ch), _p(pt), seed, leaf_budget, _p(out), ctypes.byref(nl))
     return int(ev), [(int(out[2 * i]), int(out[2 * i + 1])) for i in range(nl.value)]
+
+
+def tree_hyperplane(p1, p2, angular):
+    """(hyperplane, offset) of a split through p1, p2 (builder.rs:249-308)."""
+    p1, p2 = _f(p1), _f(p2)
+    hp = np.empty(p1.size, np.float32)
+    off = lib().orc_tree_hyperplane(_p(p1), _p(p2), p1.size, int(bool(angular)), _p(hp))
+    return hp, np.float32(off)
+
+
+def tree_route_points(hyperplanes, offsets, children, points):
+    """Leaf node each point reaches (budget-1 routing, flat_tree.rs:253-273);
+    -1 where a margin on its path is a tie (|m| < 1e-8)."""
+    hp = _f(hyperplanes)
+    off = _f(offsets)
+    ch = np.ascontiguousarray(children, np.int32)
+    pts = _f(points)
+    out = np.empty(pts.shape[0], np.int32)
+    lib().orc_tree_route_points(hp.shape[0], hp.shape[1], _p(hp), _p(off), _p(ch), _p(pts), pts.shape[0], _p(out))
+    return out
 
 
 def search_graph_from_knn(knn_idx, knn_dist, data, kind, mult=1.5):

@@ -650,6 +650,11 @@ struct TreeBuilder {  // builder.rs:138-348
     while (i2 == i1 && n > 1) i2 = rng.next_index(n);
     const float* p1 = data + (size_t)idx[i1] * dim;
     const float* p2 = data + (size_t)idx[i2] * dim;
+    return split_hyperplane(p1, p2, dim, angular, hp.data());
+  }
+  // builder.rs:249-308: the hyperplane of two split points (euclidean
+  // perpendicular bisector, or angular difference of the normalized points)
+  static float split_hyperplane(const float* p1, const float* p2, size_t dim, bool angular, float* hp) {
     if (angular) {  // :281-308
       float n1 = 0.f, n2 = 0.f;
       for (size_t i = 0; i < dim; ++i) n1 += p1[i] * p1[i];
@@ -657,7 +662,7 @@ struct TreeBuilder {  // builder.rs:138-348
       n1 = std::sqrt(n1);
       n2 = std::sqrt(n2);
       if (n1 < 1e-8f || n2 < 1e-8f) {
-        std::fill(hp.begin(), hp.end(), 0.f);
+        std::fill(hp, hp + dim, 0.f);
         return 0.f;
       }
       for (size_t i = 0; i < dim; ++i) hp[i] = p2[i] / n2 - p1[i] / n1;
@@ -1419,6 +1424,34 @@ int32_t orc_tree_search_leaves(int32_t n_nodes, int32_t dim, const float* hyperp
   }
   *n_leaves = (int32_t)leaves.size();
   return ev;
+}
+
+float orc_tree_hyperplane(const float* p1, const float* p2, int32_t dim, int32_t angular, float* hp) {
+  return TreeBuilder::split_hyperplane(p1, p2, (size_t)dim, angular != 0, hp);
+}
+
+// flat_tree.rs:253-273 (leaf budget 1) for many points: the side of every node
+// is margin > 0 (margin = dot_a + offset, builder.rs:331); a margin with
+// |m| < 1e-8 is a random side in the reference, reported here as a tie
+// (leaf_node = -1) instead of drawn.
+void orc_tree_route_points(int32_t n_nodes, int32_t dim, const float* hyperplanes, const float* offsets,
+                           const int32_t* children, const float* points, int64_t n, int32_t* leaf_node) {
+  (void)n_nodes;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    const float* x = points + (size_t)i * (size_t)dim;
+    size_t node = 0;
+    int32_t out = 0;
+    while (children[2 * node] > 0) {
+      const float margin = dot_a(x, hyperplanes + node * (size_t)dim, dim) + offsets[node];
+      if (std::fabs(margin) < 1e-8f) {
+        out = -1;
+        break;
+      }
+      node = (size_t)children[2 * node + (margin > 0.f ? 1 : 0)];
+    }
+    leaf_node[i] = out < 0 ? -1 : (int32_t)node;
+  }
 }
 
 int64_t orc_search_graph_from_knn(const int32_t* knn_idx, const float* knn_dist, const float* data,

@@ -112,6 +112,13 @@ int32_t orc_tree_search_leaves(int32_t n_nodes, int32_t dim, const float* hyperp
                                const float* point, uint64_t seed, int32_t leaf_budget,
                                int32_t* out_leaves, int32_t* n_leaves);
 
+/* Hyperplane and offset of a split through points p1, p2 (builder.rs:249-308). */
+float orc_tree_hyperplane(const float* p1, const float* p2, int32_t dim, int32_t angular, float* hp);
+/* Leaf node reached by each of n points under the budget-1 routing rule
+ * (flat_tree.rs:253-273); -1 where a margin on the path is a tie (|m| < 1e-8). */
+void orc_tree_route_points(int32_t n_nodes, int32_t dim, const float* hyperplanes, const float* offsets,
+                           const int32_t* children, const float* points, int64_t n, int32_t* leaf_node);
+
 /* ---- search graph (search_graph.rs:263-567) ----------------------------- */
 /* From a sorted dense kNN graph: returns nnz; indptr[n+1], indices[cap]. */
 int64_t orc_search_graph_from_knn(const int32_t* knn_idx, const float* knn_dist,

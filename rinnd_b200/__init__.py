@@ -303,6 +303,24 @@ class RINND:
         L.check(L.lib.rinnd_vertex_order(self._h, L.ptr(out)))
         return out
 
+    def export_search_tree(self, with_pivots=False):
+        """The first retained RP tree in original id space (lib.rs:1105-1128):
+        (hyperplanes float32[n_nodes, dim], offsets float32[n_nodes],
+        children int32[n_nodes, 2], leaf_indices int32[N]).  With
+        ``with_pivots`` a fifth array int32[n_nodes, 2] holds the two points
+        whose split defined each internal node (-1 for leaves)."""
+        m = ctypes.c_int64(0)
+        L.check(L.lib.rinnd_export_search_tree(self._h, ctypes.byref(m), None, None, None, None, None))
+        n = m.value
+        hp = np.empty((n, self.dim), np.float32)
+        off = np.empty(n, np.float32)
+        ch = np.empty((n, 2), np.int32)
+        ind = np.empty(self.n_points, np.int32)
+        piv = np.empty((n, 2), np.int32) if with_pivots else None
+        L.check(L.lib.rinnd_export_search_tree(self._h, None, L.ptr(hp), L.ptr(off), L.ptr(ch), L.ptr(ind),
+                                               L.ptr(piv) if with_pivots else None))
+        return (hp, off, ch, ind, piv) if with_pivots else (hp, off, ch, ind)
+
     def search_stats(self, reset=False) -> dict:
         """Distance evaluations, node expansions and visited-table overflows of
         the searches since the build (or the last reset)."""

@@ -91,6 +91,7 @@ SIGNATURES = {
     "rinnd_search_graph_nnz": (ctypes.c_int, [_P, _P]),
     "rinnd_search_graph": (ctypes.c_int, [_P, _P, _P, _P]),
     "rinnd_vertex_order": (ctypes.c_int, [_P, _P]),
+    "rinnd_export_search_tree": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "rinnd_quantize": (ctypes.c_int, [_P, _i32]),
     "rinnd_query_quantized": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _i32, _i32, _P, _P]),
     "rinnd_quantize_rows": (ctypes.c_int, [_P, _i64, _i32, _i32, _P, _P, _P]),

@@ -775,6 +775,79 @@ int rinnd_vertex_order(const rinnd_index* idx, int32_t* out) {
   });
 }
 
+int rinnd_export_search_tree(rinnd_index* idx, int64_t* n_nodes, float* hyperplanes, float* offsets,
+                             int32_t* children, int32_t* indices, int32_t* pivots) {
+  return guarded([&] {
+    check_index(idx);
+    require(idx->n_search_trees >= 1, "no retained search tree is available");
+    std::lock_guard<std::mutex> lock(idx->mu);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    cudaStream_t st = idx->st;
+    const Forest& f = idx->forest;
+    const size_t total = (size_t)f.n_nodes;
+    std::vector<int32_t> ch(2 * total);
+    f.children.to_host(ch.data(), 2 * total);
+    RINND_CUDA(cudaStreamSynchronize(st));
+    // the first tree (root node 0) in depth-first preorder, the reference's node
+    // numbering (tree/builder.rs:172-226 assigns ids on entry, left subtree first)
+    std::vector<int32_t> order;
+    std::vector<int32_t> local(total, -1);
+    std::vector<int32_t> stack{0};
+    while (!stack.empty()) {
+      const int32_t g = stack.back();
+      stack.pop_back();
+      local[(size_t)g] = (int32_t)order.size();
+      order.push_back(g);
+      if (ch[2 * (size_t)g] > 0) {
+        stack.push_back(ch[2 * (size_t)g + 1]);
+        stack.push_back(ch[2 * (size_t)g]);
+      }
+    }
+    const size_t m = order.size();
+    if (n_nodes) *n_nodes = (int64_t)m;
+    if (!hyperplanes && !offsets && !children && !indices && !pivots) return;
+    if (children)
+      for (size_t i = 0; i < m; ++i) {
+        const size_t g = (size_t)order[i];
+        const bool leaf = ch[2 * g] <= 0;
+        children[2 * i] = leaf ? ch[2 * g] : local[(size_t)ch[2 * g]];
+        children[2 * i + 1] = leaf ? ch[2 * g + 1] : local[(size_t)ch[2 * g + 1]];
+      }
+    if (offsets || pivots) {
+      std::vector<float> off(total);
+      std::vector<int32_t> pv(2 * total);
+      f.offsets.to_host(off.data(), total);
+      f.pivots.to_host(pv.data(), 2 * total);
+      RINND_CUDA(cudaStreamSynchronize(st));
+      for (size_t i = 0; i < m; ++i) {
+        const size_t g = (size_t)order[i];
+        if (offsets) offsets[i] = off[g];
+        if (pivots) {
+          pivots[2 * i] = pv[2 * g];
+          pivots[2 * i + 1] = pv[2 * g + 1];
+        }
+      }
+    }
+    if (hyperplanes) {
+      DVec<int32_t> ord(m, st);
+      ord.from_host(order.data(), m);
+      DVec<float> rows(m * (size_t)idx->Dp, st);
+      gather_rows(f.hyperplanes.p, ord.p, (int64_t)m, idx->Dp, rows.p, st);
+      RINND_CUDA(cudaMemcpy2DAsync(hyperplanes, sizeof(float) * idx->D, rows.p, sizeof(float) * idx->Dp,
+                                   sizeof(float) * idx->D, m, cudaMemcpyDeviceToHost, st));
+      RINND_CUDA(cudaStreamSynchronize(st));
+    }
+    if (indices) {  // leaf order of the first tree in original ids (index.rs:145-154)
+      const size_t N = (size_t)idx->N;
+      std::vector<int32_t> ti(N), vo(N);
+      idx->tree_idx.to_host(ti.data(), N);
+      idx->vertex_order.to_host(vo.data(), N);
+      RINND_CUDA(cudaStreamSynchronize(st));
+      for (size_t i = 0; i < N; ++i) indices[i] = vo[(size_t)ti[i]];
+    }
+  });
+}
+
 int rinnd_storage_info_get(const rinnd_index* idx, rinnd_storage_info* info) {
   return guarded([&] {
     check_index(idx);

@@ -23,6 +23,7 @@ struct Forest {
   DVec<int32_t> children;     // 2 * n_nodes
   DVec<float> offsets;        // n_nodes
   DVec<float> hyperplanes;    // n_nodes * Dp (zeros for leaves)
+  DVec<int32_t> pivots;       // 2 * n_nodes: the two points whose split is the node's hyperplane (-1: leaf)
   DVec<int4> leaves;          // (tree, start, end, node)
   int64_t n_nodes = 0;
   int64_t n_leaves = 0;

@@ -34,7 +34,8 @@ __global__ void k_init_perm(int32_t* perm, int N, int T) {
 
 // builder.rs:228-308 make_split (+ euclidean / angular hyperplanes).
 __global__ void k_split_params(const Seg* segs, int S, const int32_t* perm, int N, const float* X,
-                               int D, int Dp, bool angular, uint64_t seed, float* hp, float* off) {
+                               int D, int Dp, bool angular, uint64_t seed, float* hp, float* off,
+                               int32_t* piv) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S) return;
   Seg g = segs[s];
@@ -48,6 +49,8 @@ __global__ void k_split_params(const Seg* segs, int S, const int32_t* perm, int 
   if (i2 == i1 && size > 1) i2 = (i1 + 1) % size;
   const float* p1 = X + (size_t)P[i1] * Dp;
   const float* p2 = X + (size_t)P[i2] * Dp;
+  piv[2 * s] = P[i1];
+  piv[2 * s + 1] = P[i2];
   float* H = hp + (size_t)s * Dp;
   float o = 0.f;
   if (angular) {
@@ -192,9 +195,11 @@ __global__ void k_outcome(const Seg* segs, int S, const long long* gs, const int
 }
 
 __device__ __forceinline__ void emit_leaf(int tree, int start, int end, int node, int32_t* children,
-                                          float* offsets, int4* leaves,
+                                          float* offsets, int32_t* pivots, int4* leaves,
                                           unsigned long long* counters) {
   offsets[node] = 0.f;
+  pivots[2 * (size_t)node] = -1;
+  pivots[2 * (size_t)node + 1] = -1;
   children[2 * (size_t)node] = -start;
   children[2 * (size_t)node + 1] = -end;
   unsigned long long li = atomicAdd(&counters[0], 1ull);
@@ -204,16 +209,16 @@ __device__ __forceinline__ void emit_leaf(int tree, int start, int end, int node
 
 __global__ void k_finalize(const Seg* segs, int S, const int32_t* nleft, const int32_t* next_off,
                            const int32_t* node_off, long long node_base, const float* hp,
-                           const float* off, int Dp, int leaf_size, int depth, int max_depth,
-                           int32_t* children, float* offsets, float* hyperplanes, Seg* next,
-                           int4* leaves, unsigned long long* counters) {
+                           const float* off, const int32_t* piv, int Dp, int leaf_size, int depth,
+                           int max_depth, int32_t* children, float* offsets, float* hyperplanes,
+                           int32_t* pivots, Seg* next, int4* leaves, unsigned long long* counters) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S) return;
   Seg g = segs[s];
   int size = g.end - g.start;
   int nl = nleft[s];
   if (!(nl > 0 && nl < size)) {  // builder.rs:198-210 degenerate split -> leaf
-    emit_leaf(g.tree, g.start, g.end, g.node, children, offsets, leaves, counters);
+    emit_leaf(g.tree, g.start, g.end, g.node, children, offsets, pivots, leaves, counters);
     return;
   }
   int c0 = (int)(node_base + node_off[s]);
@@ -221,6 +226,8 @@ __global__ void k_finalize(const Seg* segs, int S, const int32_t* nleft, const i
   children[2 * (size_t)g.node] = c0;
   children[2 * (size_t)g.node + 1] = c1;
   offsets[g.node] = off[s];
+  pivots[2 * (size_t)g.node] = piv[2 * s];
+  pivots[2 * (size_t)g.node + 1] = piv[2 * s + 1];
   const float4* src = reinterpret_cast<const float4*>(hp + (size_t)s * Dp);
   float4* dst = reinterpret_cast<float4*>(hyperplanes + (size_t)g.node * Dp);
   for (int i = 0; i < Dp / 4; ++i) dst[i] = src[i];
@@ -231,16 +238,16 @@ __global__ void k_finalize(const Seg* segs, int S, const int32_t* nleft, const i
     if (sz > leaf_size && depth + 1 < max_depth) {
       next[o++] = Seg{g.tree, cs[j], ce[j], cid[j]};
     } else {
-      emit_leaf(g.tree, cs[j], ce[j], cid[j], children, offsets, leaves, counters);
+      emit_leaf(g.tree, cs[j], ce[j], cid[j], children, offsets, pivots, leaves, counters);
     }
   }
 }
 
-__global__ void k_root_leaves(int T, int N, int32_t* children, float* offsets, int4* leaves,
+__global__ void k_root_leaves(int T, int N, int32_t* children, float* offsets, int32_t* pivots, int4* leaves,
                               unsigned long long* counters) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= T) return;
-  emit_leaf(t, 0, N, t, children, offsets, leaves, counters);
+  emit_leaf(t, 0, N, t, children, offsets, pivots, leaves, counters);
 }
 
 template <class T>
@@ -271,6 +278,7 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
   size_t node_cap = (size_t)T * 64;
   f.children.alloc(2 * node_cap, st);
   f.offsets.alloc(node_cap, st);
+  f.pivots.alloc(2 * node_cap, st);
   f.hyperplanes.alloc(node_cap * (size_t)Dp, st);
   f.hyperplanes.fill_bytes(0);
   f.n_nodes = T;
@@ -283,7 +291,7 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
   if (N > leaf_size && max_depth > 0) {
     for (int t = 0; t < T; ++t) h_roots.push_back(Seg{t, 0, N, t});
   } else {
-    k_root_leaves<<<1, 32, 0, st>>>(T, N, f.children.p, f.offsets.p, f.leaves.p, counters.p);
+    k_root_leaves<<<1, 32, 0, st>>>(T, N, f.children.p, f.offsets.p, f.pivots.p, f.leaves.p, counters.p);
     RINND_LAUNCH_CHECK();
   }
   int S = (int)h_roots.size();
@@ -298,8 +306,9 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
     DVec<long long> gs((size_t)S, st), ge((size_t)S, st);
     k_seg_bounds<<<grid_for(S, 256), 256, 0, st>>>(segs.p, S, N, gs.p, ge.p);
     DVec<float> hp((size_t)S * Dp, st), off((size_t)S, st);
+    DVec<int32_t> piv(2 * (size_t)S, st);
     k_split_params<<<grid_for(S, 128), 128, 0, st>>>(segs.p, S, f.perm.p, N, X, D, Dp, angular,
-                                                     seed, hp.p, off.p);
+                                                     seed, hp.p, off.p, piv.p);
     RINND_LAUNCH_CHECK();
     RINND_CUDA(cudaMemsetAsync(seg_of.p, 0xFF, sizeof(int32_t) * (size_t)total, st));
     k_fill_segmap<<<std::min(S, 148 * 16), 256, 0, st>>>(gs.p, ge.p, S, seg_of.p);
@@ -337,6 +346,7 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
     if (need_nodes > f.offsets.n) {
       f.children.grow(2 * need_nodes, 2 * (size_t)f.n_nodes, st);
       f.offsets.grow(need_nodes, (size_t)f.n_nodes, st);
+      f.pivots.grow(2 * need_nodes, 2 * (size_t)f.n_nodes, st);
       f.hyperplanes.grow(f.offsets.n * (size_t)Dp, (size_t)f.n_nodes * Dp, st);
       RINND_CUDA(cudaMemsetAsync(f.hyperplanes.p + (size_t)f.n_nodes * Dp, 0,
                                  sizeof(float) * (f.hyperplanes.n - (size_t)f.n_nodes * Dp), st));
@@ -345,9 +355,9 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
     if (need_leaves > f.leaves.n) f.leaves.grow(need_leaves, (size_t)h_counters[0], st);
     DVec<Seg> next((size_t)std::max(S_next, 1), st);
     k_finalize<<<grid_for(S, 128), 128, 0, st>>>(segs.p, S, nleft.p, next_off.p, node_off.p,
-                                                 f.n_nodes, hp.p, off.p, Dp, leaf_size, depth,
+                                                 f.n_nodes, hp.p, off.p, piv.p, Dp, leaf_size, depth,
                                                  max_depth, f.children.p, f.offsets.p,
-                                                 f.hyperplanes.p, next.p, f.leaves.p, counters.p);
+                                                 f.hyperplanes.p, f.pivots.p, next.p, f.leaves.p, counters.p);
     RINND_LAUNCH_CHECK();
     f.n_nodes += new_nodes;
     segs = std::move(next);

@@ -171,3 +171,25 @@ def test_normalize_rows_sequential_sum(orc):
     inv = np.float32(1.0) / np.sqrt(nsq)
     want = np.where((nsq <= np.float32(1e-12))[:, None], X, X * inv[:, None])
     np.testing.assert_array_equal(out.view(np.uint32), want.astype(np.float32).view(np.uint32))
+
+
+def test_tree_hyperplane_known_answers(orc):
+    """builder.rs:249-308 on hand-checked points: the euclidean split of (0,0)
+    and (2,0) is the bisector x = 1 (normal (1,0), offset -1); the angular split
+    of (1,0) and (0,1) is normal (-1,1)/sqrt(2) with offset 0; coincident or
+    zero points give the zero hyperplane."""
+    hp, off = orc.tree_hyperplane([0.0, 0.0], [2.0, 0.0], angular=False)
+    assert hp.tolist() == [1.0, 0.0] and off == -1.0
+    hp, off = orc.tree_hyperplane([1.0, 0.0], [0.0, 1.0], angular=True)
+    r = np.float32(1.0) / np.sqrt(np.float32(2.0))
+    assert np.allclose(hp, [-r, r], atol=1e-7) and off == 0.0
+    hp, off = orc.tree_hyperplane([3.0, 4.0], [3.0, 4.0], angular=False)
+    assert hp.tolist() == [0.0, 0.0] and off == 0.0
+    hp, off = orc.tree_hyperplane([0.0, 0.0], [1.0, 1.0], angular=True)
+    assert hp.tolist() == [0.0, 0.0] and off == 0.0
+    # routing by margin sign: the side of x = 1
+    hyperplanes = np.array([[1.0, 0.0], [0.0, 0.0], [0.0, 0.0]], np.float32)
+    offsets = np.array([-1.0, 0.0, 0.0], np.float32)
+    children = np.array([[1, 2], [0, -1], [-1, -2]], np.int32)
+    pts = np.array([[0.0, 5.0], [3.0, -1.0], [1.0, 0.0]], np.float32)
+    assert orc.tree_route_points(hyperplanes, offsets, children, pts).tolist() == [1, 2, -1]
