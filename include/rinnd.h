@@ -59,6 +59,11 @@ extern "C" {
 #define RINND_Q8_PER_VECTOR_COSINE 0  /* "int8"  */
 #define RINND_Q8_GLOBAL_SYMMETRIC 1   /* "sq8u"  */
 #define RINND_Q8_PER_VECTOR_SYMMETRIC 2 /* "sq8p" */
+/* "sq8d" (no counterpart in the reference's encoders): one symmetric scale per
+ * dimension, scale_j = max_i |x_ij| / 127 over the index rows, code =
+ * clamp(round(x / scale_j), +-127); the search similarity is the reference's
+ * quantized_i8_per_dimension_dot (core/distance/quantized.rs:42-56). */
+#define RINND_Q8_PER_DIMENSION 3
 
 /* Local-join tile arithmetic (no counterpart in the reference, whose join is FP32):
  * FP32 evaluates every candidate pair in FP32; BF16 filters the pairs with BF16
@@ -74,7 +79,7 @@ typedef struct rinnd_build_params {
   int32_t n_neighbors;              /* default 30                                  */
   int32_t n_trees;                  /* default 8                                   */
   int32_t n_search_trees;           /* default 1                                   */
-  int32_t search_tree_leaf_budget;  /* default 1 (only 1 is implemented)           */
+  int32_t search_tree_leaf_budget;  /* default 1; leaves seeded per search tree (<= 256) */
   int32_t leaf_size;                /* <= 0: clamp(5k, 60, 256)  (index.rs:617-619) */
   int32_t max_candidates;           /* <= 0: min(k, 60)          (index.rs:620-622) */
   int32_t n_iters;                  /* <= 0: max(5, ceil(log2 N)) (index.rs:623-625) */
@@ -208,6 +213,28 @@ RINND_EXPORT int rinnd_quantize(rinnd_index* idx, int32_t encoding);
 RINND_EXPORT int rinnd_query_quantized(rinnd_index* idx, const float* queries, int64_t nq, int32_t k,
                           float epsilon, int32_t candidate_width, int32_t rerank_width,
                           int32_t* out_idx, float* out_dist);
+/* tree_quantization="int8" (crates/rinnd/src/lib.rs:681-704, QuantizedFlatTree
+ * core/tree/flat_tree.rs:35-183): int8 codes and one scale per node of the
+ * search trees' hyperplanes; quantized queries then route with the
+ * reconstructed margin dot(codes) * scale * tree_query_scale + offset.  Needs a
+ * quantized index with a per-vector encoding (int8 or sq8p). */
+RINND_EXPORT int rinnd_quantize_trees(rinnd_index* idx);
+/* retain_fp32_data=False (lib.rs:712-716): frees the FP32 rows of a quantized
+ * index; afterwards FP32 queries and exact reranks fail with RINND_ERR_INVALID. */
+RINND_EXPORT int rinnd_release_fp32(rinnd_index* idx);
+/* FlatTree::search_leaves (flat_tree.rs:239-311) of retained tree `tree` for nq
+ * host queries (normalized like the index's queries) with the search kernel's
+ * routing: up to `budget` leaves per query as (start, end) ranges into the
+ * tree's leaf order (out_leaves, nq x budget x 2) and their count (out_counts).
+ * quantized != 0 routes the queries' int8 codes over the int8 routing trees.
+ * Tied margins (|m| < 1e-8) take a side from the query's search stream. */
+RINND_EXPORT int rinnd_tree_search_leaves(rinnd_index* idx, const float* queries, int64_t nq, int32_t tree,
+                                          int32_t budget, int32_t quantized, int32_t* out_leaves,
+                                          int32_t* out_counts);
+/* Per-dimension encoder (RINND_Q8_PER_DIMENSION) for host rows (n x d f32):
+ * codes (n x d int8) and the d per-dimension scales. */
+RINND_EXPORT int rinnd_quantize_rows_per_dimension(const float* data, int64_t n, int32_t d, int8_t* codes,
+                                                   float* dim_scales);
 /* Row encoder of QuantizedI8Index::new (lib.rs:159-223) on the GPU for host rows
  * (n x d f32): codes (n x d int8), per-row scales (inv_norms) and the global
  * multiplier 127 / max|x|. */
@@ -266,7 +293,10 @@ typedef struct rinnd_storage_info {
   char encoding[32];
   int64_t code_bytes, metadata_bytes, retained_fp32_bytes;
   double encode_seconds;
-  int64_t device_bytes;
+  int64_t device_bytes;           /* device memory the index holds (no counterpart) */
+  /* quantized_tree_storage_info / released bytes (lib.rs:1037-1061) */
+  int64_t tree_code_bytes, tree_scale_bytes, tree_offset_bytes, tree_topology_bytes;
+  int64_t released_fp32_tree_bytes, released_fp32_data_bytes, retained_fp32_tree_topology_bytes;
 } rinnd_storage_info;
 RINND_EXPORT int rinnd_storage_info_get(const rinnd_index* idx, rinnd_storage_info* info);
 

@@ -84,7 +84,12 @@ def lib():
             "orc_exact_knn_f64": (None, [ctypes.c_int, _P, _i64, _P, _i64, _i32, _i32, _i32, _P, _P]),
             "orc_max_threads": (_i32, []),
             "orc_tree_hyperplane": (_f32, [_P, _P, _i32, _i32, _P]),
+            "orc_quantize_per_dimension": (None, [_P, _i64, _i32, _P, _P]),
+            "orc_quantize_queries_per_dimension": (None, [_P, _i64, _i32, _P, _P]),
             "orc_tree_route_points": (None, [_i32, _i32, _P, _P, _P, _P, _i64, _P]),
+            "orc_quantize_tree_hyperplanes": (None, [_i32, _i32, _P, _P, _P]),
+            "orc_tree_search_leaves_quantized": (_i32, [_i32, _i32, _P, _P, _P, _P, _f32, _u64, _i32, _P, _P]),
+            "orc_query_quantized_trees": (_i32, [_P, _P, _i64, _i32, _f32, _i32, _i32, _i32, _i32, _P, _P]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -208,6 +213,30 @@ def tree_search_leaves(hyperplanes, offsets, children, point, seed, leaf_budget)
     return int(ev), [(int(out[2 * i]), int(out[2 * i + 1])) for i in range(nl.value)]
 
 
+def quantize_tree_hyperplanes(hyperplanes):
+    """QuantizedFlatTree codes and per-node scales (flat_tree.rs:47-64)."""
+    hp = _f(hyperplanes)
+    codes = np.empty(hp.shape, np.int8)
+    scales = np.empty(hp.shape[0], np.float32)
+    lib().orc_quantize_tree_hyperplanes(hp.shape[0], hp.shape[1], _p(hp), _p(codes), _p(scales))
+    return codes, scales
+
+
+def tree_search_leaves_quantized(hyperplanes, offsets, children, qcodes, qscale, seed, leaf_budget):
+    """QuantizedFlatTree::search_leaves (flat_tree.rs:106-183) on the int8 form of
+    an FP32 tree, for a query's int8 codes and tree_query_scale."""
+    hp = _f(hyperplanes)
+    off = _f(offsets)
+    ch = np.ascontiguousarray(children, np.int32)
+    qc = np.ascontiguousarray(qcodes, np.int8)
+    n_nodes, dim = hp.shape
+    out = np.empty(2 * max(leaf_budget, 1), np.int32)
+    nl = ctypes.c_int32(0)
+    ev = lib().orc_tree_search_leaves_quantized(n_nodes, dim, _p(hp), _p(off), _p(ch), _p(qc), float(qscale), seed,
+                                                leaf_budget, _p(out), ctypes.byref(nl))
+    return int(ev), [(int(out[2 * i]), int(out[2 * i + 1])) for i in range(nl.value)]
+
+
 def tree_hyperplane(p1, p2, angular):
     """(hyperplane, offset) of a split through p1, p2 (builder.rs:249-308)."""
     p1, p2 = _f(p1), _f(p2)
@@ -284,6 +313,25 @@ def quantize_queries(queries, encoding, global_mult):
     scales = np.empty(n, np.float32)
     lib().orc_quantize_queries(_p(queries), n, d, encoding, global_mult, _p(codes), _p(scales))
     return codes, scales
+
+
+def quantize_per_dimension(data):
+    """Per-dimension symmetric int8 codes and the per-dimension scales."""
+    data = _f(data)
+    n, d = data.shape
+    codes = np.empty((n, d), np.int8)
+    scales = np.empty(d, np.float32)
+    lib().orc_quantize_per_dimension(_p(data), n, d, _p(codes), _p(scales))
+    return codes, scales
+
+
+def quantize_queries_per_dimension(queries, dim_scales):
+    queries = _f(queries)
+    n, d = queries.shape
+    codes = np.empty((n, d), np.int8)
+    sc = _f(dim_scales)
+    lib().orc_quantize_queries_per_dimension(_p(queries), n, d, _p(sc), _p(codes))
+    return codes
 
 
 def normalize_rows(data):
@@ -380,13 +428,14 @@ class OracleIndex:
         lib().orc_query_one(self._h, _p(q), k, epsilon, _p(idx), _p(dist))
         return idx, dist
 
-    def query_quantized(self, queries, k=10, epsilon=0.1, encoding=0, candidate_width=0, rerank_width=0):
+    def query_quantized(self, queries, k=10, epsilon=0.1, encoding=0, candidate_width=0, rerank_width=0,
+                        quantize_trees=False):
         q = _f(queries)
         nq = q.shape[0]
         idx = np.empty((nq, k), np.int32)
         dist = np.empty((nq, k), np.float32)
-        rc = lib().orc_query_quantized(self._h, _p(q), nq, k, epsilon, encoding, candidate_width, rerank_width,
-                                       _p(idx), _p(dist))
+        rc = lib().orc_query_quantized_trees(self._h, _p(q), nq, k, epsilon, encoding, candidate_width, rerank_width,
+                                             int(bool(quantize_trees)), _p(idx), _p(dist))
         if rc != 0:
             raise ValueError("invalid quantized widths")
         return idx, dist

@@ -558,13 +558,22 @@ struct FlatTree {
   // flat_tree.rs:239-311 search_leaves
   int search_leaves(const float* point, FastRng& rng, size_t budget,
                     std::vector<std::pair<size_t, size_t>>& leaves) const {
+    return search_leaves_with(
+        [&](size_t node) { return dot_a(point, &hyperplanes[node * dim], (int)dim) + offsets[node]; }, rng, budget,
+        leaves);
+  }
+  // search_leaves with the node margin given by `margin` (FP32 hyperplanes
+  // above; the int8 routing tree's reconstructed margin, flat_tree.rs:96-183)
+  template <class M>
+  int search_leaves_with(M&& margin_of, FastRng& rng, size_t budget,
+                         std::vector<std::pair<size_t, size_t>>& leaves) const {
     leaves.clear();
     if (n_nodes == 0 || budget == 0) return 0;
     int evals = 0;
     if (budget == 1) {
       size_t node = 0;
       while (children[2 * node] > 0) {
-        float margin = dot_a(point, &hyperplanes[node * dim], (int)dim) + offsets[node];
+        float margin = margin_of(node);
         ++evals;
         size_t side = std::fabs(margin) < 1e-8f ? (size_t)rng.next_bool() : (size_t)(margin > 0.f);
         node = (size_t)children[2 * node + side];
@@ -592,7 +601,7 @@ struct FlatTree {
         leaves.push_back({(size_t)(-children[2 * node]), (size_t)(-children[2 * node + 1])});
         continue;
       }
-      float margin = dot_a(point, &hyperplanes[node * dim], (int)dim) + offsets[node];
+      float margin = margin_of(node);
       ++evals;
       size_t side = std::fabs(margin) < 1e-8f ? (size_t)rng.next_bool() : (size_t)(margin > 0.f);
       frontier.push_back({pr.first, (size_t)children[2 * node + side]});
@@ -707,6 +716,30 @@ struct TreeBuilder {  // builder.rs:138-348
     return left;
   }
 };
+
+// flat_tree.rs:47-64 QuantizedFlatTree::quantize_hyperplanes: per node scale =
+// max|h| / 127 (0 for zero hyperplanes, leaves included), code =
+// (h / scale).round().clamp(-127, 127).
+static void quantize_hyperplanes(const float* hp, size_t n_nodes, size_t dim, int8_t* codes, float* scales) {
+  for (size_t v = 0; v < n_nodes; ++v) {
+    const float* h = hp + v * dim;
+    float mx = 0.f;
+    for (size_t j = 0; j < dim; ++j) mx = std::max(mx, std::fabs(h[j]));
+    const float sc = mx > 0.f ? mx / 127.0f : 0.f;
+    scales[v] = sc;
+    for (size_t j = 0; j < dim; ++j) {
+      float c = sc > 0.f ? std::round(h[j] / sc) : 0.f;
+      if (c != c) c = 0.f;
+      codes[v * dim + j] = (int8_t)std::min(std::max(c, -127.0f), 127.0f);
+    }
+  }
+}
+
+// flat_tree.rs:96-103 QuantizedFlatTree::margin: ((dot as f32) * scale) * query_scale + offset.
+static inline float quantized_margin(const int8_t* codes, const float* scales, const float* offsets, size_t dim,
+                                     size_t node, const int8_t* q, float qscale) {
+  return (float)i8_dot(codes + node * dim, q, (int)dim) * scales[node] * qscale + offsets[node];
+}
 
 // builder.rs:72-86 build_rp_tree
 static FlatTree build_rp_tree(const float* data, size_t n, size_t dim, size_t leaf_size,
@@ -1426,6 +1459,38 @@ int32_t orc_tree_search_leaves(int32_t n_nodes, int32_t dim, const float* hyperp
   return ev;
 }
 
+int32_t orc_tree_search_leaves_quantized(int32_t n_nodes, int32_t dim, const float* hyperplanes,
+                                         const float* offsets, const int32_t* children, const int8_t* qcodes,
+                                         float qscale, uint64_t seed, int32_t leaf_budget, int32_t* out_leaves,
+                                         int32_t* n_leaves) {
+  FlatTree t;
+  t.dim = (size_t)dim;
+  t.n_nodes = (size_t)n_nodes;
+  t.offsets.assign(offsets, offsets + n_nodes);
+  t.children.assign(children, children + 2 * (size_t)n_nodes);
+  std::vector<int8_t> codes((size_t)n_nodes * (size_t)dim);
+  std::vector<float> scales((size_t)n_nodes);
+  quantize_hyperplanes(hyperplanes, (size_t)n_nodes, (size_t)dim, codes.data(), scales.data());
+  FastRng rng(seed);
+  std::vector<std::pair<size_t, size_t>> leaves;
+  int ev = t.search_leaves_with(
+      [&](size_t node) {
+        return quantized_margin(codes.data(), scales.data(), t.offsets.data(), (size_t)dim, node, qcodes, qscale);
+      },
+      rng, (size_t)leaf_budget, leaves);
+  for (size_t i = 0; i < leaves.size(); ++i) {
+    out_leaves[2 * i] = (int32_t)leaves[i].first;
+    out_leaves[2 * i + 1] = (int32_t)leaves[i].second;
+  }
+  *n_leaves = (int32_t)leaves.size();
+  return ev;
+}
+
+void orc_quantize_tree_hyperplanes(int32_t n_nodes, int32_t dim, const float* hyperplanes, int8_t* codes,
+                                   float* scales) {
+  quantize_hyperplanes(hyperplanes, (size_t)n_nodes, (size_t)dim, codes, scales);
+}
+
 float orc_tree_hyperplane(const float* p1, const float* p2, int32_t dim, int32_t angular, float* hp) {
   return TreeBuilder::split_hyperplane(p1, p2, (size_t)dim, angular != 0, hp);
 }
@@ -1679,6 +1744,33 @@ void orc_quantize_queries(const float* queries, int64_t nq, int32_t dim, int32_t
   }
 }
 
+// Per-dimension symmetric int8 encoding, the operand format of
+// quantized_i8_per_dimension_dot (core/distance/quantized.rs:42-56: one
+// dequantization scale per dimension, shared by queries and rows).  The
+// reference has no production encoder for it; this one follows its other
+// symmetric encoders (lib.rs:185-199, flat_tree.rs:47-64): scale_j = max_i |x_ij| / 127
+// over the index rows (0 when the column is zero), code = clamp(round(x / scale_j),
+// -127, 127) with round half away from zero, 0 where scale_j = 0.
+void orc_quantize_per_dimension(const float* data, int64_t n, int32_t dim, int8_t* codes, float* dim_scales) {
+  for (int j = 0; j < dim; ++j) {
+    float mx = 0.f;
+    for (int64_t r = 0; r < n; ++r) mx = std::max(mx, std::fabs(data[r * dim + j]));
+    dim_scales[j] = mx > 0.f ? mx / 127.0f : 0.f;
+  }
+  orc_quantize_queries_per_dimension(data, n, dim, dim_scales, codes);
+}
+
+void orc_quantize_queries_per_dimension(const float* queries, int64_t nq, int32_t dim, const float* dim_scales,
+                                        int8_t* codes) {
+  for (int64_t r = 0; r < nq; ++r)
+    for (int j = 0; j < dim; ++j) {
+      const float sc = dim_scales[j];
+      float v = sc > 0.f ? std::round(queries[r * dim + j] / sc) : 0.f;
+      if (v != v) v = 0.f;
+      codes[r * dim + j] = (int8_t)std::min(std::max(v, -127.0f), 127.0f);
+    }
+}
+
 // lib.rs:1131-1146 normalize_rows_inplace: sequential f32 sum of squares; rows
 // with norm^2 <= 1e-12 are left unchanged; x *= 1/sqrt(norm^2).
 void orc_normalize_rows(float* data, int64_t n, int32_t dim) {
@@ -1699,6 +1791,16 @@ void orc_normalize_rows(float* data, int64_t n, int32_t dim) {
 int32_t orc_query_quantized(const orc_index* ix, const float* queries, int64_t nq, int32_t k,
                             float epsilon, int32_t encoding, int32_t candidate_width,
                             int32_t rerank_width, int32_t* out_idx, float* out_dist) {
+  return orc_query_quantized_trees(ix, queries, nq, k, epsilon, encoding, candidate_width, rerank_width, 0, out_idx,
+                                   out_dist);
+}
+
+// With quantize_trees != 0 the search trees route over int8 routing trees
+// (QuantizedFlatTree, flat_tree.rs:35-183; lib.rs:231-240) with the query's
+// int8 codes and tree_query_scale = max|q| / 127 (lib.rs:283-296, greedy.rs:109-146).
+int32_t orc_query_quantized_trees(const orc_index* ix, const float* queries, int64_t nq, int32_t k,
+                                  float epsilon, int32_t encoding, int32_t candidate_width,
+                                  int32_t rerank_width, int32_t quantize_trees, int32_t* out_idx, float* out_dist) {
   size_t resolved = candidate_width == 0 ? (size_t)std::max(k, rerank_width) : (size_t)candidate_width;
   if (resolved < (size_t)k || (size_t)rerank_width > resolved ||
       !(candidate_width == 0 || rerank_width == 0 || rerank_width >= k))
@@ -1706,12 +1808,23 @@ int32_t orc_query_quantized(const orc_index* ix, const float* queries, int64_t n
   bool rerank = candidate_width == 0 ? rerank_width > k : rerank_width > 0;
   size_t dim = ix->dim, n = ix->n;
   std::vector<int8_t> codes(n * dim);
-  std::vector<float> inv(n);
-  float gm;
-  orc_quantize_rows(ix->data.data(), (int64_t)n, (int32_t)dim, encoding, codes.data(), inv.data(), &gm);
+  std::vector<float> inv(n), dsc(dim);
+  float gm = 0.f;
+  const bool per_dim = encoding == 3;
+  if (per_dim) orc_quantize_per_dimension(ix->data.data(), (int64_t)n, (int32_t)dim, codes.data(), dsc.data());
+  else orc_quantize_rows(ix->data.data(), (int64_t)n, (int32_t)dim, encoding, codes.data(), inv.data(), &gm);
   float gds = gm > 0.f ? 1.0f / gm : 0.f;
   Workspace ws(n, resolved);
   std::vector<int8_t> qc(dim);
+  std::vector<std::vector<int8_t>> tcodes(ix->trees.size());
+  std::vector<std::vector<float>> tscales(ix->trees.size());
+  if (quantize_trees)
+    for (size_t t = 0; t < ix->trees.size(); ++t) {
+      const FlatTree& tr = ix->trees[t];
+      tcodes[t].resize(tr.n_nodes * dim);
+      tscales[t].resize(tr.n_nodes);
+      quantize_hyperplanes(tr.hyperplanes.data(), tr.n_nodes, dim, tcodes[t].data(), tscales[t].data());
+    }
   for (int64_t qi = 0; qi < nq; ++qi) {
     const float* q = queries + qi * (int64_t)dim;
     float mult;
@@ -1726,17 +1839,35 @@ int32_t orc_query_quantized(const orc_index* ix, const float* queries, int64_t n
       float v = std::round(q[j] * mult);
       qc[j] = (int8_t)std::min(std::max(v, -127.0f), 127.0f);
     }
+    if (per_dim) orc_quantize_queries_per_dimension(q, 1, (int32_t)dim, dsc.data(), qc.data());
     int32_t nsq = i8_dot(qc.data(), qc.data(), (int)dim);
     float qinv = encoding == 0 ? (nsq > 0 ? 1.0f / std::sqrt((float)nsq) : 0.f)
                                : (encoding == 1 ? gds : (mult > 0.f ? 1.0f / mult : 0.f));
     FastRng rng(ix->seed);  // index.rs:298: quantized queries seed with rng_seed only
     ws.reset(resolved);
     auto dist_to = [&](int32_t i) {
-      float sim = (float)i8_dot(qc.data(), &codes[(size_t)i * dim], (int)dim) * qinv * inv[(size_t)i];
+      // per-dimension codes: the reconstructed inner product (quantized.rs:48-56)
+      float sim = per_dim ? orc_i8_per_dimension_dot(qc.data(), &codes[(size_t)i * dim], dsc.data(), (int32_t)dim)
+                          : (float)i8_dot(qc.data(), &codes[(size_t)i * dim], (int)dim) * qinv * inv[(size_t)i];
       return 1.0f - std::min(std::max(sim, -1.0f), 1.0f);
     };
-    for (auto& t : ix->trees) {
-      t.search_leaves(q, rng, ix->leaf_budget, ws.leaves);
+    float tqs = 0.f;
+    if (quantize_trees) {
+      float mx = 0.f;
+      for (size_t j = 0; j < dim; ++j) mx = std::max(mx, std::fabs(q[j]));
+      tqs = mx > 0.f ? mx / 127.0f : 0.f;
+    }
+    for (size_t ti = 0; ti < ix->trees.size(); ++ti) {
+      const FlatTree& t = ix->trees[ti];
+      if (quantize_trees)
+        t.search_leaves_with(
+            [&](size_t node) {
+              return quantized_margin(tcodes[ti].data(), tscales[ti].data(), t.offsets.data(), dim, node, qc.data(),
+                                      tqs);
+            },
+            rng, ix->leaf_budget, ws.leaves);
+      else
+        t.search_leaves(q, rng, ix->leaf_budget, ws.leaves);
       for (auto& l : ws.leaves)
         for (size_t p = l.first; p < l.second; ++p) {
           int32_t idx = t.indices[p];

@@ -112,6 +112,15 @@ int32_t orc_tree_search_leaves(int32_t n_nodes, int32_t dim, const float* hyperp
                                const float* point, uint64_t seed, int32_t leaf_budget,
                                int32_t* out_leaves, int32_t* n_leaves);
 
+/* QuantizedFlatTree (flat_tree.rs:35-183): per-node int8 codes and scales of
+ * the hyperplanes (:47-64), and search_leaves over them (:106-183) for a query's
+ * int8 codes and tree_query_scale. */
+void orc_quantize_tree_hyperplanes(int32_t n_nodes, int32_t dim, const float* hyperplanes, int8_t* codes,
+                                   float* scales);
+int32_t orc_tree_search_leaves_quantized(int32_t n_nodes, int32_t dim, const float* hyperplanes,
+                                         const float* offsets, const int32_t* children, const int8_t* qcodes,
+                                         float qscale, uint64_t seed, int32_t leaf_budget, int32_t* out_leaves,
+                                         int32_t* n_leaves);
 /* Hyperplane and offset of a split through points p1, p2 (builder.rs:249-308). */
 float orc_tree_hyperplane(const float* p1, const float* p2, int32_t dim, int32_t angular, float* hp);
 /* Leaf node reached by each of n points under the budget-1 routing rule
@@ -150,13 +159,26 @@ void orc_query_one(const orc_index* idx, const float* query, int32_t k, float ep
                    int32_t* out_idx, float* out_dist);
 
 /* ---- int8 serving (crates/rinnd/src/lib.rs:159-358, index.rs:283-334) -- */
-/* encoding: 0 int8 per-vector cosine, 1 sq8u global symmetric, 2 sq8p per-vector. */
+/* encoding: 0 int8 per-vector cosine, 1 sq8u global symmetric, 2 sq8p per-vector
+ * (orc_query_quantized also takes 3: per-dimension symmetric codes). */
 void orc_quantize_rows(const float* data, int64_t n, int32_t dim, int32_t encoding,
                        int8_t* codes, float* inv_norms, float* global_mult);
 /* quantize_query (lib.rs:325-358) with the index's global multiplier `global_mult`
  * (used by encoding 1 only): codes nq x dim, per-query scale (query_inv_norm). */
 void orc_quantize_queries(const float* queries, int64_t nq, int32_t dim, int32_t encoding,
                           float global_mult, int8_t* codes, float* scales);
+/* Per-dimension symmetric int8 codes for quantized_i8_per_dimension_dot
+ * (quantized.rs:42-56): dim_scales[j] = max_i |x_ij| / 127, codes = clamp(round(x /
+ * scale_j), +-127) (encoding 3 of orc_query_quantized).  The query form uses the
+ * index's scales. */
+void orc_quantize_per_dimension(const float* data, int64_t n, int32_t dim, int8_t* codes, float* dim_scales);
+void orc_quantize_queries_per_dimension(const float* queries, int64_t nq, int32_t dim, const float* dim_scales,
+                                        int8_t* codes);
+/* orc_query_quantized with int8 routing trees when quantize_trees != 0
+ * (tree_quantization="int8", lib.rs:681-704). */
+int32_t orc_query_quantized_trees(const orc_index* idx, const float* queries, int64_t nq, int32_t k,
+                                  float epsilon, int32_t encoding, int32_t candidate_width,
+                                  int32_t rerank_width, int32_t quantize_trees, int32_t* out_idx, float* out_dist);
 /* normalize_rows_inplace (lib.rs:1131-1146). */
 void orc_normalize_rows(float* data, int64_t n, int32_t dim);
 int32_t orc_query_quantized(const orc_index* idx, const float* queries, int64_t nq,

@@ -38,7 +38,9 @@ _ANGULAR = {"cosine", "inner_product", "dot"}  # index.rs:606-614
 # Local-join tile arithmetic (an addition of the B200 engine): "bf16" filters
 # pairs with tensor-core BF16 Gram tiles and recomputes survivors in FP32.
 _PRECISIONS = {"fp32": L.PRECISION_FP32, "bf16": L.PRECISION_BF16}
-_ENCODINGS = {"int8": L.Q8_PER_VECTOR_COSINE, "sq8u": L.Q8_GLOBAL_SYMMETRIC, "sq8p": L.Q8_PER_VECTOR_SYMMETRIC}
+_ENCODINGS = {"int8": L.Q8_PER_VECTOR_COSINE, "sq8u": L.Q8_GLOBAL_SYMMETRIC, "sq8p": L.Q8_PER_VECTOR_SYMMETRIC,
+              # an addition of the B200 engine: per-dimension scales (quantized.rs:42-56)
+              "sq8d": L.Q8_PER_DIMENSION}
 
 
 def version() -> str:
@@ -101,7 +103,7 @@ def _prepare(data, *, metric, n_neighbors, n_trees, n_search_trees, search_tree_
     modes.update({m: (True, e) for m, e in _ENCODINGS.items()})
     if cosine_distance_mode not in modes:
         raise ValueError(f"Unknown cosine_distance_mode: {cosine_distance_mode}; expected 'log', 'direct', "
-                         "'int8', 'sq8u', or 'sq8p'")
+                         "'int8', 'sq8u', 'sq8p', or 'sq8d'")
     direct_cosine, encoding = modes[cosine_distance_mode]
     if tree_quantization not in ("none", "int8"):
         raise ValueError(f"Unknown tree_quantization: {tree_quantization}; expected 'none' or 'int8'")
@@ -111,10 +113,11 @@ def _prepare(data, *, metric, n_neighbors, n_trees, n_search_trees, search_tree_
     if quantize_trees and encoding == L.Q8_GLOBAL_SYMMETRIC:
         raise ValueError("tree_quantization='int8' is incompatible with cosine_distance_mode='sq8u'; use "
                          "tree_quantization='none'")
+    if quantize_trees and encoding == L.Q8_PER_DIMENSION:
+        raise ValueError("tree_quantization='int8' is incompatible with cosine_distance_mode='sq8d'; use "
+                         "tree_quantization='none'")
     if direct_cosine and not normalize_cosine:
         raise ValueError("direct and quantized cosine modes require metric='cosine' and normalize=True")
-    if quantize_trees:
-        raise ValueError("tree_quantization='int8' is not implemented by the B200 engine")
     if retain_fp32_data is None:
         retain_fp32_data = (not quantize_trees) or quantized_rerank_width > 0
 
@@ -166,7 +169,8 @@ def _prepare(data, *, metric, n_neighbors, n_trees, n_search_trees, search_tree_
 
     state = {"n_points": n_points, "dim": dim, "n_neighbors": int(n_neighbors), "metric": metric,
              "encoding": encoding, "candidate_width": int(quantized_candidate_width),
-             "rerank_width": int(quantized_rerank_width), "retain_fp32": bool(retain_fp32_data)}
+             "rerank_width": int(quantized_rerank_width), "retain_fp32": bool(retain_fp32_data),
+             "quantize_trees": quantize_trees, "leaf_budget": max(int(search_tree_leaf_budget), 1)}
     return data, p, state
 
 
@@ -202,8 +206,16 @@ class RINND:
         self._candidate_width = state["candidate_width"]
         self._rerank_width = state["rerank_width"]
         self._retain_fp32 = state["retain_fp32"]
+        self._leaf_budget = state["leaf_budget"]
         if self._encoding is not None:
+            # QuantizedI8Index::new (lib.rs:159-276): codes, int8 routing trees, released FP32 rows
             L.check(L.lib.rinnd_quantize(self._h, self._encoding))
+            if state["quantize_trees"]:
+                L.check(L.lib.rinnd_quantize_trees(self._h))
+            if not self._retain_fp32:
+                L.check(L.lib.rinnd_release_fp32(self._h))
+        else:
+            self._retain_fp32 = True  # only a quantized index releases its rows
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -321,6 +333,22 @@ class RINND:
                                                L.ptr(piv) if with_pivots else None))
         return (hp, off, ch, ind, piv) if with_pivots else (hp, off, ch, ind)
 
+    def search_tree_leaves(self, query_data, tree=0, leaf_budget=None, quantized=False):
+        """The leaves FlatTree::search_leaves (flat_tree.rs:239-311) visits in
+        retained tree `tree` for each query, as the search seeds them: a list
+        per query of (start, end) ranges into the tree's leaf order (the
+        `leaf_indices` of export_search_tree for tree 0).  `quantized` routes the
+        queries' int8 codes over the int8 routing trees."""
+        q = _as_f32_2d(query_data, "query_data")
+        self._check_dim(q.shape[1])
+        b = int(leaf_budget) if leaf_budget is not None else self._leaf_budget
+        n = q.shape[0]
+        out = np.empty((n, b, 2), np.int32)
+        cnt = np.empty(n, np.int32)
+        L.check(L.lib.rinnd_tree_search_leaves(self._h, L.ptr(q), n, int(tree), b, int(bool(quantized)), L.ptr(out),
+                                               L.ptr(cnt)))
+        return [[(int(s), int(e)) for s, e in out[i, :cnt[i]]] for i in range(n)]
+
     def search_stats(self, reset=False) -> dict:
         """Distance evaluations, node expansions and visited-table overflows of
         the searches since the build (or the last reset)."""
@@ -341,9 +369,18 @@ class RINND:
         info = {
             "encoding": s.encoding.decode(), "code_bytes": int(s.code_bytes),
             "metadata_bytes": int(s.metadata_bytes), "retained_fp32_bytes": int(s.retained_fp32_bytes),
-            "encode_seconds": float(s.encode_seconds), "device_bytes": int(s.device_bytes),
+            "encode_seconds": float(s.encode_seconds),
+            "tree_code_bytes": int(s.tree_code_bytes), "tree_scale_bytes": int(s.tree_scale_bytes),
+            "tree_offset_bytes": int(s.tree_offset_bytes), "tree_topology_bytes": int(s.tree_topology_bytes),
+            "hypothetical_releasable_fp32_tree_bytes": 0,
+            "released_fp32_tree_bytes": int(s.released_fp32_tree_bytes),
+            "released_fp32_data_bytes": int(s.released_fp32_data_bytes),
+            "retained_fp32_tree_topology_bytes": int(s.retained_fp32_tree_topology_bytes),
+            "device_bytes": int(s.device_bytes),
         }
-        info["allocated_bytes"] = info["code_bytes"] + info["metadata_bytes"] + info["retained_fp32_bytes"]
+        info["allocated_bytes"] = sum(info[k] for k in (
+            "code_bytes", "metadata_bytes", "retained_fp32_bytes", "retained_fp32_tree_topology_bytes",
+            "tree_code_bytes", "tree_scale_bytes", "tree_offset_bytes", "tree_topology_bytes"))
         info["bytes_per_vector"] = info["allocated_bytes"] / self.n_points
         return info
 

@@ -21,7 +21,7 @@ ERR_INVALID, ERR_OOM, ERR_CUDA, ERR_NO_DEVICE, ERR_INTERNAL, ERR_BUSY = -1, -2, 
 DIST_SQEUCLIDEAN, DIST_MANHATTAN, DIST_COSINE, DIST_ALT_COSINE, DIST_ALT_DOT, DIST_DIRECT_COSINE, \
     DIST_INNER_PRODUCT, DIST_ALT_INNER_PRODUCT = range(8)
 CORR_NONE, CORR_SQRT, CORR_ALT_COSINE, CORR_ALT_IP = range(4)
-Q8_PER_VECTOR_COSINE, Q8_GLOBAL_SYMMETRIC, Q8_PER_VECTOR_SYMMETRIC = range(3)
+Q8_PER_VECTOR_COSINE, Q8_GLOBAL_SYMMETRIC, Q8_PER_VECTOR_SYMMETRIC, Q8_PER_DIMENSION = range(4)
 PRECISION_FP32, PRECISION_BF16 = range(2)
 JOIN_CHUNKED_FP32, JOIN_PIPELINED_FP32, JOIN_TENSOR_BF16 = range(3)  # rinnd_build_info.join_form
 
@@ -71,6 +71,9 @@ class StorageInfo(ctypes.Structure):
     _fields_ = [
         ("encoding", ctypes.c_char * 32), ("code_bytes", _i64), ("metadata_bytes", _i64),
         ("retained_fp32_bytes", _i64), ("encode_seconds", _f64), ("device_bytes", _i64),
+        ("tree_code_bytes", _i64), ("tree_scale_bytes", _i64), ("tree_offset_bytes", _i64),
+        ("tree_topology_bytes", _i64), ("released_fp32_tree_bytes", _i64), ("released_fp32_data_bytes", _i64),
+        ("retained_fp32_tree_topology_bytes", _i64),
     ]
 
 
@@ -95,6 +98,10 @@ SIGNATURES = {
     "rinnd_quantize": (ctypes.c_int, [_P, _i32]),
     "rinnd_query_quantized": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _i32, _i32, _P, _P]),
     "rinnd_quantize_rows": (ctypes.c_int, [_P, _i64, _i32, _i32, _P, _P, _P]),
+    "rinnd_quantize_rows_per_dimension": (ctypes.c_int, [_P, _i64, _i32, _P, _P]),
+    "rinnd_quantize_trees": (ctypes.c_int, [_P]),
+    "rinnd_release_fp32": (ctypes.c_int, [_P]),
+    "rinnd_tree_search_leaves": (ctypes.c_int, [_P, _P, _i64, _i32, _i32, _i32, _P, _P]),
     "rinnd_search_stats_get": (ctypes.c_int, [_P, _P, _P, _P, _i32]),
     "rinnd_server_params_default": (ctypes.c_int, [_P]),
     "rinnd_server_create": (ctypes.c_int, [_P, _P, _P]),

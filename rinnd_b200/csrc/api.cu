@@ -224,6 +224,11 @@ struct rinnd_index {
   int encoding = -1;
   DVec<int8_t> codes;
   DVec<float> inv_norms;
+  DVec<float> dim_scales;        // per-dimension encoding: Dq scales
+  // int8 routing trees (tree_quantization="int8", lib.rs:681-704): codes and scales of every forest node
+  DVec<int8_t> tree_codes;
+  DVec<float> tree_scales;
+  bool fp32_released = false;    // rows X freed (retain_fp32_data=False): no FP32 search or rerank
   float global_mult = 0.f;
   int Dq = 0;
   double encode_seconds = 0.0;
@@ -256,10 +261,15 @@ struct rinnd_index {
     s.hyperplanes = forest.hyperplanes.p;
     s.tree_idx = tree_idx.p;
     s.leaf_budget = p.search_tree_leaf_budget;
+    s.tree_depth = forest.levels;
+    s.frontier_cap = s.leaf_budget > 1 ? s.leaf_budget * std::max(forest.levels, 1) + 2 : 0;
+    s.tree_codes = tree_codes.p;
+    s.tree_scales = tree_scales.p;
     s.vertex_order = vertex_order.p;
     s.seed = p.random_seed;
     s.codes = codes.p;
     s.inv_norms = inv_norms.p;
+    s.dim_scales = encoding == Q8_PER_DIMENSION ? dim_scales.p : nullptr;
     s.Dq = Dq;
     return s;
   }
@@ -275,7 +285,7 @@ void validate_params(const rinnd_build_params* p, int64_t n, int d) {
   require(p->n_neighbors >= 1 && p->n_neighbors <= 128, "n_neighbors must be in [1, 128]");
   require(p->n_trees >= 0 && p->n_trees <= 64, "n_trees must be in [0, 64]");
   require(p->n_search_trees >= 0, "n_search_trees must be >= 0");
-  require(p->search_tree_leaf_budget <= 1, "search_tree_leaf_budget > 1 is not implemented");
+  require(p->search_tree_leaf_budget <= 256, "search_tree_leaf_budget must be <= 256");
   require(p->distance_kind >= 0 && p->distance_kind < DK_COUNT, "unknown distance kind");
   require(p->correction >= 0 && p->correction <= CK_ALT_IP, "unknown correction");
   require(p->diversify_prob >= 1.0f, "diversify_prob < 1 is not implemented");
@@ -458,6 +468,7 @@ void query_impl(rinnd_index* ix, const float* q, bool on_device, int64_t nq, int
   require(k >= 1 && k <= 256, "k must be in [1, 256]");
   if (nq == 0) return;
   require(q != nullptr && out_idx != nullptr && out_dist != nullptr, "query/output pointers must not be null");
+  require(!ix->fp32_released, "FP32 search is unavailable because FP32 vector data was released");
   std::lock_guard<std::mutex> lock(ix->mu);
   RINND_CUDA(cudaSetDevice(ix->device));
   cudaStream_t st = user_st ? user_st : ix->st;
@@ -594,8 +605,11 @@ int rinnd_server_create(rinnd_index* idx, const rinnd_server_params* p, rinnd_se
     require(p->max_inflight >= 1 && p->max_inflight <= 64, "max_inflight must be in [1, 64]");
     require(p->max_k >= 1 && p->max_k <= 256, "max_k must be in [1, 256]");
     require(p->max_pending_queries >= p->max_batch_queries, "max_pending_queries must be >= max_batch_queries");
+    require(p->quantized || !idx->fp32_released, "FP32 search is unavailable because FP32 vector data was released");
     if (p->quantized) {
       require(idx->encoding >= 0, "a quantized server needs a quantized index (rinnd_quantize)");
+      require(!(idx->fp32_released && p->rerank_width > 0),
+              "exact reranking is unavailable because FP32 vector data was released");
       require(p->candidate_width >= 0 && p->rerank_width >= 0, "quantized widths must be >= 0");
       require(quantized_width(1, p->candidate_width, p->rerank_width) <= 256, "candidate width must be <= 256");
     }
@@ -853,14 +867,51 @@ int rinnd_storage_info_get(const rinnd_index* idx, rinnd_storage_info* info) {
     check_index(idx);
     require(info != nullptr, "info must not be null");
     std::memset(info, 0, sizeof(*info));
-    static const char* names[] = {"int8_per_vector_cosine", "sq8u_global_symmetric", "sq8p_per_vector_symmetric"};
+    static const char* names[] = {"int8_per_vector_cosine", "sq8u_global_symmetric", "sq8p_per_vector_symmetric",
+                                  "sq8d_per_dimension_symmetric"};
     const char* enc = idx->encoding >= 0 ? names[idx->encoding] : "fp32";
     std::snprintf(info->encoding, sizeof(info->encoding), "%s", enc);
     if (idx->encoding >= 0) {
-      info->code_bytes = (int64_t)idx->N * idx->D;
-      info->metadata_bytes = (int64_t)idx->N * 4;
-      info->retained_fp32_bytes = (int64_t)idx->N * idx->D * 4 + (int64_t)idx->N * idx->k * 4;
+      // QuantizedI8Index::storage_info / quantized_tree_storage_info (lib.rs:474-539),
+      // retained_fp32_bytes (core/index.rs:94-101): rows (unless released), neighbor
+      // distances and the FP32 search trees' hyperplanes and offsets (unless quantized)
+      const int64_t N = idx->N, D = idx->D;
+      int64_t nodes = 0;
+      if (idx->n_search_trees > 0) {
+        std::vector<int32_t> ch(2 * (size_t)idx->forest.n_nodes);
+        RINND_CUDA(cudaSetDevice(idx->device));
+        idx->forest.children.to_host(ch.data(), ch.size());
+        RINND_CUDA(cudaStreamSynchronize(idx->st));
+        for (int t = 0; t < idx->n_search_trees; ++t) {  // nodes of each retained tree
+          std::vector<int32_t> stack{t};
+          while (!stack.empty()) {
+            const int32_t g = stack.back();
+            stack.pop_back();
+            ++nodes;
+            if (ch[2 * (size_t)g] > 0) {
+              stack.push_back(ch[2 * (size_t)g]);
+              stack.push_back(ch[2 * (size_t)g + 1]);
+            }
+          }
+        }
+      }
+      const int64_t topo = nodes * 8 + (int64_t)idx->n_search_trees * N * 4;
+      const bool qtrees = idx->tree_codes.p != nullptr;
+      info->code_bytes = N * D;
+      info->metadata_bytes = idx->encoding == Q8_PER_DIMENSION ? D * 4 : N * 4;
+      info->retained_fp32_bytes =
+          (idx->fp32_released ? 0 : N * D * 4) + N * idx->k * 4 + (qtrees ? 0 : nodes * (D + 1) * 4);
       info->encode_seconds = idx->encode_seconds;
+      if (qtrees) {
+        info->tree_code_bytes = nodes * D;
+        info->tree_scale_bytes = nodes * 4;
+        info->tree_offset_bytes = nodes * 4;
+        info->tree_topology_bytes = topo;
+        info->released_fp32_tree_bytes = nodes * D * 4 + nodes * 4 + topo;
+      } else {
+        info->retained_fp32_tree_topology_bytes = topo;
+      }
+      info->released_fp32_data_bytes = idx->fp32_released ? N * D * 4 : 0;
     } else {
       info->code_bytes = (int64_t)idx->N * idx->D * 4;
     }
@@ -1035,10 +1086,10 @@ int rinnd_device_count(int32_t* count) {
 int rinnd_quantize(rinnd_index* idx, int32_t encoding) {
   return guarded([&] {
     check_index(idx);
-    require(encoding >= RINND_Q8_PER_VECTOR_COSINE && encoding <= RINND_Q8_PER_VECTOR_SYMMETRIC,
-            "unknown int8 encoding");
+    require(encoding >= RINND_Q8_PER_VECTOR_COSINE && encoding <= RINND_Q8_PER_DIMENSION, "unknown int8 encoding");
     require(idx->kind == DK_DIRECT_COSINE,
             "int8 quantization requires an index built with the direct cosine distance on normalized rows");
+    require(!idx->fp32_released, "the FP32 rows were released: the index can no longer be encoded");
     std::lock_guard<std::mutex> lock(idx->mu);
     RINND_CUDA(cudaSetDevice(idx->device));
     cudaStream_t st = idx->st;
@@ -1047,8 +1098,16 @@ int rinnd_quantize(rinnd_index* idx, int32_t encoding) {
     const int Dq = round_up(idx->D, 16);
     const float gm = quant_global_multiplier(idx->X.p, (long long)idx->N * idx->Dp, st);
     idx->codes.alloc((size_t)idx->N * Dq, st);
-    idx->inv_norms.alloc((size_t)idx->N, st);
-    quantize_rows(idx->X.p, idx->N, idx->D, idx->Dp, Dq, encoding, gm, idx->codes.p, idx->inv_norms.p, st);
+    if (encoding == Q8_PER_DIMENSION) {
+      idx->inv_norms.release();
+      idx->dim_scales.alloc((size_t)Dq, st);
+      quant_dim_scales(idx->X.p, idx->N, idx->D, idx->Dp, Dq, idx->dim_scales.p, st);
+    } else {
+      idx->dim_scales.release();
+      idx->inv_norms.alloc((size_t)idx->N, st);
+    }
+    quantize_rows(idx->X.p, idx->N, idx->D, idx->Dp, Dq, encoding, gm, idx->dim_scales.p, idx->codes.p,
+                  idx->inv_norms.p, st);
     RINND_CUDA(cudaStreamSynchronize(st));
     idx->Dq = Dq;
     idx->global_mult = gm;
@@ -1073,6 +1132,7 @@ int rinnd_query_quantized(rinnd_index* idx, const float* queries, int64_t nq, in
             "quantized rerank width must be zero or at least k");
     require(resolved <= 256, "quantized candidate width must be <= 256");
     const bool rerank = candidate_width == 0 ? rerank_width > k : rerank_width > 0;
+    require(!(rerank && idx->fp32_released), "exact reranking is unavailable because FP32 vector data was released");
     if (nq == 0) return;
     require(queries && out_idx && out_dist, "query/output pointers must not be null");
     std::lock_guard<std::mutex> lock(idx->mu);
@@ -1083,7 +1143,8 @@ int rinnd_query_quantized(rinnd_index* idx, const float* queries, int64_t nq, in
     if (idx->normalize) normalize_rows(Q.p, nq, idx->D, idx->Dp, st);
     DVec<int8_t> Q8((size_t)nq * idx->Dq, st);
     DVec<float> qs((size_t)nq, st);
-    quantize_rows(Q.p, nq, idx->D, idx->Dp, idx->Dq, idx->encoding, idx->global_mult, Q8.p, qs.p, st);
+    quantize_rows(Q.p, nq, idx->D, idx->Dp, idx->Dq, idx->encoding, idx->global_mult, idx->dim_scales.p, Q8.p, qs.p,
+                  st);
     DVec<int32_t> oi((size_t)nq * k, st);
     DVec<float> od((size_t)nq * k, st);
     greedy_search_quantized(idx->search_view(), Q.p, Q8.p, qs.p, (int)nq, resolved, k, rerank ? rerank_width : 0,
@@ -1099,7 +1160,7 @@ int rinnd_quantize_rows(const float* data, int64_t n, int32_t d, int32_t encodin
   return guarded([&] {
     require(n >= 0 && d >= 1, "invalid shape");
     require(encoding >= RINND_Q8_PER_VECTOR_COSINE && encoding <= RINND_Q8_PER_VECTOR_SYMMETRIC,
-            "unknown int8 encoding");
+            "unknown int8 encoding (per-dimension codes: rinnd_quantize_rows_per_dimension)");
     if (n == 0) {
       if (global_multiplier) *global_multiplier = 0.f;
       return;
@@ -1113,12 +1174,98 @@ int rinnd_quantize_rows(const float* data, int64_t n, int32_t d, int32_t encodin
     const float gm = quant_global_multiplier(X.p, n * Dp, sg.s);
     DVec<int8_t> C((size_t)n * Dq, sg.s);
     DVec<float> S((size_t)n, sg.s);
-    quantize_rows(X.p, n, d, Dp, Dq, encoding, gm, C.p, S.p, sg.s);
+    quantize_rows(X.p, n, d, Dp, Dq, encoding, gm, nullptr, C.p, S.p, sg.s);
     RINND_CUDA(cudaMemcpy2DAsync(codes, (size_t)d, C.p, (size_t)Dq, (size_t)d, (size_t)n, cudaMemcpyDeviceToHost,
                                  sg.s));
     S.to_host(scales, (size_t)n);
     RINND_CUDA(cudaStreamSynchronize(sg.s));
     if (global_multiplier) *global_multiplier = gm;
+  });
+}
+
+int rinnd_quantize_trees(rinnd_index* idx) {
+  return guarded([&] {
+    check_index(idx);
+    require(idx->encoding >= 0, "tree_quantization='int8' is available only with a quantized cosine_distance_mode");
+    require(idx->encoding != Q8_GLOBAL_SYMMETRIC,
+            "tree_quantization='int8' is incompatible with cosine_distance_mode='sq8u'; use tree_quantization='none'");
+    require(idx->encoding != Q8_PER_DIMENSION,
+            "tree_quantization='int8' is incompatible with cosine_distance_mode='sq8d'; use tree_quantization='none'");
+    std::lock_guard<std::mutex> lock(idx->mu);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    cudaStream_t st = idx->st;
+    const long long nn = (long long)idx->forest.n_nodes;
+    const int Dq = round_up(idx->D, 16);
+    idx->tree_codes.alloc((size_t)std::max<long long>(nn, 1) * Dq, st);
+    idx->tree_scales.alloc((size_t)std::max<long long>(nn, 1), st);
+    quantize_tree_hyperplanes(idx->forest.hyperplanes.p, nn, idx->D, idx->Dp, Dq, idx->tree_codes.p,
+                              idx->tree_scales.p, st);
+    RINND_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int rinnd_release_fp32(rinnd_index* idx) {
+  return guarded([&] {
+    check_index(idx);
+    require(idx->encoding >= 0, "only a quantized index can release its FP32 rows");
+    std::lock_guard<std::mutex> lock(idx->mu);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    idx->X.release();
+    idx->fp32_released = true;
+    RINND_CUDA(cudaStreamSynchronize(idx->st));
+  });
+}
+
+int rinnd_tree_search_leaves(rinnd_index* idx, const float* queries, int64_t nq, int32_t tree, int32_t budget,
+                             int32_t quantized, int32_t* out_leaves, int32_t* out_counts) {
+  return guarded([&] {
+    check_index(idx);
+    require(nq >= 0, "number of queries must be >= 0");
+    require(tree >= 0 && tree < idx->n_search_trees, "tree index out of range of the retained search trees");
+    require(budget >= 1 && budget <= 256, "leaf budget must be in [1, 256]");
+    require(!quantized || idx->tree_codes.p != nullptr, "the index has no int8 routing trees");
+    if (nq == 0) return;
+    require(queries && out_leaves && out_counts, "pointers must not be null");
+    std::lock_guard<std::mutex> lock(idx->mu);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    cudaStream_t st = idx->st;
+    DVec<float> Q;
+    load_rows(queries, false, nq, idx->D, idx->D, idx->Dp, Q, st);
+    if (idx->normalize) normalize_rows(Q.p, nq, idx->D, idx->Dp, st);
+    DVec<int8_t> Q8;
+    DVec<float> qs;
+    if (quantized) {
+      Q8.alloc((size_t)nq * idx->Dq, st);
+      qs.alloc((size_t)nq, st);
+      quantize_rows(Q.p, nq, idx->D, idx->Dp, idx->Dq, idx->encoding, idx->global_mult, idx->dim_scales.p, Q8.p,
+                    qs.p, st);
+    }
+    DVec<int32_t> ol((size_t)nq * budget * 2, st), oc((size_t)nq, st);
+    tree_leaves(idx->search_view(), Q.p, quantized ? Q8.p : nullptr, (int)nq, tree, budget, 0, ol.p, oc.p, st,
+                idx->search_stats.p);
+    ol.to_host(out_leaves, (size_t)nq * budget * 2);
+    oc.to_host(out_counts, (size_t)nq);
+    RINND_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int rinnd_quantize_rows_per_dimension(const float* data, int64_t n, int32_t d, int8_t* codes, float* dim_scales) {
+  return guarded([&] {
+    require(n >= 1 && d >= 1, "invalid shape");
+    require(data && codes && dim_scales, "pointers must not be null");
+    ensure_device(0);
+    StreamGuard sg;
+    const int Dp = round_up(d, 4), Dq = round_up(d, 16);
+    DVec<float> X;
+    load_rows(data, false, n, d, d, Dp, X, sg.s);
+    DVec<float> S((size_t)Dq, sg.s);
+    quant_dim_scales(X.p, n, d, Dp, Dq, S.p, sg.s);
+    DVec<int8_t> C((size_t)n * Dq, sg.s);
+    quantize_rows(X.p, n, d, Dp, Dq, Q8_PER_DIMENSION, 0.f, S.p, C.p, nullptr, sg.s);
+    RINND_CUDA(cudaMemcpy2DAsync(codes, (size_t)d, C.p, (size_t)Dq, (size_t)d, (size_t)n, cudaMemcpyDeviceToHost,
+                                 sg.s));
+    S.to_host(dim_scales, (size_t)d);
+    RINND_CUDA(cudaStreamSynchronize(sg.s));
   });
 }
 

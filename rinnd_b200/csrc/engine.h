@@ -133,11 +133,18 @@ struct SearchIndex {
   const float* hyperplanes = nullptr;
   const int32_t* tree_idx = nullptr;     // n_trees * N leaf order (internal ids)
   int leaf_budget = 1;
+  int frontier_cap = 0;                  // spill-frontier entries per query (leaf_budget > 1)
+  int tree_depth = 0;                    // most internal nodes on a root-to-leaf path
+  // int8 routing trees (QuantizedFlatTree, flat_tree.rs:35-183): per-node codes
+  // (n_nodes x Dq) and scales; used by quantized queries when non-null
+  const int8_t* tree_codes = nullptr;
+  const float* tree_scales = nullptr;
   const int32_t* vertex_order = nullptr; // internal -> original id
   uint64_t seed = 42;
   // int8 codes (optional)
   const int8_t* codes = nullptr;         // N x Dq (Dq = round_up(D,16))
   const float* inv_norms = nullptr;
+  const float* dim_scales = nullptr;     // per-dimension codes: Dq scales (null otherwise)
   int Dq = 0;
 };
 struct SearchStats {
@@ -163,6 +170,13 @@ struct QueryMeta {
 void greedy_search_packed(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq,
                           int max_width, const QueryMeta& meta, int32_t* out_idx, float* out_dist, cudaStream_t st,
                           unsigned long long* dstats);
+// FlatTree::search_leaves of tree `tree` for nq device queries (nq x Dp FP32
+// rows; with Q8, their int8 codes route over the int8 routing trees): up to
+// `budget` leaves (start, end) per query into out_leaves (nq x budget x 2) and
+// the count into out_counts.
+void tree_leaves(const SearchIndex& ix, const float* Q, const int8_t* Q8, int nq, int tree, int budget,
+                 uint64_t qid_base, int32_t* out_leaves, int32_t* out_counts, cudaStream_t st,
+                 unsigned long long* dstats);
 // Quantized search (index.rs:283-334): int8 query codes Q8 (nq x Dq) with scales
 // qinv; the result list holds k_search entries; with rerank > 0 the first
 // `rerank` results are re-ordered by their exact FP32 distance to Q (index.rs:103-126);
@@ -172,12 +186,26 @@ void greedy_search_quantized(const SearchIndex& ix, const float* Q, const int8_t
                              cudaStream_t st, unsigned long long* dstats);
 
 // ---- int8 scalar quantization (quantize.cu) -------------------------------------
-enum Q8Encoding : int { Q8_PER_VECTOR_COSINE = 0, Q8_GLOBAL_SYMMETRIC = 1, Q8_PER_VECTOR_SYMMETRIC = 2 };
+enum Q8Encoding : int {
+  Q8_PER_VECTOR_COSINE = 0,
+  Q8_GLOBAL_SYMMETRIC = 1,
+  Q8_PER_VECTOR_SYMMETRIC = 2,
+  Q8_PER_DIMENSION = 3  // one scale per dimension (quantized.rs:42-56)
+};
 // 127 / max |x| over `total` floats (0 if all zero), lib.rs:163-174.
 float quant_global_multiplier(const float* X, long long total, cudaStream_t st);
-// Codes (n x Dq, zero-padded beyond D) and per-row scales of rows X (n x Dp).
-void quantize_rows(const float* X, long long n, int D, int Dp, int Dq, int encoding, float gmult, int8_t* codes,
-                   float* scale, cudaStream_t st);
+// int8 routing-tree codes (n_nodes x Dq) and per-node scales of hyperplanes H
+// (n_nodes x Dp), flat_tree.rs:47-64.
+void quantize_tree_hyperplanes(const float* H, long long n_nodes, int D, int Dp, int Dq, int8_t* codes, float* scales,
+                               cudaStream_t st);
+// Per-dimension scales of rows X (n x Dp): dim_scales[j] = max_i |x_ij| / 127
+// (0 for a zero column and for j >= D), Dq entries.
+void quant_dim_scales(const float* X, long long n, int D, int Dp, int Dq, float* dim_scales, cudaStream_t st);
+// Codes (n x Dq, zero-padded beyond D) and per-row scales of rows X (n x Dp);
+// the per-dimension encoding takes its scales from dim_scales (device, Dq
+// entries) and writes no row scales (scale may be null).
+void quantize_rows(const float* X, long long n, int D, int Dp, int Dq, int encoding, float gmult,
+                   const float* dim_scales, int8_t* codes, float* scale, cudaStream_t st);
 
 // ---- utilities (util.cu) ------------------------------------------------------
 void distance_pairs(int kind, const float* A, const float* B, int64_t n, int D, int Dp,

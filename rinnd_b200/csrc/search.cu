@@ -2,9 +2,12 @@
 //
 // Restates the reference query path (core/search/greedy.rs:70-241, 365-413;
 // core/index.rs:157-202, 283-334) with one warp per query:
-//   * tree seeding: hard descent of each retained RP tree (flat_tree.rs:253-273;
-//     margin = dot(q, hyperplane) + offset in the reference dot order, |m| < 1e-8
-//     -> random side), every unvisited leaf point pushed to results and seeds;
+//   * tree seeding: each retained RP tree's search_leaves (flat_tree.rs:239-311):
+//     hard descent with a leaf budget of 1, else the spill search over a
+//     priority frontier; margin = dot(q, hyperplane) + offset in the reference
+//     dot order (or the int8 routing tree's reconstructed margin for quantized
+//     queries, flat_tree.rs:96-183), |m| < 1e-8 -> random side; every unvisited
+//     leaf point is pushed to results and seeds;
 //   * fill_random up to k seeds (greedy.rs:148-163);
 //   * traverse (greedy.rs:165-201): pop the nearest seed; stop when the result
 //     list is full and the seed is >= bound, bound = max + eps * (max - min_distance)
@@ -33,13 +36,14 @@ constexpr int WPB = 4;  // warps per block
 constexpr int HASH_PROBES = 32;
 
 struct WarpLayout {
-  int dp, kmax, s, h;
+  int dp, kmax, s, h, f;  // f: spill-frontier entries (0 with a leaf budget of 1)
   __host__ __device__ size_t q_off() const { return 0; }
   __host__ __device__ size_t res_off() const { return (size_t)dp * 4; }
   __host__ __device__ size_t seed_off() const { return res_off() + (size_t)kmax * 8; }
   __host__ __device__ size_t batch_off() const { return seed_off() + (size_t)2 * s * 8; }
   __host__ __device__ size_t vis_off() const { return batch_off() + 32 * 8; }
-  __host__ __device__ size_t bytes() const { return vis_off() + (size_t)h * 4; }
+  __host__ __device__ size_t fr_off() const { return vis_off() + (size_t)h * 4; }
+  __host__ __device__ size_t bytes() const { return fr_off() + (size_t)f * 8; }
 };
 
 __host__ __device__ __forceinline__ int seed_capacity(int width) {
@@ -87,6 +91,25 @@ __host__ __device__ __forceinline__ int visited_capacity(int width) {
 template <bool QUANT>
 __device__ __forceinline__ float dist_to(const SearchIndex& ix, const float* q, const int8_t* q8,
                                          float qinv, int32_t id) {
+  if (QUANT && ix.dim_scales) {
+    // per-dimension codes: quantized_i8_per_dimension_dot (quantized.rs:48-56),
+    // ((a * b) * s_j) * s_j summed sequentially over the dimensions
+    const int4* b = reinterpret_cast<const int4*>(ix.codes + (size_t)id * ix.Dq);
+    float acc = 0.f;
+    for (int t = 0; t < ix.Dq / 16; ++t) {
+      const int4 y = __ldg(b + t);
+      const int8_t* yb = reinterpret_cast<const int8_t*>(&y);
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const int j = 16 * t + u;
+        if (j < ix.D) {
+          const float s = __ldg(ix.dim_scales + j);
+          acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(__fmul_rn((float)q8[j], (float)yb[u]), s), s));
+        }
+      }
+    }
+    return __fsub_rn(1.0f, fminf(fmaxf(acc, -1.0f), 1.0f));
+  }
   if (QUANT) {
     const int4* a = reinterpret_cast<const int4*>(q8);
     const int4* b = reinterpret_cast<const int4*>(ix.codes + (size_t)id * ix.Dq);
@@ -198,6 +221,111 @@ __device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int
   tail = min(na + nb, S);
 }
 
+// tree_query_scale of a quantized query (lib.rs:283-296): max|q| / 127 of the
+// FP32 query, 0 for a zero query.  Whole warp.
+__device__ __forceinline__ float tree_query_scale(const float* qf, int D) {
+  const int lane = threadIdx.x & 31;
+  float mx = 0.f;
+  for (int t = lane; t < D; t += 32) mx = fmaxf(mx, fabsf(qf[t]));
+  for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  return mx > 0.f ? __fdiv_rn(mx, 127.0f) : 0.f;
+}
+
+// Margin of a query at an internal node: the FP32 hyperplane's dot in the
+// reference order plus the offset (builder.rs:331), or with int8 routing trees
+// (qtrees) the reconstructed margin dot(codes) * scale * tree_query_scale +
+// offset (flat_tree.rs:96-103).  Every lane computes the same value.
+__device__ __forceinline__ float tree_margin(const SearchIndex& ix, bool qtrees, const float* qf, const int8_t* q8,
+                                             float tqs, int node) {
+  if (qtrees) {
+    const int4* a = reinterpret_cast<const int4*>(q8);
+    const int4* b = reinterpret_cast<const int4*>(ix.tree_codes + (size_t)node * ix.Dq);
+    int acc = 0;
+    for (int t = 0; t < ix.Dq / 16; ++t) {
+      const int4 x = a[t], y = __ldg(b + t);
+      acc = __dp4a(x.x, y.x, acc);
+      acc = __dp4a(x.y, y.y, acc);
+      acc = __dp4a(x.z, y.z, acc);
+      acc = __dp4a(x.w, y.w, acc);
+    }
+    return __fadd_rn(__fmul_rn(__fmul_rn((float)acc, ix.tree_scales[node]), tqs), ix.offsets[node]);
+  }
+  return __fadd_rn(exact_dot_a(qf, ix.hyperplanes + (size_t)node * ix.Dp, ix.D), ix.offsets[node]);
+}
+
+// FlatTree::search_leaves (flat_tree.rs:239-311), whole warp: calls
+// on_leaf(start, end) for each leaf found, in order.  budget 1: hard descent
+// (margin > 0 -> right, |m| < 1e-8 -> random side).  Otherwise the spill
+// search over a frontier of (priority, node) kept in insertion order in `fr`
+// (fcap entries): take the first entry of least priority (min_by over
+// total_cmp; priorities are non-negative so their bits order them), emit a
+// leaf, or split an internal node into the near child (same priority) and the
+// far child (priority max(p, |margin|)), until `budget` leaves.  A frontier
+// that would exceed fcap (not reachable with fcap = budget * depth + 2) ends
+// the search early and is counted in *overflow.
+template <class LeafF>
+__device__ void tree_search_leaves(const SearchIndex& ix, int root, int budget, uint64_t* fr, int fcap, QRng& rng,
+                                   bool qtrees, const float* qf, const int8_t* q8, float tqs,
+                                   unsigned long long* overflow, LeafF&& on_leaf) {
+  const int lane = threadIdx.x & 31;
+  auto side_of = [&](float margin) -> int {
+    if (fabsf(margin) < 1e-8f) return rng.next_bool() ? 1 : 0;
+    return margin > 0.f ? 1 : 0;
+  };
+  if (budget <= 1 || fcap < 3) {
+    int node = root;
+    while (ix.children[2 * (size_t)node] > 0)
+      node = ix.children[2 * (size_t)node + side_of(tree_margin(ix, qtrees, qf, q8, tqs, node))];
+    on_leaf(-ix.children[2 * (size_t)node], -ix.children[2 * (size_t)node + 1]);
+    return;
+  }
+  int nfr = 1, nleaves = 0;
+  if (lane == 0) fr[0] = (uint64_t)(uint32_t)root;
+  __syncwarp();
+  while (nleaves < budget && nfr > 0) {
+    uint64_t best = ~0ull;
+    for (int e = lane; e < nfr; e += 32) {
+      const uint64_t key = (fr[e] & 0xFFFFFFFF00000000ull) | (uint32_t)e;
+      best = key < best ? key : best;
+    }
+    for (int o = 16; o; o >>= 1) {
+      const uint64_t other = __shfl_xor_sync(0xffffffffu, best, o);
+      best = other < best ? other : best;
+    }
+    const int pos = (int)(uint32_t)best;
+    const uint64_t entry = fr[pos];
+    __syncwarp();
+    for (int c0 = pos; c0 < nfr - 1; c0 += 32) {  // Vec::remove: shift the tail left
+      const int e = c0 + lane;
+      const uint64_t v = e + 1 < nfr ? fr[e + 1] : 0ull;
+      __syncwarp();
+      if (e + 1 < nfr) fr[e] = v;
+      __syncwarp();
+    }
+    --nfr;
+    const int node = (int)(uint32_t)entry;
+    const float prio = __uint_as_float((uint32_t)(entry >> 32));
+    if (ix.children[2 * (size_t)node] <= 0) {
+      on_leaf(-ix.children[2 * (size_t)node], -ix.children[2 * (size_t)node + 1]);
+      ++nleaves;
+      continue;
+    }
+    const float margin = tree_margin(ix, qtrees, qf, q8, tqs, node);
+    const int side = side_of(margin);
+    const float far = fmaxf(prio, fabsf(margin));
+    if (nfr + 2 > fcap) {
+      if (lane == 0) atomicAdd(overflow, 1ull);
+      break;
+    }
+    if (lane == 0) {
+      fr[nfr] = ((uint64_t)__float_as_uint(prio) << 32) | (uint32_t)ix.children[2 * (size_t)node + side];
+      fr[nfr + 1] = ((uint64_t)__float_as_uint(far) << 32) | (uint32_t)ix.children[2 * (size_t)node + 1 - side];
+    }
+    __syncwarp();
+    nfr += 2;
+  }
+}
+
 // k: result-list width; k_out: entries written to oi/od; rerank (QUANT only):
 // number of leading results re-ordered by exact FP32 distance before output;
 // rng_seed: the query's random stream.
@@ -256,24 +384,25 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
     seeds_merge(seeds, bbuf, L.s, scap, cur, head, tail, sorted, __popc(m));
   };
 
-  // ---- tree seeding (greedy.rs:70-99, leaf budget 1) ----
+  // ---- tree seeding (greedy.rs:70-146): the points of the leaves each tree's
+  // search_leaves returns (flat_tree.rs:239-311), in leaf order ----
+  // Margins: FP32 hyperplanes (dot in the reference order + offset, builder.rs:331),
+  // or for quantized queries over int8 routing trees the reconstructed margin
+  // dot(codes) * scale * tree_query_scale + offset (flat_tree.rs:96-103), with
+  // tree_query_scale = max|q| / 127 of the FP32 query (lib.rs:283-296).
+  const bool qtrees = QUANT && ix.tree_codes != nullptr;
+  const float tqs = qtrees ? tree_query_scale(Qrow, ix.D) : 0.f;
+  uint64_t* fr = reinterpret_cast<uint64_t*>(wsm + L.fr_off());
   for (int t = 0; t < ix.n_trees; ++t) {
-    int node = ix.tree_roots[t];
-    while (ix.children[2 * (size_t)node] > 0) {
-      float margin = __fadd_rn(exact_dot_a(QUANT ? Qrow : q, ix.hyperplanes + (size_t)node * ix.Dp, ix.D),
-                               ix.offsets[node]);
-      int side;
-      if (fabsf(margin) < 1e-8f) side = rng.next_bool() ? 1 : 0;
-      else side = margin > 0.f ? 1 : 0;
-      node = ix.children[2 * (size_t)node + side];
-    }
-    int start = -ix.children[2 * (size_t)node], end = -ix.children[2 * (size_t)node + 1];
     const int32_t* tidx = ix.tree_idx + (size_t)t * ix.N;
-    for (int p0 = start; p0 < end; p0 += 32) {
-      int p = p0 + lane;
-      int32_t id = p < end ? tidx[p] : -1;
-      push_all(id, id >= 0);
-    }
+    tree_search_leaves(ix, ix.tree_roots[t], L.f > 0 ? ix.leaf_budget : 1, fr, L.f, rng, qtrees,
+                       QUANT ? Qrow : q, q8, tqs, &stats[3], [&](int start, int end) {
+                         for (int p0 = start; p0 < end; p0 += 32) {
+                           int p = p0 + lane;
+                           int32_t id = p < end ? tidx[p] : -1;
+                           push_all(id, id >= 0);
+                         }
+                       });
   }
   // ---- fill_random (greedy.rs:148-163) ----
   {
@@ -420,6 +549,38 @@ __global__ void __launch_bounds__(WPB * 32)
   }
 }
 
+// search_leaves of one tree for a batch of queries (warp per query), with the
+// search kernel's own routing code: leaves (start, end) in order into
+// out[q * budget * 2 ...], their count into cnt[q].  Random sides of tied
+// margins use the query's search stream (seed + qid_base + q; quantized
+// queries the seed alone).
+__global__ void __launch_bounds__(WPB * 32)
+    k_tree_leaves(SearchIndex ix, const float* Q, const int8_t* Q8, int nq, int tree, int budget, int fcap,
+                  uint64_t qid_base, int32_t* out, int32_t* cnt, unsigned long long* stats) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t* fr = reinterpret_cast<uint64_t*>(smem) + (size_t)w * fcap;
+  const bool qtrees = Q8 != nullptr;
+  for (int qi = blockIdx.x * WPB + w; qi < nq; qi += gridDim.x * WPB) {
+    const float* qf = Q + (size_t)qi * ix.Dp;
+    const int8_t* q8 = qtrees ? Q8 + (size_t)qi * ix.Dq : nullptr;
+    QRng rng{ix.seed + (qtrees ? 0ull : qid_base + (uint64_t)qi), 0};
+    const float tqs = qtrees ? tree_query_scale(qf, ix.D) : 0.f;
+    int n = 0;
+    int32_t* o = out + (size_t)qi * budget * 2;
+    tree_search_leaves(ix, ix.tree_roots[tree], budget, fr, fcap, rng, qtrees, qf, q8, tqs, &stats[3],
+                       [&](int start, int end) {
+                         if (lane == 0 && n < budget) {
+                           o[2 * n] = start;
+                           o[2 * n + 1] = end;
+                         }
+                         ++n;
+                       });
+    if (lane == 0) cnt[qi] = n < budget ? n : budget;
+    __syncwarp();
+  }
+}
+
 WarpLayout layout_for(const SearchIndex& ix, int k) {
   if (k > 256) throw std::invalid_argument("k must be <= 256");
   WarpLayout L;
@@ -427,9 +588,11 @@ WarpLayout layout_for(const SearchIndex& ix, int k) {
   L.kmax = k <= 32 ? 32 : (k <= 128 ? 128 : 256);
   L.s = seed_capacity(L.kmax);
   L.h = L.kmax <= 32 ? visited_capacity(L.kmax) : 0;  // wider searches use a global-memory table
+  L.f = ix.leaf_budget > 1 ? ix.frontier_cap : 0;
   set_smem_limit_once(reinterpret_cast<const void*>(k_search<false>), 200 * 1024);
   set_smem_limit_once(reinterpret_cast<const void*>(k_search<true>), 200 * 1024);
-  if (L.bytes() * WPB > 200 * 1024) throw std::invalid_argument("query dimension too large for search shared memory");
+  if (L.bytes() * WPB > 200 * 1024)
+    throw std::invalid_argument("query dimension and search_tree_leaf_budget too large for search shared memory");
   return L;
 }
 
@@ -492,6 +655,23 @@ void greedy_search_quantized(const SearchIndex& ix, const float* Q, const int8_t
   k_search<true><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, width, k_out, rerank, eps, 0,
                                                             QueryMeta{}, L, gv.p(), gv.cap, out_idx, out_dist,
                                                             dstats);
+  RINND_LAUNCH_CHECK();
+}
+
+void tree_leaves(const SearchIndex& ix, const float* Q, const int8_t* Q8, int nq, int tree, int budget,
+                 uint64_t qid_base, int32_t* out_leaves, int32_t* out_counts, cudaStream_t st,
+                 unsigned long long* dstats) {
+  if (nq <= 0) return;
+  if (tree < 0 || tree >= ix.n_trees) throw std::invalid_argument("tree index out of range");
+  if (budget < 1) throw std::invalid_argument("leaf budget must be >= 1");
+  if (Q8 && !ix.tree_codes) throw std::invalid_argument("the index has no int8 routing trees");
+  const int fcap = budget > 1 ? budget * std::max(ix.tree_depth, 1) + 2 : 3;
+  const size_t smem = (size_t)WPB * fcap * 8;
+  if (smem > 200 * 1024) throw std::invalid_argument("search_tree_leaf_budget too large for this forest");
+  set_smem_limit_once(reinterpret_cast<const void*>(k_tree_leaves), 200 * 1024);
+  const int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
+  k_tree_leaves<<<blocks, WPB * 32, smem, st>>>(ix, Q, Q8, nq, tree, budget, fcap, qid_base, out_leaves, out_counts,
+                                                dstats);
   RINND_LAUNCH_CHECK();
 }
 

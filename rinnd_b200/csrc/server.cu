@@ -178,7 +178,8 @@ bool Server::launch(Slot& s) {
   meta.stream = s.dstream.p;
   meta.out_off = s.doff.p;
   if (view.quantized) {
-    quantize_rows(s.dq.p, nq, D, Dp, view.index.Dq, view.encoding, view.global_mult, s.dq8.p, s.dqs.p, st);
+    quantize_rows(s.dq.p, nq, D, Dp, view.index.Dq, view.encoding, view.global_mult, view.index.dim_scales, s.dq8.p,
+                  s.dqs.p, st);
     greedy_search_packed(view.index, s.dq.p, s.dq8.p, s.dqs.p, nq, max_width, meta, s.didx.p, s.ddist.p, st,
                          view.stats);
   } else {

@@ -138,3 +138,66 @@ def test_released_fp32_rejects_rerank(rb, orc):
     assert ids.shape == (4, 6)
     with pytest.raises(ValueError, match="FP32 vector data was released"):
         ix.query_quantized(Q, k=6, candidate_width=18, rerank_width=12)
+
+
+def test_per_dimension_encoder_bit_exact(rb, orc):
+    """sq8d codes and per-dimension scales equal the restatement's: zero
+    columns, half-away ties (x / scale = k + 0.5) and saturation included."""
+    from rinnd_b200 import _lib as L
+
+    X = np.concatenate([gmm(3000, 96, 30, seed=23), edge_rows(96)]).astype(np.float32)
+    X[:, 7] = 0.0  # a zero column: scale 0, codes 0
+    X[10, 3] = 127.0 * 4.0
+    X[11, 3] = 2.5 * 4.0  # scale of column 3 is 4.0: code 2.5 rounds away from zero
+    X[12, 3] = -2.5 * 4.0
+    n, d = X.shape
+    codes = np.empty((n, d), np.int8)
+    scales = np.empty(d, np.float32)
+    L.check(L.lib.rinnd_quantize_rows_per_dimension(L.ptr(X), n, d, L.ptr(codes), L.ptr(scales)))
+    oc, osc = orc.quantize_per_dimension(X)
+    np.testing.assert_array_equal(scales.view(np.uint32), osc.view(np.uint32))
+    np.testing.assert_array_equal(codes, oc)
+    assert codes[11, 3] == 3 and codes[12, 3] == -3 and scales[7] == 0.0
+
+
+@pytest.mark.parametrize("rerank", [False, True])
+def test_per_dimension_search_distances_and_recall(rb, orc, rerank):
+    """Every returned distance of an sq8d search is 1 - clamp(per-dimension
+    dot) of the returned pair, computed by the oracle's
+    quantized_i8_per_dimension_dot (quantized.rs:48-56) bit for bit; with an
+    exact rerank the distances are the FP32 direct cosine of the pair.  Recall@10
+    vs exact cosine is not below the oracle's sq8d search minus 0.5 point."""
+    X, Q, ix = _setup(rb, orc, "sq8d", seed=13)
+    Xn, Qn = orc.normalize_rows(X), orc.normalize_rows(Q)
+    kw = dict(candidate_width=30, rerank_width=20) if rerank else {}
+    ids, dists = ix.query_quantized(Q, k=10, epsilon=0.1, **kw)
+    codes, scales = orc.quantize_per_dimension(Xn)
+    qc = orc.quantize_queries_per_dimension(Qn, scales)
+    for i in range(len(Q)):
+        v = ids[i][ids[i] >= 0]
+        if rerank:
+            want = orc.distance_pairs(DIRECT_COSINE, np.repeat(Qn[i:i + 1], len(v), 0), Xn[v]).astype(np.float32)
+        else:
+            sims = np.array([orc.i8_per_dimension_dot(qc[i], codes[j], scales) for j in v], np.float32)
+            want = np.float32(1.0) - np.clip(sims, np.float32(-1.0), np.float32(1.0))
+        np.testing.assert_array_equal(dists[i][: len(v)].view(np.uint32), want.view(np.uint32))
+    truth = _exact_cosine(orc, Xn, Qn, 10)
+    oix = orc.OracleIndex(Xn, n_neighbors=15, distance_kind=DIRECT_COSINE, angular=True,
+                          correction=orc.CORR_NONE, random_seed=3)
+    oids, _ = oix.query_quantized(Qn, k=10, epsilon=0.1, encoding=3, **kw)
+    assert recall(ids, truth) >= recall(oids, truth) - 0.005
+    assert ix.storage_info()["encoding"] == "sq8d_per_dimension_symmetric"
+
+
+def test_per_dimension_server_results_equal_alone(rb, orc):
+    """The continuous-batching server over an sq8d index returns what the index's
+    own quantized query returns."""
+    X, Q, ix = _setup(rb, orc, "sq8d", n=8000, nq=300, seed=17, quantized_candidate_width=24,
+                      quantized_rerank_width=12)
+    srv = rb.Server(ix)
+    rids = [srv.submit(Q[i:i + 30], k=8) for i in range(0, 300, 30)]
+    got = [srv.result(r) for r in rids]
+    srv.close()
+    alone_i, alone_d = ix.query_quantized(Q, k=8, candidate_width=24, rerank_width=12)
+    np.testing.assert_array_equal(np.concatenate([g[0] for g in got]), alone_i)
+    np.testing.assert_array_equal(np.concatenate([g[1] for g in got]).view(np.uint32), alone_d.view(np.uint32))
