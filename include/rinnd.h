@@ -85,7 +85,7 @@ typedef struct rinnd_build_params {
   int32_t n_iters;                  /* <= 0: max(5, ceil(log2 N)) (index.rs:623-625) */
   float delta;                      /* default 0.001                               */
   uint64_t random_seed;             /* default 42                                  */
-  float diversify_prob;             /* default 1.0 (only 1.0 is implemented)       */
+  float diversify_prob;             /* default 1.0: chance a qualifying prune is taken */
   float pruning_degree_multiplier;  /* default 1.5                                 */
   int32_t angular;                  /* angular RP splits (index.rs:606-614)        */
   int32_t distance_kind;            /* RINND_DIST_*                                */

@@ -257,7 +257,7 @@ def tree_route_points(hyperplanes, offsets, children, points):
     return out
 
 
-def search_graph_from_knn(knn_idx, knn_dist, data, kind, mult=1.5):
+def search_graph_from_knn(knn_idx, knn_dist, data, kind, mult=1.5, diversify_prob=1.0):
     knn_idx = np.ascontiguousarray(knn_idx, np.int32)
     knn_dist = _f(knn_dist)
     data = _f(data)
@@ -266,8 +266,8 @@ def search_graph_from_knn(knn_idx, knn_dist, data, kind, mult=1.5):
     indptr = np.empty(n + 1, np.int32)
     indices = np.empty(cap, np.int32)
     md = ctypes.c_float(0)
-    nnz = lib().orc_search_graph_from_knn(_p(knn_idx), _p(knn_dist), _p(data), n, k, data.shape[1], kind, 1.0, mult,
-                                          _p(indptr), _p(indices), cap, ctypes.byref(md))
+    nnz = lib().orc_search_graph_from_knn(_p(knn_idx), _p(knn_dist), _p(data), n, k, data.shape[1], kind,
+                                          float(diversify_prob), mult, _p(indptr), _p(indices), cap, ctypes.byref(md))
     return indptr, indices[:nnz].copy(), md.value
 
 

@@ -1035,11 +1035,15 @@ struct CSR {
   size_t n = 0;
 };
 
-// search_graph.rs:432-473 diversify_row (prune probability 1: no RNG consumed)
+// search_graph.rs:432-473 diversify_row.  A qualifying prune (:457-460) is
+// taken always at probability >= 1 (no draw), else when an f32 draw is below
+// the probability; the reference draws from rand::thread_rng() (OS-seeded, not
+// reproducible), this restatement from a FastRng seeded per row.
 static void diversify_row(const int32_t* ri, const float* rd, size_t len, const float* data,
                           size_t dim, int kind, size_t max_degree,
-                          std::vector<std::pair<int32_t, float>>& out) {
+                          std::vector<std::pair<int32_t, float>>& out, float prob = 1.0f, uint64_t rseed = 0) {
   out.clear();
+  FastRng rng(rseed);
   for (size_t pos = 0; pos < len; ++pos) {
     int32_t j = ri[pos];
     if (j < 0) break;
@@ -1048,8 +1052,10 @@ static void diversify_row(const int32_t* ri, const float* rd, size_t len, const 
     for (auto& cd : out) {
       float dcj = distance_impl(kind, data + (size_t)cd.first * dim, data + (size_t)j * dim, (int)dim);
       if (cd.second > FLT_MIN && dcj < dij) {
-        keep = false;
-        break;
+        if (prob >= 1.0f || rng.next_float() < prob) {
+          keep = false;
+          break;
+        }
       }
     }
     if (keep) {
@@ -1059,11 +1065,12 @@ static void diversify_row(const int32_t* ri, const float* rd, size_t len, const 
   }
 }
 
-// search_graph.rs:478-523 diversify_sorted_csr
+// search_graph.rs:478-523 diversify_sorted_csr (prune probability as diversify_row)
 static void diversify_sorted(const int32_t* ri, const float* rd, const std::vector<size_t>& order,
                              const float* data, size_t dim, int kind, size_t max_degree,
-                             std::vector<std::pair<int32_t, float>>& out) {
+                             std::vector<std::pair<int32_t, float>>& out, float prob = 1.0f, uint64_t rseed = 0) {
   out.clear();
+  FastRng rng(rseed);
   for (size_t pos : order) {
     int32_t j = ri[pos];
     if (j < 0) continue;
@@ -1072,8 +1079,10 @@ static void diversify_sorted(const int32_t* ri, const float* rd, const std::vect
     for (auto& cd : out) {
       float dcj = distance_impl(kind, data + (size_t)cd.first * dim, data + (size_t)j * dim, (int)dim);
       if (cd.second > FLT_MIN && dcj < dij) {
-        keep = false;
-        break;
+        if (prob >= 1.0f || rng.next_float() < prob) {
+          keep = false;
+          break;
+        }
       }
     }
     if (keep) {
@@ -1132,12 +1141,13 @@ static CSR weighted_union_pruned(const std::vector<std::vector<std::pair<int32_t
 // search_graph.rs:263-360 from_dense_diversified
 static CSR from_dense_diversified(const int32_t* ni, const float* nd, const float* data, size_t n,
                                   size_t k, size_t dim, int kind, float mult, int nt,
-                                  float* min_distance) {
+                                  float* min_distance, float prob = 1.0f, uint64_t seed = 0) {
   size_t max_degree = (size_t)std::round(mult * (float)k);  // f32::round, half away from zero
   std::vector<std::vector<std::pair<int32_t, float>>> fwd(n), rev(n);
 #pragma omp parallel for schedule(dynamic, 256) num_threads(nt)
   for (long i = 0; i < (long)n; ++i)
-    diversify_row(ni + (size_t)i * k, nd + (size_t)i * k, k, data, dim, kind, max_degree, fwd[(size_t)i]);
+    diversify_row(ni + (size_t)i * k, nd + (size_t)i * k, k, data, dim, kind, max_degree, fwd[(size_t)i], prob,
+                  seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(i + 1)));
   // forward CSR with data (:299-309) and transpose (:526-567)
   std::vector<int32_t> fptr(n + 1, 0), findx;
   std::vector<float> fdat;
@@ -1177,7 +1187,8 @@ static CSR from_dense_diversified(const int32_t* ni, const float* nd, const floa
     std::iota(order.begin(), order.end(), 0);
     const float* rd = &tdat[s];
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return rd[a] < rd[b]; });
-    diversify_sorted(&tidx[s], rd, order, data, dim, kind, max_degree, rev[i]);
+    diversify_sorted(&tidx[s], rd, order, data, dim, kind, max_degree, rev[i], prob,
+                     ~seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(i + 1)));
   }
   CSR g = weighted_union_pruned(fwd, rev, n, max_degree);
   float md = INFINITY;  // :353-357
@@ -1523,9 +1534,8 @@ int64_t orc_search_graph_from_knn(const int32_t* knn_idx, const float* knn_dist,
                                   int32_t n, int32_t k, int32_t dim, int kind, float diversify_prob,
                                   float mult, int32_t* indptr, int32_t* indices, int64_t cap,
                                   float* min_distance) {
-  (void)diversify_prob;  // prune probability < 1 consumes thread_rng; only 1.0 is restated
   CSR g = from_dense_diversified(knn_idx, knn_dist, data, (size_t)n, (size_t)k, (size_t)dim, kind,
-                                 mult, num_threads_of(0), min_distance);
+                                 mult, num_threads_of(0), min_distance, diversify_prob, 42);
   std::memcpy(indptr, g.indptr.data(), sizeof(int32_t) * ((size_t)n + 1));
   int64_t nnz = (int64_t)g.indices.size();
   if (nnz <= cap) std::memcpy(indices, g.indices.data(), sizeof(int32_t) * (size_t)nnz);
@@ -1607,7 +1617,8 @@ orc_index* orc_build(const float* data, int64_t n_, int32_t dim_, const orc_para
   ix->iters = (int)iters;
   g.sort_all();
   ix->graph = from_dense_diversified(g.indices.data(), g.distances.data(), data, n, k, dim, ix->kind,
-                                     p->pruning_degree_multiplier, nt, &ix->min_distance);
+                                     p->pruning_degree_multiplier, nt, &ix->min_distance, p->diversify_prob,
+                                     p->random_seed);
   ix->nbr_idx = g.indices;
   ix->nbr_dist.resize(g.distances.size());
   for (size_t i = 0; i < g.distances.size(); ++i) ix->nbr_dist[i] = correct(ix->corr, g.distances[i]);

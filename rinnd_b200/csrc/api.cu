@@ -288,7 +288,7 @@ void validate_params(const rinnd_build_params* p, int64_t n, int d) {
   require(p->search_tree_leaf_budget <= 256, "search_tree_leaf_budget must be <= 256");
   require(p->distance_kind >= 0 && p->distance_kind < DK_COUNT, "unknown distance kind");
   require(p->correction >= 0 && p->correction <= CK_ALT_IP, "unknown correction");
-  require(p->diversify_prob >= 1.0f, "diversify_prob < 1 is not implemented");
+  require(p->diversify_prob == p->diversify_prob, "diversify_prob must not be NaN");
   require(p->pruning_degree_multiplier > 0.f, "pruning_degree_multiplier must be positive");
   require(p->precision == RINND_PRECISION_FP32 || p->precision == RINND_PRECISION_BF16, "unknown precision");
 }
@@ -394,7 +394,7 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   // diversified CSR (index.rs:656-666) on the original order
   float min_d = 0.f;
   build_search_graph(knn_idx.p, knn_raw.p, X0.p, N, k, D, Dp, ix->kind, pin->pruning_degree_multiplier, st,
-                     tmp, ix->graph_orig, &min_d);
+                     tmp, ix->graph_orig, &min_d, pin->diversify_prob, pin->random_seed);
   ix->min_distance = min_d;
   // corrected neighbor distances (index.rs:669-673)
   apply_correction_dev(knn_raw.p, (int64_t)N * k, ix->corr, st);

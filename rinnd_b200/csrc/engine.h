@@ -111,10 +111,12 @@ struct Csr {
   DVec<int32_t> indices;  // nnz
   int64_t nnz = 0;
 };
-// search_graph.rs:263-360 from a sorted dense kNN graph (raw distances).
+// search_graph.rs:263-360 from a sorted dense kNN graph (raw distances); a
+// qualifying prune is taken with probability prune_prob (diversify_prob, 1 = always).
 void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const float* X, int N,
                         int k, int D, int Dp, int kind, float mult, cudaStream_t st,
-                        TempStorage& tmp, Csr& out, float* min_distance_host);
+                        TempStorage& tmp, Csr& out, float* min_distance_host, float prune_prob = 1.0f,
+                        uint64_t seed = 0);
 // search_graph.rs:199-229: row new_v = old row order[new_v], neighbors mapped by inverse.
 void reorder_csr(const Csr& in, const int32_t* order, const int32_t* inverse, cudaStream_t st,
                  TempStorage& tmp, Csr& out);

@@ -25,10 +25,27 @@ namespace {
 
 constexpr int WARPS = 4;
 
+// Prune probability (diversify_prob): the reference draws rand::thread_rng()'s
+// f32 for every pruning decision that qualifies and prunes when the draw is below
+// the probability (search_graph.rs:457-460, :506-509), an OS-seeded stream.  Here the draw of
+// the decision (row, candidate j, retained c) is a keyed hash, 24-bit uniform
+// like rand's f32: the outcome is reproducible, and since each decision has its
+// own draw, "some retained c prunes j" does not depend on the order the retained
+// entries are tested in.  prob >= 1 prunes every qualifying decision (no draw).
+struct PruneDraw {
+  float prob;
+  uint64_t seed;
+};
+__device__ __forceinline__ bool prune_draw(const PruneDraw& pd, int row, int32_t j, int32_t c) {
+  if (pd.prob >= 1.0f) return true;
+  const uint64_t h = hash3(pd.seed ^ 0xD17E55ull, ((uint64_t)(uint32_t)row << 32) | (uint32_t)j, (uint32_t)c);
+  return (float)(h >> 40) * 5.9604644775390625e-08f < pd.prob;  // (h >> 40) / 2^24
+}
+
 // Warp-cooperative RNG-style prune step: does any retained c (in smem) prune j?
 __device__ __forceinline__ bool pruned_by_retained(const int32_t* ret_id, const float* ret_d, int nret,
                                                    int32_t j, float dij, const float* X, int D,
-                                                   int Dp, int kind) {
+                                                   int Dp, int kind, const PruneDraw& pd, int row) {
   const int lane = threadIdx.x & 31;
   for (int r0 = 0; r0 < nret; r0 += 32) {
     int r = r0 + lane;
@@ -37,7 +54,7 @@ __device__ __forceinline__ bool pruned_by_retained(const int32_t* ret_id, const 
       float dic = ret_d[r];
       if (dic > FLT_MIN) {
         float dcj = exact_distance(kind, X + (size_t)ret_id[r] * Dp, X + (size_t)j * Dp, D);
-        pr = dcj < dij;
+        pr = dcj < dij && prune_draw(pd, row, j, ret_id[r]);
       }
     }
     if (__any_sync(0xffffffffu, pr)) return true;
@@ -49,7 +66,7 @@ template <int MAXR>
 __global__ void k_diversify_fwd(const int32_t* knn_idx, const float* knn_dist, int N, int k,
                                 const float* X, int D, int Dp, int kind, int max_degree,
                                 int32_t* fwd_idx, float* fwd_dist, int32_t* fwd_cnt,
-                                uint32_t* min_key) {
+                                uint32_t* min_key, PruneDraw pd) {
   __shared__ int32_t s_id[WARPS][MAXR];
   __shared__ float s_d[WARPS][MAXR];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -61,7 +78,7 @@ __global__ void k_diversify_fwd(const int32_t* knn_idx, const float* knn_dist, i
     int32_t j = knn_idx[(size_t)row * k + pos];
     if (j < 0) break;
     float dij = knn_dist[(size_t)row * k + pos];
-    bool pruned = pruned_by_retained(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind);
+    bool pruned = pruned_by_retained(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind, pd, row);
     if (!pruned) {
       if (lane == 0) {
         s_id[w][nret] = j;
@@ -121,7 +138,7 @@ __device__ __forceinline__ StagedWarp staged_warp(unsigned char* smem, int w, in
 
 // The n candidates (cid/dpos filled, synchronized) -> sw.ret[0, nret); returns nret.
 __device__ __forceinline__ int staged_prune(const StagedWarp& sw, int n, const float* X, int D, int Dp, int kind,
-                                            int max_degree) {
+                                            int max_degree, const PruneDraw& pd, int row) {
   const int lane = threadIdx.x & 31, rs = Dp + 4, q4 = Dp / 4;
   // every 16-byte piece of every candidate row in flight at once (cp.async, L2 only)
   for (int e = lane; e < n * q4; e += 32) {
@@ -148,7 +165,7 @@ __device__ __forceinline__ int staged_prune(const StagedWarp& sw, int n, const f
     bool pr = false;
     if (lane < nret) {
       const int c = sw.ret[lane];
-      pr = sw.dpos[c] > FLT_MIN && sw.M[c * SK + pos] < dij;
+      pr = sw.dpos[c] > FLT_MIN && sw.M[c * SK + pos] < dij && prune_draw(pd, row, sw.cid[pos], sw.cid[c]);
     }
     if (!__any_sync(0xffffffffu, pr)) {
       if (lane == 0) sw.ret[nret] = pos;
@@ -164,7 +181,7 @@ __device__ __forceinline__ int staged_prune(const StagedWarp& sw, int n, const f
 __global__ void __launch_bounds__(32 * WARPS)
     k_diversify_fwd_staged(const int32_t* knn_idx, const float* knn_dist, int N, int k, const float* X, int D,
                            int Dp, int kind, int max_degree, int32_t* fwd_idx, float* fwd_dist, int32_t* fwd_cnt,
-                           uint32_t* min_key) {
+                           uint32_t* min_key, PruneDraw pd) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * WARPS + w;
@@ -182,7 +199,7 @@ __global__ void __launch_bounds__(32 * WARPS)
   sw.dpos[lane] = my_d;
   sw.cid[lane] = my_id;
   __syncwarp();
-  const int nret = staged_prune(sw, n, X, D, Dp, kind, max_degree);
+  const int nret = staged_prune(sw, n, X, D, Dp, kind, max_degree, pd, row);
   uint32_t local_min = KEY_INF;
   for (int r = lane; r < nret; r += 32) {
     const int pos = sw.ret[r];
@@ -225,7 +242,7 @@ __global__ void k_transpose(const int32_t* fwd_idx, const float* fwd_dist, const
 template <int MAXR>
 __global__ void k_diversify_rev(const int32_t* rev_ptr, const uint64_t* rev_key, int N,
                                 const float* X, int D, int Dp, int kind, int max_degree,
-                                int32_t* rret_idx, float* rret_dist, int32_t* rret_cnt) {
+                                int32_t* rret_idx, float* rret_dist, int32_t* rret_cnt, PruneDraw pd) {
   __shared__ int32_t s_id[WARPS][MAXR];
   __shared__ float s_d[WARPS][MAXR];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -236,7 +253,7 @@ __global__ void k_diversify_rev(const int32_t* rev_ptr, const uint64_t* rev_key,
     uint64_t key = rev_key[e];
     int32_t j = (int32_t)(uint32_t)key;
     float dij = fkey_inv((uint32_t)(key >> 32));
-    bool pruned = pruned_by_retained(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind);
+    bool pruned = pruned_by_retained(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind, pd, row);
     if (!pruned) {
       if (lane == 0) {
         s_id[w][nret] = j;
@@ -384,8 +401,10 @@ void exclusive_scan(const T* in, T* out, long long n, TempStorage& tmp, cudaStre
 
 void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const float* X, int N,
                         int k, int D, int Dp, int kind, float mult, cudaStream_t st,
-                        TempStorage& tmp, Csr& out, float* min_distance_host) {
+                        TempStorage& tmp, Csr& out, float* min_distance_host, float prune_prob,
+                        uint64_t seed) {
   const int max_degree = (int)roundf(mult * (float)k);  // f32::round (:276)
+  const PruneDraw pd_fwd{prune_prob, seed}, pd_rev{prune_prob, seed ^ 0x5EEDull};
   if (k > 128 || max_degree < 1 || max_degree > 384)
     throw std::invalid_argument("search graph supports n_neighbors <= 128 and 1 <= round(mult * k) <= 384");
   const int blocks = (N + WARPS - 1) / WARPS;
@@ -398,15 +417,15 @@ void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const flo
     set_smem_limit_once(reinterpret_cast<const void*>(k_diversify_fwd_staged), 227 * 1024);
     k_diversify_fwd_staged<<<blocks, 32 * WARPS, staged_bytes, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind,
                                                                     max_degree, fwd_idx.p, fwd_dist.p, fwd_cnt.p,
-                                                                    min_key.p);
+                                                                    min_key.p, pd_fwd);
   } else if (k <= 32)
     k_diversify_fwd<32><<<blocks, 32 * WARPS, 0, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind,
                                                       max_degree, fwd_idx.p, fwd_dist.p, fwd_cnt.p,
-                                                      min_key.p);
+                                                      min_key.p, pd_fwd);
   else
     k_diversify_fwd<128><<<blocks, 32 * WARPS, 0, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind,
                                                        max_degree, fwd_idx.p, fwd_dist.p, fwd_cnt.p,
-                                                       min_key.p);
+                                                       min_key.p, pd_fwd);
   RINND_LAUNCH_CHECK();
   // transpose
   DVec<int32_t> indeg((size_t)N + 1, st), rev_ptr((size_t)N + 1, st), cursor((size_t)N + 1, st);
@@ -437,10 +456,10 @@ void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const flo
   // sequential form beat the staged pair table there)
   if (max_degree <= 32)
     k_diversify_rev<32><<<blocks, 32 * WARPS, 0, st>>>(rev_ptr.p, rev_sorted.p, N, X, D, Dp, kind,
-                                                      max_degree, rret_idx.p, rret_dist.p, rret_cnt.p);
+                                                      max_degree, rret_idx.p, rret_dist.p, rret_cnt.p, pd_rev);
   else
     k_diversify_rev<384><<<blocks, 32 * WARPS, 0, st>>>(rev_ptr.p, rev_sorted.p, N, X, D, Dp, kind,
-                                                       max_degree, rret_idx.p, rret_dist.p, rret_cnt.p);
+                                                       max_degree, rret_idx.p, rret_dist.p, rret_cnt.p, pd_rev);
   RINND_LAUNCH_CHECK();
   // union + prune
   DVec<int32_t> rows((size_t)N * max_degree, st), cnt((size_t)N + 1, st);

@@ -138,3 +138,24 @@ def test_search_graph_with_missing_neighbors(rb, orc):
     op, oi, omd = orc.search_graph_from_knn(ki, kd, data, 0)
     gp, gi, gmd = gpu_search_graph(ki, kd, data, 0)
     assert np.array_equal(op, gp) and np.array_equal(oi, gi) and omd == gmd
+
+
+def test_diversify_prob_below_one(rb, orc):
+    """diversify_prob (search_graph.rs:457-460, :506-509): at probability 0 no
+    qualifying prune is taken, so the search graph is exactly the oracle's from
+    the same kNN rows; at 0.5 the GPU's keyed draws and the oracle's stream give
+    graphs of the same size within 2 %, between those of probability 0 and 1."""
+    X = gmm(6000, 24, 30, seed=41)
+    sizes = {}
+    for prob in (1.0, 0.5, 0.0):
+        ix = rb.RINND(X, metric="sqeuclidean", n_neighbors=12, random_state=2, diversify_prob=prob)
+        gi, gd = ix.neighbor_graph
+        indptr, indices, _ = ix.search_graph
+        oindptr, oindices, _ = orc.search_graph_from_knn(gi, gd, X, 0, mult=1.5, diversify_prob=prob)
+        if prob != 0.5:
+            np.testing.assert_array_equal(indptr, oindptr)
+            np.testing.assert_array_equal(indices, oindices)
+        else:
+            assert abs(len(indices) - len(oindices)) <= 0.02 * len(oindices), (len(indices), len(oindices))
+        sizes[prob] = len(indices)
+    assert sizes[1.0] < sizes[0.5] < sizes[0.0], sizes
