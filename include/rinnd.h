@@ -142,6 +142,17 @@ RINND_EXPORT int rinnd_build_on_stream(const float* data, int32_t data_on_device
                                        int64_t ld, const rinnd_build_params* p, void* stream,
                                        rinnd_index** out);
 RINND_EXPORT int rinnd_free(rinnd_index* idx);
+/* Index files (no counterpart in the reference, whose indices live in memory
+ * only): rinnd_save writes every resident array of the index (rows in search
+ * layout, graphs, trees, int8 codes) and `meta`, an opaque caller string (may
+ * be NULL), to `path`; rinnd_load reads such a file onto `device` and returns
+ * the index, whose queries then return exactly what the saved index's did.
+ * meta (meta_cap bytes, may be NULL) receives the stored string NUL-terminated
+ * and *meta_len (may be NULL) its full length.  A file of another format or
+ * version, or a truncated one, fails with RINND_ERR_INVALID. */
+RINND_EXPORT int rinnd_save(rinnd_index* idx, const char* path, const char* meta);
+RINND_EXPORT int rinnd_load(const char* path, int32_t device, rinnd_index** out, char* meta, int64_t meta_cap,
+                            int64_t* meta_len);
 /* ---- batched form: many independent indices ------------------------------- */
 /* One index of a batch: n x d f32 rows (row stride ld floats) on the host or,
  * with data_on_device, in device memory of params->device; params as for

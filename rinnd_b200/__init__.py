@@ -9,7 +9,9 @@ include/rinnd.h; there is no CPU path.
 from __future__ import annotations
 
 import ctypes
+import json
 import math
+import os
 import threading
 import time
 
@@ -17,7 +19,7 @@ import numpy as np
 
 from . import _lib as L
 
-__all__ = ["RINND", "version", "simd_info", "device_count"]
+__all__ = ["RINND", "Server", "build_many", "load", "version", "simd_info", "device_count"]
 
 # Metric::from_str aliases (core/distance/mod.rs:203-247).
 _ALIASES = {
@@ -198,8 +200,9 @@ class RINND:
         L.check(L.lib.rinnd_build(L.ptr(data), data.shape[0], data.shape[1], ctypes.byref(p), ctypes.byref(h)))
         self._attach(h, state)
 
-    def _attach(self, h, state):
+    def _attach(self, h, state, encode=True):
         self._h = h
+        self._state = dict(state)
         self.n_points, self.dim, self.n_neighbors = state["n_points"], state["dim"], state["n_neighbors"]
         self.metric = state["metric"]
         self._encoding = state["encoding"]
@@ -207,6 +210,8 @@ class RINND:
         self._rerank_width = state["rerank_width"]
         self._retain_fp32 = state["retain_fp32"]
         self._leaf_budget = state["leaf_budget"]
+        if not encode:
+            return
         if self._encoding is not None:
             # QuantizedI8Index::new (lib.rs:159-276): codes, int8 routing trees, released FP32 rows
             L.check(L.lib.rinnd_quantize(self._h, self._encoding))
@@ -333,6 +338,12 @@ class RINND:
                                                L.ptr(piv) if with_pivots else None))
         return (hp, off, ch, ind, piv) if with_pivots else (hp, off, ch, ind)
 
+    def save(self, path):
+        """Writes the index (every device array, and this object's settings) to
+        `path`; `load(path)` restores it.  No counterpart in the reference."""
+        meta = json.dumps({**self._state, "retain_fp32": self._retain_fp32}).encode()
+        L.check(L.lib.rinnd_save(self._h, os.fsencode(path), meta))
+
     def search_tree_leaves(self, query_data, tree=0, leaf_budget=None, quantized=False):
         """The leaves FlatTree::search_leaves (flat_tree.rs:239-311) visits in
         retained tree `tree` for each query, as the search seeds them: a list
@@ -383,6 +394,21 @@ class RINND:
             "tree_code_bytes", "tree_scale_bytes", "tree_offset_bytes", "tree_topology_bytes"))
         info["bytes_per_vector"] = info["allocated_bytes"] / self.n_points
         return info
+
+
+def load(path, device=0) -> RINND:
+    """An index written by RINND.save, on CUDA device `device`."""
+    h = ctypes.c_void_p()
+    n = ctypes.c_int64(0)
+    buf = ctypes.create_string_buffer(1 << 16)  # the settings string is a few hundred bytes
+    L.check(L.lib.rinnd_load(os.fsencode(path), int(device), ctypes.byref(h), buf, 1 << 16, ctypes.byref(n)))
+    if n.value >= (1 << 16):
+        L.lib.rinnd_free(h)
+        raise ValueError(f"{path}: the index settings are unreadable")
+    ix = RINND.__new__(RINND)
+    ix._h = None
+    ix._attach(h, json.loads(buf.value.decode()), encode=False)
+    return ix
 
 
 def build_many(datasets, params=None, n_workers=0, **common):

@@ -84,6 +84,8 @@ SIGNATURES = {
     "rinnd_build_device": (ctypes.c_int, [_P, _i64, _i32, _i64, _P, _P]),
     "rinnd_build_on_stream": (ctypes.c_int, [_P, _i32, _i64, _i32, _i64, _P, _P, _P]),
     "rinnd_free": (ctypes.c_int, [_P]),
+    "rinnd_save": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_char_p]),
+    "rinnd_load": (ctypes.c_int, [ctypes.c_char_p, _i32, _P, _P, _i64, _P]),
     "rinnd_build_many": (ctypes.c_int, [_P, _i32, _i32, _P, _P]),
     "rinnd_build_info_get": (ctypes.c_int, [_P, _P]),
     "rinnd_index_shape": (ctypes.c_int, [_P, _P, _P, _P]),

@@ -330,7 +330,11 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   ix->p.n_iters = n_iters;
   ix->p.search_tree_leaf_budget = std::max(1, pin->search_tree_leaf_budget);
 
-  reserve_pool(pin->device, build_working_set(n, Dp, k, c, pin->n_trees), st);
+  // (the BF16 precision form adds its BF16 copy of the rows and two floats per row)
+  reserve_pool(pin->device,
+               build_working_set(n, Dp, k, c, pin->n_trees) +
+                   (pin->precision == RINND_PRECISION_BF16 ? (size_t)n * (round_up(d, 16) * 2 + 8) : 0),
+               st);
   TempStorage tmp;
   DVec<float> X0;
   load_rows(data, on_device, n, d, ld, Dp, X0, st);
@@ -1180,6 +1184,224 @@ int rinnd_quantize_rows(const float* data, int64_t n, int32_t d, int32_t encodin
     S.to_host(scales, (size_t)n);
     RINND_CUDA(cudaStreamSynchronize(sg.s));
     if (global_multiplier) *global_multiplier = gm;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// ---- index file (no counterpart in the reference, whose indices live in memory
+// only): a header, then every resident array as (element count u64, bytes).
+constexpr char kFileMagic[8] = {'R', 'I', 'N', 'N', 'D', 'B', '2', '\0'};
+constexpr uint32_t kFileVersion = 1;
+
+struct FileHeader {
+  char magic[8];
+  uint32_t version, header_bytes;
+  int64_t N, n_nodes, graph_int_nnz, graph_orig_nnz;
+  int32_t D, Dp, k, kind, corr, normalize, encoding, Dq, n_search_trees, forest_levels, fp32_released, pad;
+  float global_mult, min_distance;
+  double encode_seconds;
+  rinnd_build_params params;
+  rinnd_build_info info;
+};
+
+struct File {
+  FILE* f = nullptr;
+  std::string path;
+  ~File() {
+    if (f) std::fclose(f);
+  }
+  void write(const void* p, size_t bytes) {
+    if (bytes && std::fwrite(p, 1, bytes, f) != bytes) throw std::invalid_argument("cannot write index file " + path);
+  }
+  void read(void* p, size_t bytes) {
+    if (bytes && std::fread(p, 1, bytes, f) != bytes)
+      throw std::invalid_argument("index file " + path + " is truncated or unreadable");
+  }
+};
+
+template <class T>
+void save_array(File& F, const DVec<T>& v, size_t count, cudaStream_t st) {
+  const uint64_t c = v.p ? (uint64_t)count : 0;
+  F.write(&c, sizeof(c));
+  if (!c) return;
+  std::vector<T> h((size_t)c);
+  v.to_host(h.data(), (size_t)c);
+  RINND_CUDA(cudaStreamSynchronize(st));
+  F.write(h.data(), sizeof(T) * (size_t)c);
+}
+
+template <class T>
+void load_array(File& F, DVec<T>& v, cudaStream_t st, size_t expect_max) {
+  uint64_t c = 0;
+  F.read(&c, sizeof(c));
+  require(c <= expect_max, "index file " + F.path + " has an array larger than its header allows");
+  if (!c) return;
+  std::vector<T> h((size_t)c);
+  F.read(h.data(), sizeof(T) * (size_t)c);
+  v.alloc((size_t)c, st);
+  v.from_host(h.data(), (size_t)c);
+  RINND_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace
+
+extern "C" {
+
+int rinnd_save(rinnd_index* idx, const char* path, const char* meta) {
+  return guarded([&] {
+    check_index(idx);
+    require(path != nullptr, "path must not be null");
+    std::lock_guard<std::mutex> lock(idx->mu);
+    RINND_CUDA(cudaSetDevice(idx->device));
+    cudaStream_t st = idx->st;
+    RINND_CUDA(cudaStreamSynchronize(st));
+    File F;
+    F.path = path;
+    F.f = std::fopen(path, "wb");
+    require(F.f != nullptr, std::string("cannot open index file ") + path + " for writing");
+    FileHeader h{};
+    std::memcpy(h.magic, kFileMagic, 8);
+    h.version = kFileVersion;
+    h.header_bytes = sizeof(FileHeader);
+    h.N = idx->N;
+    h.n_nodes = idx->forest.n_nodes;
+    h.graph_int_nnz = idx->graph_int.nnz;
+    h.graph_orig_nnz = idx->graph_orig.nnz;
+    h.D = idx->D;
+    h.Dp = idx->Dp;
+    h.k = idx->k;
+    h.kind = idx->kind;
+    h.corr = idx->corr;
+    h.normalize = idx->normalize ? 1 : 0;
+    h.encoding = idx->encoding;
+    h.Dq = idx->Dq;
+    h.n_search_trees = idx->n_search_trees;
+    h.forest_levels = idx->forest.levels;
+    h.fp32_released = idx->fp32_released ? 1 : 0;
+    h.global_mult = idx->global_mult;
+    h.min_distance = idx->min_distance;
+    h.encode_seconds = idx->encode_seconds;
+    h.params = idx->p;
+    h.info = idx->info;
+    F.write(&h, sizeof(h));
+    const std::string m = meta ? meta : "";
+    const uint64_t mlen = m.size();
+    F.write(&mlen, sizeof(mlen));
+    F.write(m.data(), m.size());
+    const size_t N = (size_t)idx->N, nn = (size_t)idx->forest.n_nodes;
+    save_array(F, idx->X, N * idx->Dp, st);
+    save_array(F, idx->vertex_order, N, st);
+    save_array(F, idx->graph_orig.indptr, N + 1, st);
+    save_array(F, idx->graph_orig.indices, (size_t)idx->graph_orig.nnz, st);
+    save_array(F, idx->graph_int.indptr, N + 1, st);
+    save_array(F, idx->graph_int.indices, (size_t)idx->graph_int.nnz, st);
+    save_array(F, idx->knn_idx, N * idx->k, st);
+    save_array(F, idx->knn_dist, N * idx->k, st);
+    save_array(F, idx->forest.children, 2 * nn, st);
+    save_array(F, idx->forest.offsets, nn, st);
+    save_array(F, idx->forest.hyperplanes, nn * idx->Dp, st);
+    save_array(F, idx->forest.pivots, 2 * nn, st);
+    save_array(F, idx->tree_idx, (size_t)idx->n_search_trees * N, st);
+    save_array(F, idx->tree_roots, (size_t)idx->n_search_trees, st);
+    save_array(F, idx->codes, N * idx->Dq, st);
+    save_array(F, idx->inv_norms, N, st);
+    save_array(F, idx->dim_scales, (size_t)idx->Dq, st);
+    save_array(F, idx->tree_codes, nn * idx->Dq, st);
+    save_array(F, idx->tree_scales, nn, st);
+    require(std::fflush(F.f) == 0, std::string("cannot write index file ") + path);
+  });
+}
+
+int rinnd_load(const char* path, int32_t device, rinnd_index** out, char* meta, int64_t meta_cap,
+               int64_t* meta_len) {
+  return guarded([&] {
+    require(path != nullptr && out != nullptr, "path and out must not be null");
+    *out = nullptr;
+    File F;
+    F.path = path;
+    F.f = std::fopen(path, "rb");
+    require(F.f != nullptr, std::string("cannot open index file ") + path);
+    FileHeader h{};
+    F.read(&h, sizeof(h));
+    require(std::memcmp(h.magic, kFileMagic, 8) == 0, std::string(path) + " is not a rinnd_b200 index file");
+    require(h.version == kFileVersion && h.header_bytes == sizeof(FileHeader),
+            std::string(path) + " was written by an incompatible version");
+    require(h.N >= 1 && h.D >= 1 && h.Dp == round_up(h.D, 4) && h.k >= 1 && h.n_nodes >= 0 &&
+                h.n_search_trees >= 0 && h.graph_orig_nnz >= 0 && h.graph_int_nnz >= 0,
+            std::string(path) + " has an invalid header");
+    uint64_t mlen = 0;
+    F.read(&mlen, sizeof(mlen));
+    require(mlen < (1ull << 30), std::string(path) + " has an invalid header");
+    std::string m((size_t)mlen, '\0');
+    F.read(&m[0], (size_t)mlen);
+    ensure_device(device);
+    std::unique_ptr<rinnd_index> ix(new rinnd_index());
+    ix->device = device;
+    RINND_CUDA(cudaStreamCreateWithFlags(&ix->st, cudaStreamNonBlocking));
+    cudaStream_t st = ix->st;
+    ix->N = h.N;
+    ix->D = h.D;
+    ix->Dp = h.Dp;
+    ix->k = h.k;
+    ix->kind = h.kind;
+    ix->corr = h.corr;
+    ix->normalize = h.normalize != 0;
+    ix->encoding = h.encoding;
+    ix->Dq = h.Dq;
+    ix->n_search_trees = h.n_search_trees;
+    ix->fp32_released = h.fp32_released != 0;
+    ix->global_mult = h.global_mult;
+    ix->min_distance = h.min_distance;
+    ix->encode_seconds = h.encode_seconds;
+    ix->p = h.params;
+    ix->p.device = device;
+    ix->info = h.info;
+    const size_t N = (size_t)h.N, nn = (size_t)h.n_nodes;
+    load_array(F, ix->X, st, N * h.Dp);
+    load_array(F, ix->vertex_order, st, N);
+    load_array(F, ix->graph_orig.indptr, st, N + 1);
+    load_array(F, ix->graph_orig.indices, st, (size_t)h.graph_orig_nnz);
+    load_array(F, ix->graph_int.indptr, st, N + 1);
+    load_array(F, ix->graph_int.indices, st, (size_t)h.graph_int_nnz);
+    load_array(F, ix->knn_idx, st, N * h.k);
+    load_array(F, ix->knn_dist, st, N * h.k);
+    load_array(F, ix->forest.children, st, 2 * nn);
+    load_array(F, ix->forest.offsets, st, nn);
+    load_array(F, ix->forest.hyperplanes, st, nn * h.Dp);
+    load_array(F, ix->forest.pivots, st, 2 * nn);
+    load_array(F, ix->tree_idx, st, (size_t)h.n_search_trees * N);
+    load_array(F, ix->tree_roots, st, (size_t)h.n_search_trees);
+    load_array(F, ix->codes, st, N * (size_t)std::max(h.Dq, 0));
+    load_array(F, ix->inv_norms, st, N);
+    load_array(F, ix->dim_scales, st, (size_t)std::max(h.Dq, 0));
+    load_array(F, ix->tree_codes, st, nn * (size_t)std::max(h.Dq, 0));
+    load_array(F, ix->tree_scales, st, nn);
+    require(ix->vertex_order.n == N && ix->graph_int.indptr.n == N + 1 && ix->knn_idx.n == N * h.k &&
+                (ix->fp32_released || ix->X.n == N * h.Dp),
+            std::string(path) + " is missing index arrays");
+    ix->graph_orig.N = ix->graph_int.N = (int)N;
+    ix->graph_orig.nnz = h.graph_orig_nnz;
+    ix->graph_int.nnz = h.graph_int_nnz;
+    ix->forest.n_nodes = h.n_nodes;
+    ix->forest.levels = h.forest_levels;
+    ix->forest.T = h.params.n_trees;
+    ix->forest.N = (int)N;
+    ix->forest.Dp = h.Dp;
+    ix->inverse.alloc(N, st);
+    invert_permutation(ix->vertex_order.p, (int)N, ix->inverse.p, st);
+    ix->search_stats.alloc(4, st);
+    ix->search_stats.fill_bytes(0);
+    RINND_CUDA(cudaStreamSynchronize(st));
+    if (meta_len) *meta_len = (int64_t)m.size();
+    if (meta && meta_cap > 0) {
+      const size_t n = std::min((size_t)meta_cap - 1, m.size());
+      std::memcpy(meta, m.data(), n);
+      meta[n] = '\0';
+    }
+    *out = ix.release();
   });
 }
 

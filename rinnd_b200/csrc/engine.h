@@ -72,6 +72,10 @@ struct KnnState {
   DVec<uint32_t> rcnt;
   int nreg = 0;
   unsigned int rsize = 0;
+  // BF16 precision form: BF16 copy of the rows (N x kpb) and per-row (|b|^2, rounding error bound)
+  DVec<uint16_t> xb;
+  DVec<float> rinfo;         // 2N floats
+  int kpb = 0;
   double upv_prev = -1.0;    // updates appended per vertex by the previous join (-1: none yet)
   bool seeded = false;       // rows initialized from tree leaves (their thresholds already filter)
 };
@@ -93,9 +97,11 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
 bool join_tma_supported(int c, int Dp);
 void join_tma_batch(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st);
 void join_describe(KnnState& s, int kind, cudaStream_t st);
-// Tensor-core join (join_tc.cu): BF16 Gram filter + exact FP32 recheck.
+// Tensor-core join (join_tc.cu): BF16 Gram filter + exact FP32 recheck.  prepare
+// makes the BF16 copy of the rows once per build (s.xb, s.rinfo).
 bool join_tc_supported(int kind, int c, int Dp);
-void join_tc_batch(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st);
+void join_tc_prepare(KnnState& s, const float* X, int D, int Dp, cudaStream_t st);
+void join_tc_batch(KnnState& s, const float* X, int D, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st);
 // Sorted output: idx (-1 empty), raw distance (+inf empty).
 void finalize_knn(const KnnState& s, int32_t* out_idx, float* out_dist, cudaStream_t st);
 void finalize_rows(const uint64_t* slots, int N, int k, int kp, int32_t* out_idx, float* out_dist,

@@ -736,6 +736,7 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
     const double nbatch = std::max(1.0, std::ceil(upv * (double)s.N / (0.8 * (double)s.ucap)));
     per_batch = std::max<long long>(1, (long long)std::ceil((double)s.N / nbatch));
   }
+  if (use_tc) join_tc_prepare(s, X, D, Dp, st);
   RINND_CUDA(cudaEventRecord(e0, st));
   if (use_tma) join_describe(s, kind, st);
   std::vector<cudaEvent_t> kev;  // start/stop of every join kernel launch
@@ -749,7 +750,7 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
     }
     RINND_CUDA(cudaEventRecord(kev[kev.size() - 2], st));
     if (use_tc) {
-      join_tc_batch(s, X, Dp, kind, (int)v0, v1, s.err.p, st);
+      join_tc_batch(s, X, D, Dp, kind, (int)v0, v1, s.err.p, st);
     } else if (use_tma) {
       join_tma_batch(s, X, Dp, kind, (int)v0, v1, s.err.p, st);
     } else if (s.c <= 32) {
