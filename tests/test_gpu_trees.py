@@ -40,21 +40,26 @@ def test_spill_leaves_match_oracle(rb, orc, metric, d):
 
 def test_spill_seeding_search_recall(rb, orc):
     """A larger leaf budget seeds more points per tree: recall@10 does not drop,
-    and with budget 4 the GPU search is within 0.5 point of the oracle's."""
+    and at each budget the GPU search is within 0.5 point of the oracle's (the
+    reference's default epsilon 0.1; at epsilon 0 both searches stop at the
+    first local minimum and their recall is dominated by the graphs' random
+    structure rather than by the seeding)."""
     X = gmm(30000, 32, 80, seed=33)
     Q = gmm(2000, 32, 80, seed=34)
     truth = orc.exact_knn_f64(0, X, Q, 10)[0]
-    rec = {}
+    rec, orec = {}, {}
     for budget in (1, 4):
         ix = rb.RINND(X, metric="sqeuclidean", n_neighbors=15, n_trees=4, n_search_trees=2,
                       search_tree_leaf_budget=budget, random_state=6)
-        ids, _ = ix.query(Q, k=10, epsilon=0.0)
+        ids, _ = ix.query(Q, k=10, epsilon=0.1)
         rec[budget] = recall(ids, truth)
-    oix = orc.OracleIndex(X, n_neighbors=15, n_trees=4, n_search_trees=2, search_tree_leaf_budget=4,
-                          distance_kind=0, correction=orc.CORR_NONE, random_seed=6)
-    oids, _ = oix.query(Q, k=10, epsilon=0.0)
+        oix = orc.OracleIndex(X, n_neighbors=15, n_trees=4, n_search_trees=2, search_tree_leaf_budget=budget,
+                              distance_kind=0, correction=orc.CORR_NONE, random_seed=6)
+        oids, _ = oix.query(Q, k=10, epsilon=0.1)
+        orec[budget] = recall(oids, truth)
     assert rec[4] >= rec[1] - 0.002, rec
-    assert rec[4] >= recall(oids, truth) - 0.005, (rec, recall(oids, truth))
+    for budget in (1, 4):
+        assert rec[budget] >= orec[budget] - 0.005, (rec, orec)
 
 
 @pytest.mark.parametrize("mode", ["int8", "sq8p"])
