@@ -48,6 +48,27 @@ extern "C" {
 #define RINND_DIST_DIRECT_COSINE 5      /* core/distance/alternatives.rs:131-154 */
 #define RINND_DIST_INNER_PRODUCT 6      /* core/distance/inner_product.rs:96-107 */
 #define RINND_DIST_ALT_INNER_PRODUCT 7  /* core/distance/alternatives.rs:160-193 */
+/* The reference's other metrics (built with their own distance, no correction,
+ * crates/rinnd/src/lib.rs:1276-1293), evaluated per pair by generic kernels. */
+#define RINND_DIST_CHEBYSHEV 8          /* core/distance/minkowski.rs:106-121 */
+#define RINND_DIST_CANBERRA 9           /* core/distance/minkowski.rs:165-181 */
+#define RINND_DIST_BRAYCURTIS 10        /* core/distance/minkowski.rs:191-212 */
+#define RINND_DIST_CORRELATION 11       /* core/distance/angular.rs:13-52     */
+#define RINND_DIST_TRUE_ANGULAR 12      /* core/distance/angular.rs:62-90     */
+#define RINND_DIST_TSSS 13              /* core/distance/angular.rs:99-133    */
+#define RINND_DIST_HAMMING 14           /* core/distance/binary.rs:13-32      */
+#define RINND_DIST_JACCARD 15           /* core/distance/binary.rs:42-68      */
+#define RINND_DIST_DICE 16              /* core/distance/binary.rs:142-167    */
+#define RINND_DIST_MATCHING 17          /* core/distance/binary.rs:113-132    */
+#define RINND_DIST_KULSINSKI 18         /* core/distance/binary.rs:177-203    */
+#define RINND_DIST_ROGERSTANIMOTO 19    /* core/distance/binary.rs:213-229    */
+#define RINND_DIST_RUSSELLRAO 20        /* core/distance/binary.rs:239-258    */
+#define RINND_DIST_SOKALMICHENER 21     /* core/distance/binary.rs:268-276    */
+#define RINND_DIST_SOKALSNEATH 22       /* core/distance/binary.rs:286-311    */
+#define RINND_DIST_YULE 23              /* core/distance/binary.rs:321-353    */
+#define RINND_DIST_HELLINGER 24         /* core/distance/hellinger.rs:16-44   */
+#define RINND_DIST_JENSEN_SHANNON 25    /* core/distance/hellinger.rs:98-128  */
+#define RINND_DIST_SYMMETRIC_KL 26      /* core/distance/hellinger.rs:137-166 */
 
 /* ---- corrections applied to reported distances -------------------------- */
 #define RINND_CORR_NONE 0

@@ -274,7 +274,161 @@ static float alt_cosine(const float* a, const float* b, int n) {
   return std::log2(std::sqrt(na * nb) / dot);
 }
 
+// The reference's other metrics (core/distance/{minkowski,angular,binary,
+// hellinger}.rs), plain sequential loops as written there.
+enum {
+  ORC_CHEBYSHEV = 8, ORC_CANBERRA, ORC_BRAYCURTIS, ORC_CORRELATION, ORC_TRUE_ANGULAR, ORC_TSSS, ORC_HAMMING,
+  ORC_JACCARD, ORC_DICE, ORC_MATCHING, ORC_KULSINSKI, ORC_ROGERSTANIMOTO, ORC_RUSSELLRAO, ORC_SOKALMICHENER,
+  ORC_SOKALSNEATH, ORC_YULE, ORC_HELLINGER, ORC_JENSEN_SHANNON, ORC_SYMMETRIC_KL
+};
+static float other_metric(int kind, const float* a, const float* b, int n) {
+  const float nf = (float)n;
+  switch (kind) {
+    case ORC_CHEBYSHEV: {  // minkowski.rs:106-121
+      float r = 0.f;
+      for (int i = 0; i < n; ++i) {
+        float d = std::fabs(a[i] - b[i]);
+        if (d > r) r = d;
+      }
+      return r;
+    }
+    case ORC_CANBERRA: {  // minkowski.rs:165-181
+      float s = 0.f;
+      for (int i = 0; i < n; ++i) {
+        float den = std::fabs(a[i]) + std::fabs(b[i]);
+        if (den > 0.f) s += std::fabs(a[i] - b[i]) / den;
+      }
+      return s;
+    }
+    case ORC_BRAYCURTIS: {  // minkowski.rs:191-212
+      float num = 0.f, den = 0.f;
+      for (int i = 0; i < n; ++i) {
+        num += std::fabs(a[i] - b[i]);
+        den += std::fabs(a[i] + b[i]);
+      }
+      return den > 0.f ? num / den : 0.f;
+    }
+    case ORC_CORRELATION: {  // angular.rs:13-52
+      if (n == 0) return 0.f;
+      float ma = 0.f, mb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        ma += a[i];
+        mb += b[i];
+      }
+      ma /= nf;
+      mb /= nf;
+      float dot = 0.f, na = 0.f, nb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        float sa = a[i] - ma, sb = b[i] - mb;
+        dot += sa * sb;
+        na += sa * sa;
+        nb += sb * sb;
+      }
+      if (na == 0.f && nb == 0.f) return 0.f;
+      if (dot == 0.f) return 1.f;
+      return 1.f - dot / std::sqrt(na * nb);
+    }
+    case ORC_TRUE_ANGULAR:  // angular.rs:62-90
+    case ORC_TSSS: {        // angular.rs:99-133
+      float de = 0.f, dot = 0.f, na = 0.f, nb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        float d = a[i] - b[i];
+        de += d * d;
+        dot += a[i] * b[i];
+        na += a[i] * a[i];
+        nb += b[i] * b[i];
+      }
+      const float pi = 3.14159265358979f;
+      if (kind == ORC_TRUE_ANGULAR) {
+        if (na == 0.f && nb == 0.f) return 0.f;
+        if (na == 0.f || nb == 0.f || dot <= 0.f) return FLT_MAX;
+        float sim = std::min(std::max(dot / std::sqrt(na * nb), -1.f), 1.f);
+        return 1.f - std::acos(sim) / pi;
+      }
+      na = std::sqrt(na);
+      nb = std::sqrt(nb);
+      float mag = std::fabs(na - nb);
+      float den = na * nb;
+      if (den < 1e-12f) return 0.f;
+      float cs = std::min(std::max(dot / den, -1.f), 1.f);
+      float theta = std::acos(cs) + 10.0f * (pi / 180.0f);  // f32::to_radians
+      float t = std::sqrt(de) + mag;
+      float sector = t * t * theta;
+      float triangle = den * std::sin(theta) / 2.0f;
+      return triangle * sector;
+    }
+    case ORC_HAMMING:
+    case ORC_MATCHING: {  // binary.rs:13-32, :113-132
+      if (n == 0) return 0.f;
+      uint32_t cnt = 0;
+      for (int i = 0; i < n; ++i)
+        cnt += kind == ORC_HAMMING ? (a[i] != b[i]) : ((a[i] != 0.f) != (b[i] != 0.f));
+      return (float)cnt / nf;
+    }
+    case ORC_HELLINGER: {  // hellinger.rs:16-44
+      float bc = 0.f, la = 0.f, lb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        bc += std::sqrt(a[i] * b[i]);
+        la += a[i];
+        lb += b[i];
+      }
+      if (la == 0.f && lb == 0.f) return 0.f;
+      if (la == 0.f || lb == 0.f) return 1.f;
+      float v = 1.f - bc / std::sqrt(la * lb);
+      return std::sqrt(std::max(v, 0.f));
+    }
+    case ORC_JENSEN_SHANNON:  // hellinger.rs:98-128
+    case ORC_SYMMETRIC_KL: {  // hellinger.rs:137-166
+      float la = 0.f, lb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        la += a[i];
+        lb += b[i];
+      }
+      float et = FLT_EPSILON * nf;
+      la += et;
+      lb += et;
+      float r = 0.f;
+      for (int i = 0; i < n; ++i) {
+        float px = (a[i] + FLT_EPSILON) / la, py = (b[i] + FLT_EPSILON) / lb;
+        if (kind == ORC_JENSEN_SHANNON) {
+          float m = 0.5f * (px + py);
+          r += 0.5f * (px * std::log(px / m) + py * std::log(py / m));
+        } else {
+          r += px * std::log(px / py) + py * std::log(py / px);
+        }
+      }
+      return r;
+    }
+  }
+  // binary.rs: indicator counts (exact integers in f32)
+  float tt = 0.f, tf = 0.f, ft = 0.f, ne = 0.f, nz = 0.f;
+  for (int i = 0; i < n; ++i) {
+    bool x = a[i] != 0.f, y = b[i] != 0.f;
+    if (x || y) nz += 1.f;
+    if (x && y) tt += 1.f;
+    if (x && !y) tf += 1.f;
+    if (!x && y) ft += 1.f;
+    if (x != y) ne += 1.f;
+  }
+  switch (kind) {
+    case ORC_JACCARD: return nz == 0.f ? 0.f : (nz - tt) / nz;                // binary.rs:42-68
+    case ORC_DICE: return ne == 0.f ? 0.f : ne / (2.f * tt + ne);             // :142-167
+    case ORC_KULSINSKI: return ne == 0.f ? 0.f : (ne - tt + nf) / (ne + nf);  // :177-203
+    case ORC_ROGERSTANIMOTO:                                                  // :213-229
+    case ORC_SOKALMICHENER: return (2.f * ne) / (nf + ne);                    // :268-276
+    case ORC_RUSSELLRAO: return n == 0 ? 0.f : (nf - tt) / nf;                // :239-258
+    case ORC_SOKALSNEATH: return ne == 0.f ? 0.f : ne / (0.5f * tt + ne);     // :286-311
+    case ORC_YULE: {                                                          // :321-353
+      float ff = nf - tt - tf - ft;
+      if (tf == 0.f || ft == 0.f) return 0.f;
+      return (2.f * tf * ft) / (tt * ff + tf * ft);
+    }
+  }
+  return NAN;
+}
+
 static float distance_impl(int kind, const float* a, const float* b, int n) {
+  if (kind >= ORC_CHEBYSHEV) return other_metric(kind, a, b, n);
   switch (kind) {
     case ORC_SQEUCLIDEAN: return sqeuclid(a, b, n);
     case ORC_MANHATTAN: return manhattan(a, b, n);

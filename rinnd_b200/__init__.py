@@ -27,15 +27,26 @@ _ALIASES = {
     "sqeuclidean": "sqeuclidean", "squared_euclidean": "sqeuclidean",
     "manhattan": "manhattan", "taxicab": "manhattan", "l1": "manhattan",
     "cosine": "cosine", "inner_product": "inner_product", "ip": "inner_product", "dot": "dot",
+    "chebyshev": "chebyshev", "linfinity": "chebyshev", "linfty": "chebyshev", "linf": "chebyshev",
+    "canberra": "canberra", "braycurtis": "braycurtis", "correlation": "correlation",
+    "true_angular": "true_angular", "tsss": "tsss", "hamming": "hamming", "jaccard": "jaccard", "dice": "dice",
+    "matching": "matching", "kulsinski": "kulsinski", "rogerstanimoto": "rogerstanimoto",
+    "russellrao": "russellrao", "sokalsneath": "sokalsneath", "sokalmichener": "sokalmichener", "yule": "yule",
+    "hellinger": "hellinger", "jensen_shannon": "jensen_shannon", "jensen-shannon": "jensen_shannon",
+    "symmetric_kl": "symmetric_kl", "symmetric-kl": "symmetric_kl", "symmetric_kullback_liebler": "symmetric_kl",
 }
-# Metrics the reference knows that this engine does not implement (outside the hot path).
-_KNOWN_OTHER = {
-    "chebyshev", "linfinity", "linfty", "linf", "canberra", "braycurtis", "correlation", "true_angular",
-    "tsss", "hamming", "jaccard", "dice", "matching", "kulsinski", "rogerstanimoto", "russellrao",
-    "sokalsneath", "sokalmichener", "yule", "hellinger", "jensen_shannon", "jensen-shannon",
-    "symmetric_kl", "symmetric-kl", "symmetric_kullback_liebler",
+# lib.rs:1276-1293: the metrics without a fast alternative are built with their
+# own distance and no correction (evaluated per pair by the generic kernels)
+_DIRECT = {
+    "chebyshev": L.DIST_CHEBYSHEV, "canberra": L.DIST_CANBERRA, "braycurtis": L.DIST_BRAYCURTIS,
+    "correlation": L.DIST_CORRELATION, "true_angular": L.DIST_TRUE_ANGULAR, "tsss": L.DIST_TSSS,
+    "hamming": L.DIST_HAMMING, "jaccard": L.DIST_JACCARD, "dice": L.DIST_DICE, "matching": L.DIST_MATCHING,
+    "kulsinski": L.DIST_KULSINSKI, "rogerstanimoto": L.DIST_ROGERSTANIMOTO, "russellrao": L.DIST_RUSSELLRAO,
+    "sokalmichener": L.DIST_SOKALMICHENER, "sokalsneath": L.DIST_SOKALSNEATH, "yule": L.DIST_YULE,
+    "hellinger": L.DIST_HELLINGER, "jensen_shannon": L.DIST_JENSEN_SHANNON, "symmetric_kl": L.DIST_SYMMETRIC_KL,
 }
-_ANGULAR = {"cosine", "inner_product", "dot"}  # index.rs:606-614
+# index.rs:606-614: angular RP splits
+_ANGULAR = {"cosine", "inner_product", "dot", "correlation", "true_angular", "tsss"}
 
 # Local-join tile arithmetic (an addition of the B200 engine): "bf16" filters
 # pairs with tensor-core BF16 Gram tiles and recomputes survivors in FP32.
@@ -96,8 +107,6 @@ def _prepare(data, *, metric, n_neighbors, n_trees, n_search_trees, search_tree_
                          "width is explicit")
     name = metric.lower()
     if name not in _ALIASES:
-        if name in _KNOWN_OTHER:
-            raise ValueError(f"Metric '{metric}' is not implemented by the B200 engine")
         raise ValueError(f"Unknown metric: {metric}")
     name = _ALIASES[name]
     normalize_cosine = bool(normalize) and name == "cosine"
@@ -145,8 +154,10 @@ def _prepare(data, *, metric, n_neighbors, n_trees, n_search_trees, search_tree_
             kind, corr = L.DIST_ALT_COSINE, L.CORR_ALT_COSINE
     elif name == "dot":
         kind, corr = L.DIST_ALT_DOT, L.CORR_ALT_COSINE
-    else:  # inner_product
+    elif name == "inner_product":
         kind, corr = L.DIST_ALT_INNER_PRODUCT, L.CORR_ALT_IP
+    else:
+        kind, corr = _DIRECT[name], L.CORR_NONE
 
     p = L.BuildParams()
     L.check(L.lib.rinnd_params_default(ctypes.byref(p)))

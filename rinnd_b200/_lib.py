@@ -20,6 +20,11 @@ ERR_INVALID, ERR_OOM, ERR_CUDA, ERR_NO_DEVICE, ERR_INTERNAL, ERR_BUSY = -1, -2, 
 
 DIST_SQEUCLIDEAN, DIST_MANHATTAN, DIST_COSINE, DIST_ALT_COSINE, DIST_ALT_DOT, DIST_DIRECT_COSINE, \
     DIST_INNER_PRODUCT, DIST_ALT_INNER_PRODUCT = range(8)
+# the reference's other metrics (core/distance/{minkowski,angular,binary,hellinger}.rs)
+DIST_CHEBYSHEV, DIST_CANBERRA, DIST_BRAYCURTIS, DIST_CORRELATION, DIST_TRUE_ANGULAR, DIST_TSSS, DIST_HAMMING, \
+    DIST_JACCARD, DIST_DICE, DIST_MATCHING, DIST_KULSINSKI, DIST_ROGERSTANIMOTO, DIST_RUSSELLRAO, \
+    DIST_SOKALMICHENER, DIST_SOKALSNEATH, DIST_YULE, DIST_HELLINGER, DIST_JENSEN_SHANNON, \
+    DIST_SYMMETRIC_KL = range(8, 27)
 CORR_NONE, CORR_SQRT, CORR_ALT_COSINE, CORR_ALT_IP = range(4)
 Q8_PER_VECTOR_COSINE, Q8_GLOBAL_SYMMETRIC, Q8_PER_VECTOR_SYMMETRIC, Q8_PER_DIMENSION = range(4)
 PRECISION_FP32, PRECISION_BF16 = range(2)

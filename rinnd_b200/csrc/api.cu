@@ -184,7 +184,7 @@ void load_rows(const float* src, bool src_device, int64_t n, int d, int64_t ld, 
                                st));
 }
 
-bool kind_uses_norms(int kind) { return kind != DK_SQEUCLIDEAN && kind != DK_MANHATTAN; }
+bool kind_uses_norms(int kind) { return kind != DK_SQEUCLIDEAN && kind != DK_MANHATTAN && kind < DK_FIRST_GENERIC; }
 
 __global__ void k_tree_idx(const int32_t* perm, const int32_t* inverse, long long total, int32_t* out) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;

@@ -21,8 +21,30 @@ enum DistKind : int {
   DK_DIRECT_COSINE = 5,
   DK_INNER_PRODUCT = 6,
   DK_ALT_INNER_PRODUCT = 7,
-  DK_COUNT = 8
+  // the reference's other metrics (core/distance/{minkowski,angular,binary,hellinger}.rs),
+  // evaluated per pair by the generic kernels
+  DK_CHEBYSHEV = 8,
+  DK_CANBERRA = 9,
+  DK_BRAYCURTIS = 10,
+  DK_CORRELATION = 11,
+  DK_TRUE_ANGULAR = 12,
+  DK_TSSS = 13,
+  DK_HAMMING = 14,
+  DK_JACCARD = 15,
+  DK_DICE = 16,
+  DK_MATCHING = 17,
+  DK_KULSINSKI = 18,
+  DK_ROGERSTANIMOTO = 19,
+  DK_RUSSELLRAO = 20,
+  DK_SOKALMICHENER = 21,
+  DK_SOKALSNEATH = 22,
+  DK_YULE = 23,
+  DK_HELLINGER = 24,
+  DK_JENSEN_SHANNON = 25,
+  DK_SYMMETRIC_KL = 26,
+  DK_COUNT = 27
 };
+constexpr int DK_FIRST_GENERIC = DK_CHEBYSHEV;
 
 enum CorrKind : int { CK_NONE = 0, CK_SQRT = 1, CK_ALT_COSINE = 2, CK_ALT_IP = 3 };
 

@@ -217,8 +217,189 @@ __device__ __forceinline__ float exact_alt_cosine(const float* a, const float* b
   return log2f(__fdiv_rn(__fsqrt_rn(__fmul_rn(na, nb)), dot));
 }
 
+// ---- the reference's other metrics: scalar loops in the reference's order, every
+// operation separately rounded (Rust does not fuse a multiply and an add) ----
+// core/distance/binary.rs: counts of (a != 0, b != 0) combinations as f32 sums.
+struct BinCounts {
+  float tt, tf, ft, ne;
+};
+__device__ __forceinline__ BinCounts binary_counts(const float* a, const float* b, int n) {
+  BinCounts c{0.f, 0.f, 0.f, 0.f};
+  for (int i = 0; i < n; ++i) {
+    const bool x = a[i] != 0.f, y = b[i] != 0.f;
+    if (x && y) c.tt = __fadd_rn(c.tt, 1.0f);
+    if (x && !y) c.tf = __fadd_rn(c.tf, 1.0f);
+    if (!x && y) c.ft = __fadd_rn(c.ft, 1.0f);
+    if (x != y) c.ne = __fadd_rn(c.ne, 1.0f);
+  }
+  return c;
+}
+
+static __device__ __noinline__ float generic_distance(int kind, const float* a, const float* b, int n) {
+  const float nf = (float)n;
+  switch (kind) {
+    case DK_CHEBYSHEV: {  // minkowski.rs:106-121
+      float r = 0.f;
+      for (int i = 0; i < n; ++i) {
+        const float d = fabsf(__fsub_rn(a[i], b[i]));
+        if (d > r) r = d;
+      }
+      return r;
+    }
+    case DK_CANBERRA: {  // minkowski.rs:165-181
+      float s = 0.f;
+      for (int i = 0; i < n; ++i) {
+        const float den = __fadd_rn(fabsf(a[i]), fabsf(b[i]));
+        if (den > 0.f) s = __fadd_rn(s, __fdiv_rn(fabsf(__fsub_rn(a[i], b[i])), den));
+      }
+      return s;
+    }
+    case DK_BRAYCURTIS: {  // minkowski.rs:191-212
+      float num = 0.f, den = 0.f;
+      for (int i = 0; i < n; ++i) {
+        num = __fadd_rn(num, fabsf(__fsub_rn(a[i], b[i])));
+        den = __fadd_rn(den, fabsf(__fadd_rn(a[i], b[i])));
+      }
+      return den > 0.f ? __fdiv_rn(num, den) : 0.f;
+    }
+    case DK_CORRELATION: {  // angular.rs:13-52
+      if (n == 0) return 0.f;
+      float ma = 0.f, mb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        ma = __fadd_rn(ma, a[i]);
+        mb = __fadd_rn(mb, b[i]);
+      }
+      ma = __fdiv_rn(ma, nf);
+      mb = __fdiv_rn(mb, nf);
+      float dot = 0.f, na = 0.f, nb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        const float sa = __fsub_rn(a[i], ma), sb = __fsub_rn(b[i], mb);
+        dot = __fadd_rn(dot, __fmul_rn(sa, sb));
+        na = __fadd_rn(na, __fmul_rn(sa, sa));
+        nb = __fadd_rn(nb, __fmul_rn(sb, sb));
+      }
+      if (na == 0.f && nb == 0.f) return 0.f;
+      if (dot == 0.f) return 1.0f;
+      return __fsub_rn(1.0f, __fdiv_rn(dot, __fsqrt_rn(__fmul_rn(na, nb))));
+    }
+    case DK_TRUE_ANGULAR:  // angular.rs:62-90
+    case DK_TSSS: {        // angular.rs:99-133
+      float de = 0.f, dot = 0.f, na = 0.f, nb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        const float d = __fsub_rn(a[i], b[i]);
+        de = __fadd_rn(de, __fmul_rn(d, d));
+        dot = __fadd_rn(dot, __fmul_rn(a[i], b[i]));
+        na = __fadd_rn(na, __fmul_rn(a[i], a[i]));
+        nb = __fadd_rn(nb, __fmul_rn(b[i], b[i]));
+      }
+      if (kind == DK_TRUE_ANGULAR) {
+        if (na == 0.f && nb == 0.f) return 0.f;
+        if (na == 0.f || nb == 0.f || dot <= 0.f) return FLT_MAX;
+        const float sim = fminf(fmaxf(__fdiv_rn(dot, __fsqrt_rn(__fmul_rn(na, nb))), -1.0f), 1.0f);
+        return __fsub_rn(1.0f, __fdiv_rn(acosf(sim), 3.14159265358979f));
+      }
+      na = __fsqrt_rn(na);
+      nb = __fsqrt_rn(nb);
+      const float mag = fabsf(__fsub_rn(na, nb));
+      const float den = __fmul_rn(na, nb);
+      if (den < 1e-12f) return 0.f;
+      const float cs = fminf(fmaxf(__fdiv_rn(dot, den), -1.0f), 1.0f);
+      // + 10 degrees in radians: 10 * (pi / 180) in f32 arithmetic (f32::to_radians)
+      const float theta = __fadd_rn(acosf(cs), __fmul_rn(10.0f, __fdiv_rn(3.14159265358979f, 180.0f)));
+      const float t = __fadd_rn(__fsqrt_rn(de), mag);
+      const float sector = __fmul_rn(__fmul_rn(t, t), theta);
+      const float triangle = __fdiv_rn(__fmul_rn(den, sinf(theta)), 2.0f);
+      return __fmul_rn(triangle, sector);
+    }
+    case DK_HAMMING: {  // binary.rs:13-32
+      if (n == 0) return 0.f;
+      unsigned cnt = 0;
+      for (int i = 0; i < n; ++i) cnt += a[i] != b[i];
+      return __fdiv_rn((float)cnt, nf);
+    }
+    case DK_MATCHING: {  // binary.rs:113-132
+      if (n == 0) return 0.f;
+      unsigned cnt = 0;
+      for (int i = 0; i < n; ++i) cnt += (a[i] != 0.f) != (b[i] != 0.f);
+      return __fdiv_rn((float)cnt, nf);
+    }
+    case DK_RUSSELLRAO: {  // binary.rs:239-258
+      if (n == 0) return 0.f;
+      const BinCounts c = binary_counts(a, b, n);
+      return __fdiv_rn(__fsub_rn(nf, c.tt), nf);
+    }
+    case DK_JACCARD:
+    case DK_DICE:
+    case DK_KULSINSKI:
+    case DK_ROGERSTANIMOTO:
+    case DK_SOKALMICHENER:
+    case DK_SOKALSNEATH:
+    case DK_YULE: {
+      const BinCounts c = binary_counts(a, b, n);
+      switch (kind) {
+        case DK_JACCARD: {  // binary.rs:42-68 (non-zero in either = tt + ne, exact integer counts)
+          const float nnz = __fadd_rn(c.tt, c.ne);
+          return nnz == 0.f ? 0.f : __fdiv_rn(__fsub_rn(nnz, c.tt), nnz);
+        }
+        case DK_DICE:  // binary.rs:142-167
+          return c.ne == 0.f ? 0.f : __fdiv_rn(c.ne, __fadd_rn(__fmul_rn(2.0f, c.tt), c.ne));
+        case DK_KULSINSKI:  // binary.rs:177-203
+          return c.ne == 0.f ? 0.f : __fdiv_rn(__fadd_rn(__fsub_rn(c.ne, c.tt), nf), __fadd_rn(c.ne, nf));
+        case DK_SOKALSNEATH:  // binary.rs:286-311
+          return c.ne == 0.f ? 0.f : __fdiv_rn(c.ne, __fadd_rn(__fmul_rn(0.5f, c.tt), c.ne));
+        case DK_YULE: {  // binary.rs:321-353
+          const float ff = __fsub_rn(__fsub_rn(__fsub_rn(nf, c.tt), c.tf), c.ft);
+          if (c.tf == 0.f || c.ft == 0.f) return 0.f;
+          return __fdiv_rn(__fmul_rn(__fmul_rn(2.0f, c.tf), c.ft),
+                           __fadd_rn(__fmul_rn(c.tt, ff), __fmul_rn(c.tf, c.ft)));
+        }
+        default:  // rogerstanimoto, binary.rs:213-229; sokalmichener is the same, :268-276
+          return __fdiv_rn(__fmul_rn(2.0f, c.ne), __fadd_rn(nf, c.ne));
+      }
+    }
+    case DK_HELLINGER: {  // hellinger.rs:16-44
+      float bc = 0.f, la = 0.f, lb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        bc = __fadd_rn(bc, __fsqrt_rn(__fmul_rn(a[i], b[i])));
+        la = __fadd_rn(la, a[i]);
+        lb = __fadd_rn(lb, b[i]);
+      }
+      if (la == 0.f && lb == 0.f) return 0.f;
+      if (la == 0.f || lb == 0.f) return 1.0f;
+      const float v = __fsub_rn(1.0f, __fdiv_rn(bc, __fsqrt_rn(__fmul_rn(la, lb))));
+      return __fsqrt_rn(fmaxf(v, 0.f));
+    }
+    case DK_JENSEN_SHANNON:  // hellinger.rs:98-128
+    case DK_SYMMETRIC_KL: {  // hellinger.rs:137-166
+      float la = 0.f, lb = 0.f;
+      for (int i = 0; i < n; ++i) {
+        la = __fadd_rn(la, a[i]);
+        lb = __fadd_rn(lb, b[i]);
+      }
+      const float et = __fmul_rn(FLT_EPSILON, nf);
+      la = __fadd_rn(la, et);
+      lb = __fadd_rn(lb, et);
+      float r = 0.f;
+      for (int i = 0; i < n; ++i) {
+        const float px = __fdiv_rn(__fadd_rn(a[i], FLT_EPSILON), la);
+        const float py = __fdiv_rn(__fadd_rn(b[i], FLT_EPSILON), lb);
+        if (kind == DK_JENSEN_SHANNON) {
+          const float m = __fmul_rn(0.5f, __fadd_rn(px, py));
+          const float t = __fadd_rn(__fmul_rn(px, logf(__fdiv_rn(px, m))), __fmul_rn(py, logf(__fdiv_rn(py, m))));
+          r = __fadd_rn(r, __fmul_rn(0.5f, t));
+        } else {
+          r = __fadd_rn(r, __fadd_rn(__fmul_rn(px, logf(__fdiv_rn(px, py))), __fmul_rn(py, logf(__fdiv_rn(py, px)))));
+        }
+      }
+      return r;
+    }
+  }
+  return __int_as_float(0x7fc00000);
+}
+
 // Dispatch.  `n` is the true dimension; rows may be padded beyond it.
 __device__ __forceinline__ float exact_distance(int kind, const float* a, const float* b, int n) {
+  if (kind >= DK_FIRST_GENERIC) return generic_distance(kind, a, b, n);
   switch (kind) {
     case DK_SQEUCLIDEAN: return exact_sqeuclid(a, b, n);
     case DK_MANHATTAN: return exact_manhattan(a, b, n);
@@ -243,8 +424,10 @@ __device__ __forceinline__ float exact_distance(int kind, const float* a, const 
 
 // Metrics evaluated from (dot, |a|^2, |b|^2) in the tiled join kernels.
 __host__ __device__ __forceinline__ bool kind_is_dot(int kind) {
-  return kind != DK_SQEUCLIDEAN && kind != DK_MANHATTAN;
+  return kind != DK_SQEUCLIDEAN && kind != DK_MANHATTAN && kind < DK_FIRST_GENERIC;
 }
+// Metrics the tiled joins do not evaluate (the generic per-pair kernels do).
+__host__ __device__ __forceinline__ bool kind_is_generic(int kind) { return kind >= DK_FIRST_GENERIC; }
 __device__ __forceinline__ float finalize_dot(int kind, float dot, float na, float nb) {
   switch (kind) {
     case DK_COSINE: {

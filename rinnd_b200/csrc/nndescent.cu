@@ -300,6 +300,104 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Generic metrics (the reference's other metrics, core/distance/{minkowski,
+// angular,binary,hellinger}.rs): the same pairs and pushes as the tiled joins,
+// each pair's distance evaluated by one thread with exact_distance from the rows
+// in global memory (the tiles' dot / difference forms do not apply to them).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void emit_generic(UpdateBuf ub, uint32_t row, uint64_t key, uint64_t* slots, uint32_t* thr,
+                                             int k, int kp, unsigned long long* counters) {
+  const unsigned long long at = atomicAdd(ub.count, 1ull);
+  if (at < ub.cap) {
+    ub.row[at] = row;
+    ub.key[at] = key;
+  } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
+    atomicAdd(&counters[0], 1ull);
+  }
+}
+
+// Pair (p, q) of ids with thresholds tp, tq: pushed into each row it beats.
+__device__ __forceinline__ void generic_pair(int kind, const float* X, int D, int Dp, int32_t p, int32_t q, uint32_t tp,
+                                             uint32_t tq, UpdateBuf ub, uint64_t* slots, uint32_t* thr, int k, int kp,
+                                             unsigned long long* counters) {
+  const float d = exact_distance(kind, X + (size_t)p * Dp, X + (size_t)q * Dp, D);
+  const uint32_t kd = fkey(d);
+  if (kd < tp) emit_generic(ub, (uint32_t)p, ((uint64_t)kd << 32) | (uint32_t)q | 0x80000000u, slots, thr, k, kp, counters);
+  if (kd < tq) emit_generic(ub, (uint32_t)q, ((uint64_t)kd << 32) | (uint32_t)p | 0x80000000u, slots, thr, k, kp, counters);
+}
+
+// One CTA per vertex (grid-stride over [v0, v1)): new x new (q after p) and new x old (q != p).
+template <int MAXC>
+__global__ void k_local_join_generic(const uint64_t* cand_new, const uint64_t* cand_old, int v0, int v1, int c, int cp,
+                                     const float* __restrict__ X, int D, int Dp, int kind, uint64_t* slots, uint32_t* thr,
+                                     int k, int kp, UpdateBuf ub, unsigned long long* counters) {
+  __shared__ int32_t ids[2 * MAXC];
+  __shared__ uint32_t th[2 * MAXC];
+  __shared__ int s_na, s_nb;
+  for (int v = v0 + blockIdx.x; v < v1; v += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x < 32) {  // compact valid ids, new first then old
+      const int lane = threadIdx.x;
+      int base = 0;
+      for (int list = 0; list < 2; ++list) {
+        const uint64_t* L = (list ? cand_old : cand_new) + (size_t)v * cp;
+        for (int t0 = 0; t0 < c; t0 += 32) {
+          const int t = t0 + lane;
+          const int32_t id = t < c ? slot_id(L[t]) : -1;
+          const unsigned m = __ballot_sync(0xffffffffu, id >= 0);
+          if (id >= 0) ids[base + __popc(m & ((1u << lane) - 1))] = id;
+          base += __popc(m);
+        }
+        if (list == 0 && lane == 0) s_na = base;
+      }
+      if (lane == 0) s_nb = base;
+    }
+    __syncthreads();
+    const int na = s_na, nb = s_nb;
+    if (na == 0) continue;  // uniform across the CTA
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) th[t] = __ldcg(thr + ids[t]);
+    __syncthreads();
+    unsigned int pairs = 0;
+    for (int e = threadIdx.x; e < na * nb; e += blockDim.x) {
+      const int i = e / nb, j = e - i * nb;
+      const bool valid = j < na ? j > i : ids[j] != ids[i];  // mod.rs:396, :424
+      if (!valid) continue;
+      ++pairs;
+      generic_pair(kind, X, D, Dp, ids[i], ids[j], th[i], th[j], ub, slots, thr, k, kp, counters);
+    }
+    for (int o = 16; o; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&counters[2], (unsigned long long)pairs);
+    if (threadIdx.x == 0) atomicAdd(&counters[3], (unsigned long long)nb);
+  }
+}
+
+// Leaf jobs (leaf, block a, block b) of BS points: the pairs of initialize_from_leaves
+// (mod.rs:203-300), evaluated per thread.
+__global__ void k_leaf_join_generic(const int4* jobs, long long j0, long long j1, const int4* leaves, const int32_t* perm,
+                                    int N, int BS, const float* __restrict__ X, int D, int Dp, int kind, uint64_t* slots,
+                                    uint32_t* thr, int k, int kp, UpdateBuf ub, unsigned long long* counters) {
+  for (long long jb = j0 + blockIdx.x; jb < j1; jb += gridDim.x) {
+    const int4 job = jobs[jb];
+    const int4 leaf = leaves[job.x];
+    const int32_t* P = perm + (size_t)leaf.x * N + leaf.y;
+    const int L = leaf.z - leaf.y;
+    const int a0 = job.y * BS, b0 = job.z * BS;
+    const int na = min(BS, L - a0), nb = min(BS, L - b0);
+    const bool tri = job.y == job.z;
+    unsigned int pairs = 0;
+    for (int e = threadIdx.x; e < na * nb; e += blockDim.x) {
+      const int i = e / nb, j = e - i * nb;
+      if (tri && j <= i) continue;
+      ++pairs;
+      const int32_t p = P[a0 + i], q = P[b0 + j];
+      generic_pair(kind, X, D, Dp, p, q, __ldcg(thr + p), __ldcg(thr + q), ub, slots, thr, k, kp, counters);
+    }
+    for (int o = 16; o; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&counters[2], (unsigned long long)pairs);
+  }
+}
+
 // Lock-free pushes of buffered updates (heap.cuh protocol).
 // Entry handled in place e of n: consecutive entries of the leaf initialization
 // come from one leaf block and target the same few rows (all racing for an
@@ -640,7 +738,6 @@ UpdateBuf update_buf(KnnState& s) { return UpdateBuf{s.urow.p, s.ukey.p, s.count
 
 void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int kind,
                cudaStream_t st) {
-  (void)D;
   if (f.n_leaves == 0) return;
   ensure_update_buffer(s, st);
   const int BS = f.max_leaf <= 32 ? 32 : 64;
@@ -659,8 +756,17 @@ void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int 
   k_leaf_job_emit<<<grid_for(f.n_leaves, 256, 148 * 32), 256, 0, st>>>(f.leaves.p, f.n_leaves, BS, off.p, jobs.p);
   RINND_LAUNCH_CHECK();
   const float* norms = s.norms.p;
+  const bool generic = kind_is_generic(kind);
   auto launch = [&](long long j0, long long j1, int pass) {
     const int grid = (int)std::min<long long>(j1 - j0, 148LL * 16);
+    if (generic) {  // every job through the update buffer (no direct first pass)
+      if (pass == 0) {
+        k_leaf_join_generic<<<grid, 128, 0, st>>>(jobs.p, j0, j1, f.leaves.p, f.perm.p, f.N, BS, X, D, Dp, kind,
+                                                  s.slots.p, s.thr.p, s.k, s.kp, update_buf(s), s.counters.p);
+        RINND_LAUNCH_CHECK();
+      }
+      return;
+    }
     if (BS == 32)
       k_leaf_join<32, 128><<<grid, 128, 0, st>>>(jobs.p, j0, j1, f.leaves.p, f.perm.p, f.N, X, Dp, kind, norms,
                                                  s.slots.p, s.thr.p, s.k, s.kp, update_buf(s), s.counters.p, pass);
@@ -707,7 +813,6 @@ void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st) {
 }
 
 JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st) {
-  (void)D;
   ensure_update_buffer(s, st);
   RINND_CUDA(cudaMemsetAsync(s.counters.p, 0, sizeof(unsigned long long), st));
   RINND_CUDA(cudaMemsetAsync(s.counters.p + 2, 0, 2 * sizeof(unsigned long long), st));
@@ -715,8 +820,9 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
   cudaEvent_t e0, e1;
   RINND_CUDA(cudaEventCreate(&e0));
   RINND_CUDA(cudaEventCreate(&e1));
-  const bool use_tc = s.precision == 1 && join_tc_supported(kind, s.c, Dp);
-  const bool use_tma = use_tc || (s.use_tma && join_tma_supported(s.c, Dp));
+  const bool generic = kind_is_generic(kind);
+  const bool use_tc = !generic && s.precision == 1 && join_tc_supported(kind, s.c, Dp);
+  const bool use_tma = !generic && (use_tc || (s.use_tma && join_tma_supported(s.c, Dp)));
   if (s.err.n == 0) {
     s.err.alloc(1, st);
     s.err.fill_bytes(0);
@@ -753,6 +859,16 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
       join_tc_batch(s, X, D, Dp, kind, (int)v0, v1, s.err.p, st);
     } else if (use_tma) {
       join_tma_batch(s, X, Dp, kind, (int)v0, v1, s.err.p, st);
+    } else if (generic) {
+      if (s.c <= 32)
+        k_local_join_generic<32><<<grid, 128, 0, st>>>(s.cand_new.p, s.cand_old.p, (int)v0, v1, s.c, s.cp, X, D, Dp,
+                                                        kind, s.slots.p, s.thr.p, s.k, s.kp, update_buf(s),
+                                                        s.counters.p);
+      else
+        k_local_join_generic<64><<<grid, 128, 0, st>>>(s.cand_new.p, s.cand_old.p, (int)v0, v1, s.c, s.cp, X, D, Dp,
+                                                        kind, s.slots.p, s.thr.p, s.k, s.kp, update_buf(s),
+                                                        s.counters.p);
+      RINND_LAUNCH_CHECK();
     } else if (s.c <= 32) {
       k_local_join<32, 128><<<grid, 128, 0, st>>>(s.cand_new.p, s.cand_old.p, (int)v0, v1, s.c, s.cp, X, Dp, kind,
                                                   s.norms.p, s.slots.p, s.thr.p, s.k, s.kp, update_buf(s),
