@@ -543,10 +543,12 @@ def run_precision(args, world, rank, local_rank):
 def run_serving(args, world, rank, local_rank):
     """The serving form on one GPU (replicas per rank otherwise): a 10M x 96
     index of L2-normalised Gaussian-mixture rows (1000 clusters), cosine, k=30,
-    built with the BF16 join (FP32 recheck); int8 per-vector search codes with
-    an exact FP32 rerank behind the continuous-batching server.  Request sizes
-    are log-uniform in [1, 4096], k in {10, 100}, epsilon 0.1, arrivals Poisson
-    at 0.5 / 0.8 / 0.95 of the measured saturated QPS."""
+    built with the BF16 join (FP32 recheck); int8 per-dimension search codes
+    (sq8d) with an exact FP32 rerank behind the continuous-batching server.
+    Request sizes are log-uniform in [1, 4096], k in {10, 100}, epsilon 0.1,
+    arrivals Poisson at 0.5 / 0.8 / 0.95 of the measured saturated QPS.  Beside
+    it, the plain FP32 search (no codes, no server) at several epsilons and
+    widths, to compare throughput at equal recall@10."""
     import torch
 
     import rinnd_b200
@@ -580,14 +582,14 @@ def run_serving(args, world, rank, local_rank):
     L.check(L.lib.rinnd_build_device(ctypes.c_void_p(X.data_ptr()), n, d, d, ctypes.byref(p), ctypes.byref(h)))
     t_build = time.perf_counter() - t0
     t0 = time.perf_counter()
-    L.check(L.lib.rinnd_quantize(h, L.Q8_PER_VECTOR_COSINE))
+    L.check(L.lib.rinnd_quantize(h, L.Q8_PER_DIMENSION))
     t_encode = time.perf_counter() - t0
-    # a RINND view of the built index for the server and the plain FP32 search
+    # a RINND view of the built (and encoded) index for the server
     ix = rinnd_b200.RINND.__new__(rinnd_b200.RINND)
     ix._h = None
-    ix._attach(h, {"n_points": n, "dim": d, "n_neighbors": 30, "metric": "cosine", "encoding": None,
-                   "candidate_width": 0, "rerank_width": 100, "retain_fp32": True})
-    ix._encoding = L.Q8_PER_VECTOR_COSINE  # codes made above
+    ix._attach(h, {"n_points": n, "dim": d, "n_neighbors": 30, "metric": "cosine", "encoding": L.Q8_PER_DIMENSION,
+                   "candidate_width": 0, "rerank_width": 100, "retain_fp32": True, "quantize_trees": False,
+                   "leaf_budget": 1}, encode=False)
     # exact cosine top-10 of 1000 sampled queries (FP64, the recall checker)
     ns = 1000
     qs = Qd[:ns].double()
@@ -665,30 +667,41 @@ def run_serving(args, world, rank, local_rank):
     rid = srv.submit(Q[:ns], k=10, epsilon=0.1)
     qi, _ = srv.result(rid)
     srv.close()
-    fi = torch.empty((10000, 10), dtype=torch.int32, device=dev)
-    fd = torch.empty((10000, 10), dtype=torch.float32, device=dev)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    L.check(L.lib.rinnd_query_device(h, ctypes.c_void_p(Qd.data_ptr()), 10000, d, 10, 0.1, 0,
-                                     ctypes.c_void_p(fi.data_ptr()), ctypes.c_void_p(fd.data_ptr()), None))
-    torch.cuda.synchronize()
-    t_fp32 = time.perf_counter() - t0
-    fp32_ids = fi[:ns].cpu().numpy()
+    rec_q = recall(qi, truth)
+    # the plain FP32 search (rinnd_query_device, 10k queries) at several operating
+    # points: result width k (top 10 of it scored) and epsilon
+    fp32_points = []
+    for kw, eps in ((10, 0.1), (10, 0.3), (30, 0.1), (30, 0.3), (100, 0.1), (100, 0.3)):
+        fi = torch.empty((10000, kw), dtype=torch.int32, device=dev)
+        fd = torch.empty((10000, kw), dtype=torch.float32, device=dev)
+        L.check(L.lib.rinnd_query_device(h, ctypes.c_void_p(Qd.data_ptr()), 2000, d, kw, eps, 0,
+                                         ctypes.c_void_p(fi.data_ptr()), ctypes.c_void_p(fd.data_ptr()), None))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.check(L.lib.rinnd_query_device(h, ctypes.c_void_p(Qd.data_ptr()), 10000, d, kw, eps, 0,
+                                         ctypes.c_void_p(fi.data_ptr()), ctypes.c_void_p(fd.data_ptr()), None))
+        torch.cuda.synchronize()
+        t_fp32 = time.perf_counter() - t0
+        fp32_points.append({"width": kw, "epsilon": eps, "qps": 10000 / t_fp32,
+                            "recall@10": recall(fi[:ns, :10].cpu().numpy(), truth)})
+    reach = [pnt for pnt in fp32_points if pnt["recall@10"] >= rec_q - 0.005]
+    fp32_equal = max(reach, key=lambda pnt: pnt["qps"]) if reach else None
     if rank == 0:
         line = {
             "metric": "serving QPS and p50/p99 latency at recall@10 (10M x 96, int8 + FP32 rerank)",
             "value": qps_sat, "unit": "queries/s", "n_gpus": world, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int8 search / f32 rerank", "data": "synthetic",
             "config": {"workload": f"serving: {n} x {d} L2-normalised GMM (1000 clusters), cosine, k=30, BF16 join + "
-                                   "FP32 recheck build; int8 per-vector codes, candidate width max(k, 100), rerank 100; "
-                                   "requests log-uniform 1-4096 queries, k in {10, 100}, eps 0.1, Poisson arrivals",
+                                   "FP32 recheck build; int8 per-dimension codes, candidate width max(k, 100), "
+                                   "rerank 100; requests log-uniform 1-4096 queries, k in {10, 100}, eps 0.1, "
+                                   "Poisson arrivals",
                        "parallelism": f"replicas{world}"},
             "build_s": t_build, "encode_s": t_encode, "saturated": {"qps": qps_sat, "p50_ms": st_sat["p50_ms"],
                                                                      "p99_ms": st_sat["p99_ms"]},
             "loads": loads,
-            "recall@10": {"server_int8_rerank": recall(qi, truth), "plain_fp32_search": recall(fp32_ids, truth),
-                          "sample_queries": ns},
-            "plain_fp32_search_qps": 10000 / t_fp32,
+            "recall@10": {"server_int8_rerank": rec_q, "sample_queries": ns},
+            "plain_fp32_search": fp32_points,
+            "plain_fp32_at_equal_recall": fp32_equal,
         }
         print(json.dumps(line), flush=True)
     L.check(L.lib.rinnd_free(h))
