@@ -39,6 +39,7 @@ using namespace joinc;
 constexpr int NSTAGE = 2;   // row stages (72 KB: three CTAs per SM beat a deeper prefetch)
 constexpr int NCONS = 8;    // consumer warps
 constexpr int NT = 32 * (1 + NCONS);
+constexpr int JB = 2;       // candidate rows per work item (each against 4 new rows)
 
 struct Layout {
   int maxc, dp, rs, dstride;  // rs: row stride (floats); dstride: descriptor stride (ints)
@@ -83,9 +84,9 @@ __global__ void k_cand_describe(const uint64_t* cand_new, const uint64_t* cand_o
   __syncwarp();
   if (norms)
     for (int r = lane; r < nb; r += 32) reinterpret_cast<float*>(d)[Desc::nrm(maxc) + r] = norms[ids[r]];
-  // items of quad iq: candidate rows j in [4 iq + 1, nb)
+  // items of quad iq: JB consecutive candidate rows each, starting at row 4 iq + 1
   const int nq = (na + 3) >> 2;
-  int cnt = (lane < nq) ? max(0, nb - (4 * lane + 1)) : 0;
+  int cnt = (lane < nq) ? (max(0, nb - (4 * lane + 1)) + JB - 1) / JB : 0;
   int incl = cnt;
   for (int o = 1; o < 32; o <<= 1) {
     int y = __shfl_up_sync(0xffffffffu, incl, o);
@@ -109,7 +110,7 @@ struct Bars {
 };
 
 template <int MAXC>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 3)
     k_join_ws(const int32_t* __restrict__ desc, int v0, int v1, const float* __restrict__ X, int Dp, int kind,
               uint64_t* slots, uint32_t* thr, int k, int kp, Layout L, uint32_t* urow_buf, uint64_t* ukey_buf,
               unsigned long long* ucount, uint32_t* rcnt, unsigned int rsize, unsigned long long* counters,
@@ -276,69 +277,96 @@ __global__ void __launch_bounds__(NT)
       const int item = b0 + ct;
       const bool active = item < items;
       int iq = 0, j = 0;
-      unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
+      unsigned long long acc[4 * JB];
+#pragma unroll
+      for (int p = 0; p < 4 * JB; ++p) acc[p] = 0ull;
       if (active) {
         for (int q = 1; q < nq; ++q) iq += (sd[4 + q] <= item);
-        j = 4 * iq + 1 + (item - sd[4 + iq]);
-        const ulonglong2* pb = reinterpret_cast<const ulonglong2*>(rows + (size_t)j * L.rs);
+        j = 4 * iq + 1 + JB * (item - sd[4 + iq]);
+        // candidate rows j .. j + JB - 1 (a row past nb repeats row nb - 1; its results are discarded)
+        const ulonglong2* pb[JB];
+#pragma unroll
+        for (int v = 0; v < JB; ++v)
+          pb[v] = reinterpret_cast<const ulonglong2*>(rows + (size_t)min(j + v, nb - 1) * L.rs);
         const ulonglong2* pa = reinterpret_cast<const ulonglong2*>(rows + (size_t)(4 * iq) * L.rs);
         const int ars = L.rs / 4;
         if (kind == DK_SQEUCLIDEAN) {
-#pragma unroll 4
+#pragma unroll 2
           for (int q = 0; q < Dp / 4; ++q) {
-            const ulonglong2 b = pb[q];
+            ulonglong2 b[JB];
+#pragma unroll
+            for (int v = 0; v < JB; ++v) b[v] = pb[v][q];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
               const ulonglong2 a = pa[u * ars + q];
-              const unsigned long long d01 = f2_sub(a.x, b.x), d23 = f2_sub(a.y, b.y);
-              acc[u] = f2_fma(d01, d01, acc[u]);
-              acc[u] = f2_fma(d23, d23, acc[u]);
+#pragma unroll
+              for (int v = 0; v < JB; ++v) {
+                const unsigned long long d01 = f2_sub(a.x, b[v].x), d23 = f2_sub(a.y, b[v].y);
+                acc[4 * v + u] = f2_fma(d01, d01, acc[4 * v + u]);
+                acc[4 * v + u] = f2_fma(d23, d23, acc[4 * v + u]);
+              }
             }
           }
         } else if (kind == DK_MANHATTAN) {
           const unsigned long long absmask = 0x7FFFFFFF7FFFFFFFull;
-#pragma unroll 4
+#pragma unroll 2
           for (int q = 0; q < Dp / 4; ++q) {
-            const ulonglong2 b = pb[q];
+            ulonglong2 b[JB];
+#pragma unroll
+            for (int v = 0; v < JB; ++v) b[v] = pb[v][q];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
               const ulonglong2 a = pa[u * ars + q];
-              acc[u] = f2_add(acc[u], f2_sub(a.x, b.x) & absmask);
-              acc[u] = f2_add(acc[u], f2_sub(a.y, b.y) & absmask);
+#pragma unroll
+              for (int v = 0; v < JB; ++v) {
+                acc[4 * v + u] = f2_add(acc[4 * v + u], f2_sub(a.x, b[v].x) & absmask);
+                acc[4 * v + u] = f2_add(acc[4 * v + u], f2_sub(a.y, b[v].y) & absmask);
+              }
             }
           }
         } else {
-#pragma unroll 4
+#pragma unroll 2
           for (int q = 0; q < Dp / 4; ++q) {
-            const ulonglong2 b = pb[q];
+            ulonglong2 b[JB];
+#pragma unroll
+            for (int v = 0; v < JB; ++v) b[v] = pb[v][q];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
               const ulonglong2 a = pa[u * ars + q];
-              acc[u] = f2_fma(a.x, b.x, acc[u]);
-              acc[u] = f2_fma(a.y, b.y, acc[u]);
+#pragma unroll
+              for (int v = 0; v < JB; ++v) {
+                acc[4 * v + u] = f2_fma(a.x, b[v].x, acc[4 * v + u]);
+                acc[4 * v + u] = f2_fma(a.y, b[v].y, acc[4 * v + u]);
+              }
             }
           }
         }
       }
-      // validity and thresholds -> emit bits (u: push into A row; 4+u: into B row)
-      uint32_t kd[4];
+      // validity and thresholds -> emit bits (bit p = 4 v + u: push into A row; 16 + p: into B row)
+      uint32_t kd[4 * JB];
       unsigned emit = 0;
       int n_emit = 0;
-      const int32_t bid = active ? ids[j] : -1;
-      const uint32_t bthr = active ? sthr[j] : 0u;
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        kd[u] = 0;
-        const int ia = 4 * iq + u;
-        if (active && ia < na) {
-          const bool valid = (j < na) ? (j > ia) : (bid != ids[ia]);  // mod.rs:396, :424
-          if (valid) {
-            ++pairs_total;
-            float d = f2_sum(acc[u]);
-            if (is_dot) d = finalize_dot(kind, d, snrm[ia], snrm[j]);
-            kd[u] = fkey(d);
-            if (kd[u] < sthr[ia]) { emit |= 1u << u; ++n_emit; }
-            if (kd[u] < bthr) { emit |= 16u << u; ++n_emit; }
+      for (int v = 0; v < JB; ++v) {
+        const int jv = j + v;
+        const bool have = active && jv < nb;
+        const int32_t bid = have ? ids[jv] : -1;
+        const uint32_t bthr = have ? sthr[jv] : 0u;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int p = 4 * v + u;
+          kd[p] = 0;
+          const int ia = 4 * iq + u;
+          if (have && ia < na) {
+            const bool valid = (jv < na) ? (jv > ia) : (bid != ids[ia]);  // mod.rs:396, :424
+            if (valid) {
+              ++pairs_total;
+              float d = f2_sum(acc[p]);
+              if (is_dot) d = finalize_dot(kind, d, snrm[ia], snrm[jv]);
+              kd[p] = fkey(d);
+              if (kd[p] < sthr[ia]) { emit |= 1u << p; ++n_emit; }
+              if (kd[p] < bthr) { emit |= 0x10000u << p; ++n_emit; }
+            }
           }
         }
       }
@@ -354,14 +382,15 @@ __global__ void __launch_bounds__(NT)
       base = __shfl_sync(0xffffffffu, base, 0) + (unsigned int)(incl - n_emit);
       if (emit) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int p = 0; p < 4 * JB; ++p) {
 #pragma unroll
           for (int side = 0; side < 2; ++side) {
-            if (!(emit & ((side ? 16u : 1u) << u))) continue;
-            const int32_t aid = ids[4 * iq + u];
+            if (!(emit & ((side ? 0x10000u : 1u) << p))) continue;
+            const int32_t aid = ids[4 * iq + (p & 3)];
+            const int32_t bid = ids[j + (p >> 2)];
             const int32_t row = side ? bid : aid;
             const int32_t other = side ? aid : bid;
-            const uint64_t key = ((uint64_t)kd[u] << 32) | (uint32_t)other | 0x80000000u;
+            const uint64_t key = ((uint64_t)kd[p] << 32) | (uint32_t)other | 0x80000000u;
             if (base < rsize) {
               urow_reg[base] = (uint32_t)row;
               ukey_reg[base] = key;
