@@ -115,8 +115,29 @@ typedef struct rinnd_build_params {
   int32_t verbose;
   int32_t device;                   /* CUDA device ordinal, default 0              */
   int32_t precision;                /* RINND_PRECISION_*: local-join tile arithmetic */
-  int32_t reserved[6];
+  int32_t join_tuning;              /* RINND_TUNE_*: tile shape of the pipelined FP32 join */
+  int32_t reserved[5];
 } rinnd_build_params;
+
+/* Tile shape of the pipelined FP32 local join (row stages in flight per CTA,
+ * candidate rows per work item, CTAs per SM).  RINND_TUNE_TABLE (default): the
+ * shape tuned earlier in this process for the build's (device, padded
+ * dimension, list length class, metric class, grouped) key, else one tuned now
+ * by timing every shape on a sample of the first iteration's candidate lists
+ * (the heaps are restored afterwards, so the build's result distribution does
+ * not change); RINND_TUNE_FIXED: the default shape, no trials; RINND_TUNE_RETUNE:
+ * trials even when the table has the key.  rinnd_join_tile_table lists the
+ * table: 8 ints per row (device, Dp, list class 32|64, metric class 0 squared
+ * Euclidean / 1 Manhattan / 2 dot forms, grouped, stages, rows per item, CTAs
+ * per SM with 0 = as many as shared memory allows); rows = NULL just counts. */
+#define RINND_TUNE_TABLE 0
+#define RINND_TUNE_FIXED 1
+#define RINND_TUNE_RETUNE 2
+RINND_EXPORT int rinnd_join_tile_table(int32_t* rows, int32_t cap, int32_t* n_rows);
+RINND_EXPORT int rinnd_join_tile_table_clear(void);
+/* Stores one table row (8 ints as above): later builds of that key with
+ * RINND_TUNE_TABLE (and rinnd_nndescent_step) run the shape without trials. */
+RINND_EXPORT int rinnd_join_tile_set(const int32_t* row);
 
 typedef struct rinnd_index rinnd_index;
 
@@ -137,13 +158,21 @@ typedef struct rinnd_build_info {
   uint64_t join_kernel_launches; /* local-join kernel launches (ms_join_kernel covers these) */
   uint64_t join_updates;         /* updates the join kernels appended for the heap pushes */
   int32_t join_form;             /* RINND_JOIN_* of the last iteration's local join      */
+  int32_t group_items;           /* indices built together with this one (1 = alone; see
+                                    rinnd_build_many_ex): times and counters are the group's */
+  int32_t join_tile_stages;      /* tile shape the pipelined FP32 join ran (RINND_TUNE_*) */
+  int32_t join_tile_rows;
+  int32_t join_tile_ctas_per_sm;
+  int32_t join_tile_tuned;       /* 1: this build ran the tile trials                     */
 } rinnd_build_info;
 
 /* Local-join kernels (rinnd_build_info.join_form).  The pipelined FP32 join
  * holds a vertex's candidate rows in shared memory (rows padded to Dp =
  * round_up(D, 4) floats: Dp <= 424 with candidate lists of <= 32, Dp <= 204 with
- * longer lists); the tensor-core form (precision BF16) needs lists of <= 32, a
- * non-Manhattan metric and Dp <= 304; other builds use the chunked FP32 join. */
+ * longer lists); the tensor-core form (precision BF16) needs lists of <= 32 and
+ * a non-Manhattan metric of the tiled family (any D: the Gram tiles stream K
+ * in chunks); other builds use the chunked FP32 join (the generic metrics their
+ * per-pair kernel). */
 #define RINND_JOIN_CHUNKED_FP32 0
 #define RINND_JOIN_PIPELINED_FP32 1
 #define RINND_JOIN_TENSOR_BF16 2
@@ -186,13 +215,44 @@ typedef struct rinnd_batch_item {
   int64_t ld;
   const rinnd_build_params* params;
 } rinnd_batch_item;
-/* Builds n_items independent indices concurrently (no counterpart in the
- * reference, which builds one index per call): n_workers host threads (0 =
- * min(n_items, 16)) take items longest first (estimated n * d * k) and each
- * build runs on its own stream, so the builds' kernels overlap on the device.
- * out[i] receives index i (NULL on failure) and status[i] (may be NULL) its
- * status code.  Returns RINND_OK when every item built, else the first failing
- * item's code with its message in rinnd_last_error(). */
+/* Options of the batched form. */
+typedef struct rinnd_batch_options {
+  int32_t n_workers;          /* host threads driving groups (0 = min(tasks, 16))                 */
+  int32_t grouped;            /* 1 (default): indices of one NN-Descent shape are built as a group */
+  int64_t max_group_points;   /* rows per group at most (default 8 Mi; 0 = no cap)                  */
+  int32_t capture_iterations; /* 1 (default): each grouped iteration runs as one CUDA graph          */
+  int32_t reserved;
+} rinnd_batch_options;
+RINND_EXPORT int rinnd_batch_options_default(rinnd_batch_options* o);
+/* Builds n_items independent indices (no counterpart in the reference, which
+ * builds one index per call).  Grouped (the default): items with equal device,
+ * d, distance kind, normalize, angular, n_neighbors, resolved candidate-list
+ * length, resolved leaf size and precision form a group (split to at most
+ * max_group_points rows) whose NN-Descent runs once over all its rows: one
+ * forest pass with every index's trees as root segments, one leaf
+ * initialization, and per iteration one candidate pass and one join launch
+ * family whose persistent CTAs walk the vertices of every index in the group.
+ * Each index keeps its own n_iters cap and delta test (its rows stop sampling
+ * candidates once it stops); trees, candidate draws and priorities are keyed by
+ * the group's first index's random_seed and the rows' positions in the group,
+ * so an index's graph is a valid build of its parameters but not bit-identical
+ * to its one-at-a-time build.  Search graph, reorder and search trees are made
+ * per index; each index's build_info reports the group's phase times and
+ * counters with group_items = the group's size.  With capture_iterations, a
+ * group's iteration (candidate pass, join launches, update applications and
+ * the counter read-back) is stream-captured into a CUDA graph and launched as
+ * one unit; later iterations update the executable graph in place, and
+ * ms_join then covers the whole iteration (ms_candidates and ms_join_kernel
+ * are 0).  Items alone in their group,
+ * or all items with grouped = 0, are built as by rinnd_build, concurrently on
+ * one stream each.  n_workers host threads take groups longest first
+ * (estimated n * d * k).  An item whose data or params are invalid fails
+ * alone.  out[i] receives index i (NULL on failure) and status[i] (may be NULL)
+ * its status code.  Returns RINND_OK when every item built, else the first
+ * failing item's code with its message in rinnd_last_error(). */
+RINND_EXPORT int rinnd_build_many_ex(const rinnd_batch_item* items, int32_t n_items,
+                                     const rinnd_batch_options* options, rinnd_index** out, int32_t* status);
+/* rinnd_build_many_ex with the default options and n_workers. */
 RINND_EXPORT int rinnd_build_many(const rinnd_batch_item* items, int32_t n_items, int32_t n_workers,
                                   rinnd_index** out, int32_t* status);
 RINND_EXPORT int rinnd_build_info_get(const rinnd_index* idx, rinnd_build_info* info);

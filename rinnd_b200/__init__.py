@@ -51,6 +51,9 @@ _ANGULAR = {"cosine", "inner_product", "dot", "correlation", "true_angular", "ts
 # Local-join tile arithmetic (an addition of the B200 engine): "bf16" filters
 # pairs with tensor-core BF16 Gram tiles and recomputes survivors in FP32.
 _PRECISIONS = {"fp32": L.PRECISION_FP32, "bf16": L.PRECISION_BF16}
+# tile shape of the pipelined FP32 join: the process's tuned table (tuning a new
+# key on first use), the fixed default shape, or fresh trials
+_TUNINGS = {"table": L.TUNE_TABLE, "fixed": L.TUNE_FIXED, "retune": L.TUNE_RETUNE}
 _ENCODINGS = {"int8": L.Q8_PER_VECTOR_COSINE, "sq8u": L.Q8_GLOBAL_SYMMETRIC, "sq8p": L.Q8_PER_VECTOR_SYMMETRIC,
               # an addition of the B200 engine: per-dimension scales (quantized.rs:42-56)
               "sq8d": L.Q8_PER_DIMENSION}
@@ -95,11 +98,13 @@ def _validate_quantized_widths(k: int, candidate_width: int, rerank_width: int) 
 def _prepare(data, *, metric, n_neighbors, n_trees, n_search_trees, search_tree_leaf_budget, leaf_size,
              max_candidates, n_iters, delta, random_state, diversify_prob, pruning_degree_multiplier, verbose,
              normalize, cosine_distance_mode, quantized_candidate_width, quantized_rerank_width, tree_quantization,
-             retain_fp32_data, device, precision):
+             retain_fp32_data, device, precision, join_tuning="table"):
     """Validates the constructor arguments (lib.rs:616-755) and maps them to
     build parameters; returns (rows, params, state for RINND._attach)."""
     if precision not in _PRECISIONS:
         raise ValueError(f"Unknown precision: {precision}; expected 'fp32' or 'bf16'")
+    if join_tuning not in _TUNINGS:
+        raise ValueError(f"Unknown join_tuning: {join_tuning}; expected 'table', 'fixed' or 'retune'")
     data = _as_f32_2d(data)
     n_points, dim = data.shape
     if quantized_candidate_width > 0 and quantized_rerank_width > quantized_candidate_width:
@@ -179,13 +184,13 @@ def _prepare(data, *, metric, n_neighbors, n_trees, n_search_trees, search_tree_
     p.verbose = int(bool(verbose))
     p.device = int(device)
     p.precision = _PRECISIONS[precision]
+    p.join_tuning = _TUNINGS[join_tuning]
 
     state = {"n_points": n_points, "dim": dim, "n_neighbors": int(n_neighbors), "metric": metric,
              "encoding": encoding, "candidate_width": int(quantized_candidate_width),
              "rerank_width": int(quantized_rerank_width), "retain_fp32": bool(retain_fp32_data),
              "quantize_trees": quantize_trees, "leaf_budget": max(int(search_tree_leaf_budget), 1)}
     return data, p, state
-
 
 
 class RINND:
@@ -196,7 +201,7 @@ class RINND:
                  random_state=None, diversify_prob=1.0, pruning_degree_multiplier=1.5, verbose=False,
                  normalize=False, cosine_distance_mode="log", quantized_candidate_width=0,
                  quantized_rerank_width=0, tree_quantization="none", retain_fp32_data=None, device=0,
-                 precision="fp32"):
+                 precision="fp32", join_tuning="table"):
         self._h = None
         data, p, state = _prepare(data, metric=metric, n_neighbors=n_neighbors, n_trees=n_trees,
                                   n_search_trees=n_search_trees, search_tree_leaf_budget=search_tree_leaf_budget,
@@ -206,7 +211,8 @@ class RINND:
                                   normalize=normalize, cosine_distance_mode=cosine_distance_mode,
                                   quantized_candidate_width=quantized_candidate_width,
                                   quantized_rerank_width=quantized_rerank_width, tree_quantization=tree_quantization,
-                                  retain_fp32_data=retain_fp32_data, device=device, precision=precision)
+                                  retain_fp32_data=retain_fp32_data, device=device, precision=precision,
+                                  join_tuning=join_tuning)
         h = ctypes.c_void_p()
         L.check(L.lib.rinnd_build(L.ptr(data), data.shape[0], data.shape[1], ctypes.byref(p), ctypes.byref(h)))
         self._attach(h, state)
@@ -422,13 +428,19 @@ def load(path, device=0) -> RINND:
     return ix
 
 
-def build_many(datasets, params=None, n_workers=0, **common):
+def build_many(datasets, params=None, n_workers=0, grouped=True, max_group_points=8 << 20, capture_iterations=True,
+               **common):
     """Builds many independent indices in one call (the batched form; no
     counterpart in the reference).  `datasets` is a sequence of float32 [N, D]
     arrays of any sizes and dimensions; `params` an optional sequence of per-index
     keyword dicts (metric, n_neighbors, precision, ...) merged over `common`.
-    Builds run concurrently, longest first, each on its own stream
-    (rinnd_build_many).  Returns a list of RINND, one per dataset."""
+    With `grouped`, indices of one NN-Descent shape (dimension, metric, k,
+    candidates, leaf size, precision) run their NN-Descent together as one
+    group of at most `max_group_points` rows, each index keeping its own
+    iteration cap and delta test, and with `capture_iterations` each group
+    iteration runs as one CUDA graph; otherwise (and for indices alone in their
+    group) each is built as by RINND, concurrently on its own stream
+    (rinnd_build_many_ex).  Returns a list of RINND, one per dataset."""
     datasets = list(datasets)
     params = list(params) if params is not None else [{} for _ in datasets]
     if len(params) != len(datasets):
@@ -437,7 +449,8 @@ def build_many(datasets, params=None, n_workers=0, **common):
                     leaf_size=None, max_candidates=None, n_iters=None, delta=0.001, random_state=None,
                     diversify_prob=1.0, pruning_degree_multiplier=1.5, verbose=False, normalize=False,
                     cosine_distance_mode="log", quantized_candidate_width=0, quantized_rerank_width=0,
-                    tree_quantization="none", retain_fp32_data=None, device=0, precision="fp32")
+                    tree_quantization="none", retain_fp32_data=None, device=0, precision="fp32",
+                    join_tuning="table")
     prepared = []
     for data, kw in zip(datasets, params):
         args = dict(defaults)
@@ -456,7 +469,11 @@ def build_many(datasets, params=None, n_workers=0, **common):
         items[i].params = ctypes.addressof(p)
     handles = (ctypes.c_void_p * n)()
     status = (ctypes.c_int32 * n)()
-    rc = L.lib.rinnd_build_many(items, n, int(n_workers), handles, status)
+    opts = L.BatchOptions()
+    L.check(L.lib.rinnd_batch_options_default(ctypes.byref(opts)))
+    opts.n_workers, opts.grouped, opts.max_group_points = int(n_workers), int(bool(grouped)), int(max_group_points)
+    opts.capture_iterations = int(bool(capture_iterations))
+    rc = L.lib.rinnd_build_many_ex(items, n, ctypes.byref(opts), handles, status)
     out = []
     for i, (_, _, state) in enumerate(prepared):
         if handles[i]:

@@ -28,6 +28,7 @@ DIST_CHEBYSHEV, DIST_CANBERRA, DIST_BRAYCURTIS, DIST_CORRELATION, DIST_TRUE_ANGU
 CORR_NONE, CORR_SQRT, CORR_ALT_COSINE, CORR_ALT_IP = range(4)
 Q8_PER_VECTOR_COSINE, Q8_GLOBAL_SYMMETRIC, Q8_PER_VECTOR_SYMMETRIC, Q8_PER_DIMENSION = range(4)
 PRECISION_FP32, PRECISION_BF16 = range(2)
+TUNE_TABLE, TUNE_FIXED, TUNE_RETUNE = range(3)
 JOIN_CHUNKED_FP32, JOIN_PIPELINED_FP32, JOIN_TENSOR_BF16 = range(3)  # rinnd_build_info.join_form
 
 _i32, _i64, _u64, _f32, _f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_float, ctypes.c_double
@@ -40,7 +41,7 @@ class BuildParams(ctypes.Structure):
         ("leaf_size", _i32), ("max_candidates", _i32), ("n_iters", _i32), ("delta", _f32),
         ("random_seed", _u64), ("diversify_prob", _f32), ("pruning_degree_multiplier", _f32),
         ("angular", _i32), ("distance_kind", _i32), ("correction", _i32), ("normalize", _i32),
-        ("verbose", _i32), ("device", _i32), ("precision", _i32), ("reserved", _i32 * 6),
+        ("verbose", _i32), ("device", _i32), ("precision", _i32), ("join_tuning", _i32), ("reserved", _i32 * 5),
     ]
 
 
@@ -52,12 +53,18 @@ class BuildInfo(ctypes.Structure):
         ("pairs_evaluated", _u64), ("pushes_accepted", _u64), ("push_contention", _u64),
         ("search_graph_nnz", _i64), ("min_distance", _f32), ("join_rows_gathered", _u64),
         ("ms_join_kernel", _f64), ("kernel_launches", _u64), ("join_kernel_launches", _u64),
-        ("join_updates", _u64), ("join_form", _i32),
+        ("join_updates", _u64), ("join_form", _i32), ("group_items", _i32), ("join_tile_stages", _i32),
+        ("join_tile_rows", _i32), ("join_tile_ctas_per_sm", _i32), ("join_tile_tuned", _i32),
     ]
 
 
 class BatchItem(ctypes.Structure):
     _fields_ = [("data", _P), ("n", _i64), ("d", _i32), ("data_on_device", _i32), ("ld", _i64), ("params", _P)]
+
+
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("n_workers", _i32), ("grouped", _i32), ("max_group_points", _i64), ("capture_iterations", _i32),
+                ("reserved", _i32)]
 
 
 class ServerParams(ctypes.Structure):
@@ -92,6 +99,11 @@ SIGNATURES = {
     "rinnd_save": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_char_p]),
     "rinnd_load": (ctypes.c_int, [ctypes.c_char_p, _i32, _P, _P, _i64, _P]),
     "rinnd_build_many": (ctypes.c_int, [_P, _i32, _i32, _P, _P]),
+    "rinnd_batch_options_default": (ctypes.c_int, [_P]),
+    "rinnd_build_many_ex": (ctypes.c_int, [_P, _i32, _P, _P, _P]),
+    "rinnd_join_tile_table": (ctypes.c_int, [_P, _i32, _P]),
+    "rinnd_join_tile_table_clear": (ctypes.c_int, []),
+    "rinnd_join_tile_set": (ctypes.c_int, [_P]),
     "rinnd_build_info_get": (ctypes.c_int, [_P, _P]),
     "rinnd_index_shape": (ctypes.c_int, [_P, _P, _P, _P]),
     "rinnd_query": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _P, _P]),

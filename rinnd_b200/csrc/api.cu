@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <set>
@@ -291,6 +292,61 @@ void validate_params(const rinnd_build_params* p, int64_t n, int d) {
   require(p->diversify_prob == p->diversify_prob, "diversify_prob must not be NaN");
   require(p->pruning_degree_multiplier > 0.f, "pruning_degree_multiplier must be positive");
   require(p->precision == RINND_PRECISION_FP32 || p->precision == RINND_PRECISION_BF16, "unknown precision");
+  require(p->join_tuning >= RINND_TUNE_TABLE && p->join_tuning <= RINND_TUNE_RETUNE, "unknown join_tuning mode");
+}
+
+// The index from its sorted kNN rows (ids local to the index, raw distances):
+// diversified CSR (index.rs:656-666) on the original order, corrected neighbor
+// distances (:669-673), vertex order = the first retained tree's leaf order and
+// the rows gathered in it (:679-715), search trees.  X0 = the index's rows in
+// original order (N x Dp); ix->forest holds the trees (perm: tree t's leaf
+// order at t * N), of which the first n_search_trees are kept.  Runs on ix->st
+// and synchronizes it.
+void finish_index(rinnd_index* ix, const float* X0, DVec<int32_t>&& knn_idx, DVec<float>&& knn_raw,
+                  TempStorage& tmp) {
+  const rinnd_build_params* pin = &ix->p;
+  cudaStream_t st = ix->st;
+  const int N = (int)ix->N, D = ix->D, Dp = ix->Dp, k = ix->k;
+  // diversified CSR (index.rs:656-666) on the original order
+  float min_d = 0.f;
+  build_search_graph(knn_idx.p, knn_raw.p, X0, N, k, D, Dp, ix->kind, pin->pruning_degree_multiplier, st,
+                     tmp, ix->graph_orig, &min_d, pin->diversify_prob, pin->random_seed);
+  ix->min_distance = min_d;
+  // corrected neighbor distances (index.rs:669-673)
+  apply_correction_dev(knn_raw.p, (int64_t)N * k, ix->corr, st);
+  ix->knn_idx = std::move(knn_idx);
+  ix->knn_dist = std::move(knn_raw);
+  // vertex order = first retained tree's leaf order (index.rs:679-715)
+  ix->n_search_trees = std::min(std::max(pin->n_search_trees, 0), std::max(pin->n_trees, 0));
+  ix->vertex_order.alloc((size_t)N, st);
+  if (ix->n_search_trees > 0) {
+    RINND_CUDA(cudaMemcpyAsync(ix->vertex_order.p, ix->forest.perm.p, sizeof(int32_t) * N,
+                               cudaMemcpyDeviceToDevice, st));
+  } else {
+    k_iota<<<grid_for(N, 256), 256, 0, st>>>(ix->vertex_order.p, N);
+    RINND_LAUNCH_CHECK();
+  }
+  ix->inverse.alloc((size_t)N, st);
+  invert_permutation(ix->vertex_order.p, N, ix->inverse.p, st);
+  ix->X.alloc((size_t)N * Dp, st);
+  gather_rows(X0, ix->vertex_order.p, N, Dp, ix->X.p, st);
+  reorder_csr(ix->graph_orig, ix->vertex_order.p, ix->inverse.p, st, tmp, ix->graph_int);
+  if (ix->n_search_trees > 0) {
+    long long tot = (long long)ix->n_search_trees * N;
+    ix->tree_idx.alloc((size_t)tot, st);
+    k_tree_idx<<<grid_for(tot, 256, 148 * 64), 256, 0, st>>>(ix->forest.perm.p, ix->inverse.p, tot,
+                                                              ix->tree_idx.p);
+    RINND_LAUNCH_CHECK();
+    std::vector<int32_t> roots(ix->n_search_trees);
+    for (int t = 0; t < ix->n_search_trees; ++t) roots[t] = t;
+    ix->tree_roots.alloc(roots.size(), st);
+    ix->tree_roots.from_host(roots.data(), roots.size());
+  }
+  ix->forest.perm.release();
+  ix->forest.leaves.release();
+  ix->search_stats.alloc(4, st);
+  ix->search_stats.fill_bytes(0);
+  RINND_CUDA(cudaStreamSynchronize(st));
 }
 
 void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
@@ -355,6 +411,8 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   leaf_init(ks, ix->forest, X0.p, D, Dp, ix->kind, st);
   RINND_CUDA(cudaStreamSynchronize(st));
   double t2 = now_ms();
+  bool tile_tuned = false;
+  choose_join_tile(ks, X0.p, D, Dp, ix->kind, pin->random_seed, pin->join_tuning, st, &tile_tuned);
   const size_t conv = (size_t)(pin->delta * (float)k * (float)N);  // mod.rs:157
   uint64_t pairs_total = 0, pushes_total = 0, rows_total = 0;
   double ms_cand = 0, ms_join = 0, ms_join_kernel = 0;
@@ -392,50 +450,12 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   finalize_knn(ks, knn_idx.p, knn_raw.p, st);
   unsigned long long hc[4];
   RINND_CUDA(cudaMemcpyAsync(hc, ks.counters.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+  const JoinTile tile = ks.tile;
   ks = KnnState();  // release heap and candidate rows
   RINND_CUDA(cudaStreamSynchronize(st));
   double t4 = now_ms();
-  // diversified CSR (index.rs:656-666) on the original order
-  float min_d = 0.f;
-  build_search_graph(knn_idx.p, knn_raw.p, X0.p, N, k, D, Dp, ix->kind, pin->pruning_degree_multiplier, st,
-                     tmp, ix->graph_orig, &min_d, pin->diversify_prob, pin->random_seed);
-  ix->min_distance = min_d;
-  // corrected neighbor distances (index.rs:669-673)
-  apply_correction_dev(knn_raw.p, (int64_t)N * k, ix->corr, st);
-  ix->knn_idx = std::move(knn_idx);
-  ix->knn_dist = std::move(knn_raw);
-  // vertex order = first retained tree's leaf order (index.rs:679-715)
-  ix->n_search_trees = std::min(std::max(pin->n_search_trees, 0), std::max(pin->n_trees, 0));
-  ix->vertex_order.alloc((size_t)N, st);
-  if (ix->n_search_trees > 0) {
-    RINND_CUDA(cudaMemcpyAsync(ix->vertex_order.p, ix->forest.perm.p, sizeof(int32_t) * N,
-                               cudaMemcpyDeviceToDevice, st));
-  } else {
-    k_iota<<<grid_for(N, 256), 256, 0, st>>>(ix->vertex_order.p, N);
-    RINND_LAUNCH_CHECK();
-  }
-  ix->inverse.alloc((size_t)N, st);
-  invert_permutation(ix->vertex_order.p, N, ix->inverse.p, st);
-  ix->X.alloc((size_t)N * Dp, st);
-  gather_rows(X0.p, ix->vertex_order.p, N, Dp, ix->X.p, st);
+  finish_index(ix.get(), X0.p, std::move(knn_idx), std::move(knn_raw), tmp);
   X0.release();
-  reorder_csr(ix->graph_orig, ix->vertex_order.p, ix->inverse.p, st, tmp, ix->graph_int);
-  if (ix->n_search_trees > 0) {
-    long long tot = (long long)ix->n_search_trees * N;
-    ix->tree_idx.alloc((size_t)tot, st);
-    k_tree_idx<<<grid_for(tot, 256, 148 * 64), 256, 0, st>>>(ix->forest.perm.p, ix->inverse.p, tot,
-                                                              ix->tree_idx.p);
-    RINND_LAUNCH_CHECK();
-    std::vector<int32_t> roots(ix->n_search_trees);
-    for (int t = 0; t < ix->n_search_trees; ++t) roots[t] = t;
-    ix->tree_roots.alloc(roots.size(), st);
-    ix->tree_roots.from_host(roots.data(), roots.size());
-  }
-  ix->forest.perm.release();
-  ix->forest.leaves.release();
-  ix->search_stats.alloc(4, st);
-  ix->search_stats.fill_bytes(0);
-  RINND_CUDA(cudaStreamSynchronize(st));
   double t5 = now_ms();
   rinnd_build_info& inf = ix->info;
   inf.iterations = iters;
@@ -460,7 +480,415 @@ void build_impl(const float* data, bool on_device, int64_t n, int d, int64_t ld,
   inf.push_contention = hc[1];
   inf.search_graph_nnz = ix->graph_orig.nnz;
   inf.min_distance = ix->min_distance;
+  inf.group_items = 1;
+  inf.join_tile_stages = tile.nstage;
+  inf.join_tile_rows = tile.jb;
+  inf.join_tile_ctas_per_sm = tile.per_sm;
+  inf.join_tile_tuned = tile_tuned ? 1 : 0;
   *out = ix.release();
+}
+
+// ---- grouped batched build --------------------------------------------------
+// rinnd_build_many puts indices that share the shape of their NN-Descent state
+// (device, d, metric, normalization, tree kind, k, candidate-list length, leaf
+// size, precision) into groups and builds each group's NN-Descent as ONE set of
+// device rows: one forest pass (every index's trees are root segments of the
+// same level-synchronous split), one leaf initialization, and per iteration one
+// candidate pass and one join whose persistent CTAs walk the vertices of all the
+// group's indices.  Each index keeps its own delta test and iteration cap: its
+// rows are frozen (sample no candidates) once it stops, so its graph is the one
+// its own NN-Descent run would produce from the same trees.  Random streams are
+// keyed by the group's first index's seed and the rows' positions in the group.
+// The search graph, reorder and search trees are then made per index.
+
+// Parameters a build resolves from its inputs (index.rs:617-625, nndescent/mod.rs:89).
+struct Resolved {
+  int leaf_size, max_cand, n_iters, c;
+};
+Resolved resolve_params(const rinnd_build_params* p, int64_t n) {
+  const int k = p->n_neighbors;
+  Resolved r;
+  r.leaf_size = p->leaf_size > 0 ? p->leaf_size : std::max(60, std::min(5 * k, 256));
+  r.max_cand = p->max_candidates > 0 ? p->max_candidates : std::min(k, 60);
+  r.n_iters = p->n_iters > 0 ? p->n_iters : std::max(5, (int)std::ceil(std::log2((double)n)));
+  r.c = std::min(std::min(r.max_cand, 60), k);
+  return r;
+}
+
+struct BatchMember {
+  int32_t item;                 // position in the caller's batch
+  const rinnd_batch_item* it;
+  Resolved r;
+};
+
+struct GroupKey {
+  int device, d, kind, normalize, angular, k, c, leaf_size, precision;
+  bool operator<(const GroupKey& o) const {
+    const int a[9] = {device, d, kind, normalize, angular, k, c, leaf_size, precision};
+    const int b[9] = {o.device, o.d, o.kind, o.normalize, o.angular, o.k, o.c, o.leaf_size, o.precision};
+    return std::lexicographical_compare(a, a + 9, b, b + 9);
+  }
+};
+
+// row -> item by binary search over the item offsets
+__global__ void k_row_items(const int64_t* off, int n_items, int N, int32_t* out) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (off[mid] <= r) lo = mid;
+      else hi = mid - 1;
+    }
+    out[r] = lo;
+  }
+}
+
+// group row ids -> ids local to the row's index
+__global__ void k_localize_ids(int32_t* idx, long long total, int k, const int32_t* row_item, const int64_t* off) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int32_t id = idx[e];
+    if (id >= 0) idx[e] = id - (int32_t)off[row_item[e / k]];
+  }
+}
+
+// Copies the nodes src[0..cnt) of the group forest into an index's own forest
+// (point ids made local); children were remapped on the host.
+__global__ void k_gather_nodes(const int32_t* src, long long cnt, int Dp, const float* offsets, const float* hp,
+                               const int32_t* pivots, int32_t base, float* o_offsets, float* o_hp,
+                               int32_t* o_pivots) {
+  const long long total = cnt * (long long)Dp;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long j = e / Dp;
+    const int t = (int)(e - j * Dp);
+    const int32_t s = src[j];
+    o_hp[e] = hp[(size_t)s * Dp + t];
+    if (t == 0) {
+      o_offsets[j] = offsets[s];
+      const int32_t p0 = pivots[2 * (size_t)s], p1 = pivots[2 * (size_t)s + 1];
+      o_pivots[2 * j] = p0 >= 0 ? p0 - base : -1;
+      o_pivots[2 * j + 1] = p1 >= 0 ? p1 - base : -1;
+    }
+  }
+}
+
+// tree t's leaf order of the index's rows: perm[t * Ntot + base + p] - base
+__global__ void k_local_perm(const int32_t* perm, long long Ntot, int T, int32_t base, int n, int32_t* out) {
+  const long long total = (long long)T * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long t = e / n, p = e - t * n;
+    out[e] = perm[t * Ntot + base + p] - base;
+  }
+}
+
+// The index's own forest from the group forest (children on the host): its
+// first `keep` trees renumbered with roots 0..keep-1 followed by the other
+// nodes in breadth-first order; leaf bounds and pivots made local.  levels and
+// n_leaves count all `trees` trees of the index.
+void extract_forest(const Forest& g, const std::vector<int32_t>& ch, int n_items, int item, int trees, int keep,
+                    int64_t base, int n, cudaStream_t st, Forest& out) {
+  std::vector<int32_t> src, lch;
+  std::vector<std::pair<int32_t, int>> q;  // (group node, depth)
+  int64_t n_leaves = 0;
+  int levels = 0;
+  for (int t = 0; t < trees; ++t) {
+    const bool kept = t < keep;
+    q.clear();
+    q.push_back({(int32_t)(t * n_items + item), 0});
+    if (kept) {
+      // roots first: reserve slot t
+      if (src.size() < (size_t)keep) src.resize((size_t)keep, -1);
+      src[(size_t)t] = q[0].first;
+    }
+    for (size_t h = 0; h < q.size(); ++h) {
+      const int32_t nd = q[h].first;
+      const int dep = q[h].second;
+      const int32_t c0 = ch[2 * (size_t)nd], c1 = ch[2 * (size_t)nd + 1];
+      if (c1 <= 0) {
+        ++n_leaves;
+        continue;
+      }
+      levels = std::max(levels, dep + 1);
+      q.push_back({c0, dep + 1});
+      q.push_back({c1, dep + 1});
+    }
+    if (!kept) continue;
+    for (size_t h = 1; h < q.size(); ++h) src.push_back(q[h].first);
+  }
+  // group node -> local id
+  std::vector<std::pair<int32_t, int32_t>> map;
+  map.reserve(src.size());
+  for (size_t j = 0; j < src.size(); ++j) map.push_back({src[j], (int32_t)j});
+  std::sort(map.begin(), map.end());
+  auto local = [&](int32_t nd) {
+    auto itr = std::lower_bound(map.begin(), map.end(), std::make_pair(nd, (int32_t)INT32_MIN));
+    return itr->second;
+  };
+  lch.resize(2 * src.size());
+  for (size_t j = 0; j < src.size(); ++j) {
+    const int32_t c0 = ch[2 * (size_t)src[j]], c1 = ch[2 * (size_t)src[j] + 1];
+    if (c1 <= 0) {  // leaf: {-start, -end} within the tree's slice
+      lch[2 * j] = c0 + (int32_t)base;
+      lch[2 * j + 1] = c1 + (int32_t)base;
+    } else {
+      lch[2 * j] = local(c0);
+      lch[2 * j + 1] = local(c1);
+    }
+  }
+  const long long cnt = (long long)src.size();
+  out.T = keep;
+  out.N = n;
+  out.Dp = g.Dp;
+  out.n_nodes = cnt;
+  out.n_leaves = n_leaves;
+  out.levels = levels;
+  out.max_leaf = g.max_leaf;
+  out.children.alloc(std::max<size_t>(lch.size(), 2), st);
+  out.offsets.alloc(std::max<size_t>(src.size(), 1), st);
+  out.pivots.alloc(std::max<size_t>(2 * src.size(), 2), st);
+  out.hyperplanes.alloc(std::max<size_t>(src.size(), 1) * (size_t)g.Dp, st);
+  out.perm.alloc(std::max<size_t>((size_t)keep * n, 1), st);
+  if (cnt > 0) {
+    out.children.from_host(lch.data(), lch.size());
+    DVec<int32_t> d_src((size_t)cnt, st);
+    d_src.from_host(src.data(), (size_t)cnt);
+    k_gather_nodes<<<grid_for(cnt * g.Dp, 256, 148 * 32), 256, 0, st>>>(
+        d_src.p, cnt, g.Dp, g.offsets.p, g.hyperplanes.p, g.pivots.p, (int32_t)base, out.offsets.p,
+        out.hyperplanes.p, out.pivots.p);
+    RINND_LAUNCH_CHECK();
+    k_local_perm<<<grid_for((long long)keep * n, 256, 148 * 32), 256, 0, st>>>(g.perm.p, g.N, keep, (int32_t)base,
+                                                                            n, out.perm.p);
+    RINND_LAUNCH_CHECK();
+    RINND_CUDA(cudaStreamSynchronize(st));  // host arrays and d_src are released at scope exit
+  }
+}
+
+// Builds one group; out[m.item] / codes[m.item] / msgs[m.item] receive each
+// member's index or error.
+void build_group(const std::vector<BatchMember>& mem, bool capture, rinnd_index** out, std::vector<int32_t>& codes,
+                 std::vector<std::string>& msgs) {
+  const rinnd_build_params& gp = *mem[0].it->params;
+  const int n_items = (int)mem.size();
+  auto fail_all = [&](int code) {
+    for (const BatchMember& m : mem) {
+      codes[(size_t)m.item] = code;
+      msgs[(size_t)m.item] = g_last_error;
+    }
+  };
+  // the group's rows and NN-Descent state live in this scope
+  std::vector<int64_t> off((size_t)n_items + 1, 0);
+  for (int i = 0; i < n_items; ++i) off[(size_t)i + 1] = off[(size_t)i] + mem[(size_t)i].it->n;
+  const int64_t Ntot = off.back();
+  const int D = mem[0].it->d, Dp = round_up(D, 4), k = gp.n_neighbors;
+  const Resolved R0 = mem[0].r;
+  StreamGuard sg;
+  cudaStream_t st = sg.s;
+  TempStorage tmp;
+  DVec<float> X0;
+  DVec<int32_t> gidx;
+  DVec<float> graw;
+  DVec<int64_t> d_off;
+  DVec<int32_t> row_item;
+  Forest gf;
+  std::vector<int32_t> iters((size_t)n_items, 0);
+  std::vector<int32_t> ch;
+  double ms_forest = 0, ms_leaf = 0, ms_iters = 0, ms_cand = 0, ms_join = 0, ms_join_kernel = 0, ms_sort = 0;
+  uint64_t pairs_total = 0, pushes_total = 0, rows_total = 0, join_launches = 0, join_updates = 0;
+  unsigned long long hc[4] = {0, 0, 0, 0};
+  int join_form = RINND_JOIN_CHUNKED_FP32;
+  JoinTile tile;
+  bool tile_tuned = false;
+  const unsigned long long launches0 = launch_counter();
+  const double t_start = now_ms();
+  int code = guarded([&] {
+    ensure_device(gp.device);
+    require(Ntot < (int64_t)INT32_MAX - 1, "a group holds at most 2^31-2 points");
+    const int N = (int)Ntot;
+    int T = 0;
+    for (const BatchMember& m : mem) T = std::max(T, std::max(m.it->params->n_trees, 0));
+    reserve_pool(gp.device,
+                 build_working_set(Ntot, Dp, k, R0.c, T) +
+                     (gp.precision == RINND_PRECISION_BF16 ? (size_t)Ntot * (round_up(D, 16) * 2 + 8) : 0),
+                 st);
+    X0.alloc((size_t)Ntot * Dp, st);
+    if (Dp != D) X0.fill_bytes(0);
+    for (int i = 0; i < n_items; ++i) {
+      const rinnd_batch_item& it = *mem[(size_t)i].it;
+      const int64_t ld = it.ld > 0 ? it.ld : it.d;
+      RINND_CUDA(cudaMemcpy2DAsync(X0.p + (size_t)off[(size_t)i] * Dp, sizeof(float) * Dp, it.data,
+                                   sizeof(float) * ld, sizeof(float) * D, (size_t)it.n,
+                                   it.data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    }
+    if (gp.normalize) normalize_rows(X0.p, Ntot, D, Dp, st);
+    KnnState ks;
+    ks.precision = gp.precision;
+    if (kind_uses_norms(gp.distance_kind)) {
+      ks.norms.alloc((size_t)N, st);
+      compute_norms(X0.p, N, D, Dp, ks.norms.p, st);
+    }
+    d_off.alloc(off.size(), st);
+    d_off.from_host(off.data(), off.size());
+    row_item.alloc((size_t)N, st);
+    k_row_items<<<grid_for(N, 256, 148 * 16), 256, 0, st>>>(d_off.p, n_items, N, row_item.p);
+    RINND_LAUNCH_CHECK();
+    RINND_CUDA(cudaStreamSynchronize(st));
+    double t0 = now_ms();
+    ForestItems fi;
+    fi.off = off;
+    for (const BatchMember& m : mem) fi.trees.push_back(std::max(m.it->params->n_trees, 0));
+    build_forest(X0.p, N, D, Dp, T, R0.leaf_size, gp.angular != 0, 200, gp.random_seed, st, tmp, gf, &fi);
+    RINND_CUDA(cudaStreamSynchronize(st));
+    double t1 = now_ms();
+    knn_init(ks, N, k, R0.c, st);
+    leaf_init(ks, gf, X0.p, D, Dp, gp.distance_kind, st);
+    ks.row_item.alloc((size_t)N, st);
+    RINND_CUDA(cudaMemcpyAsync(ks.row_item.p, row_item.p, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, st));
+    ks.item_active.alloc((size_t)n_items, st);
+    ks.item_changes.alloc((size_t)n_items, st);
+    RINND_CUDA(cudaStreamSynchronize(st));
+    double t2 = now_ms();
+    choose_join_tile(ks, X0.p, D, Dp, gp.distance_kind, gp.random_seed, gp.join_tuning, st, &tile_tuned);
+    std::vector<uint8_t> active((size_t)n_items, 1);
+    std::vector<unsigned long long> changes((size_t)n_items, 0);
+    int max_iters = 0;
+    for (const BatchMember& m : mem) max_iters = std::max(max_iters, m.r.n_iters);
+    IterationGraph ig;
+    for (int it = 0; it < max_iters; ++it) {
+      int n_active = 0;
+      for (int i = 0; i < n_items; ++i) n_active += active[(size_t)i];
+      if (n_active == 0) break;
+      RINND_CUDA(cudaMemcpyAsync(ks.item_active.p, active.data(), (size_t)n_items, cudaMemcpyHostToDevice, st));
+      JoinStats js;
+      const double a = now_ms();
+      if (capture) {  // candidates + join + applications as one CUDA graph
+        js = iteration_graph(ks, ig, gp.random_seed, it, X0.p, D, Dp, gp.distance_kind, st, changes.data(),
+                             n_items);
+        ms_join += now_ms() - a;
+      } else {
+        ks.item_changes.fill_bytes(0);
+        build_candidates(ks, gp.random_seed, it, st);
+        RINND_CUDA(cudaStreamSynchronize(st));
+        const double b = now_ms();
+        js = local_join(ks, X0.p, D, Dp, gp.distance_kind, st);
+        const double e = now_ms();
+        RINND_CUDA(cudaMemcpyAsync(changes.data(), ks.item_changes.p, sizeof(unsigned long long) * n_items,
+                                   cudaMemcpyDeviceToHost, st));
+        RINND_CUDA(cudaStreamSynchronize(st));
+        ms_cand += b - a;
+        ms_join += e - b;
+      }
+      ms_join_kernel += js.kernel_ms;
+      join_launches += (uint64_t)js.launches;
+      join_updates += js.appended;
+      join_form = js.form;
+      pairs_total += js.pairs;
+      pushes_total += js.changes;
+      rows_total += js.rows;
+      if (gp.verbose)
+        std::printf("Group of %d: iteration %d, %d indices active, %llu updates (%llu pairs)\n", n_items, it + 1,
+                    n_active, js.changes, js.pairs);
+      for (int i = 0; i < n_items; ++i) {
+        if (!active[(size_t)i]) continue;
+        const BatchMember& m = mem[(size_t)i];
+        iters[(size_t)i] = it + 1;
+        // mod.rs:157 delta test per index
+        const size_t conv = (size_t)(m.it->params->delta * (float)k * (float)m.it->n);
+        if ((size_t)changes[(size_t)i] <= conv || it + 1 >= m.r.n_iters) active[(size_t)i] = 0;
+      }
+    }
+    double t3 = now_ms();
+    gidx.alloc((size_t)N * k, st);
+    graw.alloc((size_t)N * k, st);
+    finalize_knn(ks, gidx.p, graw.p, st);
+    k_localize_ids<<<grid_for((long long)N * k, 256, 148 * 32), 256, 0, st>>>(gidx.p, (long long)N * k, k,
+                                                                             row_item.p, d_off.p);
+    RINND_LAUNCH_CHECK();
+    RINND_CUDA(cudaMemcpyAsync(hc, ks.counters.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    tile = ks.tile;
+    ks = KnnState();
+    ch.resize(2 * (size_t)gf.n_nodes);
+    gf.children.to_host(ch.data(), ch.size());
+    gf.leaves.release();
+    RINND_CUDA(cudaStreamSynchronize(st));
+    double t4 = now_ms();
+    ms_forest = t1 - t0;
+    ms_leaf = t2 - t1;
+    ms_iters = t3 - t2;
+    ms_sort = t4 - t3;
+  });
+  if (code != RINND_OK) {
+    fail_all(code);
+    return;
+  }
+  // per index: kNN rows, own forest, search graph, reorder, trees
+  for (int i = 0; i < n_items; ++i) {
+    const BatchMember& m = mem[(size_t)i];
+    const rinnd_build_params* pin = m.it->params;
+    const int32_t n = (int32_t)m.it->n;
+    const double ti = now_ms();
+    codes[(size_t)m.item] = guarded([&] {
+      std::unique_ptr<rinnd_index> ix(new rinnd_index());
+      ix->device = pin->device;
+      ix->p = *pin;
+      ix->p.leaf_size = m.r.leaf_size;
+      ix->p.max_candidates = m.r.max_cand;
+      ix->p.n_iters = m.r.n_iters;
+      ix->p.search_tree_leaf_budget = std::max(1, pin->search_tree_leaf_budget);
+      RINND_CUDA(cudaStreamCreateWithFlags(&ix->st, cudaStreamNonBlocking));
+      cudaStream_t is = ix->st;
+      ix->N = n;
+      ix->D = D;
+      ix->Dp = Dp;
+      ix->k = k;
+      ix->kind = pin->distance_kind;
+      ix->corr = pin->correction;
+      ix->normalize = pin->normalize != 0;
+      const int64_t base = off[(size_t)i];
+      DVec<int32_t> kidx((size_t)n * k, is);
+      DVec<float> kraw((size_t)n * k, is);
+      RINND_CUDA(cudaMemcpyAsync(kidx.p, gidx.p + (size_t)base * k, sizeof(int32_t) * (size_t)n * k,
+                                 cudaMemcpyDeviceToDevice, is));
+      RINND_CUDA(cudaMemcpyAsync(kraw.p, graw.p + (size_t)base * k, sizeof(float) * (size_t)n * k,
+                                 cudaMemcpyDeviceToDevice, is));
+      const int trees = std::max(pin->n_trees, 0);
+      const int keep = std::min(std::max(pin->n_search_trees, 0), trees);
+      extract_forest(gf, ch, n_items, i, trees, keep, base, n, is, ix->forest);
+      TempStorage itmp;
+      finish_index(ix.get(), X0.p + (size_t)base * Dp, std::move(kidx), std::move(kraw), itmp);
+      rinnd_build_info& inf = ix->info;
+      inf.iterations = iters[(size_t)i];
+      inf.forest_levels = ix->forest.levels;
+      inf.n_leaves = ix->forest.n_leaves;
+      inf.ms_forest = ms_forest;
+      inf.ms_leaf_init = ms_leaf;
+      inf.ms_iterations = ms_iters;
+      inf.ms_candidates = ms_cand;
+      inf.ms_join = ms_join;
+      inf.ms_sort = ms_sort;
+      inf.ms_graph = now_ms() - ti;
+      inf.ms_total = now_ms() - t_start;
+      inf.pairs_evaluated = pairs_total;
+      inf.join_rows_gathered = rows_total;
+      inf.ms_join_kernel = ms_join_kernel;
+      inf.join_kernel_launches = join_launches;
+      inf.join_updates = join_updates;
+      inf.join_form = join_form;
+      inf.kernel_launches = launch_counter() - launches0;
+      inf.pushes_accepted = pushes_total;
+      inf.push_contention = hc[1];
+      inf.search_graph_nnz = ix->graph_orig.nnz;
+      inf.min_distance = ix->min_distance;
+      inf.group_items = n_items;
+      inf.join_tile_stages = tile.nstage;
+      inf.join_tile_rows = tile.jb;
+      inf.join_tile_ctas_per_sm = tile.per_sm;
+      inf.join_tile_tuned = tile_tuned ? 1 : 0;
+      out[m.item] = ix.release();
+    });
+    if (codes[(size_t)m.item] != RINND_OK) msgs[(size_t)m.item] = g_last_error;
+  }
 }
 
 void check_index(const rinnd_index* idx) { require(idx != nullptr, "index must not be null"); }
@@ -529,36 +957,101 @@ int rinnd_build_on_stream(const float* data, int32_t data_on_device, int64_t n, 
   });
 }
 
-int rinnd_build_many(const rinnd_batch_item* items, int32_t n_items, int32_t n_workers, rinnd_index** out,
-                     int32_t* status) {
+int rinnd_batch_options_default(rinnd_batch_options* o) {
+  if (!o) return fail(RINND_ERR_INVALID, "options must not be null");
+  std::memset(o, 0, sizeof(*o));
+  o->grouped = 1;
+  o->max_group_points = 8 << 20;
+  o->capture_iterations = 1;
+  return RINND_OK;
+}
+
+int rinnd_build_many_ex(const rinnd_batch_item* items, int32_t n_items, const rinnd_batch_options* opt,
+                        rinnd_index** out, int32_t* status) {
   if (n_items < 0 || (n_items > 0 && (!items || !out)))
     return fail(RINND_ERR_INVALID, "items and out must not be null and n_items >= 0");
+  rinnd_batch_options o;
+  rinnd_batch_options_default(&o);
+  if (opt) o = *opt;
   if (n_items == 0) return RINND_OK;
   for (int32_t i = 0; i < n_items; ++i) out[i] = nullptr;
-  // longest first: estimated work n * d * k
-  std::vector<int32_t> order((size_t)n_items);
-  for (int32_t i = 0; i < n_items; ++i) order[(size_t)i] = i;
-  auto cost = [&](int32_t i) {
-    const rinnd_build_params* p = items[i].params;
-    return (double)items[i].n * (double)std::max(items[i].d, 1) * (double)(p ? std::max(p->n_neighbors, 1) : 1);
-  };
-  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return cost(a) > cost(b); });
-  const int workers = std::max(1, std::min<int>(n_workers > 0 ? n_workers : 16, n_items));
   std::vector<int32_t> codes((size_t)n_items, RINND_OK);
   std::vector<std::string> msgs((size_t)n_items);
+  // validation first: an invalid item fails alone
+  std::vector<BatchMember> valid;
+  for (int32_t i = 0; i < n_items; ++i) {
+    const rinnd_batch_item& it = items[i];
+    codes[(size_t)i] = guarded([&] {
+      require(it.data != nullptr && it.params != nullptr, "batch item data and params must not be null");
+      validate_params(it.params, it.n, it.d);
+      require((it.ld > 0 ? it.ld : it.d) >= it.d, "row stride must be >= dimension");
+      valid.push_back(BatchMember{i, &it, resolve_params(it.params, it.n)});
+    });
+    if (codes[(size_t)i] != RINND_OK) msgs[(size_t)i] = g_last_error;
+  }
+  // tasks: groups of compatible items (or single items), longest first
+  struct Task {
+    std::vector<BatchMember> mem;
+    double cost = 0;
+  };
+  std::vector<Task> tasks;
+  auto cost = [](const BatchMember& m) {
+    return (double)m.it->n * (double)std::max(m.it->d, 1) * (double)std::max(m.it->params->n_neighbors, 1);
+  };
+  if (o.grouped) {
+    std::map<GroupKey, std::vector<BatchMember>> groups;
+    for (const BatchMember& m : valid) {
+      const rinnd_build_params& p = *m.it->params;
+      GroupKey key{p.device, m.it->d, p.distance_kind, p.normalize != 0, p.angular != 0, p.n_neighbors, m.r.c,
+                   m.r.leaf_size, p.precision};
+      groups[key].push_back(m);
+    }
+    const int64_t cap = o.max_group_points > 0 ? o.max_group_points : ((int64_t)INT32_MAX - 2);
+    for (auto& kv : groups) {
+      std::vector<BatchMember>& v = kv.second;
+      std::stable_sort(v.begin(), v.end(), [&](const BatchMember& a, const BatchMember& b) { return cost(a) > cost(b); });
+      Task cur;
+      int64_t pts = 0;
+      for (const BatchMember& m : v) {
+        if (!cur.mem.empty() && pts + m.it->n > cap) {
+          tasks.push_back(std::move(cur));
+          cur = Task();
+          pts = 0;
+        }
+        cur.mem.push_back(m);
+        cur.cost += cost(m);
+        pts += m.it->n;
+      }
+      if (!cur.mem.empty()) tasks.push_back(std::move(cur));
+    }
+  } else {
+    for (const BatchMember& m : valid) {
+      Task t;
+      t.mem.push_back(m);
+      t.cost = cost(m);
+      tasks.push_back(std::move(t));
+    }
+  }
+  std::stable_sort(tasks.begin(), tasks.end(), [](const Task& a, const Task& b) { return a.cost > b.cost; });
+  const int n_tasks = (int)tasks.size();
+  const int workers = std::max(1, std::min<int>(o.n_workers > 0 ? o.n_workers : 16, std::max(n_tasks, 1)));
   std::atomic<int32_t> next{0};
   auto work = [&]() {
     for (;;) {
       const int32_t t = next.fetch_add(1);
-      if (t >= n_items) return;
-      const int32_t i = order[(size_t)t];
-      const rinnd_batch_item& it = items[i];
-      codes[(size_t)i] = guarded([&] {
-        require(it.data != nullptr && it.params != nullptr, "batch item data and params must not be null");
-        build_impl(it.data, it.data_on_device != 0, it.n, it.d, it.ld > 0 ? it.ld : it.d, it.params, nullptr,
-                   &out[i]);
-      });
-      if (codes[(size_t)i] != RINND_OK) msgs[(size_t)i] = g_last_error;
+      if (t >= n_tasks) return;
+      const std::vector<BatchMember>& mem = tasks[(size_t)t].mem;
+      if (mem.size() == 1) {
+        const BatchMember& m = mem[0];
+        const rinnd_batch_item& it = *m.it;
+        codes[(size_t)m.item] = guarded([&] {
+          build_impl(it.data, it.data_on_device != 0, it.n, it.d, it.ld > 0 ? it.ld : it.d, it.params, nullptr,
+                     &out[m.item]);
+        });
+        if (codes[(size_t)m.item] != RINND_OK) msgs[(size_t)m.item] = g_last_error;
+      } else {
+        build_group(mem, o.capture_iterations != 0, out, codes, msgs);
+      }
     }
   };
   std::vector<std::thread> pool;
@@ -574,6 +1067,43 @@ int rinnd_build_many(const rinnd_batch_item* items, int32_t n_items, int32_t n_w
     }
   }
   return rc;
+}
+
+int rinnd_build_many(const rinnd_batch_item* items, int32_t n_items, int32_t n_workers, rinnd_index** out,
+                     int32_t* status) {
+  rinnd_batch_options o;
+  rinnd_batch_options_default(&o);
+  o.n_workers = n_workers;
+  return rinnd_build_many_ex(items, n_items, &o, out, status);
+}
+
+int rinnd_join_tile_table(int32_t* rows, int32_t cap, int32_t* n_rows) {
+  return guarded([&] {
+    require(cap >= 0, "cap must be >= 0");
+    const std::vector<std::array<int, 8>> t = join_tile_table();
+    if (n_rows) *n_rows = (int32_t)t.size();
+    if (rows)
+      for (size_t i = 0; i < t.size() && (int32_t)i < cap; ++i)
+        for (int j = 0; j < 8; ++j) rows[8 * i + j] = t[i][(size_t)j];
+  });
+}
+
+int rinnd_join_tile_table_clear(void) {
+  return guarded([&] { join_tile_table_clear(); });
+}
+
+int rinnd_join_tile_set(const int32_t* row) {
+  return guarded([&] {
+    require(row != nullptr, "row must not be null");
+    require(row[2] == 32 || row[2] == 64, "list class must be 32 or 64");
+    require(row[3] >= 0 && row[3] <= 2 && (row[4] == 0 || row[4] == 1), "unknown metric class or grouped flag");
+    JoinTile t{row[5], row[6], row[7]};
+    require((t.nstage == 2 || t.nstage == 3) && (t.jb == 1 || t.jb == 2) && t.per_sm >= 0,
+            "stages must be 2 or 3, rows per item 1 or 2, CTAs per SM >= 0");
+    require(row[2] == 32 || (t.nstage == 2 && t.jb == 1), "lists longer than 32 run the default shape only");
+    require(join_tile_fits(row[2], row[1], t), "the tile shape does not fit shared memory at this dimension");
+    join_tile_store(row[0], row[1], row[2], row[3], row[4], t);
+  });
 }
 
 int rinnd_search_stats_get(rinnd_index* idx, uint64_t* evaluations, uint64_t* expansions,
@@ -1055,6 +1585,7 @@ int rinnd_nndescent_step(const float* data, int64_t n, int32_t d, int32_t k, int
     dd.from_host(hd.data(), hd.size());
     df.from_host(hf.data(), hf.size());
     if (!hr.empty()) heap_push_batch(ks, (long long)hr.size(), dr.p, di.p, dd.p, df.p, st);
+    join_tile_lookup(ks, Dp, kind);  // the table's tile shape for this key, if any (else the default)
     build_candidates(ks, seed, iteration, st);
     JoinStats js = local_join(ks, X.p, d, Dp, kind, st);
     DVec<int32_t> oi((size_t)N * k, st);

@@ -3,7 +3,9 @@
 #include <stdint.h>
 
 #include "devmem.cuh"
+#include "heap.cuh"
 
+#include <array>
 #include <string>
 
 namespace rinnd {
@@ -30,8 +32,16 @@ struct Forest {
   int max_leaf = 0;
   int levels = 0;
 };
+// Several indices' rows in one forest (a grouped build): item i owns rows
+// [off[i], off[i+1]) and trees 0..trees[i]-1 (trees[i] <= T); the root of
+// (tree t, item i) is node t * n_items + i.  Splits never cross item bounds.
+struct ForestItems {
+  std::vector<int64_t> off;  // n_items + 1
+  std::vector<int> trees;    // n_items
+};
 void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bool angular,
-                  int max_depth, uint64_t seed, cudaStream_t st, TempStorage& tmp, Forest& out);
+                  int max_depth, uint64_t seed, cudaStream_t st, TempStorage& tmp, Forest& out,
+                  const ForestItems* items = nullptr);
 
 // Raises `kernel`'s dynamic shared-memory limit to `bytes` once per (kernel,
 // current device); safe to call from concurrent host threads (api.cu).  Later
@@ -46,6 +56,13 @@ struct BuildStats {
   unsigned long long contention = 0;
   double ms_forest = 0, ms_leaf = 0, ms_iters = 0, ms_sort = 0, ms_graph = 0, ms_total = 0;
   double ms_candidates = 0, ms_join = 0;
+};
+
+// Tile shape of the pipelined FP32 join: row stages in flight per CTA (2 or 3),
+// candidate rows per work item (1 or 2) and CTAs launched per SM (0 = as many
+// as shared memory allows).  Candidate lists longer than 32 run (2, 1, 0).
+struct JoinTile {
+  int nstage = 2, jb = 1, per_sm = 0;
 };
 
 struct KnnState {
@@ -63,6 +80,7 @@ struct KnnState {
   DVec<int> err;             // device error flag of pipelined kernels
   DVec<int32_t> desc;        // per-vertex join descriptors (counts, item prefix, ids, thresholds, norms)
   bool use_tma = true;       // bulk-copy pipelined join when shared memory allows
+  JoinTile tile;             // tile shape of the pipelined FP32 join
   int precision = 0;         // 0: FP32 join tiles; 1: BF16 tensor-core filter + FP32 recheck
   DVec<uint32_t> urow;       // update buffer: destination rows
   DVec<uint64_t> ukey;       // update buffer: slot keys
@@ -78,6 +96,14 @@ struct KnnState {
   int kpb = 0;
   double upv_prev = -1.0;    // updates appended per vertex by the previous join (-1: none yet)
   bool seeded = false;       // rows initialized from tree leaves (their thresholds already filter)
+  // Grouped build (several indices' rows in one state; empty otherwise):
+  // row_item[r] = index of row r; item_active[i] = 0 once index i stopped
+  // iterating; item_changes[i] = accepted pushes into index i's rows since reset.
+  DVec<int32_t> row_item;
+  DVec<uint8_t> item_active;
+  DVec<unsigned long long> item_changes;
+  ItemCount item_count() const { return ItemCount{row_item.p, item_changes.p}; }
+  GroupRows group_rows() const { return GroupRows{row_item.p, item_active.p}; }
 };
 
 void knn_init(KnnState& s, int N, int k, int c, cudaStream_t st);
@@ -93,14 +119,73 @@ struct JoinStats {
   int launches = 0;        // join kernel launches
   int form = 0;            // RINND_JOIN_* of the kernel that ran
 };
+// One local join: plan (host decisions and every allocation / kernel attribute
+// the join needs), enqueue (stream work only: capturable in a CUDA graph), and
+// collect (counters read back -> stats).  local_join does the three in order,
+// timing each join kernel launch with events.
+constexpr int JOIN_MAX_GRID = 148 * 64;  // upper bound of any join launch's grid
+struct JoinPlan {
+  bool generic = false, use_tc = false, use_tma = false;
+  long long per_batch = 1;  // vertices per join launch (each followed by its update application)
+};
+JoinPlan join_plan(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st);
+void join_enqueue(KnnState& s, const JoinPlan& p, const float* X, int D, int Dp, int kind, cudaStream_t st,
+                  std::vector<cudaEvent_t>* kernel_events);
+JoinStats join_collect(KnnState& s, const JoinPlan& p, const unsigned long long* counters, int err);
 JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st);
+void candidates_reserve(KnnState& s, cudaStream_t st);
+// One NN-Descent iteration (candidate pass, join launches, update applications,
+// counter read-back) captured by stream capture into a CUDA graph and launched;
+// later iterations update the instantiated graph in place (cudaGraphExecUpdate)
+// when its topology is unchanged.  item_changes_host (n_items) receives the
+// grouped build's per-index change counts.
+struct IterationGraph {
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long* host = nullptr;  // pinned: 7 counters, error flag, per-index changes
+  size_t host_words = 0;
+  int launches = 0, updates = 0;       // graph launches; of them, in-place updates of the executable
+  IterationGraph() = default;
+  IterationGraph(const IterationGraph&) = delete;
+  IterationGraph& operator=(const IterationGraph&) = delete;
+  ~IterationGraph();
+};
+JoinStats iteration_graph(KnnState& s, IterationGraph& g, uint64_t seed, int iter, const float* X, int D, int Dp,
+                          int kind, cudaStream_t st, unsigned long long* item_changes_host, int n_items);
 bool join_tma_supported(int c, int Dp);
+bool join_tile_fits(int c, int Dp, const JoinTile& t);
+// Join tile tuner (join_tma.cu).  join_tune times every tile shape that fits on
+// the vertices [0, sample) of the current candidate lists, leaves the heaps as
+// they were, stores the fastest shape in s.tile and in the process-wide table,
+// and returns it; join_tile_lookup loads a tuned shape for s's key from the
+// table (false when none is stored).  Table rows: device, Dp, list class (32 or
+// 64), metric class (0 squared Euclidean, 1 Manhattan, 2 dot forms), grouped,
+// stages, rows per item, CTAs per SM.
+struct TileTrial {
+  JoinTile tile;
+  float ms;         // best of the timed trials on the sample
+  int vertices;     // sample size
+};
+JoinTile join_tune(KnnState& s, const float* X, int Dp, int kind, long long sample, cudaStream_t st,
+                   std::vector<TileTrial>* trials = nullptr);
+bool join_tile_lookup(KnnState& s, int Dp, int kind);
+// The build's join tile by rinnd_build_params.join_tuning (RINND_TUNE_*): the
+// fixed default, the table's shape for this key, or one tuned now on the
+// first iteration's candidates (heaps left as they were).  Call before the
+// first iteration; *tuned (may be null) tells whether trials ran.
+JoinTile choose_join_tile(KnnState& s, const float* X, int D, int Dp, int kind, uint64_t seed, int mode,
+                          cudaStream_t st, bool* tuned);
+std::vector<std::array<int, 8>> join_tile_table();
+void join_tile_table_clear();
+void join_tile_store(int device, int Dp, int list_class, int metric_class, int grouped, const JoinTile& t);
 void join_tma_batch(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st);
+void join_tma_reserve(const KnnState& s, int Dp);   // kernel attributes of join_tma_batch
 void join_describe(KnnState& s, int kind, cudaStream_t st);
+void join_describe_reserve(KnnState& s);           // descriptor storage of join_describe
 // Tensor-core join (join_tc.cu): BF16 Gram filter + exact FP32 recheck.  prepare
 // makes the BF16 copy of the rows once per build (s.xb, s.rinfo).
 bool join_tc_supported(int kind, int c, int Dp);
 void join_tc_prepare(KnnState& s, const float* X, int D, int Dp, cudaStream_t st);
+void join_tc_reserve(int kind);                     // kernel attributes of join_tc_batch
 void join_tc_batch(KnnState& s, const float* X, int D, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st);
 // Sorted output: idx (-1 empty), raw distance (+inf empty).
 void finalize_knn(const KnnState& s, int32_t* out_idx, float* out_dist, cudaStream_t st);

@@ -243,11 +243,13 @@ __global__ void k_finalize(const Seg* segs, int S, const int32_t* nleft, const i
   }
 }
 
-__global__ void k_root_leaves(int T, int N, int32_t* children, float* offsets, int32_t* pivots, int4* leaves,
-                              unsigned long long* counters) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= T) return;
-  emit_leaf(t, 0, N, t, children, offsets, pivots, leaves, counters);
+// Roots that are leaves already (an item of at most leaf_size points, or max_depth 0).
+__global__ void k_root_leaves(const int4* roots, int n, int32_t* children, float* offsets, int32_t* pivots,
+                              int4* leaves, unsigned long long* counters) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int4 g = roots[r];
+  emit_leaf(g.x, g.y, g.z, g.w, children, offsets, pivots, leaves, counters);
 }
 
 template <class T>
@@ -261,7 +263,15 @@ void exclusive_scan(const T* in, T* out, long long n, TempStorage& tmp, cudaStre
 }  // namespace
 
 void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bool angular,
-                  int max_depth, uint64_t seed, cudaStream_t st, TempStorage& tmp, Forest& f) {
+                  int max_depth, uint64_t seed, cudaStream_t st, TempStorage& tmp, Forest& f,
+                  const ForestItems* items) {
+  ForestItems one;
+  if (items == nullptr) {
+    one.off = {0, (int64_t)N};
+    one.trees = {T};
+    items = &one;
+  }
+  const int n_items = (int)items->trees.size();
   f.T = T;
   f.N = N;
   f.Dp = Dp;
@@ -275,23 +285,37 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
   k_init_perm<<<grid_for(total, 256, 148 * 64), 256, 0, st>>>(inv.p, N, T);  // identity is its own inverse
   RINND_LAUNCH_CHECK();
 
-  size_t node_cap = (size_t)T * 64;
+  // Root of (tree t, item i) is node t * n_items + i (node t for a single item);
+  // roots of trees an item does not have stay unused.
+  const size_t n_roots = (size_t)T * n_items;
+  size_t node_cap = std::max<size_t>(n_roots * 64, 64);
   f.children.alloc(2 * node_cap, st);
+  f.children.fill_bytes(0);
   f.offsets.alloc(node_cap, st);
   f.pivots.alloc(2 * node_cap, st);
   f.hyperplanes.alloc(node_cap * (size_t)Dp, st);
   f.hyperplanes.fill_bytes(0);
-  f.n_nodes = T;
-  size_t leaf_cap = (size_t)T * 64;
+  f.n_nodes = (int64_t)n_roots;
+  size_t leaf_cap = std::max<size_t>(n_roots * 64, 64);
   f.leaves.alloc(leaf_cap, st);
   DVec<unsigned long long> counters(2, st);  // [0] n_leaves, [1] max leaf size
   counters.fill_bytes(0);
 
   std::vector<Seg> h_roots;
-  if (N > leaf_size && max_depth > 0) {
-    for (int t = 0; t < T; ++t) h_roots.push_back(Seg{t, 0, N, t});
-  } else {
-    k_root_leaves<<<1, 32, 0, st>>>(T, N, f.children.p, f.offsets.p, f.pivots.p, f.leaves.p, counters.p);
+  std::vector<int4> h_root_leaves;
+  for (int t = 0; t < T; ++t)
+    for (int i = 0; i < n_items; ++i) {
+      if (t >= items->trees[i]) continue;
+      const int s0 = (int)items->off[i], s1 = (int)items->off[i + 1], node = t * n_items + i;
+      if (s1 - s0 > leaf_size && max_depth > 0) h_roots.push_back(Seg{t, s0, s1, node});
+      else h_root_leaves.push_back(make_int4(t, s0, s1, node));
+    }
+  if (!h_root_leaves.empty()) {
+    const int nr = (int)h_root_leaves.size();
+    DVec<int4> rl((size_t)nr, st);
+    rl.from_host(h_root_leaves.data(), (size_t)nr);
+    k_root_leaves<<<grid_for(nr, 128), 128, 0, st>>>(rl.p, nr, f.children.p, f.offsets.p, f.pivots.p, f.leaves.p,
+                                                     counters.p);
     RINND_LAUNCH_CHECK();
   }
   int S = (int)h_roots.size();

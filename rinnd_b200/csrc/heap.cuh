@@ -163,4 +163,45 @@ __device__ __forceinline__ int row_push_fast(uint64_t* row, int k, uint32_t* thr
   return row_push(row, k, thr, key, contention);
 }
 
+// Per-index accounting of a grouped build (several indices' rows in one set of
+// heaps): an accepted push into row r adds 1 to changes[row_item[r]].  Both
+// pointers are null outside grouped builds.
+struct ItemCount {
+  const int32_t* row_item;
+  unsigned long long* changes;
+  __device__ __forceinline__ void add(uint32_t row) const {
+    if (changes != nullptr) atomicAdd(&changes[row_item[row]], 1ull);
+  }
+};
+
+// Rows of indices that have finished iterating in a grouped build: frozen rows
+// sample no candidates, so the join neither reads nor changes them.
+struct GroupRows {
+  const int32_t* row_item;
+  const uint8_t* item_active;
+  __device__ __forceinline__ bool frozen(int row) const {
+    return item_active != nullptr && item_active[row_item[row]] == 0;
+  }
+};
+
+// Run-length form for kernels that apply many pushes in row order: counts are
+// held per thread while consecutive rows belong to one item.
+struct ItemTally {
+  int item = -1;
+  unsigned int n = 0;
+  __device__ __forceinline__ void add(const ItemCount& ic, uint32_t row) {
+    if (ic.changes == nullptr) return;
+    const int it = ic.row_item[row];
+    if (it != item) {
+      flush(ic);
+      item = it;
+    }
+    ++n;
+  }
+  __device__ __forceinline__ void flush(const ItemCount& ic) {
+    if (n) atomicAdd(&ic.changes[item], (unsigned long long)n);
+    n = 0;
+  }
+};
+
 }  // namespace rinnd

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(NT)
               const float2* __restrict__ rinfo, const float* __restrict__ X, int Dp, int kind, uint64_t* slots,
               uint32_t* thr, int k, int kp, TcLayout L, uint32_t* urow_buf, uint64_t* ukey_buf,
               unsigned long long* ucount, uint32_t* rcnt, unsigned int rsize, unsigned long long* counters,
-              int* err) {
+              int* err, ItemCount ic) {
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
   Bars B{bar, bar + NSTAGE, bar + 2 * NSTAGE, bar + 2 * NSTAGE + NHDR, bar + 2 * NSTAGE + 2 * NHDR,
@@ -515,6 +515,7 @@ __global__ void __launch_bounds__(NT)
             ukey_buf[(size_t)blockIdx.x * rsize + base] = key;
           } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
             atomicAdd(&counters[0], 1ull);
+            ic.add(row);
           }
           ++base;
         }
@@ -560,7 +561,7 @@ void launch_tc(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, cu
   k_join_tc<SQ><<<grid, NT, smem, st>>>(s.desc.p, v0, v1, reinterpret_cast<const __nv_bfloat16*>(s.xb.p),
                                         reinterpret_cast<const float2*>(s.rinfo.p), X, Dp, kind, s.slots.p, s.thr.p,
                                         s.k, s.kp, L, s.urow.p, s.ukey.p, s.counters.p + 4, s.rcnt.p, s.rsize,
-                                        s.counters.p, err);
+                                        s.counters.p, err, s.item_count());
   RINND_LAUNCH_CHECK();
 }
 
@@ -569,6 +570,12 @@ void launch_tc(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, cu
 bool join_tc_supported(int kind, int c, int Dp) {
   (void)Dp;  // K is streamed in chunks: any row width
   return kind != DK_MANHATTAN && c <= MAXC;
+}
+
+void join_tc_reserve(int kind) {
+  const void* kern = kind == DK_SQEUCLIDEAN ? reinterpret_cast<const void*>(k_join_tc<true>)
+                                            : reinterpret_cast<const void*>(k_join_tc<false>);
+  set_smem_limit_once(kern, 227 * 1024);
 }
 
 void join_tc_prepare(KnnState& s, const float* X, int D, int Dp, cudaStream_t st) {

@@ -28,6 +28,10 @@
 // Every wait is bounded.  A wait that runs out sets the device error flag and a
 // shared abort flag; all warps leave, the producer first waiting (bounded) for
 // every copy it issued.  The host turns the flag into an error.
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "engine.h"
 #include "join_common.cuh"
 
@@ -36,29 +40,31 @@ namespace {
 
 using namespace joinc;
 
-constexpr int NSTAGE = 2;   // row stages (72 KB: three CTAs per SM beat a deeper prefetch)
+// Tile shape (JoinTile, chosen per build by join_tune): NSTAGE row stages in
+// flight per CTA (pipeline depth), JB candidate rows per work item (each
+// against 4 new rows), and the CTAs launched per SM.
 constexpr int NCONS = 8;    // consumer warps
 constexpr int NT = 32 * (1 + NCONS);
-constexpr int JB = 2;       // candidate rows per work item (each against 4 new rows)
 
 struct Layout {
   int maxc, dp, rs, dstride;  // rs: row stride (floats); dstride: descriptor stride (ints)
-  __host__ __device__ size_t bar_bytes() const { return 8 * (2 * NSTAGE + NDESC) + 16; }
+  int ns;                     // row stages (the kernel's NSTAGE)
+  __host__ __device__ size_t bar_bytes() const { return 8 * (2 * ns + NDESC) + 16; }
   __host__ __device__ size_t desc_off() const { return (bar_bytes() + 15) / 16 * 16; }
   __host__ __device__ size_t stage_off() const { return desc_off() + (size_t)NDESC * dstride * 4; }
   __host__ __device__ size_t rows_off() const { return (size_t)dstride * 4; }  // within a stage
   // rows read: B rows j < nb and A quads up to row na + 3 <= 2 * maxc - 1
   __host__ __device__ size_t stage_bytes() const { return rows_off() + (size_t)(2 * maxc) * rs * 4; }
-  __host__ __device__ size_t bytes() const { return stage_off() + NSTAGE * stage_bytes(); }
+  __host__ __device__ size_t bytes() const { return stage_off() + ns * stage_bytes(); }
 };
 
-Layout make_layout(int c, int Dp) {
+Layout make_layout(int c, int Dp, int ns = 2) {
   const int maxc = c <= 32 ? 32 : 64;
-  return Layout{maxc, Dp, Dp + 4, Desc::stride(maxc)};
+  return Layout{maxc, Dp, Dp + 4, Desc::stride(maxc), ns};
 }
 
 __global__ void k_cand_describe(const uint64_t* cand_new, const uint64_t* cand_old, int N, int c, int cp, int maxc,
-                                int dstride, const float* norms, int32_t* desc) {
+                                int dstride, int JB, const float* norms, int32_t* desc) {
   const int v = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (v >= N) return;
   int32_t* d = desc + (size_t)v * dstride;
@@ -109,12 +115,15 @@ struct Bars {
   int* abort_flag;
 };
 
-template <int MAXC>
+// GROUPED: rows of several indices (per-index accounting of direct pushes).
+template <int MAXC, bool GROUPED, int NSTAGE, int JB>
 __global__ void __launch_bounds__(NT, 3)
     k_join_ws(const int32_t* __restrict__ desc, int v0, int v1, const float* __restrict__ X, int Dp, int kind,
-              uint64_t* slots, uint32_t* thr, int k, int kp, Layout L, uint32_t* urow_buf, uint64_t* ukey_buf,
+              uint64_t* slots, uint32_t* thr, int k, int kp, Layout Lin, uint32_t* urow_buf, uint64_t* ukey_buf,
               unsigned long long* ucount, uint32_t* rcnt, unsigned int rsize, unsigned long long* counters,
-              int* err) {
+              int* err, ItemCount ic) {
+  Layout L = Lin;
+  L.ns = NSTAGE;  // (the launch passes the same; a constant folds the offsets)
   extern __shared__ __align__(16) unsigned char smem[];
   Bars B{reinterpret_cast<uint64_t*>(smem), reinterpret_cast<uint64_t*>(smem) + NSTAGE,
          reinterpret_cast<uint64_t*>(smem) + 2 * NSTAGE,
@@ -291,7 +300,7 @@ __global__ void __launch_bounds__(NT, 3)
         const ulonglong2* pa = reinterpret_cast<const ulonglong2*>(rows + (size_t)(4 * iq) * L.rs);
         const int ars = L.rs / 4;
         if (kind == DK_SQEUCLIDEAN) {
-#pragma unroll 2
+#pragma unroll(JB == 1 ? 4 : 2)
           for (int q = 0; q < Dp / 4; ++q) {
             ulonglong2 b[JB];
 #pragma unroll
@@ -309,7 +318,7 @@ __global__ void __launch_bounds__(NT, 3)
           }
         } else if (kind == DK_MANHATTAN) {
           const unsigned long long absmask = 0x7FFFFFFF7FFFFFFFull;
-#pragma unroll 2
+#pragma unroll(JB == 1 ? 4 : 2)
           for (int q = 0; q < Dp / 4; ++q) {
             ulonglong2 b[JB];
 #pragma unroll
@@ -325,7 +334,7 @@ __global__ void __launch_bounds__(NT, 3)
             }
           }
         } else {
-#pragma unroll 2
+#pragma unroll(JB == 1 ? 4 : 2)
           for (int q = 0; q < Dp / 4; ++q) {
             ulonglong2 b[JB];
 #pragma unroll
@@ -396,6 +405,7 @@ __global__ void __launch_bounds__(NT, 3)
               ukey_reg[base] = key;
             } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
               atomicAdd(&counters[0], 1ull);
+              if constexpr (GROUPED) ic.add((uint32_t)row);
             }
             ++base;
           }
@@ -423,12 +433,49 @@ __global__ void __launch_bounds__(NT, 3)
   if (ct == 0 && rows_total) atomicAdd(&counters[3], rows_total);
 }
 
-template <int MAXC>
-void launch_join(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, cudaStream_t st, const Layout& L,
-                 int* err) {
+using JoinKernel = void (*)(const int32_t*, int, int, const float*, int, int, uint64_t*, uint32_t*, int, int, Layout,
+                           uint32_t*, uint64_t*, unsigned long long*, uint32_t*, unsigned int, unsigned long long*, int*,
+                           ItemCount);
+
+// The tile shapes the tuner chooses among (candidate lists of <= 32; longer
+// lists run the default shape).
+template <int MAXC, bool G>
+JoinKernel pick_kernel(int ns, int jb) {
+  if constexpr (MAXC == 32) {
+    if (ns == 3) return jb == 1 ? k_join_ws<MAXC, G, 3, 1> : k_join_ws<MAXC, G, 3, 2>;
+    return jb == 1 ? k_join_ws<MAXC, G, 2, 1> : k_join_ws<MAXC, G, 2, 2>;
+  } else {
+    (void)ns;
+    (void)jb;
+    return k_join_ws<MAXC, G, 2, 1>;
+  }
+}
+
+JoinTile effective_tile(const KnnState& s) {
+  JoinTile t = s.tile;
+  if (t.nstage != 2 && t.nstage != 3) t.nstage = 2;
+  if (t.jb != 1 && t.jb != 2) t.jb = 1;
+  if (s.c > 32) {  // one shape for long lists
+    t.nstage = 2;
+    t.jb = 1;
+  }
+  return t;
+}
+
+JoinKernel join_kernel(const KnnState& s, const JoinTile& t) {
+  const bool grouped = s.item_changes.p != nullptr;
+  if (s.c <= 32) return grouped ? pick_kernel<32, true>(t.nstage, t.jb) : pick_kernel<32, false>(t.nstage, t.jb);
+  return grouped ? pick_kernel<64, true>(t.nstage, t.jb) : pick_kernel<64, false>(t.nstage, t.jb);
+}
+
+void launch_join(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, cudaStream_t st, int* err) {
+  const JoinTile t = effective_tile(s);
+  const Layout L = make_layout(s.c, Dp, t.nstage);
   const size_t smem = L.bytes();
-  set_smem_limit_once(reinterpret_cast<const void*>(k_join_ws<MAXC>), 227 * 1024);
-  const int per_sm = std::max(1, (int)((227 * 1024) / (smem + 1024)));
+  JoinKernel kern = join_kernel(s, t);
+  set_smem_limit_once(reinterpret_cast<const void*>(kern), 227 * 1024);
+  int per_sm = std::max(1, (int)((227 * 1024) / (smem + 1024)));
+  if (t.per_sm > 0) per_sm = std::min(per_sm, t.per_sm);
   const int grid = std::min(v1 - v0, 148 * per_sm);
   if (grid <= 0) return;
   // one region of the update buffer per CTA (k_apply_regions reads them back)
@@ -436,28 +483,148 @@ void launch_join(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, 
   RINND_CUDA(cudaMemsetAsync(s.rcnt.p, 0, sizeof(uint32_t) * grid, st));
   s.nreg = grid;
   s.rsize = (unsigned int)std::min<unsigned long long>(s.ucap / (unsigned long long)grid, 0xFFFFFFFFull);
-  k_join_ws<MAXC><<<grid, NT, smem, st>>>(s.desc.p, v0, v1, X, Dp, kind, s.slots.p, s.thr.p, s.k, s.kp, L,
-                                          s.urow.p, s.ukey.p, s.counters.p + 4, s.rcnt.p, s.rsize, s.counters.p,
-                                          err);
+  kern<<<grid, NT, smem, st>>>(s.desc.p, v0, v1, X, Dp, kind, s.slots.p, s.thr.p, s.k, s.kp, L, s.urow.p, s.ukey.p,
+                               s.counters.p + 4, s.rcnt.p, s.rsize, s.counters.p, err, s.item_count());
   RINND_LAUNCH_CHECK();
 }
 
 }  // namespace
 
-bool join_tma_supported(int c, int Dp) { return make_layout(c, Dp).bytes() <= 220 * 1024; }
+bool join_tma_supported(int c, int Dp) { return make_layout(c, Dp, 2).bytes() <= 220 * 1024; }
+bool join_tile_fits(int c, int Dp, const JoinTile& t) { return make_layout(c, Dp, t.nstage).bytes() <= 220 * 1024; }
+
+void join_describe_reserve(KnnState& s) {
+  const Layout L = make_layout(s.c, 4);
+  if (s.desc.n < (size_t)s.N * L.dstride) s.desc.alloc((size_t)s.N * L.dstride, s.slots.st);
+}
+
+void join_tma_reserve(const KnnState& s, int Dp) {
+  (void)Dp;
+  set_smem_limit_once(reinterpret_cast<const void*>(join_kernel(s, effective_tile(s))), 227 * 1024);
+}
 
 void join_describe(KnnState& s, int kind, cudaStream_t st) {
   const Layout L = make_layout(s.c, 4);
   if (s.desc.n < (size_t)s.N * L.dstride) s.desc.alloc((size_t)s.N * L.dstride, st);
   k_cand_describe<<<grid_for((long long)s.N * 32, 256), 256, 0, st>>>(
-      s.cand_new.p, s.cand_old.p, s.N, s.c, s.cp, L.maxc, L.dstride, kind_is_dot(kind) ? s.norms.p : nullptr, s.desc.p);
+      s.cand_new.p, s.cand_old.p, s.N, s.c, s.cp, L.maxc, L.dstride, effective_tile(s).jb,
+      kind_is_dot(kind) ? s.norms.p : nullptr, s.desc.p);
   RINND_LAUNCH_CHECK();
 }
 
 void join_tma_batch(KnnState& s, const float* X, int Dp, int kind, int v0, int v1, int* err, cudaStream_t st) {
-  const Layout L = make_layout(s.c, Dp);
-  if (L.maxc == 32) launch_join<32>(s, X, Dp, kind, v0, v1, st, L, err);
-  else launch_join<64>(s, X, Dp, kind, v0, v1, st, L, err);
+  launch_join(s, X, Dp, kind, v0, v1, st, err);
+}
+
+// ---- tile tuner -------------------------------------------------------------
+// Tuned shapes are kept per (device, Dp, list class, metric class, grouped) for
+// the life of the process.
+namespace {
+using TileKey = std::tuple<int, int, int, int, int>;
+std::mutex g_tile_mu;
+std::map<TileKey, JoinTile> g_tiles;
+
+TileKey tile_key(const KnnState& s, int Dp, int kind) {
+  int dev = 0;
+  RINND_CUDA(cudaGetDevice(&dev));
+  const int kclass = kind == DK_SQEUCLIDEAN ? 0 : kind == DK_MANHATTAN ? 1 : 2;
+  return TileKey{dev, Dp, s.c <= 32 ? 32 : 64, kclass, s.item_changes.p != nullptr ? 1 : 0};
+}
+}  // namespace
+
+bool join_tile_lookup(KnnState& s, int Dp, int kind) {
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  auto it = g_tiles.find(tile_key(s, Dp, kind));
+  if (it == g_tiles.end()) return false;
+  s.tile = it->second;
+  return true;
+}
+
+std::vector<std::array<int, 8>> join_tile_table() {
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  std::vector<std::array<int, 8>> out;
+  for (const auto& kv : g_tiles) {
+    const TileKey& k = kv.first;
+    out.push_back({std::get<0>(k), std::get<1>(k), std::get<2>(k), std::get<3>(k), std::get<4>(k), kv.second.nstage,
+                   kv.second.jb, kv.second.per_sm});
+  }
+  return out;
+}
+
+void join_tile_store(int device, int Dp, int list_class, int metric_class, int grouped, const JoinTile& t) {
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  g_tiles[TileKey{device, Dp, list_class, metric_class, grouped}] = t;
+}
+
+void join_tile_table_clear() {
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  g_tiles.clear();
+}
+
+// Times every tile shape on the same vertex sample of the current candidate
+// lists (built by the caller) and keeps the fastest in s.tile and the table.
+// Trials append to the update buffer but their updates are never applied, and
+// the few pushes a full buffer region sends directly are undone by restoring
+// the rows and thresholds afterwards, so the heaps are those the caller had.
+JoinTile join_tune(KnnState& s, const float* X, int Dp, int kind, long long sample, cudaStream_t st,
+                   std::vector<TileTrial>* trials) {
+  const size_t nslots = (size_t)s.N * s.kp;
+  DVec<uint64_t> slots0(nslots, st);
+  DVec<uint32_t> thr0((size_t)s.N, st);
+  DVec<unsigned long long> cnt0(8, st);
+  RINND_CUDA(cudaMemcpyAsync(slots0.p, s.slots.p, sizeof(uint64_t) * nslots, cudaMemcpyDeviceToDevice, st));
+  RINND_CUDA(cudaMemcpyAsync(thr0.p, s.thr.p, sizeof(uint32_t) * s.N, cudaMemcpyDeviceToDevice, st));
+  RINND_CUDA(cudaMemcpyAsync(cnt0.p, s.counters.p, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToDevice, st));
+  const int v1 = (int)std::min<long long>(s.N, std::max<long long>(1, sample));
+  std::vector<JoinTile> cands;
+  for (int ns : {2, 3})
+    for (int jb : {2, 1})
+      for (int per_sm : {0, 2}) {
+        JoinTile t{ns, jb, per_sm};
+        if (s.c > 32 && !(ns == 2 && jb == 1)) continue;
+        if (!join_tile_fits(s.c, Dp, t)) continue;
+        cands.push_back(t);
+      }
+  const JoinTile saved = s.tile;
+  std::vector<float> best(cands.size(), 1e30f);
+  cudaEvent_t e0, e1;
+  RINND_CUDA(cudaEventCreate(&e0));
+  RINND_CUDA(cudaEventCreate(&e1));
+  for (int round = 0; round < 2; ++round)
+    for (size_t i = 0; i < cands.size(); ++i) {
+      s.tile = cands[i];
+      join_tma_reserve(s, Dp);
+      join_describe(s, kind, st);
+      RINND_CUDA(cudaMemsetAsync(s.counters.p + 4, 0, sizeof(unsigned long long), st));
+      RINND_CUDA(cudaEventRecord(e0, st));
+      join_tma_batch(s, X, Dp, kind, 0, v1, s.err.p, st);
+      RINND_CUDA(cudaEventRecord(e1, st));
+      s.nreg = 0;  // the trial's updates are dropped
+      RINND_CUDA(cudaMemcpyAsync(s.slots.p, slots0.p, sizeof(uint64_t) * nslots, cudaMemcpyDeviceToDevice, st));
+      RINND_CUDA(cudaMemcpyAsync(s.thr.p, thr0.p, sizeof(uint32_t) * s.N, cudaMemcpyDeviceToDevice, st));
+      RINND_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      RINND_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (round > 0) best[i] = std::min(best[i], ms);
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  RINND_CUDA(cudaMemcpyAsync(s.counters.p, cnt0.p, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToDevice, st));
+  int herr = 0;
+  RINND_CUDA(cudaMemcpyAsync(&herr, s.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  RINND_CUDA(cudaStreamSynchronize(st));
+  if (herr) throw CudaError("join tuning: a shared-memory pipeline stage did not complete within its wait limit");
+  size_t pick = 0;
+  for (size_t i = 0; i < cands.size(); ++i) {
+    if (best[i] < best[pick]) pick = i;
+    if (trials) trials->push_back(TileTrial{cands[i], best[i], v1});
+  }
+  JoinTile chosen = cands.empty() ? saved : cands[pick];
+  s.tile = chosen;
+  join_tma_reserve(s, Dp);
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  g_tiles[tile_key(s, Dp, kind)] = chosen;
+  return chosen;
 }
 
 }  // namespace rinnd

@@ -22,6 +22,8 @@
 // every thread accumulates a 4x4 block of pair distances in registers.
 #include <cub/cub.cuh>
 
+#include <cstring>
+
 #include <vector>
 
 #include "dist.cuh"
@@ -89,6 +91,7 @@ struct UpdateBuf {
   uint64_t* key;
   unsigned long long* count;  // total appended (may exceed cap)
   unsigned long long cap;
+  ItemCount ic;               // per-index accounting of direct pushes (grouped builds)
 };
 
 __device__ __forceinline__ void stage_rows(const float* __restrict__ X, int Dp, int c0, const int32_t* ids,
@@ -246,6 +249,7 @@ __device__ __forceinline__ void join_pairs(PairSmem<MAXA, MAXB, AROWS>& sm, int 
           ub.key[base] = key;
         } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
           atomicAdd(&counters[0], 1ull);
+          ub.ic.add(row);
         }
         ++base;
       }
@@ -314,6 +318,7 @@ __device__ __forceinline__ void emit_generic(UpdateBuf ub, uint32_t row, uint64_
     ub.key[at] = key;
   } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
     atomicAdd(&counters[0], 1ull);
+    ub.ic.add(row);
   }
 }
 
@@ -410,19 +415,24 @@ __device__ __forceinline__ unsigned long long spread_entry(unsigned long long e,
 
 __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, const unsigned long long* count,
                                 unsigned long long cap, uint64_t* slots, uint32_t* thr, int k, int kp,
-                                unsigned long long* counters, bool spread) {
+                                unsigned long long* counters, bool spread, ItemCount ic) {
   const unsigned long long n = min(*count, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     atomicAdd(&counters[5], n);
     atomicAdd(&counters[6], *count);  // appended, including overflow pushed directly
   }
   unsigned int mine = 0;
+  ItemTally tally;
   for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
        e += (unsigned long long)gridDim.x * blockDim.x) {
     const unsigned long long x = spread ? spread_entry(e, n) : e;
     uint32_t r = urow[x];
-    mine += row_push(slots + (size_t)r * kp, k, thr + r, ukey[x], &counters[1]);
+    if (row_push(slots + (size_t)r * kp, k, thr + r, ukey[x], &counters[1])) {
+      ++mine;
+      tally.add(ic, r);
+    }
   }
+  tally.flush(ic);
   for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&counters[0], (unsigned long long)mine);
 }
@@ -431,7 +441,7 @@ __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, cons
 // updates from entry r * rsize; `sub` blocks share a region.
 __global__ void k_apply_regions(const uint32_t* urow, const uint64_t* ukey, const uint32_t* rcnt, int nreg,
                                 unsigned int rsize, int sub, const unsigned long long* count, uint64_t* slots,
-                                uint32_t* thr, int k, int kp, unsigned long long* counters) {
+                                uint32_t* thr, int k, int kp, unsigned long long* counters, ItemCount ic) {
   const int r = blockIdx.x / sub, part = blockIdx.x - r * sub;
   if (r >= nreg) return;
   const unsigned int cnt = rcnt[r];
@@ -441,12 +451,17 @@ __global__ void k_apply_regions(const uint32_t* urow, const uint64_t* ukey, cons
   }
   const size_t base = (size_t)r * rsize;
   unsigned int mine = 0;
+  ItemTally tally;
   // (in order: the join's updates rarely share rows within a warp, and reads
   // in order are cheaper than spread ones)
   for (unsigned int e = part * blockDim.x + threadIdx.x; e < cnt; e += sub * blockDim.x) {
     const uint32_t row = urow[base + e];
-    mine += row_push(slots + (size_t)row * kp, k, thr + row, ukey[base + e], &counters[1]);
+    if (row_push(slots + (size_t)row * kp, k, thr + row, ukey[base + e], &counters[1])) {
+      ++mine;
+      tally.add(ic, row);
+    }
   }
+  tally.flush(ic);
   for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&counters[0], (unsigned long long)mine);
 }
@@ -527,11 +542,23 @@ __device__ __forceinline__ uint32_t cand_priority(uint64_t seed, int iter, int r
 
 template <int P>
 __global__ void k_cand_forward(const uint64_t* slots, int N, int k, int kp, int c, int cp, uint64_t* cnew,
-                               uint64_t* cold, uint32_t* thr_new, uint32_t* thr_old, uint64_t seed, int iter) {
+                               uint64_t* cold, uint32_t* thr_new, uint32_t* thr_old, uint64_t seed, int iter,
+                               GroupRows grp) {
   __shared__ uint64_t buf[4][P];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * 4 + w;
   if (row >= N) return;
+  if (grp.frozen(row)) {  // a finished index of a grouped build: empty lists that accept no offer
+    for (int t = lane; t < c; t += 32) {
+      cnew[(size_t)row * cp + t] = CAND_EMPTY;
+      cold[(size_t)row * cp + t] = CAND_EMPTY;
+    }
+    if (lane == 0) {
+      thr_new[row] = 0u;
+      thr_old[row] = 0u;
+    }
+    return;
+  }
   uint64_t* b = buf[w];
   for (int flag = 1; flag >= 0; --flag) {
     int n = 0;
@@ -592,7 +619,7 @@ __global__ void k_cand_forward(const uint64_t* slots, int N, int k, int kp, int 
 
 __global__ void k_cand_reverse(const uint64_t* slots, int N, int k, int kp, int c, int cp, uint64_t* cnew,
                                uint64_t* cold, uint32_t* thr_new, uint32_t* thr_old, uint64_t seed, int iter,
-                               unsigned long long* contention) {
+                               unsigned long long* contention, GroupRows grp) {
   long long total = (long long)N * k;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
@@ -600,7 +627,7 @@ __global__ void k_cand_reverse(const uint64_t* slots, int N, int k, int kp, int 
     int j = (int)(e % k);
     uint64_t sl = slots[(size_t)i * kp + j];
     int32_t id = slot_id(sl);
-    if (id < 0) continue;
+    if (id < 0 || grp.frozen(i)) continue;  // (a frozen row's neighbors are frozen rows too)
     const bool nw = slot_new(sl);
     uint64_t key = ((uint64_t)cand_priority(seed, iter, i, id) << 32) | (uint32_t)i;
     row_push_fast((nw ? cnew : cold) + (size_t)id * cp, c, (nw ? thr_new : thr_old) + id, key, contention);
@@ -724,16 +751,17 @@ void apply_pending(KnnState& s, cudaStream_t st, bool spread = false) {
   if (s.nreg > 0) {
     const int sub = std::max(1, (148 * 16) / s.nreg);
     k_apply_regions<<<s.nreg * sub, 256, 0, st>>>(s.urow.p, s.ukey.p, s.rcnt.p, s.nreg, s.rsize, sub,
-                                                  s.counters.p + 4, s.slots.p, s.thr.p, s.k, s.kp, s.counters.p);
+                                                  s.counters.p + 4, s.slots.p, s.thr.p, s.k, s.kp, s.counters.p,
+                                                  s.item_count());
     RINND_LAUNCH_CHECK();
     s.nreg = 0;
     return;
   }
   k_apply_updates<<<148 * 16, 256, 0, st>>>(s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap, s.slots.p, s.thr.p,
-                                            s.k, s.kp, s.counters.p, spread);
+                                            s.k, s.kp, s.counters.p, spread, s.item_count());
   RINND_LAUNCH_CHECK();
 }
-UpdateBuf update_buf(KnnState& s) { return UpdateBuf{s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap}; }
+UpdateBuf update_buf(KnnState& s) { return UpdateBuf{s.urow.p, s.ukey.p, s.counters.p + 4, s.ucap, s.item_count()}; }
 }  // namespace
 
 void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int kind,
@@ -787,79 +815,94 @@ void leaf_init(KnnState& s, const Forest& f, const float* X, int D, int Dp, int 
   }
 }
 
-void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st) {
+void candidates_reserve(KnnState& s, cudaStream_t st) {
   if (s.cthr.n < 2 * (size_t)s.N) s.cthr.alloc(2 * (size_t)s.N, st);
+}
+
+void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st) {
+  candidates_reserve(s, st);
   uint32_t* thr_new = s.cthr.p;
   uint32_t* thr_old = s.cthr.p + s.N;
   const int grid = (s.N + 3) / 4;
   if (s.k <= 32)
     k_cand_forward<32><<<grid, 128, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p,
-                                             thr_new, thr_old, seed, iter);
+                                             thr_new, thr_old, seed, iter, s.group_rows());
   else if (s.k <= 64)
     k_cand_forward<64><<<grid, 128, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p,
-                                             thr_new, thr_old, seed, iter);
+                                             thr_new, thr_old, seed, iter, s.group_rows());
   else
     k_cand_forward<128><<<grid, 128, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p,
-                                              thr_new, thr_old, seed, iter);
+                                              thr_new, thr_old, seed, iter, s.group_rows());
   RINND_LAUNCH_CHECK();
   long long total = (long long)s.N * s.k;
   k_cand_reverse<<<grid_for(total, 256, 148 * 64), 256, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp,
                                                                 s.cand_new.p, s.cand_old.p, thr_new, thr_old,
-                                                                seed, iter, &s.counters.p[1]);
+                                                                seed, iter, &s.counters.p[1], s.group_rows());
   RINND_LAUNCH_CHECK();
   k_mark_old<<<grid_for((long long)s.N * 32, 256), 256, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.cand_new.p,
                                                                  s.c, s.cp);
   RINND_LAUNCH_CHECK();
 }
 
-JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st) {
+JoinPlan join_plan(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st) {
   ensure_update_buffer(s, st);
-  RINND_CUDA(cudaMemsetAsync(s.counters.p, 0, sizeof(unsigned long long), st));
-  RINND_CUDA(cudaMemsetAsync(s.counters.p + 2, 0, 2 * sizeof(unsigned long long), st));
-  RINND_CUDA(cudaMemsetAsync(s.counters.p + 5, 0, 2 * sizeof(unsigned long long), st));
-  cudaEvent_t e0, e1;
-  RINND_CUDA(cudaEventCreate(&e0));
-  RINND_CUDA(cudaEventCreate(&e1));
-  const bool generic = kind_is_generic(kind);
-  const bool use_tc = !generic && s.precision == 1 && join_tc_supported(kind, s.c, Dp);
-  const bool use_tma = !generic && (use_tc || (s.use_tma && join_tma_supported(s.c, Dp)));
+  JoinPlan p;
+  p.generic = kind_is_generic(kind);
+  p.use_tc = !p.generic && s.precision == 1 && join_tc_supported(kind, s.c, Dp);
+  p.use_tma = !p.generic && (p.use_tc || (s.use_tma && join_tma_supported(s.c, Dp)));
   if (s.err.n == 0) {
     s.err.alloc(1, st);
     s.err.fill_bytes(0);
   }
+  // one region of the update buffer per join CTA: enough counts for any grid
+  if (s.rcnt.n < (size_t)JOIN_MAX_GRID) s.rcnt.alloc((size_t)JOIN_MAX_GRID, st);
   // The chunked kernel batches for its worst case, 4 c^2 updates per vertex (2 directions x
   // c new x 2c candidates).  The pipelined kernel batches for the expected count: the
   // previous iteration's appended updates per vertex (an estimate before the first), with
   // the buffer filled to 80%; rows tightened by one batch's pushes filter the next.
-  long long per_batch =
+  p.per_batch =
       std::max<long long>(1, (long long)(s.ucap / (4ull * (unsigned long long)s.c * (unsigned long long)s.c)));
-  if (use_tma) {
+  if (p.use_tma) {
     // First join: rows seeded from the tree leaves already filter most pairs
     // (~0.09 c^2 updates per vertex measured on 1M-point mixtures, k = 30);
     // unseeded rows (no trees) pass nearly every pair.
     const double first = (s.seeded ? 0.25 : 1.2) * (double)s.c * (double)s.c;
     const double upv = s.upv_prev >= 0 ? 1.1 * s.upv_prev : first;
     const double nbatch = std::max(1.0, std::ceil(upv * (double)s.N / (0.8 * (double)s.ucap)));
-    per_batch = std::max<long long>(1, (long long)std::ceil((double)s.N / nbatch));
+    p.per_batch = std::max<long long>(1, (long long)std::ceil((double)s.N / nbatch));
+    join_describe_reserve(s);
   }
-  if (use_tc) join_tc_prepare(s, X, D, Dp, st);
-  RINND_CUDA(cudaEventRecord(e0, st));
-  if (use_tma) join_describe(s, kind, st);
-  std::vector<cudaEvent_t> kev;  // start/stop of every join kernel launch
-  for (long long v0 = 0; v0 < s.N; v0 += per_batch) {
-    int v1 = (int)std::min<long long>(s.N, v0 + per_batch);
+  if (p.use_tc) {
+    join_tc_prepare(s, X, D, Dp, st);
+    join_tc_reserve(kind);
+  } else if (p.use_tma) {
+    join_tma_reserve(s, Dp);
+  }
+  return p;
+}
+
+void join_enqueue(KnnState& s, const JoinPlan& p, const float* X, int D, int Dp, int kind, cudaStream_t st,
+                  std::vector<cudaEvent_t>* kev) {
+  RINND_CUDA(cudaMemsetAsync(s.counters.p, 0, sizeof(unsigned long long), st));
+  RINND_CUDA(cudaMemsetAsync(s.counters.p + 2, 0, 2 * sizeof(unsigned long long), st));
+  RINND_CUDA(cudaMemsetAsync(s.counters.p + 5, 0, 2 * sizeof(unsigned long long), st));
+  if (p.use_tma) join_describe(s, kind, st);
+  for (long long v0 = 0; v0 < s.N; v0 += p.per_batch) {
+    int v1 = (int)std::min<long long>(s.N, v0 + p.per_batch);
     RINND_CUDA(cudaMemsetAsync(s.counters.p + 4, 0, sizeof(unsigned long long), st));
     int grid = (int)std::min<long long>(v1 - v0, 148LL * 16);
-    for (int e = 0; e < 2; ++e) {
-      kev.emplace_back();
-      RINND_CUDA(cudaEventCreate(&kev.back()));
+    if (kev) {
+      for (int e = 0; e < 2; ++e) {
+        kev->emplace_back();
+        RINND_CUDA(cudaEventCreate(&kev->back()));
+      }
+      RINND_CUDA(cudaEventRecord((*kev)[kev->size() - 2], st));
     }
-    RINND_CUDA(cudaEventRecord(kev[kev.size() - 2], st));
-    if (use_tc) {
+    if (p.use_tc) {
       join_tc_batch(s, X, D, Dp, kind, (int)v0, v1, s.err.p, st);
-    } else if (use_tma) {
+    } else if (p.use_tma) {
       join_tma_batch(s, X, Dp, kind, (int)v0, v1, s.err.p, st);
-    } else if (generic) {
+    } else if (p.generic) {
       if (s.c <= 32)
         k_local_join_generic<32><<<grid, 128, 0, st>>>(s.cand_new.p, s.cand_old.p, (int)v0, v1, s.c, s.cp, X, D, Dp,
                                                         kind, s.slots.p, s.thr.p, s.k, s.kp, update_buf(s),
@@ -880,17 +923,39 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
                                                   s.counters.p);
       RINND_LAUNCH_CHECK();
     }
-    RINND_CUDA(cudaEventRecord(kev.back(), st));
+    if (kev) RINND_CUDA(cudaEventRecord(kev->back(), st));
     apply_pending(s, st);
   }
+}
+
+JoinStats join_collect(KnnState& s, const JoinPlan& p, const unsigned long long* h, int herr) {
+  if (herr) throw CudaError("local join: a shared-memory pipeline stage did not complete within its wait limit");
+  JoinStats js;
+  js.form = p.use_tc ? RINND_JOIN_TENSOR_BF16 : p.use_tma ? RINND_JOIN_PIPELINED_FP32 : RINND_JOIN_CHUNKED_FP32;
+  js.changes = h[0];
+  js.pairs = h[2];
+  js.rows = h[3];
+  js.updates = h[5];
+  js.appended = h[6];
+  s.upv_prev = (double)h[6] / (double)s.N;
+  return js;
+}
+
+JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaStream_t st) {
+  const JoinPlan p = join_plan(s, X, D, Dp, kind, st);
+  cudaEvent_t e0, e1;
+  RINND_CUDA(cudaEventCreate(&e0));
+  RINND_CUDA(cudaEventCreate(&e1));
+  std::vector<cudaEvent_t> kev;  // start/stop of every join kernel launch
+  RINND_CUDA(cudaEventRecord(e0, st));
+  join_enqueue(s, p, X, D, Dp, kind, st, &kev);
   RINND_CUDA(cudaEventRecord(e1, st));
   unsigned long long h[7];
   int herr = 0;
   RINND_CUDA(cudaMemcpyAsync(h, s.counters.p, sizeof(h), cudaMemcpyDeviceToHost, st));
   RINND_CUDA(cudaMemcpyAsync(&herr, s.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   RINND_CUDA(cudaStreamSynchronize(st));
-  if (herr) throw CudaError("local join: a shared-memory pipeline stage did not complete within its wait limit");
-  JoinStats js;
+  JoinStats js = join_collect(s, p, h, herr);
   RINND_CUDA(cudaEventElapsedTime(&js.total_ms, e0, e1));
   for (size_t e = 0; e < kev.size(); e += 2) {
     float ms = 0.f;
@@ -898,16 +963,113 @@ JoinStats local_join(KnnState& s, const float* X, int D, int Dp, int kind, cudaS
     js.kernel_ms += ms;
   }
   js.launches = (int)(kev.size() / 2);
-  js.form = use_tc ? RINND_JOIN_TENSOR_BF16 : use_tma ? RINND_JOIN_PIPELINED_FP32 : RINND_JOIN_CHUNKED_FP32;
   for (cudaEvent_t ev : kev) cudaEventDestroy(ev);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  js.changes = h[0];
-  js.pairs = h[2];
-  js.rows = h[3];
-  js.updates = h[5];
-  js.appended = h[6];
-  s.upv_prev = (double)h[6] / (double)s.N;
+  return js;
+}
+
+JoinTile choose_join_tile(KnnState& s, const float* X, int D, int Dp, int kind, uint64_t seed, int mode,
+                          cudaStream_t st, bool* tuned) {
+  if (tuned) *tuned = false;
+  if (mode == RINND_TUNE_FIXED) {
+    s.tile = JoinTile();
+    return s.tile;
+  }
+  const JoinPlan p = join_plan(s, X, D, Dp, kind, st);
+  if (!p.use_tma || p.use_tc) return s.tile;
+  if (mode != RINND_TUNE_RETUNE && join_tile_lookup(s, Dp, kind)) return s.tile;
+  // the first iteration's candidate lists, sampled; the heaps (with their
+  // flags) are put back so the iteration itself starts from the same state
+  const size_t nslots = (size_t)s.N * s.kp;
+  DVec<uint64_t> slots0(nslots, st);
+  DVec<uint32_t> thr0((size_t)s.N, st);
+  RINND_CUDA(cudaMemcpyAsync(slots0.p, s.slots.p, sizeof(uint64_t) * nslots, cudaMemcpyDeviceToDevice, st));
+  RINND_CUDA(cudaMemcpyAsync(thr0.p, s.thr.p, sizeof(uint32_t) * s.N, cudaMemcpyDeviceToDevice, st));
+  build_candidates(s, seed, 0, st);
+  join_tune(s, X, Dp, kind, std::min<long long>(p.per_batch, 131072), st);
+  RINND_CUDA(cudaMemcpyAsync(s.slots.p, slots0.p, sizeof(uint64_t) * nslots, cudaMemcpyDeviceToDevice, st));
+  RINND_CUDA(cudaMemcpyAsync(s.thr.p, thr0.p, sizeof(uint32_t) * s.N, cudaMemcpyDeviceToDevice, st));
+  RINND_CUDA(cudaStreamSynchronize(st));
+  if (tuned) *tuned = true;
+  return s.tile;
+}
+
+IterationGraph::~IterationGraph() {
+  if (exec) cudaGraphExecDestroy(exec);
+  if (host) cudaFreeHost(host);
+}
+
+JoinStats iteration_graph(KnnState& s, IterationGraph& g, uint64_t seed, int iter, const float* X, int D, int Dp,
+                          int kind, cudaStream_t st, unsigned long long* item_changes_host, int n_items) {
+  // host-side preparation (allocations, BF16 copy, kernel attributes) happens
+  // outside the capture; the graph holds only stream work
+  const JoinPlan p = join_plan(s, X, D, Dp, kind, st);
+  candidates_reserve(s, st);
+  const size_t host_words = 8 + (size_t)std::max(n_items, 0);
+  if (g.host_words < host_words) {
+    if (g.host) cudaFreeHost(g.host);
+    g.host = nullptr;
+    RINND_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&g.host), host_words * sizeof(unsigned long long),
+                             cudaHostAllocDefault));
+    g.host_words = host_words;
+  }
+  cudaGraph_t graph = nullptr;
+  RINND_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  try {
+    if (n_items > 0 && s.item_changes.p)
+      RINND_CUDA(cudaMemsetAsync(s.item_changes.p, 0, sizeof(unsigned long long) * n_items, st));
+    build_candidates(s, seed, iter, st);
+    join_enqueue(s, p, X, D, Dp, kind, st, nullptr);
+    RINND_CUDA(cudaMemcpyAsync(g.host, s.counters.p, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    RINND_CUDA(cudaMemcpyAsync(g.host + 7, s.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (n_items > 0 && s.item_changes.p)
+      RINND_CUDA(cudaMemcpyAsync(g.host + 8, s.item_changes.p, sizeof(unsigned long long) * n_items,
+                                 cudaMemcpyDeviceToHost, st));
+  } catch (...) {
+    cudaStreamEndCapture(st, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  RINND_CUDA(cudaStreamEndCapture(st, &graph));
+  bool updated = false;
+  if (g.exec) {
+    cudaGraphExecUpdateResultInfo info;
+    updated = cudaGraphExecUpdate(g.exec, graph, &info) == cudaSuccess;
+    if (!updated) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+    }
+  }
+  if (!g.exec) {
+    const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      RINND_CUDA(e);
+    }
+  }
+  g.updates += updated ? 1 : 0;
+  g.launches += 1;
+  cudaEvent_t e0, e1;
+  RINND_CUDA(cudaEventCreate(&e0));
+  RINND_CUDA(cudaEventCreate(&e1));
+  RINND_CUDA(cudaEventRecord(e0, st));
+  const cudaError_t le = cudaGraphLaunch(g.exec, st);
+  RINND_CUDA(cudaEventRecord(e1, st));
+  cudaGraphDestroy(graph);
+  RINND_CUDA(le);
+  RINND_CUDA(cudaStreamSynchronize(st));
+  unsigned long long h[7];
+  for (int i = 0; i < 7; ++i) h[i] = g.host[i];
+  int herr = 0;
+  std::memcpy(&herr, g.host + 7, sizeof(int));
+  if (item_changes_host)
+    for (int i = 0; i < n_items; ++i) item_changes_host[i] = g.host[8 + i];
+  JoinStats js = join_collect(s, p, h, herr);
+  RINND_CUDA(cudaEventElapsedTime(&js.total_ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   return js;
 }
 

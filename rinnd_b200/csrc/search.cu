@@ -20,10 +20,13 @@
 //
 // Per-warp state lives in shared memory: the query, the result list (sorted by
 // (distance, id)), the seed set as a sorted array merged warp-parallel with each
-// batch of accepted neighbors, and an open-addressing visited table.
-// Deviations, all bounded and counted: the seed set keeps at most S entries
-// (the farthest are dropped), and a visited table that cannot place an id after
-// 32 probes treats the id as unvisited (results are still deduplicated).
+// batch of accepted neighbors, and an open-addressing visited table.  Both are
+// bounded (S seeds, a fixed table), while the reference's seed heap and visited
+// bitset are not: a query whose search would exceed either (a seed dropped, or
+// an id the table cannot place within 32 probes) is recorded, and a second
+// launch re-runs exactly those queries from scratch with per-warp global-memory
+// state sized to the index (a visited bitset of N bits and seed arrays of N
+// entries), so every query's result is the one of the unbounded search.
 // Neighbor and tie order follow (distance, id); the reference's BinaryHeap
 // orders exact distance ties by its internal layout.
 #include "dist.cuh"
@@ -61,19 +64,31 @@ struct QRng {  // counter-based per-query stream (seed + query id, as index.rs:1
   __device__ uint32_t next_index(uint32_t n) { return (uint32_t)(((next() >> 32) * (uint64_t)n) >> 32); }
 };
 
-// Visited table: returns true if id was already present (VisitedSet::check_and_mark).
-// An id that finds no free slot within HASH_PROBES probes is counted and treated
-// as visited: it is skipped, which keeps the work of a search bounded.
-__device__ __forceinline__ bool visited_check_and_mark(int32_t* tab, int h, int32_t id,
-                                                       unsigned long long* overflow) {
-  uint32_t pos = ((uint32_t)id * 2654435761u) & (uint32_t)(h - 1);
+// Visited set (VisitedSet::check_and_mark): returns true if id was already
+// present.  Bounded form: an open-addressing table of h entries; an id that
+// finds no free slot within HASH_PROBES probes is counted, treated as visited
+// and marks the search as lost (it will be re-run exactly).  Exact form: a
+// bitset of N bits (bits != null).
+struct Visited {
+  int32_t* tab;
+  int h;
+  uint32_t* bits;
+  bool lost;
+};
+__device__ __forceinline__ bool visited_check_and_mark(Visited& v, int32_t id, unsigned long long* overflow) {
+  if (v.bits) {
+    const uint32_t m = 1u << (id & 31);
+    return (atomicOr(&v.bits[id >> 5], m) & m) != 0u;
+  }
+  uint32_t pos = ((uint32_t)id * 2654435761u) & (uint32_t)(v.h - 1);
   for (int p = 0; p < HASH_PROBES; ++p) {
-    int32_t old = atomicCAS(&tab[pos], -1, id);
+    int32_t old = atomicCAS(&v.tab[pos], -1, id);
     if (old == -1) return false;
     if (old == id) return true;
-    pos = (pos + 1) & (uint32_t)(h - 1);
+    pos = (pos + 1) & (uint32_t)(v.h - 1);
   }
   atomicAdd(overflow, 1ull);
+  v.lost = true;
   return true;
 }
 
@@ -185,11 +200,13 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
 
 // Merge the sorted batch (one key per lane, ascending, ~0 = none; nb valid) into
 // the sorted seed array A[head, tail) -> C[0, min(na + nb, S)); the two arrays
-// are `stride` entries apart (stride >= S).
+// are `stride` entries apart (stride >= S).  Dropping seeds beyond S marks the
+// search as lost (warp-uniform).
 __device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int stride, int S, int& cur,
-                                            int& head, int& tail, uint64_t bkey, int nb) {
+                                            int& head, int& tail, uint64_t bkey, int nb, bool& lost) {
   const int lane = threadIdx.x & 31;
   if (nb == 0) return;
+  if (tail - head + nb > S) lost = true;
   bbuf[lane] = bkey;
   __syncwarp();
   const uint64_t* A = seeds + (size_t)cur * stride;
@@ -329,15 +346,23 @@ __device__ void tree_search_leaves(const SearchIndex& ix, int root, int budget, 
 // k: result-list width; k_out: entries written to oi/od; rerank (QUANT only):
 // number of leading results re-ordered by exact FP32 distance before output;
 // rng_seed: the query's random stream.
+// X (exact re-run, may be null): this warp's visited bitset (N bits) and seed
+// arrays (2 x N entries) in global memory, used instead of the bounded
+// shared-memory state.  Returns true when the bounded state overflowed.
+struct ExactState {
+  uint32_t* bits;
+  uint64_t* seeds;
+};
 template <bool QUANT>
-__device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_t* Q8row,
+__device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_t* Q8row,
                            float qinv, uint64_t rng_seed, int k, int k_out, int rerank, float eps,
-                           const WarpLayout& L, unsigned char* wsm, int32_t* gvis, int32_t* oi,
+                           const WarpLayout& L, unsigned char* wsm, int32_t* gvis, ExactState X, int32_t* oi,
                            float* od, unsigned long long* stats) {
   const int lane = threadIdx.x & 31;
   float* q = reinterpret_cast<float*>(wsm + L.q_off());
   uint64_t* res = reinterpret_cast<uint64_t*>(wsm + L.res_off());
-  uint64_t* seeds = reinterpret_cast<uint64_t*>(wsm + L.seed_off());
+  uint64_t* seeds = X.seeds ? X.seeds : reinterpret_cast<uint64_t*>(wsm + L.seed_off());
+  const int sstride = X.seeds ? ix.N : L.s;  // seed arrays: entries apart, and capacity
   int32_t* vis = reinterpret_cast<int32_t*>(wsm + L.vis_off());
   uint64_t* bbuf = reinterpret_cast<uint64_t*>(wsm + L.batch_off());
   int8_t* q8 = reinterpret_cast<int8_t*>(q);  // QUANT: codes stored in the query slot
@@ -349,12 +374,18 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
   }
   const int vcap = visited_capacity(k);
   if (gvis) vis = gvis;  // global-memory table of this warp
-  for (int t = lane; t < vcap; t += 32) vis[t] = -1;
+  Visited V{vis, vcap, X.bits, false};
+  if (X.bits) {
+    for (int t = lane; t < (ix.N + 31) / 32; t += 32) X.bits[t] = 0u;
+  } else {
+    for (int t = lane; t < vcap; t += 32) vis[t] = -1;
+  }
   __syncwarp();
   QRng rng{rng_seed, 0};
   // seed-set capacity from this query's own width (not the batch's), so a
   // query's result does not depend on the queries it is batched with
-  const int scap = seed_capacity(k);
+  const int scap = X.seeds ? ix.N : seed_capacity(k);
+  bool lost = false;  // bounded state overflowed (warp-uniform)
   int rc = 0, cur = 0, head = 0, tail = 0;
   unsigned long long evals = 0, expansions = 0;
   unsigned long long* overflow = &stats[2];
@@ -366,7 +397,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
     bool fresh = false;
     float d = 0.f;
     if (have) {
-      fresh = !visited_check_and_mark(vis, vcap, my_id, overflow);
+      fresh = !visited_check_and_mark(V, my_id, overflow);
       if (fresh) d = dist_to<QUANT>(ix, q, q8, qinv, my_id);
     }
     unsigned m = __ballot_sync(0xffffffffu, fresh);
@@ -381,7 +412,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
       result_push(res, rc, k, dj, ij);
     }
     uint64_t sorted = warp_sort32(bkey);
-    seeds_merge(seeds, bbuf, L.s, scap, cur, head, tail, sorted, __popc(m));
+    seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(m), lost);
   };
 
   // ---- tree seeding (greedy.rs:70-146): the points of the leaves each tree's
@@ -419,7 +450,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
       for (int r = 0; r < 32 && r0 + r < need; ++r) {
         int32_t x = __shfl_sync(0xffffffffu, id, r);
         bool f = false;
-        if (lane == 0) f = !visited_check_and_mark(vis, vcap, x, overflow);
+        if (lane == 0) f = !visited_check_and_mark(V, x, overflow);
         f = __shfl_sync(0xffffffffu, f, 0);
         if (lane == r) fresh = f;
       }
@@ -434,14 +465,14 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
         result_push(res, rc, k, __shfl_sync(0xffffffffu, d, j), __shfl_sync(0xffffffffu, id, j));
       }
       uint64_t sorted = warp_sort32(fresh ? rkey(d, id) : ~0ull);
-      seeds_merge(seeds, bbuf, L.s, scap, cur, head, tail, sorted, __popc(m));
+      seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(m), lost);
     }
   }
   // ---- traverse (greedy.rs:165-201) ----
   float mx = result_max(res, rc);
   float bound = bound_of(mx);
   while (head < tail) {
-    uint64_t top = seeds[(size_t)cur * L.s + head];
+    uint64_t top = seeds[(size_t)cur * sstride + head];
     ++head;
     float vd = fkey_inv((uint32_t)(top >> 32));
     int32_t v = (int32_t)(uint32_t)top;
@@ -454,7 +485,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
     for (int c0 = s; c0 < e; c0 += 32) {
       int c = c0 + lane;
       int32_t nb = c < e ? ix.indices[c] : -1;
-      bool fresh = nb >= 0 && !visited_check_and_mark(vis, vcap, nb, overflow);
+      bool fresh = nb >= 0 && !visited_check_and_mark(V, nb, overflow);
       float d = fresh ? dist_to<QUANT>(ix, q, q8, qinv, nb) : 0.f;
       unsigned m = __ballot_sync(0xffffffffu, fresh);
       evals += __popc(m);
@@ -475,7 +506,7 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
       }
       bool acc = (acc_mask >> lane) & 1u;
       uint64_t sorted = warp_sort32(acc ? rkey(d, nb) : ~0ull);
-      seeds_merge(seeds, bbuf, L.s, scap, cur, head, tail, sorted, __popc(acc_mask));
+      seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(acc_mask), lost);
     }
   }
   // ---- exact rerank of the first `rerank` results (index.rs:103-126): exact
@@ -516,19 +547,41 @@ __device__ void search_one(const SearchIndex& ix, const float* Qrow, const int8_
     atomicAdd(&stats[1], expansions);
   }
   __syncwarp();
+  return __any_sync(0xffffffffu, lost || V.lost);
 }
+
+// Queries a bounded search could not finish exactly: the first launch appends
+// their indices (count, list); the exact launch re-runs the listed queries with
+// per-warp global-memory state (xbits: words_per_warp words; xseeds: 2 N
+// entries per warp).
+struct Redo {
+  unsigned int* count;
+  int32_t* list;
+  uint32_t* xbits;
+  uint64_t* xseeds;
+  long long words_per_warp;
+};
 
 template <bool QUANT>
 __global__ void __launch_bounds__(WPB * 32)
     k_search(SearchIndex ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k, int k_out,
              int rerank, float eps, uint64_t qid_base, QueryMeta meta, WarpLayout L, int32_t* gvis, int gcap,
-             int32_t* out_idx, float* out_dist, unsigned long long* stats) {
+             int32_t* out_idx, float* out_dist, unsigned long long* stats, Redo redo, bool exact) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   unsigned char* wsm = smem + (size_t)w * L.bytes();
-  int32_t* my_gvis = gvis ? gvis + (size_t)(blockIdx.x * WPB + w) * gcap : nullptr;
+  const long long gw = (long long)blockIdx.x * WPB + w;
+  int32_t* my_gvis = gvis ? gvis + (size_t)gw * gcap : nullptr;
+  ExactState X{nullptr, nullptr};
+  if (exact) {
+    X.bits = redo.xbits + (size_t)gw * redo.words_per_warp;
+    X.seeds = redo.xseeds + (size_t)gw * 2 * ix.N;
+  }
   const int total_warps = gridDim.x * WPB;
-  for (int qi = blockIdx.x * WPB + w; qi < nq; qi += total_warps) {
+  const int n_run = exact ? (int)min((unsigned int)nq, *redo.count) : nq;
+  for (int t = blockIdx.x * WPB + w; t < n_run; t += total_warps) {
+    const int qi = exact ? redo.list[t] : t;
     int qk = k, qko = k_out, qr = rerank;
     float qe = eps;
     // FP32 queries seed with seed + query index (index.rs:165); quantized
@@ -543,9 +596,10 @@ __global__ void __launch_bounds__(WPB * 32)
       stream = QUANT ? 0ull : meta.stream[qi];
       off = meta.out_off[qi];
     }
-    search_one<QUANT>(ix, Q + (size_t)qi * ix.Dp, QUANT ? Q8 + (size_t)qi * ix.Dq : nullptr,
-                      QUANT ? qinv[qi] : 0.f, ix.seed + stream, qk, qko, qr, qe, L, wsm, my_gvis, out_idx + off,
-                      out_dist + off, stats);
+    const bool lost = search_one<QUANT>(ix, Q + (size_t)qi * ix.Dp, QUANT ? Q8 + (size_t)qi * ix.Dq : nullptr,
+                                        QUANT ? qinv[qi] : 0.f, ix.seed + stream, qk, qko, qr, qe, L, wsm, my_gvis, X,
+                                        out_idx + off, out_dist + off, stats);
+    if (lost && !exact && lane == 0) redo.list[atomicAdd(redo.count, 1u)] = qi;
   }
 }
 
@@ -609,6 +663,44 @@ struct GlobalVisited {
   int32_t* p() const { return buf.p; }
 };
 
+// Per-warp global-memory state of the exact re-run: a visited bitset of N bits
+// and two seed arrays of N entries each; as many warps as fit EXACT_BYTES (at
+// least one, at most EXACT_MAX_WARPS).
+constexpr size_t EXACT_BYTES = 256ull << 20;
+constexpr int EXACT_MAX_WARPS = 128;
+
+// The bounded launch over all queries, then the exact launch over the queries
+// it recorded (their outputs are overwritten).  Both are enqueued on `st`; the
+// exact launch finds the recorded count on the device.
+template <bool QUANT>
+void run_search(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k, int k_out,
+                int rerank, float eps, uint64_t qid_base, const QueryMeta& meta, const WarpLayout& L,
+                int32_t* out_idx, float* out_dist, cudaStream_t st, unsigned long long* dstats) {
+  const int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
+  GlobalVisited gv(L, blocks, st);
+  DVec<unsigned int> count(1, st);
+  count.fill_bytes(0);
+  DVec<int32_t> list((size_t)nq, st);
+  Redo redo{count.p, list.p, nullptr, nullptr, 0};
+  k_search<QUANT><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base,
+                                                             meta, L, gv.p(), gv.cap, out_idx, out_dist, dstats, redo,
+                                                             false);
+  RINND_LAUNCH_CHECK();
+  const long long words = ((long long)(ix.N + 31) / 32 + 3) / 4 * 4;  // 16-byte multiple per warp
+  const size_t per_warp = (size_t)words * 4 + (size_t)2 * ix.N * 8;
+  const int warps = (int)std::max<size_t>(1, std::min<size_t>(EXACT_BYTES / per_warp, EXACT_MAX_WARPS));
+  const int xblocks = (std::min(warps, nq) + WPB - 1) / WPB;
+  DVec<uint32_t> xbits((size_t)xblocks * WPB * words, st);
+  DVec<uint64_t> xseeds((size_t)xblocks * WPB * 2 * ix.N, st);
+  redo.xbits = xbits.p;
+  redo.xseeds = xseeds.p;
+  redo.words_per_warp = words;
+  k_search<QUANT><<<xblocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base,
+                                                              meta, L, nullptr, 0, out_idx, out_dist, dstats, redo,
+                                                              true);
+  RINND_LAUNCH_CHECK();
+}
+
 }  // namespace
 
 void greedy_search(const SearchIndex& ix, const float* Q, int nq, int k, float eps,
@@ -616,11 +708,8 @@ void greedy_search(const SearchIndex& ix, const float* Q, int nq, int k, float e
                    unsigned long long* dstats) {
   if (nq <= 0) return;
   const WarpLayout L = layout_for(ix, k);
-  int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
-  GlobalVisited gv(L, blocks, st);
-  k_search<false><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, nullptr, nullptr, nq, k, k, 0, eps, qid_base,
-                                                             QueryMeta{}, L, gv.p(), gv.cap, out_idx, out_dist, dstats);
-  RINND_LAUNCH_CHECK();
+  run_search<false>(ix, Q, nullptr, nullptr, nq, k, k, 0, eps, qid_base, QueryMeta{}, L, out_idx, out_dist, st,
+                    dstats);
 }
 
 void greedy_search_packed(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq,
@@ -632,15 +721,10 @@ void greedy_search_packed(const SearchIndex& ix, const float* Q, const int8_t* Q
   const bool quant = Q8 != nullptr;
   if (quant && (!ix.codes || ix.Dq % 16 != 0)) throw std::invalid_argument("index has no int8 codes");
   const WarpLayout L = layout_for(ix, max_width);
-  int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
-  GlobalVisited gv(L, blocks, st);
   if (quant)
-    k_search<true><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, 0, 0, 0, 0.f, 0, meta, L, gv.p(),
-                                                              gv.cap, out_idx, out_dist, dstats);
+    run_search<true>(ix, Q, Q8, qinv, nq, 0, 0, 0, 0.f, 0, meta, L, out_idx, out_dist, st, dstats);
   else
-    k_search<false><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, nullptr, nullptr, nq, 0, 0, 0, 0.f, 0, meta, L,
-                                                               gv.p(), gv.cap, out_idx, out_dist, dstats);
-  RINND_LAUNCH_CHECK();
+    run_search<false>(ix, Q, nullptr, nullptr, nq, 0, 0, 0, 0.f, 0, meta, L, out_idx, out_dist, st, dstats);
 }
 
 void greedy_search_quantized(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq,
@@ -650,12 +734,7 @@ void greedy_search_quantized(const SearchIndex& ix, const float* Q, const int8_t
   if (!ix.codes || ix.Dq % 16 != 0) throw std::invalid_argument("index has no int8 codes");
   if (k_out > width || rerank > width) throw std::invalid_argument("invalid quantized widths");
   const WarpLayout L = layout_for(ix, width);
-  int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
-  GlobalVisited gv(L, blocks, st);
-  k_search<true><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, width, k_out, rerank, eps, 0,
-                                                            QueryMeta{}, L, gv.p(), gv.cap, out_idx, out_dist,
-                                                            dstats);
-  RINND_LAUNCH_CHECK();
+  run_search<true>(ix, Q, Q8, qinv, nq, width, k_out, rerank, eps, 0, QueryMeta{}, L, out_idx, out_dist, st, dstats);
 }
 
 void tree_leaves(const SearchIndex& ix, const float* Q, const int8_t* Q8, int nq, int tree, int budget,

@@ -129,7 +129,7 @@ def test_quantized_width_validation():
 
 
 STRUCTS = {"rinnd_build_params": "BuildParams", "rinnd_build_info": "BuildInfo", "rinnd_batch_item": "BatchItem",
-           "rinnd_server_params": "ServerParams", "rinnd_server_stats": "ServerStats",
+           "rinnd_batch_options": "BatchOptions", "rinnd_server_params": "ServerParams", "rinnd_server_stats": "ServerStats",
            "rinnd_storage_info": "StorageInfo"}
 
 
@@ -163,3 +163,21 @@ def test_ctypes_mirrors_match_the_header_layout(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(cls), cname
         for field, _ in cls._fields_:
             assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)
+
+
+def test_join_tile_table_rejects_shapes_that_do_not_exist():
+    """rinnd_join_tile_set validates a row on the host (no device needed)."""
+    from rinnd_b200 import _lib as L
+
+    for row in [(0, 64, 32, 0, 0, 4, 2, 0), (0, 64, 32, 0, 0, 2, 3, 0), (0, 64, 64, 0, 0, 3, 1, 0),
+                (0, 64, 48, 0, 0, 2, 2, 0), (0, 64, 32, 5, 0, 2, 2, 0), (0, 4000, 32, 0, 0, 3, 2, 0)]:
+        with pytest.raises(ValueError):
+            L.check(L.lib.rinnd_join_tile_set((ctypes.c_int32 * 8)(*row)))
+    L.check(L.lib.rinnd_join_tile_set((ctypes.c_int32 * 8)(0, 64, 32, 0, 0, 3, 1, 2)))
+    n = ctypes.c_int32(0)
+    rows = (ctypes.c_int32 * 8)()
+    L.check(L.lib.rinnd_join_tile_table(rows, 1, ctypes.byref(n)))
+    assert n.value == 1 and tuple(rows) == (0, 64, 32, 0, 0, 3, 1, 2)
+    L.check(L.lib.rinnd_join_tile_table_clear())
+    L.check(L.lib.rinnd_join_tile_table(None, 0, ctypes.byref(n)))
+    assert n.value == 0

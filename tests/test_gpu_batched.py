@@ -58,3 +58,43 @@ def test_build_many_reports_the_failing_item(rb):
     with pytest.raises(ValueError, match="batch item 1"):
         rb.build_many(datasets, params)
     assert rb.build_many([], []) == []
+
+
+def test_grouped_build_keeps_each_index_own_stop_rule(rb, orc):
+    """One group (same d, metric, k) of uneven sizes: every index stops by its
+    own iteration cap and delta test, its graph holds only its own points, and
+    its recall is no more than 0.5 point below its one-at-a-time build's."""
+    sizes = [12000, 2500, 7000, 300, 18]
+    data = [gmm(n, 64, 20, seed=70 + i) for i, n in enumerate(sizes)]
+    params = [{"metric": "sqeuclidean", "n_neighbors": 15, "random_state": 5 + i} for i in range(len(sizes))]
+    params[2]["n_iters"] = 2
+    many = rb.build_many(data, params, grouped=True)
+    for X, kw, ix in zip(data, params, many):
+        n = X.shape[0]
+        info = ix.build_info
+        assert info["group_items"] == len(sizes)
+        cap = kw.get("n_iters") or max(5, int(np.ceil(np.log2(n))))
+        assert 1 <= info["iterations"] <= cap
+        gi, gd = ix.neighbor_graph
+        assert gi.shape == (n, 15)
+        valid = gi >= 0
+        assert np.all(gi[valid] < n)
+        assert not np.any(gi == np.arange(n)[:, None])
+        assert np.all(np.diff(gd, axis=1)[np.all(valid, axis=1)] >= 0)
+        if n >= 300:
+            one = rb.RINND(X, **kw)
+            r_many = graph_recall(orc, X, gi, "sqeuclidean", 15, m=min(400, n))
+            r_one = graph_recall(orc, X, one.neighbor_graph[0], "sqeuclidean", 15, m=min(400, n))
+            assert r_many >= r_one - 0.005, (n, r_many, r_one)
+        else:  # the whole index is one leaf: its rows are exact
+            assert np.all(valid)
+            assert graph_recall(orc, X, gi, "sqeuclidean", 15, m=n) == 1.0
+    assert many[2].build_info["iterations"] == 2
+    qi, qd = many[0].query(data[0][:50], k=10)
+    assert np.all((qi >= 0) & (qi < sizes[0]))
+
+
+def test_ungrouped_option_builds_each_index_alone(rb):
+    datasets, params = make_batch(4, seed=8)
+    many = rb.build_many(datasets, params, grouped=False)
+    assert all(ix.build_info["group_items"] == 1 for ix in many)

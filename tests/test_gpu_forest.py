@@ -42,6 +42,31 @@ def test_forest_matches_oracle_splits_and_routing(rb, orc, metric, d, n, leaf):
     if metric == "cosine":
         X = np.abs(X) + np.float32(0.1)
     ix = rb.RINND(X, metric=metric, n_neighbors=10, n_trees=3, n_search_trees=1, leaf_size=leaf, random_state=9)
+    check_exported_tree(orc, X, ix, metric, leaf)
+
+
+def test_grouped_build_forests_match_oracle(rb, orc):
+    """Indices built as one group (rinnd_build_many_ex, grouped) share one
+    forest pass; each index's exported tree must still be a complete tree over
+    its own points with the oracle's splits and routing, including an index
+    small enough to be a single leaf."""
+    sizes, trees = [20000, 3000, 25, 9000], [3, 2, 3, 4]
+    data = [gmm(n, 32, 25, seed=40 + i) for i, n in enumerate(sizes)]
+    params = [dict(metric="sqeuclidean", n_neighbors=10, n_trees=t, n_search_trees=1, leaf_size=30, random_state=9)
+              for t in trees]
+    many = rb.build_many(data, params, grouped=True)
+    for X, ix in zip(data, many):
+        assert ix.build_info["group_items"] == len(sizes)
+        if X.shape[0] <= 30:
+            hp, off, ch, ind = ix.export_search_tree()
+            assert ch.shape == (1, 2) and ch[0, 0] == 0 and ch[0, 1] == -X.shape[0]
+            assert np.array_equal(np.sort(ind), np.arange(X.shape[0]))
+            continue
+        check_exported_tree(orc, X, ix, "sqeuclidean", 30)
+
+
+def check_exported_tree(orc, X, ix, metric, leaf):
+    n = X.shape[0]
     hp, off, ch, ind, piv = ix.export_search_tree(with_pivots=True)
     m = hp.shape[0]
     assert off.shape == (m,) and ch.shape == (m, 2) and piv.shape == (m, 2)
