@@ -73,6 +73,8 @@ def parse_args():
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="serving workload: seconds per offered load")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"],
                     help="local-join tiles of the timed builds (the precision form is also reported beside fp32)")
+    ap.add_argument("--join-tuning", default="table", choices=["table", "fixed", "retune"],
+                    help="tile shape of the FP32 join: tuned table (default), fixed default shape, fresh trials")
     ap.add_argument("--items", type=int, default=512, help="batched workload: number of indices")
     ap.add_argument("--check-items", type=int, default=16,
                     help="batched workload: indices whose recall is compared with one-at-a-time builds")
@@ -771,6 +773,7 @@ def main():
     p.distance_kind, p.correction, p.random_seed, p.device = L.DIST_SQEUCLIDEAN, L.CORR_NONE, 42, local_rank
     p.verbose = int(args.verbose)
     p.precision = 1 if args.precision == "bf16" else 0
+    p.join_tuning = {"table": L.TUNE_TABLE, "fixed": L.TUNE_FIXED, "retune": L.TUNE_RETUNE}[args.join_tuning]
 
     def build(src_ptr, on_device):
         h = ctypes.c_void_p()
@@ -1001,7 +1004,10 @@ def main():
                                            "sort": i.ms_sort, "graph": i.ms_graph} for i in infos]},
             "counters": {"pairs_evaluated": int(inf.pairs_evaluated), "pushes_accepted": int(inf.pushes_accepted),
                          "push_contention": int(inf.push_contention), "join_rows": int(inf.join_rows_gathered),
-                         "iterations": int(inf.iterations), "n_leaves": int(inf.n_leaves)},
+                         "iterations": int(inf.iterations), "n_leaves": int(inf.n_leaves),
+                         "join_tile": {"stages": int(inf.join_tile_stages), "rows_per_item": int(inf.join_tile_rows),
+                                       "ctas_per_sm": int(inf.join_tile_ctas_per_sm),
+                                       "mode": args.join_tuning}},
             "phases_ms": {"forest": inf.ms_forest, "leaf_init": inf.ms_leaf_init, "iterations": inf.ms_iterations,
                           "candidates": inf.ms_candidates, "join": inf.ms_join, "sort": inf.ms_sort,
                           "graph": inf.ms_graph, "total": inf.ms_total},

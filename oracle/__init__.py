@@ -67,6 +67,8 @@ def lib():
             "orc_weighted_union_pruned": (_i64, [_i32, _P, _P, _P, _P, _P, _P, _i32, _P, _P]),
             "orc_params_default": (None, [_P]),
             "orc_build": (_P, [_P, _i64, _i32, _P]),
+            "orc_index_from_parts": (_P, [_P, _i64, _i32, ctypes.c_int32, ctypes.c_int32, _P, _P, _f32, _i32, _P,
+                                          _P, _P, _P, _P, _i32, _P, _u64, _i32]),
             "orc_free": (None, [_P]),
             "orc_index_k": (_i32, [_P]),
             "orc_neighbor_graph": (None, [_P, _P, _P]),
@@ -374,6 +376,32 @@ class OracleIndex:
         n, d = self.data.shape
         self.n, self.dim, self.k = n, d, n_neighbors
         self._h = lib().orc_build(_p(self.data), n, d, ctypes.byref(p))
+
+    @classmethod
+    def from_parts(cls, data, *, kind, correction, indptr, indices, min_distance, vertex_order, trees=(),
+                   leaf_budget=1, seed=42, n_threads=0):
+        """A search-only index over another index's graph and trees (internal
+        order: `data` rows, CSR `indptr`/`indices` and each tree's leaf order are
+        in internal ids; `vertex_order` maps internal to original ids).  `trees`
+        is a sequence of (hyperplanes [m, dim], offsets [m], children [m, 2],
+        leaf_indices [n]) in FlatTree layout."""
+        self = cls.__new__(cls)
+        self.data = _f(data)
+        n, d = self.data.shape
+        self.n, self.dim, self.k = n, d, 0
+        self._parts = [np.ascontiguousarray(indptr, np.int32), np.ascontiguousarray(indices, np.int32),
+                       np.ascontiguousarray(vertex_order, np.int32)]
+        tn = np.array([len(t[1]) for t in trees] or [0], np.int64)
+        hp = np.ascontiguousarray(np.concatenate([t[0] for t in trees]) if trees else np.zeros((1, d)), np.float32)
+        off = np.ascontiguousarray(np.concatenate([t[1] for t in trees]) if trees else np.zeros(1), np.float32)
+        ch = np.ascontiguousarray(np.concatenate([t[2] for t in trees]) if trees else np.zeros((1, 2)), np.int32)
+        ti = np.ascontiguousarray(np.concatenate([t[3] for t in trees]) if trees else np.zeros(1), np.int32)
+        self._parts += [tn, hp, off, ch, ti]
+        self._h = lib().orc_index_from_parts(_p(self.data), n, d, int(kind), int(correction), _p(self._parts[0]),
+                                             _p(self._parts[1]), float(min_distance), len(trees), _p(tn), _p(hp),
+                                             _p(off), _p(ch), _p(ti), int(leaf_budget), _p(self._parts[2]),
+                                             int(seed), int(n_threads))
+        return self
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -1801,6 +1801,47 @@ orc_index* orc_build(const float* data, int64_t n_, int32_t dim_, const orc_para
   return ix;
 }
 
+// A search-only index from another index's parts (test infrastructure: the GPU
+// search and this search on one shared graph and tree set).  Rows, CSR and
+// tree leaf orders are in the index's internal order; vertex_order maps
+// internal ids to original ids (index.rs:679-715); the trees' nodes are
+// concatenated (tree_nodes[t] nodes each) in FlatTree layout (flat_tree.rs:14-28).
+orc_index* orc_index_from_parts(const float* data, int64_t n_, int32_t dim_, int32_t kind, int32_t corr,
+                                const int32_t* indptr, const int32_t* indices, float min_distance, int32_t n_trees,
+                                const int64_t* tree_nodes, const float* hyperplanes, const float* offsets,
+                                const int32_t* children, const int32_t* tree_indices, int32_t leaf_budget,
+                                const int32_t* vertex_order, uint64_t seed, int32_t n_threads) {
+  const size_t n = (size_t)n_, dim = (size_t)dim_;
+  orc_index* ix = new orc_index();
+  ix->n = n;
+  ix->dim = dim;
+  ix->kind = kind;
+  ix->corr = corr;
+  ix->seed = seed;
+  ix->nt = num_threads_of(n_threads);
+  ix->leaf_budget = (size_t)std::max(1, leaf_budget);
+  ix->min_distance = min_distance;
+  ix->data.assign(data, data + n * dim);
+  ix->graph.n = n;
+  ix->graph.indptr.assign(indptr, indptr + n + 1);
+  ix->graph.indices.assign(indices, indices + (size_t)indptr[n]);
+  size_t node0 = 0;
+  for (int32_t t = 0; t < n_trees; ++t) {
+    FlatTree ft;
+    ft.dim = dim;
+    ft.n_nodes = (size_t)tree_nodes[t];
+    ft.hyperplanes.assign(hyperplanes + node0 * dim, hyperplanes + (node0 + ft.n_nodes) * dim);
+    ft.offsets.assign(offsets + node0, offsets + node0 + ft.n_nodes);
+    ft.children.assign(children + 2 * node0, children + 2 * (node0 + ft.n_nodes));
+    ft.indices.assign(tree_indices + (size_t)t * n, tree_indices + (size_t)(t + 1) * n);
+    ix->trees.push_back(std::move(ft));
+    node0 += (size_t)tree_nodes[t];
+  }
+  ix->vertex_order.resize(n);
+  for (size_t i = 0; i < n; ++i) ix->vertex_order[i] = (size_t)vertex_order[i];
+  return ix;
+}
+
 void orc_free(orc_index* idx) { delete idx; }
 int32_t orc_index_k(const orc_index* idx) { return (int32_t)idx->k; }
 int32_t orc_iterations(const orc_index* idx) { return idx->iters; }

@@ -144,6 +144,11 @@ int64_t orc_weighted_union_pruned(int32_t n, const int32_t* fwd_ptr, const int32
 /* ---- full index ---------------------------------------------------------- */
 void orc_params_default(orc_params* p);
 orc_index* orc_build(const float* data, int64_t n, int32_t dim, const orc_params* p);
+orc_index* orc_index_from_parts(const float* data, int64_t n, int32_t dim, int32_t kind, int32_t corr,
+                                const int32_t* indptr, const int32_t* indices, float min_distance, int32_t n_trees,
+                                const int64_t* tree_nodes, const float* hyperplanes, const float* offsets,
+                                const int32_t* children, const int32_t* tree_indices, int32_t leaf_budget,
+                                const int32_t* vertex_order, uint64_t seed, int32_t n_threads);
 void orc_free(orc_index* idx);
 int32_t orc_index_k(const orc_index* idx);
 void orc_neighbor_graph(const orc_index* idx, int32_t* out_idx, float* out_dist);

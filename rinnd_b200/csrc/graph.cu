@@ -42,7 +42,61 @@ __device__ __forceinline__ bool prune_draw(const PruneDraw& pd, int row, int32_t
   return (float)(h >> 40) * 5.9604644775390625e-08f < pd.prob;  // (h >> 40) / 2^24
 }
 
+// exact_distance with the metric fixed at compile time (KIND >= 0) or chosen
+// at run time (KIND < 0): the fixed form carries only its metric's code, so the
+// kernels hold fewer registers and keep more warps resident.
+template <int KIND>
+__device__ __forceinline__ float pair_distance(int kind, const float* a, const float* b, int n) {
+  if constexpr (KIND == DK_SQEUCLIDEAN) return exact_sqeuclid(a, b, n);
+  else return exact_distance(kind, a, b, n);
+}
+
+// Squared Euclidean distances of the row pairs (a0, b0), (a0, b1), (a1, b0),
+// (a1, b1), each with exact_sqeuclid's arithmetic (the same chains, packed
+// pairs, horizontal sum and remainder); the four pairs share their chunk loads.
+__device__ __forceinline__ void exact_sqeuclid_2x2(const float* a0, const float* a1, const float* b0,
+                                                   const float* b1, int n, float* out) {
+  unsigned long long p[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int t = 0; t < 4; ++t) p[u][t] = 0ull;
+  const int chunks = n >> 3;
+  for (int c = 0; c < chunks; ++c) {
+    unsigned long long x0[4], x1[4], y0[4], y1[4];
+    load8p(a0 + 8 * c, x0);
+    load8p(a1 + 8 * c, x1);
+    load8p(b0 + 8 * c, y0);
+    load8p(b1 + 8 * c, y1);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      unsigned long long d = pk_sub(x0[t], y0[t]);
+      p[0][t] = pk_fma(d, d, p[0][t]);
+      d = pk_sub(x0[t], y1[t]);
+      p[1][t] = pk_fma(d, d, p[1][t]);
+      d = pk_sub(x1[t], y0[t]);
+      p[2][t] = pk_fma(d, d, p[2][t]);
+      d = pk_sub(x1[t], y1[t]);
+      p[3][t] = pk_fma(d, d, p[3][t]);
+    }
+  }
+  const float* A[4] = {a0, a0, a1, a1};
+  const float* B[4] = {b0, b1, b0, b1};
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    float s[8];
+    unpack8(p[u], s);
+    float r = hsum_a(s);
+    for (int i = chunks * 8; i < n; ++i) {
+      const float d = __fsub_rn(A[u][i], B[u][i]);
+      r = __fadd_rn(r, __fmul_rn(d, d));
+    }
+    out[u] = r;
+  }
+}
+
 // Warp-cooperative RNG-style prune step: does any retained c (in smem) prune j?
+template <int KIND>
 __device__ __forceinline__ bool pruned_by_retained(const int32_t* ret_id, const float* ret_d, int nret,
                                                    int32_t j, float dij, const float* X, int D,
                                                    int Dp, int kind, const PruneDraw& pd, int row) {
@@ -53,7 +107,7 @@ __device__ __forceinline__ bool pruned_by_retained(const int32_t* ret_id, const 
     if (r < nret) {
       float dic = ret_d[r];
       if (dic > FLT_MIN) {
-        float dcj = exact_distance(kind, X + (size_t)ret_id[r] * Dp, X + (size_t)j * Dp, D);
+        float dcj = pair_distance<KIND>(kind, X + (size_t)ret_id[r] * Dp, X + (size_t)j * Dp, D);
         pr = dcj < dij && prune_draw(pd, row, j, ret_id[r]);
       }
     }
@@ -62,7 +116,7 @@ __device__ __forceinline__ bool pruned_by_retained(const int32_t* ret_id, const 
   return false;
 }
 
-template <int MAXR>
+template <int MAXR, int KIND>
 __global__ void k_diversify_fwd(const int32_t* knn_idx, const float* knn_dist, int N, int k,
                                 const float* X, int D, int Dp, int kind, int max_degree,
                                 int32_t* fwd_idx, float* fwd_dist, int32_t* fwd_cnt,
@@ -78,7 +132,7 @@ __global__ void k_diversify_fwd(const int32_t* knn_idx, const float* knn_dist, i
     int32_t j = knn_idx[(size_t)row * k + pos];
     if (j < 0) break;
     float dij = knn_dist[(size_t)row * k + pos];
-    bool pruned = pruned_by_retained(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind, pd, row);
+    bool pruned = pruned_by_retained<KIND>(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind, pd, row);
     if (!pruned) {
       if (lane == 0) {
         s_id[w][nret] = j;
@@ -137,6 +191,7 @@ __device__ __forceinline__ StagedWarp staged_warp(unsigned char* smem, int w, in
 }
 
 // The n candidates (cid/dpos filled, synchronized) -> sw.ret[0, nret); returns nret.
+template <int KIND>
 __device__ __forceinline__ int staged_prune(const StagedWarp& sw, int n, const float* X, int D, int Dp, int kind,
                                             int max_degree, const PruneDraw& pd, int row) {
   const int lane = threadIdx.x & 31, rs = Dp + 4, q4 = Dp / 4;
@@ -149,14 +204,36 @@ __device__ __forceinline__ int staged_prune(const StagedWarp& sw, int n, const f
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
   __syncwarp();
-  // pairs a < b < n in the order (b, then a): pair e is (e - b(b-1)/2, b) with
-  // b = floor((1 + sqrt(1 + 8e)) / 2), so no lane idles on a >= b
-  for (int e = lane; e < n * (n - 1) / 2; e += 32) {
-    int b = (int)((1.0f + sqrtf((float)(8 * e + 1))) * 0.5f);
-    if (b * (b - 1) / 2 > e) --b;
-    else if ((b + 1) * b / 2 <= e) ++b;
-    const int a = e - b * (b - 1) / 2;
-    sw.M[a * SK + b] = exact_distance(kind, sw.rows + (size_t)a * rs, sw.rows + (size_t)b * rs, D);
+  if constexpr (KIND == DK_SQEUCLIDEAN) {
+    // 2 x 2 blocks of pairs: rows (2p, 2p + 1) x (2q, 2q + 1), p <= q, block e
+    // = (p, q) with q = floor((sqrt(1 + 8e) - 1) / 2); rows past n repeat row
+    // n - 1 and pairs with a >= b or b >= n are not stored
+    const int h = (n + 1) >> 1;
+    for (int e = lane; e < h * (h + 1) / 2; e += 32) {
+      int q = (int)((sqrtf((float)(8 * e + 1)) - 1.0f) * 0.5f);
+      if (q * (q + 1) / 2 > e) --q;
+      else if ((q + 1) * (q + 2) / 2 <= e) ++q;
+      const int p = e - q * (q + 1) / 2;
+      const int a0 = 2 * p, a1 = min(2 * p + 1, n - 1), b0 = 2 * q, b1 = min(2 * q + 1, n - 1);
+      float d4[4];
+      exact_sqeuclid_2x2(sw.rows + (size_t)a0 * rs, sw.rows + (size_t)a1 * rs, sw.rows + (size_t)b0 * rs,
+                         sw.rows + (size_t)b1 * rs, D, d4);
+      const int as[4] = {2 * p, 2 * p, 2 * p + 1, 2 * p + 1};
+      const int bs[4] = {2 * q, 2 * q + 1, 2 * q, 2 * q + 1};
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (as[u] < bs[u] && bs[u] < n) sw.M[as[u] * SK + bs[u]] = d4[u];
+    }
+  } else {
+    // pairs a < b < n in the order (b, then a): pair e is (e - b(b-1)/2, b) with
+    // b = floor((1 + sqrt(1 + 8e)) / 2), so no lane idles on a >= b
+    for (int e = lane; e < n * (n - 1) / 2; e += 32) {
+      int b = (int)((1.0f + sqrtf((float)(8 * e + 1))) * 0.5f);
+      if (b * (b - 1) / 2 > e) --b;
+      else if ((b + 1) * b / 2 <= e) ++b;
+      const int a = e - b * (b - 1) / 2;
+      sw.M[a * SK + b] = exact_distance(kind, sw.rows + (size_t)a * rs, sw.rows + (size_t)b * rs, D);
+    }
   }
   __syncwarp();
   int nret = 0;
@@ -178,6 +255,7 @@ __device__ __forceinline__ int staged_prune(const StagedWarp& sw, int n, const f
   return nret;
 }
 
+template <int KIND>
 __global__ void __launch_bounds__(32 * WARPS)
     k_diversify_fwd_staged(const int32_t* knn_idx, const float* knn_dist, int N, int k, const float* X, int D,
                            int Dp, int kind, int max_degree, int32_t* fwd_idx, float* fwd_dist, int32_t* fwd_cnt,
@@ -199,7 +277,7 @@ __global__ void __launch_bounds__(32 * WARPS)
   sw.dpos[lane] = my_d;
   sw.cid[lane] = my_id;
   __syncwarp();
-  const int nret = staged_prune(sw, n, X, D, Dp, kind, max_degree, pd, row);
+  const int nret = staged_prune<KIND>(sw, n, X, D, Dp, kind, max_degree, pd, row);
   uint32_t local_min = KEY_INF;
   for (int r = lane; r < nret; r += 32) {
     const int pos = sw.ret[r];
@@ -239,7 +317,7 @@ __global__ void k_transpose(const int32_t* fwd_idx, const float* fwd_dist, const
   }
 }
 
-template <int MAXR>
+template <int MAXR, int KIND>
 __global__ void k_diversify_rev(const int32_t* rev_ptr, const uint64_t* rev_key, int N,
                                 const float* X, int D, int Dp, int kind, int max_degree,
                                 int32_t* rret_idx, float* rret_dist, int32_t* rret_cnt, PruneDraw pd) {
@@ -253,7 +331,7 @@ __global__ void k_diversify_rev(const int32_t* rev_ptr, const uint64_t* rev_key,
     uint64_t key = rev_key[e];
     int32_t j = (int32_t)(uint32_t)key;
     float dij = fkey_inv((uint32_t)(key >> 32));
-    bool pruned = pruned_by_retained(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind, pd, row);
+    bool pruned = pruned_by_retained<KIND>(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind, pd, row);
     if (!pruned) {
       if (lane == 0) {
         s_id[w][nret] = j;
@@ -413,19 +491,18 @@ void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const flo
   DVec<uint32_t> min_key(1, st);
   RINND_CUDA(cudaMemcpyAsync(min_key.p, &KEY_INF, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   const size_t staged_bytes = StagedSmem::per_warp(Dp) * WARPS;
+  const bool sq = kind == DK_SQEUCLIDEAN;
   if (k <= SK && Dp <= 256) {
-    set_smem_limit_once(reinterpret_cast<const void*>(k_diversify_fwd_staged), 227 * 1024);
-    k_diversify_fwd_staged<<<blocks, 32 * WARPS, staged_bytes, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind,
-                                                                    max_degree, fwd_idx.p, fwd_dist.p, fwd_cnt.p,
-                                                                    min_key.p, pd_fwd);
-  } else if (k <= 32)
-    k_diversify_fwd<32><<<blocks, 32 * WARPS, 0, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind,
-                                                      max_degree, fwd_idx.p, fwd_dist.p, fwd_cnt.p,
-                                                      min_key.p, pd_fwd);
-  else
-    k_diversify_fwd<128><<<blocks, 32 * WARPS, 0, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind,
-                                                       max_degree, fwd_idx.p, fwd_dist.p, fwd_cnt.p,
-                                                       min_key.p, pd_fwd);
+    auto kern = sq ? k_diversify_fwd_staged<DK_SQEUCLIDEAN> : k_diversify_fwd_staged<-1>;
+    set_smem_limit_once(reinterpret_cast<const void*>(kern), 227 * 1024);
+    kern<<<blocks, 32 * WARPS, staged_bytes, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind, max_degree, fwd_idx.p,
+                                                   fwd_dist.p, fwd_cnt.p, min_key.p, pd_fwd);
+  } else {
+    auto kern = k <= 32 ? (sq ? k_diversify_fwd<32, DK_SQEUCLIDEAN> : k_diversify_fwd<32, -1>)
+                        : (sq ? k_diversify_fwd<128, DK_SQEUCLIDEAN> : k_diversify_fwd<128, -1>);
+    kern<<<blocks, 32 * WARPS, 0, st>>>(knn_idx, knn_dist, N, k, X, D, Dp, kind, max_degree, fwd_idx.p,
+                                        fwd_dist.p, fwd_cnt.p, min_key.p, pd_fwd);
+  }
   RINND_LAUNCH_CHECK();
   // transpose
   DVec<int32_t> indeg((size_t)N + 1, st), rev_ptr((size_t)N + 1, st), cursor((size_t)N + 1, st);
@@ -454,12 +531,13 @@ void build_search_graph(const int32_t* knn_idx, const float* knn_dist, const flo
   DVec<float> rret_dist((size_t)N * max_degree, st);
   // (reverse rows stay sequential: they are short, and the early exits of the
   // sequential form beat the staged pair table there)
-  if (max_degree <= 32)
-    k_diversify_rev<32><<<blocks, 32 * WARPS, 0, st>>>(rev_ptr.p, rev_sorted.p, N, X, D, Dp, kind,
-                                                      max_degree, rret_idx.p, rret_dist.p, rret_cnt.p, pd_rev);
-  else
-    k_diversify_rev<384><<<blocks, 32 * WARPS, 0, st>>>(rev_ptr.p, rev_sorted.p, N, X, D, Dp, kind,
-                                                       max_degree, rret_idx.p, rret_dist.p, rret_cnt.p, pd_rev);
+  {
+    auto kern = max_degree <= 32 ? (sq ? k_diversify_rev<32, DK_SQEUCLIDEAN> : k_diversify_rev<32, -1>)
+                : max_degree <= 64 ? (sq ? k_diversify_rev<64, DK_SQEUCLIDEAN> : k_diversify_rev<64, -1>)
+                                   : (sq ? k_diversify_rev<384, DK_SQEUCLIDEAN> : k_diversify_rev<384, -1>);
+    kern<<<blocks, 32 * WARPS, 0, st>>>(rev_ptr.p, rev_sorted.p, N, X, D, Dp, kind, max_degree, rret_idx.p,
+                                        rret_dist.p, rret_cnt.p, pd_rev);
+  }
   RINND_LAUNCH_CHECK();
   // union + prune
   DVec<int32_t> rows((size_t)N * max_degree, st), cnt((size_t)N + 1, st);

@@ -109,10 +109,13 @@ def gpu_search_graph(knn_idx, knn_dist, data, kind, mult=1.5):
 
 @pytest.mark.parametrize("kind,gen,k,d", [(0, "gmm", 15, 24), (0, "uniform", 15, 24), (3, "gmm", 15, 24),
                                          (7, "uniform", 15, 24), (1, "gmm", 15, 24), (0, "gmm", 30, 128),
-                                         (3, "gmm", 30, 300), (0, "gmm", 40, 64)])
+                                         (3, "gmm", 30, 300), (0, "gmm", 40, 64), (0, "gmm", 31, 37),
+                                         (0, "uniform", 32, 100)])
 def test_search_graph_identical_on_shared_input(rb, orc, kind, gen, k, d):
     """from_dense_diversified on the same sorted kNN graph gives the same CSR
-    (the staged and the sequential forward-diversify kernels both covered)."""
+    (the staged and the sequential forward-diversify kernels both covered, and
+    the staged kernel's 2 x 2 blocked squared-Euclidean pairs with an odd
+    candidate count and a dimension that is not a multiple of 8)."""
     data = gmm(3000, d, 30, seed=5) if gen == "gmm" else uniform(3000, d, seed=5)
     if kind == 7:
         data = np.abs(data) + np.float32(0.01)

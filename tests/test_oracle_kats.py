@@ -193,3 +193,28 @@ def test_tree_hyperplane_known_answers(orc):
     children = np.array([[1, 2], [0, -1], [-1, -2]], np.int32)
     pts = np.array([[0.0, 5.0], [3.0, -1.0], [1.0, 0.0]], np.float32)
     assert orc.tree_route_points(hyperplanes, offsets, children, pts).tolist() == [1, 2, -1]
+
+
+def test_oracle_index_from_parts_searches_like_the_built_index(orc):
+    """OracleIndex.from_parts over an oracle index's own exported graph and
+    vertex order (no search trees) answers queries exactly as that index."""
+    import numpy as np
+
+    rng = np.random.default_rng(5)
+    X = rng.normal(size=(3000, 16)).astype(np.float32)
+    Q = rng.normal(size=(60, 16)).astype(np.float32)
+    ix = orc.OracleIndex(X, n_neighbors=10, n_trees=3, n_search_trees=0, distance_kind=0,
+                         correction=orc.CORR_NONE, random_seed=9)
+    indptr, indices, md = ix.search_graph
+    vo = ix.vertex_order.astype(np.int64)
+    inv = np.empty_like(vo)
+    inv[vo] = np.arange(len(vo))
+    counts = np.diff(indptr)[vo]
+    iptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    iidx = np.concatenate([inv[indices[indptr[o]:indptr[o + 1]]] for o in vo]).astype(np.int32)
+    part = orc.OracleIndex.from_parts(X[vo], kind=0, correction=orc.CORR_NONE, indptr=iptr, indices=iidx,
+                                      min_distance=md, vertex_order=vo, seed=9)
+    a_i, a_d = ix.query(Q, k=8, epsilon=0.1)
+    b_i, b_d = part.query(Q, k=8, epsilon=0.1)
+    assert np.array_equal(a_i, b_i)
+    assert np.array_equal(a_d.view(np.uint32), b_d.view(np.uint32))
