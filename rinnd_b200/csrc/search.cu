@@ -57,11 +57,55 @@ __device__ __forceinline__ uint64_t rkey(float d, int32_t id) {
   return ((uint64_t)fkey(d) << 32) | (uint32_t)id;
 }
 
-struct QRng {  // counter-based per-query stream (seed + query id, as index.rs:165)
-  uint64_t base, ctr;
-  __device__ uint64_t next() { return mix64(base ^ mix64(++ctr)); }
-  __device__ bool next_bool() { return (next() >> 63) != 0; }
-  __device__ uint32_t next_index(uint32_t n) { return (uint32_t)(((next() >> 32) * (uint64_t)n) >> 32); }
+// The query's random stream: the reference's FastRng (core/rng.rs), i.e.
+// Xoshiro256++ (rand_xoshiro 0.6.0) seeded through SplitMix64 by
+// seed_from_u64, with rand 0.8.5's samplers: a bool is the sign bit of a
+// u32 draw (next_u32 = high word of next_u64), and gen_range(0..n) is the
+// widening-multiply draw with rejection of the low word above the zone
+// (range << lz) - 1.  Seeded with seed + query id (index.rs:165).  Every lane
+// of the warp advances the same state, so draws are warp-uniform.
+struct QRng {
+  uint64_t s0, s1, s2, s3;
+  __device__ explicit QRng(uint64_t seed) {
+    uint64_t x = seed;
+    uint64_t st[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      x += 0x9e3779b97f4a7c15ull;
+      uint64_t z = x;
+      z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+      z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+      st[i] = z ^ (z >> 31);
+    }
+    s0 = st[0];
+    s1 = st[1];
+    s2 = st[2];
+    s3 = st[3];
+  }
+  __device__ static uint64_t rotl(uint64_t v, int k) { return (v << k) | (v >> (64 - k)); }
+  __device__ uint64_t next() {
+    const uint64_t r = rotl(s0 + s3, 23) + s0;
+    const uint64_t t = s1 << 17;
+    s2 ^= s0;
+    s3 ^= s1;
+    s1 ^= s2;
+    s0 ^= s3;
+    s2 ^= t;
+    s3 = rotl(s3, 45);
+    return r;
+  }
+  __device__ bool next_bool() { return (int32_t)(uint32_t)(next() >> 32) < 0; }
+  __device__ uint32_t next_index(uint32_t n) {
+    const uint64_t range = n;
+    const uint64_t zone = (range << __clzll((long long)range)) - 1;
+    uint64_t hi = 0;
+    for (int attempt = 0; attempt < 64; ++attempt) {  // a draw is rejected with probability < 1/2
+      const uint64_t v = next();
+      hi = __umul64hi(v, range);
+      if (v * range <= zone) break;
+    }
+    return (uint32_t)hi;
+  }
 };
 
 // Visited set (VisitedSet::check_and_mark): returns true if id was already
@@ -381,7 +425,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
     for (int t = lane; t < vcap; t += 32) vis[t] = -1;
   }
   __syncwarp();
-  QRng rng{rng_seed, 0};
+  QRng rng(rng_seed);
   // seed-set capacity from this query's own width (not the batch's), so a
   // query's result does not depend on the queries it is batched with
   const int scap = X.seeds ? ix.N : seed_capacity(k);
@@ -618,7 +662,7 @@ __global__ void __launch_bounds__(WPB * 32)
   for (int qi = blockIdx.x * WPB + w; qi < nq; qi += gridDim.x * WPB) {
     const float* qf = Q + (size_t)qi * ix.Dp;
     const int8_t* q8 = qtrees ? Q8 + (size_t)qi * ix.Dq : nullptr;
-    QRng rng{ix.seed + (qtrees ? 0ull : qid_base + (uint64_t)qi), 0};
+    QRng rng(ix.seed + (qtrees ? 0ull : qid_base + (uint64_t)qi));
     const float tqs = qtrees ? tree_query_scale(qf, ix.D) : 0.f;
     int n = 0;
     int32_t* o = out + (size_t)qi * budget * 2;

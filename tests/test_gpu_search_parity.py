@@ -8,9 +8,11 @@ leaves with the same per-query random streams, so every query must return the
 same neighbors with bit-identical distances -- for queries from the indexed
 distribution and for queries far from every point, whose searches expand many
 nodes (the GPU's bounded seed set and visited table overflow on those, and the
-exact re-run must reproduce the unbounded search).  Exact distance ties, whose
-order the reference's BinaryHeap leaves to its internal layout, do not occur
-for these continuous inputs.
+exact re-run must reproduce the unbounded search).  The random fill of seeds
+and the random side of tied tree margins draw from the reference's FastRng
+stream (Xoshiro256++ seeded with seed + query id) on both sides.  Exact
+distance ties, whose order the reference's BinaryHeap leaves to its internal
+layout, do not occur for these continuous inputs.
 """
 import numpy as np
 import pytest

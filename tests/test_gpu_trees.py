@@ -40,12 +40,14 @@ def test_spill_leaves_match_oracle(rb, orc, metric, d):
 
 def test_spill_seeding_search_recall(rb, orc):
     """A larger leaf budget seeds more points per tree: recall@10 does not drop,
-    and at each budget the GPU search is within 0.5 point of the oracle's (the
-    reference's default epsilon 0.1; at epsilon 0 both searches stop at the
-    first local minimum and their recall is dominated by the graphs' random
-    structure rather than by the seeding)."""
+    and at each budget the GPU build + search is within 0.5 point of the
+    oracle's build + search (the reference's default epsilon 0.1) for queries
+    from the indexed distribution.  (Queries far from every cluster are routed
+    to a cluster by the first tree splits alone, so their recall is a property
+    of two random trees rather than of the seeding; the shared-index search
+    parity test covers them exactly.)"""
     X = gmm(30000, 32, 80, seed=33)
-    Q = gmm(2000, 32, 80, seed=34)
+    Q = gmm(32000, 32, 80, seed=33)[30000:]
     truth = orc.exact_knn_f64(0, X, Q, 10)[0]
     rec, orec = {}, {}
     for budget in (1, 4):
@@ -92,7 +94,7 @@ def test_int8_routing_trees_search(rb, orc):
     oracle's search over its own int8 routing trees, and the FP32 rows are
     released by default (no exact rerank, rinnd lib.rs:712-716)."""
     X = gmm(20000, 64, 50, seed=37)
-    Q = gmm(2000, 64, 50, seed=38)
+    Q = gmm(22000, 64, 50, seed=37)[20000:]  # the indexed distribution
     ix = rb.RINND(X, metric="cosine", normalize=True, cosine_distance_mode="int8", tree_quantization="int8",
                   n_neighbors=15, random_state=3, search_tree_leaf_budget=2)
     Xn, Qn = orc.normalize_rows(X), orc.normalize_rows(Q)

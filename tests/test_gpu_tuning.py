@@ -5,9 +5,13 @@ per CTA, candidate rows per work item, CTAs per SM); a shape changes how the
 pairs of a vertex are scheduled, never which pairs are evaluated, their
 arithmetic or the pushes.  So one NN-Descent iteration (candidate sampling +
 local join + heap pushes, core/nndescent/mod.rs:101-155, :321-491) from the
-same rows must give bit-identical rows with every shape.  The tuner times the
-shapes on a sample of the first iteration and restores the heaps it touched:
-a build that tunes reaches the recall of one that does not.
+same rows must give the same rows with every shape: bit-identical distances,
+and the same ids except where a row's last distance is tied (the push rejects
+d >= the row's max as the reference does, so which of two equally distant
+candidates keeps the last slot follows arrival order, for any one shape run
+twice as well).  The tuner times the shapes on a sample of the first iteration
+and restores the heaps it touched: a build that tunes reaches the recall of
+one that does not.
 """
 import ctypes
 
@@ -40,6 +44,19 @@ def table():
     return [tuple(rows[8 * i: 8 * i + 8]) for i in range(n.value)]
 
 
+def assert_same_rows_up_to_last_ties(ref, got, shape):
+    (ri, rd, rf), (gi, gd, gf) = ref, got
+    np.testing.assert_array_equal(rd.view(np.uint32), gd.view(np.uint32), err_msg=str(shape))
+    last = rd[:, -1:]
+    free = rd == last  # entries tied with the row's last distance
+    assert np.array_equal(np.where(free, 0, ri), np.where(free, 0, gi)), shape
+    assert np.array_equal(np.where(free, 0, rf), np.where(free, 0, gf)), shape
+    # tied entries differ only where the tie reaches the row's last slot
+    tie_rows = np.nonzero(~np.all(ri == gi, axis=1))[0]
+    assert np.all(free[tie_rows].sum(axis=1) >= 1)
+    assert len(tie_rows) <= 0.01 * len(ri), (shape, len(tie_rows))
+
+
 @pytest.mark.parametrize("kind,d", [(SQEUCLIDEAN, 64), (SQEUCLIDEAN, 32), (ALT_COSINE, 96)])
 def test_every_tile_shape_gives_the_same_iteration(rb, orc, kind, d):
     from rinnd_b200 import _lib as L
@@ -59,8 +76,7 @@ def test_every_tile_shape_gives_the_same_iteration(rb, orc, kind, d):
         if ref is None:
             ref = got
             continue
-        for a, b in zip(ref, got):
-            assert np.array_equal(a, b), shape
+        assert_same_rows_up_to_last_ties(ref, got, shape)
     L.check(L.lib.rinnd_join_tile_table_clear())
 
 
