@@ -119,11 +119,9 @@ struct Bars {
 template <int MAXC, bool GROUPED, int NSTAGE, int JB>
 __global__ void __launch_bounds__(NT, 3)
     k_join_ws(const int32_t* __restrict__ desc, int v0, int v1, const float* __restrict__ X, int Dp, int kind,
-              uint64_t* slots, uint32_t* thr, int k, int kp, Layout Lin, uint32_t* urow_buf, uint64_t* ukey_buf,
+              uint64_t* slots, uint32_t* thr, int k, int kp, Layout L, uint32_t* urow_buf, uint64_t* ukey_buf,
               unsigned long long* ucount, uint32_t* rcnt, unsigned int rsize, unsigned long long* counters,
               int* err, ItemCount ic) {
-  Layout L = Lin;
-  L.ns = NSTAGE;  // (the launch passes the same; a constant folds the offsets)
   extern __shared__ __align__(16) unsigned char smem[];
   Bars B{reinterpret_cast<uint64_t*>(smem), reinterpret_cast<uint64_t*>(smem) + NSTAGE,
          reinterpret_cast<uint64_t*>(smem) + 2 * NSTAGE,
@@ -133,8 +131,10 @@ __global__ void __launch_bounds__(NT, 3)
   unsigned int* s_done = s_ucnt + 1;  // consumer warps finished
   uint32_t* urow_reg = urow_buf + (size_t)blockIdx.x * rsize;
   uint64_t* ukey_reg = ukey_buf + (size_t)blockIdx.x * rsize;
-  int32_t* dring = reinterpret_cast<int32_t*>(smem + L.desc_off());
-  unsigned char* stage0 = smem + L.stage_off();
+  // (offsets with the stage count as a constant; the launch's L.ns is NSTAGE)
+  constexpr size_t kDescOff = (8 * (2 * NSTAGE + NDESC) + 16 + 15) / 16 * 16;
+  int32_t* dring = reinterpret_cast<int32_t*>(smem + kDescOff);
+  unsigned char* stage0 = smem + kDescOff + (size_t)NDESC * L.dstride * 4;
   const size_t sbytes = L.stage_bytes();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
@@ -282,132 +282,237 @@ __global__ void __launch_bounds__(NT, 3)
     const float* snrm = reinterpret_cast<const float*>(sd + Desc::nrm(MAXC));
     const float* rows = reinterpret_cast<const float*>(st + L.rows_off());
     if (ct == 0) rows_total += (unsigned long long)nb;
-    for (int b0 = 0; b0 < items; b0 += 32 * NCONS) {
-      const int item = b0 + ct;
-      const bool active = item < items;
-      int iq = 0, j = 0;
-      unsigned long long acc[4 * JB];
-#pragma unroll
-      for (int p = 0; p < 4 * JB; ++p) acc[p] = 0ull;
-      if (active) {
-        for (int q = 1; q < nq; ++q) iq += (sd[4 + q] <= item);
-        j = 4 * iq + 1 + JB * (item - sd[4 + iq]);
-        // candidate rows j .. j + JB - 1 (a row past nb repeats row nb - 1; its results are discarded)
-        const ulonglong2* pb[JB];
-#pragma unroll
-        for (int v = 0; v < JB; ++v)
-          pb[v] = reinterpret_cast<const ulonglong2*>(rows + (size_t)min(j + v, nb - 1) * L.rs);
-        const ulonglong2* pa = reinterpret_cast<const ulonglong2*>(rows + (size_t)(4 * iq) * L.rs);
-        const int ars = L.rs / 4;
-        if (kind == DK_SQEUCLIDEAN) {
-#pragma unroll(JB == 1 ? 4 : 2)
-          for (int q = 0; q < Dp / 4; ++q) {
-            ulonglong2 b[JB];
-#pragma unroll
-            for (int v = 0; v < JB; ++v) b[v] = pb[v][q];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const ulonglong2 a = pa[u * ars + q];
-#pragma unroll
-              for (int v = 0; v < JB; ++v) {
-                const unsigned long long d01 = f2_sub(a.x, b[v].x), d23 = f2_sub(a.y, b[v].y);
-                acc[4 * v + u] = f2_fma(d01, d01, acc[4 * v + u]);
-                acc[4 * v + u] = f2_fma(d23, d23, acc[4 * v + u]);
+    if constexpr (JB == 1) {  // one candidate row per item
+      for (int b0 = 0; b0 < items; b0 += 32 * NCONS) {
+        const int item = b0 + ct;
+        const bool active = item < items;
+        int iq = 0, j = 0;
+        unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
+        if (active) {
+          for (int q = 1; q < nq; ++q) iq += (sd[4 + q] <= item);
+          j = 4 * iq + 1 + (item - sd[4 + iq]);
+          const ulonglong2* pb = reinterpret_cast<const ulonglong2*>(rows + (size_t)j * L.rs);
+          const ulonglong2* pa = reinterpret_cast<const ulonglong2*>(rows + (size_t)(4 * iq) * L.rs);
+          const int ars = L.rs / 4;
+          if (kind == DK_SQEUCLIDEAN) {
+  #pragma unroll 4
+            for (int q = 0; q < Dp / 4; ++q) {
+              const ulonglong2 b = pb[q];
+  #pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const ulonglong2 a = pa[u * ars + q];
+                const unsigned long long d01 = f2_sub(a.x, b.x), d23 = f2_sub(a.y, b.y);
+                acc[u] = f2_fma(d01, d01, acc[u]);
+                acc[u] = f2_fma(d23, d23, acc[u]);
               }
             }
-          }
-        } else if (kind == DK_MANHATTAN) {
-          const unsigned long long absmask = 0x7FFFFFFF7FFFFFFFull;
-#pragma unroll(JB == 1 ? 4 : 2)
-          for (int q = 0; q < Dp / 4; ++q) {
-            ulonglong2 b[JB];
-#pragma unroll
-            for (int v = 0; v < JB; ++v) b[v] = pb[v][q];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const ulonglong2 a = pa[u * ars + q];
-#pragma unroll
-              for (int v = 0; v < JB; ++v) {
-                acc[4 * v + u] = f2_add(acc[4 * v + u], f2_sub(a.x, b[v].x) & absmask);
-                acc[4 * v + u] = f2_add(acc[4 * v + u], f2_sub(a.y, b[v].y) & absmask);
+          } else if (kind == DK_MANHATTAN) {
+            const unsigned long long absmask = 0x7FFFFFFF7FFFFFFFull;
+  #pragma unroll 4
+            for (int q = 0; q < Dp / 4; ++q) {
+              const ulonglong2 b = pb[q];
+  #pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const ulonglong2 a = pa[u * ars + q];
+                acc[u] = f2_add(acc[u], f2_sub(a.x, b.x) & absmask);
+                acc[u] = f2_add(acc[u], f2_sub(a.y, b.y) & absmask);
               }
             }
-          }
-        } else {
-#pragma unroll(JB == 1 ? 4 : 2)
-          for (int q = 0; q < Dp / 4; ++q) {
-            ulonglong2 b[JB];
-#pragma unroll
-            for (int v = 0; v < JB; ++v) b[v] = pb[v][q];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const ulonglong2 a = pa[u * ars + q];
-#pragma unroll
-              for (int v = 0; v < JB; ++v) {
-                acc[4 * v + u] = f2_fma(a.x, b[v].x, acc[4 * v + u]);
-                acc[4 * v + u] = f2_fma(a.y, b[v].y, acc[4 * v + u]);
+          } else {
+  #pragma unroll 4
+            for (int q = 0; q < Dp / 4; ++q) {
+              const ulonglong2 b = pb[q];
+  #pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const ulonglong2 a = pa[u * ars + q];
+                acc[u] = f2_fma(a.x, b.x, acc[u]);
+                acc[u] = f2_fma(a.y, b.y, acc[u]);
               }
             }
           }
         }
-      }
-      // validity and thresholds -> emit bits (bit p = 4 v + u: push into A row; 16 + p: into B row)
-      uint32_t kd[4 * JB];
-      unsigned emit = 0;
-      int n_emit = 0;
-#pragma unroll
-      for (int v = 0; v < JB; ++v) {
-        const int jv = j + v;
-        const bool have = active && jv < nb;
-        const int32_t bid = have ? ids[jv] : -1;
-        const uint32_t bthr = have ? sthr[jv] : 0u;
-#pragma unroll
+        // validity and thresholds -> emit bits (u: push into A row; 4+u: into B row)
+        uint32_t kd[4];
+        unsigned emit = 0;
+        int n_emit = 0;
+        const int32_t bid = active ? ids[j] : -1;
+        const uint32_t bthr = active ? sthr[j] : 0u;
+  #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const int p = 4 * v + u;
-          kd[p] = 0;
+          kd[u] = 0;
           const int ia = 4 * iq + u;
-          if (have && ia < na) {
-            const bool valid = (jv < na) ? (jv > ia) : (bid != ids[ia]);  // mod.rs:396, :424
+          if (active && ia < na) {
+            const bool valid = (j < na) ? (j > ia) : (bid != ids[ia]);  // mod.rs:396, :424
             if (valid) {
               ++pairs_total;
-              float d = f2_sum(acc[p]);
-              if (is_dot) d = finalize_dot(kind, d, snrm[ia], snrm[jv]);
-              kd[p] = fkey(d);
-              if (kd[p] < sthr[ia]) { emit |= 1u << p; ++n_emit; }
-              if (kd[p] < bthr) { emit |= 0x10000u << p; ++n_emit; }
+              float d = f2_sum(acc[u]);
+              if (is_dot) d = finalize_dot(kind, d, snrm[ia], snrm[j]);
+              kd[u] = fkey(d);
+              if (kd[u] < sthr[ia]) { emit |= 1u << u; ++n_emit; }
+              if (kd[u] < bthr) { emit |= 16u << u; ++n_emit; }
+            }
+          }
+        }
+        int incl = n_emit;
+  #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        const int warp_total = __shfl_sync(0xffffffffu, incl, 31);
+        unsigned int base = 0;
+        if (lane == 0 && warp_total) base = atomicAdd(s_ucnt, (unsigned int)warp_total);
+        base = __shfl_sync(0xffffffffu, base, 0) + (unsigned int)(incl - n_emit);
+        if (emit) {
+  #pragma unroll
+          for (int u = 0; u < 4; ++u) {
+  #pragma unroll
+            for (int side = 0; side < 2; ++side) {
+              if (!(emit & ((side ? 16u : 1u) << u))) continue;
+              const int32_t aid = ids[4 * iq + u];
+              const int32_t row = side ? bid : aid;
+              const int32_t other = side ? aid : bid;
+              const uint64_t key = ((uint64_t)kd[u] << 32) | (uint32_t)other | 0x80000000u;
+              if (base < rsize) {
+                urow_reg[base] = (uint32_t)row;
+                ukey_reg[base] = key;
+              } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
+                atomicAdd(&counters[0], 1ull);
+                if constexpr (GROUPED) ic.add((uint32_t)row);
+              }
+              ++base;
             }
           }
         }
       }
-      int incl = n_emit;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      const int warp_total = __shfl_sync(0xffffffffu, incl, 31);
-      unsigned int base = 0;
-      if (lane == 0 && warp_total) base = atomicAdd(s_ucnt, (unsigned int)warp_total);
-      base = __shfl_sync(0xffffffffu, base, 0) + (unsigned int)(incl - n_emit);
-      if (emit) {
-#pragma unroll
-        for (int p = 0; p < 4 * JB; ++p) {
-#pragma unroll
-          for (int side = 0; side < 2; ++side) {
-            if (!(emit & ((side ? 0x10000u : 1u) << p))) continue;
-            const int32_t aid = ids[4 * iq + (p & 3)];
-            const int32_t bid = ids[j + (p >> 2)];
-            const int32_t row = side ? bid : aid;
-            const int32_t other = side ? aid : bid;
-            const uint64_t key = ((uint64_t)kd[p] << 32) | (uint32_t)other | 0x80000000u;
-            if (base < rsize) {
-              urow_reg[base] = (uint32_t)row;
-              ukey_reg[base] = key;
-            } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
-              atomicAdd(&counters[0], 1ull);
-              if constexpr (GROUPED) ic.add((uint32_t)row);
+    } else {  // JB candidate rows per item
+      for (int b0 = 0; b0 < items; b0 += 32 * NCONS) {
+        const int item = b0 + ct;
+        const bool active = item < items;
+        int iq = 0, j = 0;
+        unsigned long long acc[4 * JB];
+  #pragma unroll
+        for (int p = 0; p < 4 * JB; ++p) acc[p] = 0ull;
+        if (active) {
+          for (int q = 1; q < nq; ++q) iq += (sd[4 + q] <= item);
+          j = 4 * iq + 1 + JB * (item - sd[4 + iq]);
+          // candidate rows j .. j + JB - 1 (a row past nb repeats row nb - 1; its results are discarded)
+          const ulonglong2* pb[JB];
+  #pragma unroll
+          for (int v = 0; v < JB; ++v)
+            pb[v] = reinterpret_cast<const ulonglong2*>(rows + (size_t)min(j + v, nb - 1) * L.rs);
+          const ulonglong2* pa = reinterpret_cast<const ulonglong2*>(rows + (size_t)(4 * iq) * L.rs);
+          const int ars = L.rs / 4;
+          if (kind == DK_SQEUCLIDEAN) {
+  #pragma unroll(JB == 1 ? 4 : 2)
+            for (int q = 0; q < Dp / 4; ++q) {
+              ulonglong2 b[JB];
+  #pragma unroll
+              for (int v = 0; v < JB; ++v) b[v] = pb[v][q];
+  #pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const ulonglong2 a = pa[u * ars + q];
+  #pragma unroll
+                for (int v = 0; v < JB; ++v) {
+                  const unsigned long long d01 = f2_sub(a.x, b[v].x), d23 = f2_sub(a.y, b[v].y);
+                  acc[4 * v + u] = f2_fma(d01, d01, acc[4 * v + u]);
+                  acc[4 * v + u] = f2_fma(d23, d23, acc[4 * v + u]);
+                }
+              }
             }
-            ++base;
+          } else if (kind == DK_MANHATTAN) {
+            const unsigned long long absmask = 0x7FFFFFFF7FFFFFFFull;
+  #pragma unroll(JB == 1 ? 4 : 2)
+            for (int q = 0; q < Dp / 4; ++q) {
+              ulonglong2 b[JB];
+  #pragma unroll
+              for (int v = 0; v < JB; ++v) b[v] = pb[v][q];
+  #pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const ulonglong2 a = pa[u * ars + q];
+  #pragma unroll
+                for (int v = 0; v < JB; ++v) {
+                  acc[4 * v + u] = f2_add(acc[4 * v + u], f2_sub(a.x, b[v].x) & absmask);
+                  acc[4 * v + u] = f2_add(acc[4 * v + u], f2_sub(a.y, b[v].y) & absmask);
+                }
+              }
+            }
+          } else {
+  #pragma unroll(JB == 1 ? 4 : 2)
+            for (int q = 0; q < Dp / 4; ++q) {
+              ulonglong2 b[JB];
+  #pragma unroll
+              for (int v = 0; v < JB; ++v) b[v] = pb[v][q];
+  #pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const ulonglong2 a = pa[u * ars + q];
+  #pragma unroll
+                for (int v = 0; v < JB; ++v) {
+                  acc[4 * v + u] = f2_fma(a.x, b[v].x, acc[4 * v + u]);
+                  acc[4 * v + u] = f2_fma(a.y, b[v].y, acc[4 * v + u]);
+                }
+              }
+            }
+          }
+        }
+        // validity and thresholds -> emit bits (bit p = 4 v + u: push into A row; 16 + p: into B row)
+        uint32_t kd[4 * JB];
+        unsigned emit = 0;
+        int n_emit = 0;
+  #pragma unroll
+        for (int v = 0; v < JB; ++v) {
+          const int jv = j + v;
+          const bool have = active && jv < nb;
+          const int32_t bid = have ? ids[jv] : -1;
+          const uint32_t bthr = have ? sthr[jv] : 0u;
+  #pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int p = 4 * v + u;
+            kd[p] = 0;
+            const int ia = 4 * iq + u;
+            if (have && ia < na) {
+              const bool valid = (jv < na) ? (jv > ia) : (bid != ids[ia]);  // mod.rs:396, :424
+              if (valid) {
+                ++pairs_total;
+                float d = f2_sum(acc[p]);
+                if (is_dot) d = finalize_dot(kind, d, snrm[ia], snrm[jv]);
+                kd[p] = fkey(d);
+                if (kd[p] < sthr[ia]) { emit |= 1u << p; ++n_emit; }
+                if (kd[p] < bthr) { emit |= 0x10000u << p; ++n_emit; }
+              }
+            }
+          }
+        }
+        int incl = n_emit;
+  #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        const int warp_total = __shfl_sync(0xffffffffu, incl, 31);
+        unsigned int base = 0;
+        if (lane == 0 && warp_total) base = atomicAdd(s_ucnt, (unsigned int)warp_total);
+        base = __shfl_sync(0xffffffffu, base, 0) + (unsigned int)(incl - n_emit);
+        if (emit) {
+  #pragma unroll
+          for (int p = 0; p < 4 * JB; ++p) {
+  #pragma unroll
+            for (int side = 0; side < 2; ++side) {
+              if (!(emit & ((side ? 0x10000u : 1u) << p))) continue;
+              const int32_t aid = ids[4 * iq + (p & 3)];
+              const int32_t bid = ids[j + (p >> 2)];
+              const int32_t row = side ? bid : aid;
+              const int32_t other = side ? aid : bid;
+              const uint64_t key = ((uint64_t)kd[p] << 32) | (uint32_t)other | 0x80000000u;
+              if (base < rsize) {
+                urow_reg[base] = (uint32_t)row;
+                ukey_reg[base] = key;
+              } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
+                atomicAdd(&counters[0], 1ull);
+                if constexpr (GROUPED) ic.add((uint32_t)row);
+              }
+              ++base;
+            }
           }
         }
       }
