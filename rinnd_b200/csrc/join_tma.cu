@@ -116,8 +116,10 @@ struct Bars {
 };
 
 // GROUPED: rows of several indices (per-index accounting of direct pushes).
+// (No minimum-blocks bound: asking for 3 CTAs per SM gave the same 72
+// registers but a 20 % slower one-row tile on the 1M build.)
 template <int MAXC, bool GROUPED, int NSTAGE, int JB>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT)
     k_join_ws(const int32_t* __restrict__ desc, int v0, int v1, const float* __restrict__ X, int Dp, int kind,
               uint64_t* slots, uint32_t* thr, int k, int kp, Layout L, uint32_t* urow_buf, uint64_t* ukey_buf,
               unsigned long long* ucount, uint32_t* rcnt, unsigned int rsize, unsigned long long* counters,
