@@ -390,12 +390,17 @@ __device__ void tree_search_leaves(const SearchIndex& ix, int root, int budget, 
 // k: result-list width; k_out: entries written to oi/od; rerank (QUANT only):
 // number of leading results re-ordered by exact FP32 distance before output;
 // rng_seed: the query's random stream.
-// X (exact re-run, may be null): this warp's visited bitset (N bits) and seed
-// arrays (2 x N entries) in global memory, used instead of the bounded
-// shared-memory state.  Returns true when the bounded state overflowed.
+// X (re-runs; all null in the first pass): this warp's global-memory state
+// used instead of the shared-memory one -- the wide form (a larger bounded
+// visited table and seed arrays) or the exact form (a visited bitset of N bits
+// and seed arrays of N entries, which cannot overflow).  Returns true when a
+// bounded state overflowed.
 struct ExactState {
-  uint32_t* bits;
-  uint64_t* seeds;
+  uint32_t* bits;     // exact form: visited bitset of N bits
+  uint64_t* seeds;    // two seed arrays of seed_cap entries each
+  int seed_cap;
+  int32_t* vis;       // wide form: open-addressing visited table of vis_cap entries
+  int vis_cap;
 };
 template <bool QUANT>
 __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_t* Q8row,
@@ -406,7 +411,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   float* q = reinterpret_cast<float*>(wsm + L.q_off());
   uint64_t* res = reinterpret_cast<uint64_t*>(wsm + L.res_off());
   uint64_t* seeds = X.seeds ? X.seeds : reinterpret_cast<uint64_t*>(wsm + L.seed_off());
-  const int sstride = X.seeds ? ix.N : L.s;  // seed arrays: entries apart, and capacity
+  const int sstride = X.seeds ? X.seed_cap : L.s;  // seed arrays: entries apart
   int32_t* vis = reinterpret_cast<int32_t*>(wsm + L.vis_off());
   uint64_t* bbuf = reinterpret_cast<uint64_t*>(wsm + L.batch_off());
   int8_t* q8 = reinterpret_cast<int8_t*>(q);  // QUANT: codes stored in the query slot
@@ -416,8 +421,9 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   } else {
     for (int t = lane; t < ix.Dp; t += 32) q[t] = t < ix.D ? Qrow[t] : 0.f;
   }
-  const int vcap = visited_capacity(k);
+  const int vcap = X.vis ? X.vis_cap : visited_capacity(k);
   if (gvis) vis = gvis;  // global-memory table of this warp
+  if (X.vis) vis = X.vis;
   Visited V{vis, vcap, X.bits, false};
   if (X.bits) {
     for (int t = lane; t < (ix.N + 31) / 32; t += 32) X.bits[t] = 0u;
@@ -428,7 +434,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   QRng rng(rng_seed);
   // seed-set capacity from this query's own width (not the batch's), so a
   // query's result does not depend on the queries it is batched with
-  const int scap = X.seeds ? ix.N : seed_capacity(k);
+  const int scap = X.seeds ? X.seed_cap : seed_capacity(k);
   bool lost = false;  // bounded state overflowed (warp-uniform)
   int rc = 0, cur = 0, head = 0, tail = 0;
   unsigned long long evals = 0, expansions = 0;
@@ -594,38 +600,51 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   return __any_sync(0xffffffffu, lost || V.lost);
 }
 
-// Queries a bounded search could not finish exactly: the first launch appends
-// their indices (count, list); the exact launch re-runs the listed queries with
-// per-warp global-memory state (xbits: words_per_warp words; xseeds: 2 N
-// entries per warp).
+// Queries a bounded search could not finish: a launch appends their indices to
+// (count_out, list_out), and the next launch re-runs the queries of
+// (count_in, list_in) with per-warp global-memory state: the wide pass a
+// visited table of vis_cap entries and seed arrays of seed_cap entries, the
+// exact pass a bitset of N bits (words_per_warp words) and seed arrays of N.
 struct Redo {
-  unsigned int* count;
-  int32_t* list;
+  const unsigned int* count_in;
+  const int32_t* list_in;
+  unsigned int* count_out;
+  int32_t* list_out;
   uint32_t* xbits;
   uint64_t* xseeds;
+  int32_t* xvis;
   long long words_per_warp;
+  int seed_cap, vis_cap;
 };
+enum SearchPass { PASS_BOUNDED = 0, PASS_WIDE = 1, PASS_EXACT = 2 };
 
 template <bool QUANT>
 __global__ void __launch_bounds__(WPB * 32)
     k_search(SearchIndex ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k, int k_out,
              int rerank, float eps, uint64_t qid_base, QueryMeta meta, WarpLayout L, int32_t* gvis, int gcap,
-             int32_t* out_idx, float* out_dist, unsigned long long* stats, Redo redo, bool exact) {
+             int32_t* out_idx, float* out_dist, unsigned long long* stats, Redo redo, int pass) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   unsigned char* wsm = smem + (size_t)w * L.bytes();
-  const long long gw = (long long)blockIdx.x * WPB + w;
+  const int wpb = blockDim.x >> 5;  // warps per block (the re-runs launch one-warp blocks)
+  const long long gw = (long long)blockIdx.x * wpb + w;
   int32_t* my_gvis = gvis ? gvis + (size_t)gw * gcap : nullptr;
-  ExactState X{nullptr, nullptr};
-  if (exact) {
+  ExactState X{nullptr, nullptr, 0, nullptr, 0};
+  if (pass == PASS_WIDE) {
+    X.seeds = redo.xseeds + (size_t)gw * 2 * redo.seed_cap;
+    X.seed_cap = redo.seed_cap;
+    X.vis = redo.xvis + (size_t)gw * redo.vis_cap;
+    X.vis_cap = redo.vis_cap;
+  } else if (pass == PASS_EXACT) {
     X.bits = redo.xbits + (size_t)gw * redo.words_per_warp;
     X.seeds = redo.xseeds + (size_t)gw * 2 * ix.N;
+    X.seed_cap = ix.N;
   }
-  const int total_warps = gridDim.x * WPB;
-  const int n_run = exact ? (int)min((unsigned int)nq, *redo.count) : nq;
-  for (int t = blockIdx.x * WPB + w; t < n_run; t += total_warps) {
-    const int qi = exact ? redo.list[t] : t;
+  const int total_warps = gridDim.x * wpb;
+  const int n_run = pass == PASS_BOUNDED ? nq : (int)min((unsigned int)nq, *redo.count_in);
+  for (int t = (int)gw; t < n_run; t += total_warps) {
+    const int qi = pass == PASS_BOUNDED ? t : redo.list_in[t];
     int qk = k, qko = k_out, qr = rerank;
     float qe = eps;
     // FP32 queries seed with seed + query index (index.rs:165); quantized
@@ -643,7 +662,7 @@ __global__ void __launch_bounds__(WPB * 32)
     const bool lost = search_one<QUANT>(ix, Q + (size_t)qi * ix.Dp, QUANT ? Q8 + (size_t)qi * ix.Dq : nullptr,
                                         QUANT ? qinv[qi] : 0.f, ix.seed + stream, qk, qko, qr, qe, L, wsm, my_gvis, X,
                                         out_idx + off, out_dist + off, stats);
-    if (lost && !exact && lane == 0) redo.list[atomicAdd(redo.count, 1u)] = qi;
+    if (lost && pass != PASS_EXACT && lane == 0) redo.list_out[atomicAdd(redo.count_out, 1u)] = qi;
   }
 }
 
@@ -707,41 +726,51 @@ struct GlobalVisited {
   int32_t* p() const { return buf.p; }
 };
 
-// Per-warp global-memory state of the exact re-run: a visited bitset of N bits
-// and two seed arrays of N entries each; as many warps as fit EXACT_BYTES (at
-// least one, at most EXACT_MAX_WARPS).
+// Per-warp global-memory state of the re-runs.  Wide pass: a visited table of
+// WIDE_VIS entries and seed arrays of WIDE_SEEDS entries (512 KB per warp).
+// Exact pass: a visited bitset of N bits and two seed arrays of N entries; as
+// many warps as fit EXACT_BYTES (at least one, at most EXACT_MAX_WARPS).
+constexpr int WIDE_VIS = 1 << 16;
+constexpr int WIDE_SEEDS = 1 << 14;
+constexpr int WIDE_MAX_WARPS = 256;
 constexpr size_t EXACT_BYTES = 256ull << 20;
 constexpr int EXACT_MAX_WARPS = 128;
 
-// The bounded launch over all queries, then the exact launch over the queries
-// it recorded (their outputs are overwritten).  Both are enqueued on `st`; the
-// exact launch finds the recorded count on the device.
+// The bounded launch over all queries; the wide launch over the queries it
+// recorded; the exact launch over the queries the wide launch recorded (their
+// outputs are overwritten).  All are enqueued on `st`; each re-run finds its
+// query count on the device.
 template <bool QUANT>
 void run_search(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k, int k_out,
                 int rerank, float eps, uint64_t qid_base, const QueryMeta& meta, const WarpLayout& L,
                 int32_t* out_idx, float* out_dist, cudaStream_t st, unsigned long long* dstats) {
   const int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
   GlobalVisited gv(L, blocks, st);
-  DVec<unsigned int> count(1, st);
-  count.fill_bytes(0);
-  DVec<int32_t> list((size_t)nq, st);
-  Redo redo{count.p, list.p, nullptr, nullptr, 0};
+  DVec<unsigned int> counts(2, st);
+  counts.fill_bytes(0);
+  DVec<int32_t> list1((size_t)nq, st), list2((size_t)nq, st);
+  Redo redo{nullptr, nullptr, counts.p, list1.p, nullptr, nullptr, nullptr, 0, 0, 0};
   k_search<QUANT><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base,
                                                              meta, L, gv.p(), gv.cap, out_idx, out_dist, dstats, redo,
-                                                             false);
+                                                             PASS_BOUNDED);
   RINND_LAUNCH_CHECK();
+  // wide re-run (one-warp blocks, as many as queries up to WIDE_MAX_WARPS)
+  const int wwarps = std::min(WIDE_MAX_WARPS, nq);
+  DVec<int32_t> wvis((size_t)wwarps * WIDE_VIS, st);
+  DVec<uint64_t> wseeds((size_t)wwarps * 2 * WIDE_SEEDS, st);
+  Redo wide{counts.p, list1.p, counts.p + 1, list2.p, nullptr, wseeds.p, wvis.p, 0, WIDE_SEEDS, WIDE_VIS};
+  k_search<QUANT><<<wwarps, 32, L.bytes(), st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base, meta, L,
+                                                 nullptr, 0, out_idx, out_dist, dstats, wide, PASS_WIDE);
+  RINND_LAUNCH_CHECK();
+  // exact re-run
   const long long words = ((long long)(ix.N + 31) / 32 + 3) / 4 * 4;  // 16-byte multiple per warp
   const size_t per_warp = (size_t)words * 4 + (size_t)2 * ix.N * 8;
-  const int warps = (int)std::max<size_t>(1, std::min<size_t>(EXACT_BYTES / per_warp, EXACT_MAX_WARPS));
-  const int xblocks = (std::min(warps, nq) + WPB - 1) / WPB;
-  DVec<uint32_t> xbits((size_t)xblocks * WPB * words, st);
-  DVec<uint64_t> xseeds((size_t)xblocks * WPB * 2 * ix.N, st);
-  redo.xbits = xbits.p;
-  redo.xseeds = xseeds.p;
-  redo.words_per_warp = words;
-  k_search<QUANT><<<xblocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base,
-                                                              meta, L, nullptr, 0, out_idx, out_dist, dstats, redo,
-                                                              true);
+  const int xwarps = std::min(nq, (int)std::max<size_t>(1, std::min<size_t>(EXACT_BYTES / per_warp, EXACT_MAX_WARPS)));
+  DVec<uint32_t> xbits((size_t)xwarps * words, st);
+  DVec<uint64_t> xseeds((size_t)xwarps * 2 * ix.N, st);
+  Redo exact{counts.p + 1, list2.p, nullptr, nullptr, xbits.p, xseeds.p, nullptr, words, ix.N, 0};
+  k_search<QUANT><<<xwarps, 32, L.bytes(), st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base, meta, L,
+                                                 nullptr, 0, out_idx, out_dist, dstats, exact, PASS_EXACT);
   RINND_LAUNCH_CHECK();
 }
 

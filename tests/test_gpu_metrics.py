@@ -86,6 +86,17 @@ def test_generic_build_recall_matches_oracle(rb, orc, name):
     oix = orc.OracleIndex(X, n_neighbors=k, distance_kind=kind, correction=orc.CORR_NONE,
                           angular=name in ("correlation", "true_angular", "tsss"), random_seed=4)
     oi, _ = oix.neighbor_graph
-    assert recall(gi[rows], truth) >= recall(oi[rows], truth) - 0.005
+    # tie-aware recall: a found neighbor counts when its distance is within the
+    # k-th smallest (binary metrics such as jaccard have many exactly tied
+    # distances, so which tied ids a build keeps is arrival order)
+    kth = np.sort(dist, axis=1)[:, k - 1:k]
+
+    def tie_recall(found):
+        f = found[rows]
+        d = np.take_along_axis(dist, np.where(f >= 0, f, 0), axis=1)
+        return float(np.mean((f >= 0) & (d <= kth)))
+
+    assert tie_recall(gi) >= tie_recall(oi) - 0.005, (tie_recall(gi), tie_recall(oi))
+    assert recall(gi[rows], truth) >= recall(oi[rows], truth) - 0.02
     ids, _ = ix.query(X[:200], k=5)
     assert (ids[:, 0] >= 0).all()
