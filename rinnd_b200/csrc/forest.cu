@@ -153,50 +153,6 @@ __global__ void k_margins(const int32_t* seg_of, const int32_t* inv, int N, int 
   }
 }
 
-// k_margins for a sparse level (few points still in active segments): one
-// warp per active segment walks the segment's positions four at a time (8
-// lanes per position), so finished points cost nothing.  Same margin
-// arithmetic and tie draw as k_margins, bit for bit; positions outside active
-// segments keep side 0 (is_left is cleared before the launch).
-__global__ void k_margins_sparse(const long long* seg_gstart, const long long* seg_gend, int S, const int32_t* perm,
-                                 int N, const float* X, int D, int Dp, const float* hp, const float* off,
-                                 uint64_t seed, int depth, int32_t* is_left) {
-  const int lane = threadIdx.x & 31, grp = lane >> 3, t8 = lane & 7;
-  const int warp = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-  const int nwarps = (int)(((long long)gridDim.x * blockDim.x) >> 5);
-  const int chunks = D >> 3;
-  for (int sg = warp; sg < S; sg += nwarps) {
-    const long long g0 = seg_gstart[sg], g1 = seg_gend[sg];
-    const float* h = hp + (size_t)sg * Dp;
-    const int t = (int)(g0 / N);
-    for (long long gb = g0; gb < g1; gb += 4) {
-      const long long g = gb + grp;
-      const bool have = g < g1;
-      const int32_t pid = have ? perm[g] : 0;
-      const float* x = X + (size_t)pid * Dp;
-      float acc = 0.f;
-      if (have)
-        for (int c = 0; c < chunks; ++c) acc = __fmaf_rn(x[8 * c + t8], h[8 * c + t8], acc);
-      const float up4 = __shfl_down_sync(0xffffffffu, acc, 4, 8);
-      const float a = __fadd_rn(up4, acc);
-      const float up1 = __shfl_down_sync(0xffffffffu, a, 1, 8);
-      const float b = __fadd_rn(a, up1);
-      const float up2 = __shfl_down_sync(0xffffffffu, b, 2, 8);
-      if (t8 == 0 && have) {
-        float r = __fadd_rn(b, up2);
-        for (int i = chunks * 8; i < D; ++i) r = __fadd_rn(r, __fmul_rn(x[i], h[i]));
-        const float margin = __fadd_rn(r, off[sg]);
-        int left;
-        if (fabsf(margin) < 1e-8f)
-          left = (int)(hash3(seed ^ 0x7a11u, ((uint64_t)t << 32) | (uint32_t)depth, (uint64_t)pid) >> 63);
-        else
-          left = margin < 0.f;
-        is_left[g] = left;
-      }
-    }
-  }
-}
-
 __global__ void k_scatter(const int32_t* seg_of, const long long* seg_gstart,
                           const long long* seg_gend, const int32_t* scan, const int32_t* is_left,
                           const int32_t* perm, int32_t* perm_next, int32_t* inv, int N, long long total) {
@@ -223,11 +179,9 @@ __global__ void k_seg_bounds(const Seg* segs, int S, int N, long long* gs, long 
   ge[s] = (long long)g.tree * N + g.end;
 }
 
-// Also adds the next level's active positions (the continuing children's
-// sizes) to *next_active.
 __global__ void k_outcome(const Seg* segs, int S, const long long* gs, const int32_t* scan,
                           int leaf_size, int depth, int max_depth, int32_t* nleft, int32_t* n_next,
-                          int32_t* n_node, unsigned long long* next_active) {
+                          int32_t* n_node) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S) return;
   Seg g = segs[s];
@@ -238,10 +192,6 @@ __global__ void k_outcome(const Seg* segs, int S, const long long* gs, const int
   auto cont = [&](int sz) { return (sz > leaf_size && depth + 1 < max_depth) ? 1 : 0; };
   n_next[s] = ok ? cont(nl) + cont(size - nl) : 0;
   n_node[s] = ok ? 2 : 0;
-  if (ok) {
-    const unsigned long long act = (unsigned long long)(cont(nl) * nl + cont(size - nl) * (size - nl));
-    if (act) atomicAdd(next_active, act);
-  }
 }
 
 __device__ __forceinline__ void emit_leaf(int tree, int start, int end, int node, int32_t* children,
@@ -348,7 +298,7 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
   f.n_nodes = (int64_t)n_roots;
   size_t leaf_cap = std::max<size_t>(n_roots * 64, 64);
   f.leaves.alloc(leaf_cap, st);
-  DVec<unsigned long long> counters(3, st);  // [0] n_leaves, [1] max leaf size, [2] next level's active positions
+  DVec<unsigned long long> counters(2, st);  // [0] n_leaves, [1] max leaf size
   counters.fill_bytes(0);
 
   std::vector<Seg> h_roots;
@@ -374,9 +324,7 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
   DVec<int32_t> is_left((size_t)total + 1, st), scan((size_t)total + 1, st);
   DVec<int32_t> seg_of((size_t)total, st);
   RINND_CUDA(cudaMemsetAsync(is_left.p + total, 0, sizeof(int32_t), st));
-  unsigned long long h_counters[3] = {0, 0, 0};
-  long long active = 0;  // positions in active segments this level
-  for (const Seg& g : h_roots) active += g.end - g.start;
+  unsigned long long h_counters[2] = {0, 0};
   int depth = 0;
   while (S > 0) {
     DVec<long long> gs((size_t)S, st), ge((size_t)S, st);
@@ -389,14 +337,8 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
     RINND_CUDA(cudaMemsetAsync(seg_of.p, 0xFF, sizeof(int32_t) * (size_t)total, st));
     k_fill_segmap<<<std::min(S, 148 * 16), 256, 0, st>>>(gs.p, ge.p, S, seg_of.p);
     RINND_LAUNCH_CHECK();
-    if (active * 4 < total) {  // sparse level: only the active segments' positions
-      RINND_CUDA(cudaMemsetAsync(is_left.p, 0, sizeof(int32_t) * (size_t)total, st));
-      k_margins_sparse<<<grid_for((long long)S * 32, 256, 148 * 32), 256, 0, st>>>(
-          gs.p, ge.p, S, f.perm.p, N, X, D, Dp, hp.p, off.p, seed, depth, is_left.p);
-    } else {
-      k_margins<<<grid_for((long long)N * 32, 256, 148 * 32), 256, 0, st>>>(seg_of.p, inv.p, N, T, X, D, Dp, hp.p,
-                                                                           off.p, seed, depth, is_left.p);
-    }
+    k_margins<<<grid_for((long long)N * 32, 256, 148 * 32), 256, 0, st>>>(seg_of.p, inv.p, N, T, X, D, Dp, hp.p,
+                                                                         off.p, seed, depth, is_left.p);
     RINND_LAUNCH_CHECK();
     exclusive_scan(is_left.p, scan.p, total + 1, tmp, st);
     RINND_CUDA(cudaMemcpyAsync(perm_next.p, f.perm.p, sizeof(int32_t) * (size_t)total,
@@ -411,9 +353,8 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
     DVec<int32_t> next_off((size_t)S + 1, st), node_off((size_t)S + 1, st);
     RINND_CUDA(cudaMemsetAsync(n_next.p + S, 0, sizeof(int32_t), st));
     RINND_CUDA(cudaMemsetAsync(n_node.p + S, 0, sizeof(int32_t), st));
-    RINND_CUDA(cudaMemsetAsync(counters.p + 2, 0, sizeof(unsigned long long), st));
     k_outcome<<<grid_for(S, 256), 256, 0, st>>>(segs.p, S, gs.p, scan.p, leaf_size, depth,
-                                                max_depth, nleft.p, n_next.p, n_node.p, counters.p + 2);
+                                                max_depth, nleft.p, n_next.p, n_node.p);
     RINND_LAUNCH_CHECK();
     exclusive_scan(n_next.p, next_off.p, (long long)S + 1, tmp, st);
     exclusive_scan(n_node.p, node_off.p, (long long)S + 1, tmp, st);
@@ -445,7 +386,6 @@ void build_forest(const float* X, int N, int D, int Dp, int T, int leaf_size, bo
     f.n_nodes += new_nodes;
     segs = std::move(next);
     S = S_next;
-    active = (long long)h_counters[2];
     ++depth;
   }
   RINND_CUDA(cudaMemcpyAsync(h_counters, counters.p, sizeof(h_counters), cudaMemcpyDeviceToHost, st));

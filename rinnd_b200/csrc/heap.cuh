@@ -120,25 +120,6 @@ __device__ __forceinline__ int row_push_small(uint64_t* row, int k, uint32_t* th
   return 0;
 }
 
-// Largest fkey (high word) of the k valid slots: the reject test of a push
-// (d >= the row's max, neighbor_heap.rs:156) needs only this, so a push that
-// fails it skips the duplicate scan and the 64-bit max tracking.
-__device__ __forceinline__ uint32_t row_max_fkey(const uint64_t* row, int k) {
-  const uint4* r4 = reinterpret_cast<const uint4*>(row);  // (lo, hi) word pairs
-  uint32_t mx = 0;
-  for (int j0 = 0; j0 < k; j0 += ROW_ALIGN) {
-    uint4 v[ROW_ALIGN / 2];
-#pragma unroll
-    for (int t = 0; t < ROW_ALIGN / 2; ++t) v[t] = __ldcg(r4 + j0 / 2 + t);
-#pragma unroll
-    for (int t = 0; t < ROW_ALIGN / 2; ++t) {
-      if (j0 + 2 * t < k) mx = max(mx, v[t].y);
-      if (j0 + 2 * t + 1 < k) mx = max(mx, v[t].w);
-    }
-  }
-  return mx;
-}
-
 // Returns 1 if inserted.  `key` = (fkey(v) << 32) | lo, lo's low 31 bits = id.
 // `thr` (may be null) holds an upper bound of fkey(row max value).  This form
 // scans the row in 16-slot chunks and keeps few registers: kernels whose push
@@ -147,13 +128,6 @@ __device__ __forceinline__ int row_push(uint64_t* row, int k, uint32_t* thr, uin
                                         unsigned long long* contention) {
   const uint32_t vk = (uint32_t)(key >> 32);
   if (thr != nullptr && vk >= __ldcg(thr)) return 0;
-  {  // cheap reject on the high words first (most buffered updates end here)
-    const uint32_t mx = row_max_fkey(row, k);
-    if (vk >= mx) {
-      if (thr != nullptr) atomicMin(thr, mx);
-      return 0;
-    }
-  }
   const uint32_t id = ((uint32_t)key) & 0x7FFFFFFFu;
   for (int attempt = 0; attempt < PUSH_MAX_RETRY; ++attempt) {
     RowScan s = scan_row(row, k, id);
