@@ -152,6 +152,32 @@ __device__ __forceinline__ int row_push(uint64_t* row, int k, uint32_t* thr, uin
   return 0;
 }
 
+// row_push with the reject test (d >= the row's max, neighbor_heap.rs:156) on
+// the rows' high words first: the join kernels' rare direct pushes (a full
+// update-buffer region) use it.
+__device__ __forceinline__ int row_push_hi_first(uint64_t* row, int k, uint32_t* thr, uint64_t key,
+                                                 unsigned long long* contention) {
+  const uint32_t vk = (uint32_t)(key >> 32);
+  if (thr != nullptr && vk >= __ldcg(thr)) return 0;
+  const uint4* r4 = reinterpret_cast<const uint4*>(row);  // (lo, hi) word pairs
+  uint32_t mx = 0;
+  for (int j0 = 0; j0 < k; j0 += ROW_ALIGN) {
+    uint4 v[ROW_ALIGN / 2];
+#pragma unroll
+    for (int t = 0; t < ROW_ALIGN / 2; ++t) v[t] = __ldcg(r4 + j0 / 2 + t);
+#pragma unroll
+    for (int t = 0; t < ROW_ALIGN / 2; ++t) {
+      if (j0 + 2 * t < k) mx = max(mx, v[t].y);
+      if (j0 + 2 * t + 1 < k) mx = max(mx, v[t].w);
+    }
+  }
+  if (vk >= mx) {
+    if (thr != nullptr) atomicMin(thr, mx);
+    return 0;
+  }
+  return row_push(row, k, thr, key, contention);
+}
+
 // The push of the reverse candidate offers: rows of up to 32 slots take the
 // register-snapshot form (faster there; in the update-application kernel its
 // registers cost more occupancy than the shorter scan saves).

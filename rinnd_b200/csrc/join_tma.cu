@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(NT)
               if (base < rsize) {
                 urow_reg[base] = (uint32_t)row;
                 ukey_reg[base] = key;
-              } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
+              } else if (row_push_hi_first(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
                 atomicAdd(&counters[0], 1ull);
                 if constexpr (GROUPED) ic.add((uint32_t)row);
               }
@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(NT)
               if (base < rsize) {
                 urow_reg[base] = (uint32_t)row;
                 ukey_reg[base] = key;
-              } else if (row_push(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
+              } else if (row_push_hi_first(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
                 atomicAdd(&counters[0], 1ull);
                 if constexpr (GROUPED) ic.add((uint32_t)row);
               }
