@@ -22,11 +22,14 @@
 // (distance, id)), the seed set as a sorted array merged warp-parallel with each
 // batch of accepted neighbors, and an open-addressing visited table.  Both are
 // bounded (S seeds, a fixed table), while the reference's seed heap and visited
-// bitset are not: a query whose search would exceed either (a seed dropped, or
-// an id the table cannot place within 32 probes) is recorded, and a second
-// launch re-runs exactly those queries from scratch with per-warp global-memory
-// state sized to the index (a visited bitset of N bits and seed arrays of N
-// entries), so every query's result is the one of the unbounded search.
+// bitset are not.  Dropping the farthest seeds changes nothing unless the
+// unbounded search would pop one of them (it ranks before a seed that is popped
+// while still within the bound, or the seeds run out while it is); such a
+// query, or one with an id the table cannot place within 32 probes, is
+// recorded and re-run from scratch, first with a wider bounded state in global
+// memory and, if that overflows too, with state sized to the index (a visited
+// bitset of N bits and seed arrays of N entries), so every query's result is
+// the one of the unbounded search.
 // Neighbor and tie order follow (distance, id); the reference's BinaryHeap
 // orders exact distance ties by its internal layout.
 #include "dist.cuh"
@@ -44,7 +47,7 @@ struct WarpLayout {
   __host__ __device__ size_t res_off() const { return (size_t)dp * 4; }
   __host__ __device__ size_t seed_off() const { return res_off() + (size_t)kmax * 8; }
   __host__ __device__ size_t batch_off() const { return seed_off() + (size_t)2 * s * 8; }
-  __host__ __device__ size_t vis_off() const { return batch_off() + 32 * 8; }
+  __host__ __device__ size_t vis_off() const { return batch_off() + 34 * 8; }  // batch + smallest dropped seed
   __host__ __device__ size_t fr_off() const { return vis_off() + (size_t)h * 4; }
   __host__ __device__ size_t bytes() const { return fr_off() + (size_t)f * 8; }
 };
@@ -244,13 +247,14 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
 
 // Merge the sorted batch (one key per lane, ascending, ~0 = none; nb valid) into
 // the sorted seed array A[head, tail) -> C[0, min(na + nb, S)); the two arrays
-// are `stride` entries apart (stride >= S).  Dropping seeds beyond S marks the
-// search as lost (warp-uniform).
+// are `stride` entries apart (stride >= S).  Entries merged beyond S are
+// dropped; min_drop (warp-uniform) keeps the smallest dropped key, which the
+// traversal compares with the seeds it pops and its final bound.
 __device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int stride, int S, int& cur,
-                                            int& head, int& tail, uint64_t bkey, int nb, bool& lost) {
+                                            int& head, int& tail, uint64_t bkey, int nb, uint64_t& min_drop) {
   const int lane = threadIdx.x & 31;
   if (nb == 0) return;
-  if (tail - head + nb > S) lost = true;
+  const bool drops = tail - head + nb > S;
   bbuf[lane] = bkey;
   __syncwarp();
   const uint64_t* A = seeds + (size_t)cur * stride;
@@ -265,6 +269,7 @@ __device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int
     }
     int o = i + lo;
     if (o < S) C[o] = a;
+    else if (o == S) bbuf[32] = a;  // the smallest dropped entry
   }
   if (lane < nb) {  // out = j + #(a <= b)
     uint64_t b = bkey;
@@ -275,8 +280,10 @@ __device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int
     }
     int o = lane + lo;
     if (o < S) C[o] = b;
+    else if (o == S) bbuf[32] = b;
   }
   __syncwarp();
+  if (drops) min_drop = min(min_drop, bbuf[32]);
   cur ^= 1;
   head = 0;
   tail = min(na + nb, S);
@@ -435,7 +442,11 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   // seed-set capacity from this query's own width (not the batch's), so a
   // query's result does not depend on the queries it is batched with
   const int scap = X.seeds ? X.seed_cap : seed_capacity(k);
-  bool lost = false;  // bounded state overflowed (warp-uniform)
+  // Dropped seeds change the result only if the unbounded search would pop
+  // one: when a popped seed ranks after the smallest dropped one while that
+  // one is still within the bound, or the seeds run out while it is.
+  uint64_t min_drop = ~0ull;
+  bool lost = false;  // the bounded state may have changed the result (warp-uniform)
   int rc = 0, cur = 0, head = 0, tail = 0;
   unsigned long long evals = 0, expansions = 0;
   unsigned long long* overflow = &stats[2];
@@ -462,7 +473,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
       result_push(res, rc, k, dj, ij);
     }
     uint64_t sorted = warp_sort32(bkey);
-    seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(m), lost);
+    seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(m), min_drop);
   };
 
   // ---- tree seeding (greedy.rs:70-146): the points of the leaves each tree's
@@ -515,18 +526,25 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
         result_push(res, rc, k, __shfl_sync(0xffffffffu, d, j), __shfl_sync(0xffffffffu, id, j));
       }
       uint64_t sorted = warp_sort32(fresh ? rkey(d, id) : ~0ull);
-      seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(m), lost);
+      seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(m), min_drop);
     }
   }
   // ---- traverse (greedy.rs:165-201) ----
   float mx = result_max(res, rc);
   float bound = bound_of(mx);
+  bool stopped = false;
   while (head < tail) {
     uint64_t top = seeds[(size_t)cur * sstride + head];
     ++head;
     float vd = fkey_inv((uint32_t)(top >> 32));
     int32_t v = (int32_t)(uint32_t)top;
-    if (rc >= k && vd >= bound) break;
+    if (top > min_drop) {  // the unbounded search reaches the dropped seed first
+      if (!(rc >= k && fkey_inv((uint32_t)(min_drop >> 32)) >= bound)) lost = true;
+    }
+    if (rc >= k && vd >= bound) {
+      stopped = true;
+      break;
+    }
     // With an exact visited set every node is expanded at most once; the cap
     // only matters after a visited-table overflow, where it bounds the loop.
     if (expansions >= (unsigned long long)ix.N + 64) break;
@@ -556,9 +574,12 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
       }
       bool acc = (acc_mask >> lane) & 1u;
       uint64_t sorted = warp_sort32(acc ? rkey(d, nb) : ~0ull);
-      seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(acc_mask), lost);
+      seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(acc_mask), min_drop);
     }
   }
+  // seeds ran out: the unbounded search would go on with a dropped seed
+  // within the bound
+  if (!stopped && min_drop != ~0ull && !(rc >= k && fkey_inv((uint32_t)(min_drop >> 32)) >= bound)) lost = true;
   // ---- exact rerank of the first `rerank` results (index.rs:103-126): exact
   // FP32 distance to the FP32 query, sorted by (distance, id) ----
   int nres = rc;

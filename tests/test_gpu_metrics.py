@@ -96,7 +96,8 @@ def test_generic_build_recall_matches_oracle(rb, orc, name):
         d = np.take_along_axis(dist, np.where(f >= 0, f, 0), axis=1)
         return float(np.mean((f >= 0) & (d <= kth)))
 
-    assert tie_recall(gi) >= tie_recall(oi) - 0.005, (tie_recall(gi), tie_recall(oi))
+    assert tie_recall(gi) >= tie_recall(oi) - 0.005, (tie_recall(gi), tie_recall(oi), ix.build_info["iterations"],
+                                                      oix.iterations, ix.build_info["pushes_accepted"])
     assert recall(gi[rows], truth) >= recall(oi[rows], truth) - 0.02
     ids, _ = ix.query(X[:200], k=5)
     assert (ids[:, 0] >= 0).all()
