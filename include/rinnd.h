@@ -379,6 +379,12 @@ RINND_EXPORT int rinnd_server_destroy(rinnd_server* s);
  * their table had no free slot within the probe limit).  reset != 0 zeroes them. */
 RINND_EXPORT int rinnd_search_stats_get(rinnd_index* idx, uint64_t* evaluations, uint64_t* expansions,
                                         uint64_t* visited_overflows, int32_t reset);
+/* All search counters since the last reset (8 words): evaluations, expansions,
+ * visited-table overflows, spill-frontier overflows, queries re-run with the
+ * wide bounded state, queries re-run with the exact state, 0, 0.  A query is
+ * re-run when its bounded shared-memory state could have changed its result
+ * (see rinnd_query); the re-run's result is the one returned. */
+RINND_EXPORT int rinnd_search_counters(rinnd_index* idx, uint64_t* out, int32_t reset);
 
 /* ---- storage info (crates/rinnd/src/lib.rs:1028-1077) ---------------------- */
 typedef struct rinnd_storage_info {

@@ -378,11 +378,13 @@ class RINND:
         return [[(int(s), int(e)) for s, e in out[i, :cnt[i]]] for i in range(n)]
 
     def search_stats(self, reset=False) -> dict:
-        """Distance evaluations, node expansions and visited-table overflows of
-        the searches since the build (or the last reset)."""
-        v = [ctypes.c_uint64(0) for _ in range(3)]
-        L.check(L.lib.rinnd_search_stats_get(self._h, *(ctypes.byref(x) for x in v), int(bool(reset))))
-        return {"evaluations": v[0].value, "expansions": v[1].value, "visited_overflows": v[2].value}
+        """Distance evaluations, node expansions, visited-table and spill-frontier
+        overflows, and the queries re-run with the wide and with the exact state,
+        of the searches since the build (or the last reset)."""
+        v = (ctypes.c_uint64 * 8)()
+        L.check(L.lib.rinnd_search_counters(self._h, v, int(bool(reset))))
+        return {"evaluations": v[0], "expansions": v[1], "visited_overflows": v[2], "frontier_overflows": v[3],
+                "wide_reruns": v[4], "exact_reruns": v[5]}
 
     @property
     def build_info(self) -> dict:

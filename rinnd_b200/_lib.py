@@ -104,6 +104,7 @@ SIGNATURES = {
     "rinnd_join_tile_table": (ctypes.c_int, [_P, _i32, _P]),
     "rinnd_join_tile_table_clear": (ctypes.c_int, []),
     "rinnd_join_tile_set": (ctypes.c_int, [_P]),
+    "rinnd_search_counters": (ctypes.c_int, [_P, _P, _i32]),
     "rinnd_build_info_get": (ctypes.c_int, [_P, _P]),
     "rinnd_index_shape": (ctypes.c_int, [_P, _P, _P, _P]),
     "rinnd_query": (ctypes.c_int, [_P, _P, _i64, _i32, _f32, _P, _P]),

@@ -344,7 +344,7 @@ void finish_index(rinnd_index* ix, const float* X0, DVec<int32_t>&& knn_idx, DVe
   }
   ix->forest.perm.release();
   ix->forest.leaves.release();
-  ix->search_stats.alloc(4, st);
+  ix->search_stats.alloc(8, st);
   ix->search_stats.fill_bytes(0);
   RINND_CUDA(cudaStreamSynchronize(st));
 }
@@ -1106,6 +1106,19 @@ int rinnd_join_tile_set(const int32_t* row) {
   });
 }
 
+int rinnd_search_counters(rinnd_index* idx, uint64_t* out, int32_t reset) {
+  return guarded([&] {
+    check_index(idx);
+    require(out != nullptr, "out must not be null");
+    RINND_CUDA(cudaSetDevice(idx->device));
+    unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    RINND_CUDA(cudaDeviceSynchronize());
+    RINND_CUDA(cudaMemcpy(h, idx->search_stats.p, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 8; ++i) out[i] = h[i];
+    if (reset) RINND_CUDA(cudaMemset(idx->search_stats.p, 0, sizeof(h)));
+  });
+}
+
 int rinnd_search_stats_get(rinnd_index* idx, uint64_t* evaluations, uint64_t* expansions,
                            uint64_t* visited_overflows, int32_t reset) {
   return guarded([&] {
@@ -1117,7 +1130,7 @@ int rinnd_search_stats_get(rinnd_index* idx, uint64_t* evaluations, uint64_t* ex
     if (evaluations) *evaluations = h[0];
     if (expansions) *expansions = h[1];
     if (visited_overflows) *visited_overflows = h[2];
-    if (reset) RINND_CUDA(cudaMemset(idx->search_stats.p, 0, sizeof(h)));
+    if (reset) RINND_CUDA(cudaMemset(idx->search_stats.p, 0, 8 * sizeof(unsigned long long)));
   });
 }
 
@@ -1923,7 +1936,7 @@ int rinnd_load(const char* path, int32_t device, rinnd_index** out, char* meta, 
     ix->forest.Dp = h.Dp;
     ix->inverse.alloc(N, st);
     invert_permutation(ix->vertex_order.p, (int)N, ix->inverse.p, st);
-    ix->search_stats.alloc(4, st);
+    ix->search_stats.alloc(8, st);
     ix->search_stats.fill_bytes(0);
     RINND_CUDA(cudaStreamSynchronize(st));
     if (meta_len) *meta_len = (int64_t)m.size();

@@ -28,8 +28,14 @@ constexpr int ROW_ALIGN = 16;  // slots per 128-byte line group
 
 __host__ __device__ __forceinline__ int row_stride(int k) { return (k + ROW_ALIGN - 1) / ROW_ALIGN * ROW_ALIGN; }
 
+// The order a push evicts by: distance, then id -- the new/old flag (bit 31)
+// takes no part, so among equally distant entries a new one is not evicted
+// before an old one (which would starve the next candidate samples on data
+// with many tied distances).
+constexpr uint64_t EVICT_MASK = ~(1ull << 31);
+
 struct RowScan {
-  uint64_t vmax;  // largest key (lowest index among equal keys)
+  uint64_t vmax;  // the slot value to evict: largest (distance, id), lowest index among equal
   uint64_t v2;    // largest key among the other slots
   int m;
   bool dup;
@@ -52,7 +58,7 @@ __device__ __forceinline__ RowScan scan_row(const uint64_t* row, int k, uint32_t
       if (j < k) {
         uint64_t x = (t & 1) ? v[t >> 1].y : v[t >> 1].x;
         r.dup |= (((uint32_t)x) & 0x7FFFFFFFu) == id;
-        if (first || x > r.vmax) {
+        if (first || (x & EVICT_MASK) > (r.vmax & EVICT_MASK)) {
           r.v2 = first ? 0 : r.vmax;
           r.vmax = x;
           r.m = j;
@@ -91,7 +97,7 @@ __device__ __forceinline__ int row_push_small(uint64_t* row, int k, uint32_t* th
     for (int j = 0; j < KP; ++j) {
       if (j < k) {
         dup |= (((uint32_t)v[j]) & 0x7FFFFFFFu) == id;
-        if (j > 0 && v[j] > vmax) {
+        if (j > 0 && (v[j] & EVICT_MASK) > (vmax & EVICT_MASK)) {
           vmax = v[j];
           m = j;
         }

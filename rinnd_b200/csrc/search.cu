@@ -757,6 +757,14 @@ constexpr int WIDE_MAX_WARPS = 256;
 constexpr size_t EXACT_BYTES = 256ull << 20;
 constexpr int EXACT_MAX_WARPS = 128;
 
+// stats[4] += queries re-run in the wide pass, stats[5] += in the exact pass
+__global__ void k_count_reruns(const unsigned int* counts, unsigned long long* stats) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    atomicAdd(&stats[4], (unsigned long long)counts[0]);
+    atomicAdd(&stats[5], (unsigned long long)counts[1]);
+  }
+}
+
 // The bounded launch over all queries; the wide launch over the queries it
 // recorded; the exact launch over the queries the wide launch recorded (their
 // outputs are overwritten).  All are enqueued on `st`; each re-run finds its
@@ -792,6 +800,8 @@ void run_search(const SearchIndex& ix, const float* Q, const int8_t* Q8, const f
   Redo exact{counts.p + 1, list2.p, nullptr, nullptr, xbits.p, xseeds.p, nullptr, words, ix.N, 0};
   k_search<QUANT><<<xwarps, 32, L.bytes(), st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base, meta, L,
                                                  nullptr, 0, out_idx, out_dist, dstats, exact, PASS_EXACT);
+  RINND_LAUNCH_CHECK();
+  k_count_reruns<<<1, 32, 0, st>>>(counts.p, dstats);
   RINND_LAUNCH_CHECK();
 }
 
