@@ -158,9 +158,61 @@ __device__ __forceinline__ int row_push(uint64_t* row, int k, uint32_t* thr, uin
   return 0;
 }
 
-// row_push with the reject test (d >= the row's max, neighbor_heap.rs:156) on
-// the rows' high words first: the join kernels' rare direct pushes (a full
-// update-buffer region) use it.
+// The join kernels' rare direct push (an update beyond a full update-buffer
+// region): the reject test (d >= the row's max, neighbor_heap.rs:156) on the
+// rows' high words first, then a push whose eviction compares whole slot
+// values (so among equally distant entries a new one goes first).  This form
+// is kept as measured: the push's code is inlined into the join's pair loop
+// and changes to it moved the 1M-point FP32 join between 67 and 101 ms.
+__device__ __forceinline__ int row_push_raw(uint64_t* row, int k, uint32_t* thr, uint64_t key,
+                                            unsigned long long* contention) {
+  const uint32_t vk = (uint32_t)(key >> 32);
+  const uint32_t id = ((uint32_t)key) & 0x7FFFFFFFu;
+  const ulonglong2* r2 = reinterpret_cast<const ulonglong2*>(row);
+  for (int attempt = 0; attempt < PUSH_MAX_RETRY; ++attempt) {
+    uint64_t vmax = 0, v2 = 0;
+    int m = 0;
+    bool dup = false, first = true;
+    for (int j0 = 0; j0 < k; j0 += ROW_ALIGN) {
+      ulonglong2 v[ROW_ALIGN / 2];
+#pragma unroll
+      for (int t = 0; t < ROW_ALIGN / 2; ++t) v[t] = __ldcg(r2 + j0 / 2 + t);
+#pragma unroll
+      for (int t = 0; t < ROW_ALIGN; ++t) {
+        const int j = j0 + t;
+        if (j < k) {
+          const uint64_t x = (t & 1) ? v[t >> 1].y : v[t >> 1].x;
+          dup |= (((uint32_t)x) & 0x7FFFFFFFu) == id;
+          if (first || x > vmax) {
+            v2 = first ? 0 : vmax;
+            vmax = x;
+            m = j;
+            first = false;
+          } else if (x > v2) {
+            v2 = x;
+          }
+        }
+      }
+    }
+    if (dup) return 0;
+    if (vk >= (uint32_t)(vmax >> 32)) {
+      if (thr != nullptr) atomicMin(thr, (uint32_t)(vmax >> 32));
+      return 0;
+    }
+    const unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long*>(row + m),
+                                             (unsigned long long)vmax, (unsigned long long)key);
+    if (old == vmax) {
+      if (thr != nullptr) {
+        const uint64_t nm = v2 > key ? v2 : key;
+        atomicMin(thr, (uint32_t)(nm >> 32));
+      }
+      return 1;
+    }
+  }
+  if (contention) atomicAdd(contention, 1ull);
+  return 0;
+}
+
 __device__ __forceinline__ int row_push_hi_first(uint64_t* row, int k, uint32_t* thr, uint64_t key,
                                                  unsigned long long* contention) {
   const uint32_t vk = (uint32_t)(key >> 32);
@@ -181,7 +233,7 @@ __device__ __forceinline__ int row_push_hi_first(uint64_t* row, int k, uint32_t*
     if (thr != nullptr) atomicMin(thr, mx);
     return 0;
   }
-  return row_push(row, k, thr, key, contention);
+  return row_push_raw(row, k, thr, key, contention);
 }
 
 // The push of the reverse candidate offers: rows of up to 32 slots take the

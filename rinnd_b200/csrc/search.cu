@@ -548,6 +548,8 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
     // With an exact visited set every node is expanded at most once; the cap
     // only matters after a visited-table overflow, where it bounds the loop.
     if (expansions >= (unsigned long long)ix.N + 64) break;
+    // a bounded pass stops as soon as its result is known to need the re-run
+    if (!X.bits && (lost || __any_sync(0xffffffffu, V.lost))) break;
     ++expansions;
     int s = ix.indptr[v], e = ix.indptr[v + 1];
     for (int c0 = s; c0 < e; c0 += 32) {
@@ -748,12 +750,12 @@ struct GlobalVisited {
 };
 
 // Per-warp global-memory state of the re-runs.  Wide pass: a visited table of
-// WIDE_VIS entries and seed arrays of WIDE_SEEDS entries (512 KB per warp).
+// WIDE_VIS entries and seed arrays of WIDE_SEEDS entries (256 KB per warp).
 // Exact pass: a visited bitset of N bits and two seed arrays of N entries; as
 // many warps as fit EXACT_BYTES (at least one, at most EXACT_MAX_WARPS).
-constexpr int WIDE_VIS = 1 << 16;
-constexpr int WIDE_SEEDS = 1 << 14;
-constexpr int WIDE_MAX_WARPS = 256;
+constexpr int WIDE_VIS = 1 << 15;
+constexpr int WIDE_SEEDS = 1 << 13;
+constexpr int WIDE_MAX_WARPS = 148 * 8;
 constexpr size_t EXACT_BYTES = 256ull << 20;
 constexpr int EXACT_MAX_WARPS = 128;
 
