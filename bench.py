@@ -734,7 +734,6 @@ def run_serving(args, world, rank, local_rank):
         }
         print(json.dumps(line), flush=True)
     L.check(L.lib.rinnd_free(h))
-    ix._h = None
 
 
 def main():

@@ -441,7 +441,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   QRng rng(rng_seed);
   // seed-set capacity from this query's own width (not the batch's), so a
   // query's result does not depend on the queries it is batched with
-  const int scap = X.seeds ? X.seed_cap : seed_capacity(k);
+  const int scap = X.seed_cap > 0 ? X.seed_cap : seed_capacity(k);
   // Dropped seeds change the result only if the unbounded search would pop
   // one: when a popped seed ranks after the smallest dropped one while that
   // one is still within the bound, or the seeds run out while it is.
@@ -654,8 +654,7 @@ __global__ void __launch_bounds__(WPB * 32)
   const long long gw = (long long)blockIdx.x * wpb + w;
   int32_t* my_gvis = gvis ? gvis + (size_t)gw * gcap : nullptr;
   ExactState X{nullptr, nullptr, 0, nullptr, 0};
-  if (pass == PASS_WIDE) {
-    X.seeds = redo.xseeds + (size_t)gw * 2 * redo.seed_cap;
+  if (pass == PASS_WIDE) {  // seeds in shared memory (the launch's layout holds seed_cap), table in global
     X.seed_cap = redo.seed_cap;
     X.vis = redo.xvis + (size_t)gw * redo.vis_cap;
     X.vis_cap = redo.vis_cap;
@@ -749,8 +748,9 @@ struct GlobalVisited {
   int32_t* p() const { return buf.p; }
 };
 
-// Per-warp global-memory state of the re-runs.  Wide pass: a visited table of
-// WIDE_VIS entries and seed arrays of WIDE_SEEDS entries (256 KB per warp).
+// Per-warp state of the re-runs.  Wide pass: a visited table of WIDE_VIS
+// entries in global memory and seed arrays of WIDE_SEEDS entries in shared
+// memory (128 KB: one such block per SM).
 // Exact pass: a visited bitset of N bits and two seed arrays of N entries; as
 // many warps as fit EXACT_BYTES (at least one, at most EXACT_MAX_WARPS).
 constexpr int WIDE_VIS = 1 << 15;
@@ -785,13 +785,17 @@ void run_search(const SearchIndex& ix, const float* Q, const int8_t* Q8, const f
                                                              meta, L, gv.p(), gv.cap, out_idx, out_dist, dstats, redo,
                                                              PASS_BOUNDED);
   RINND_LAUNCH_CHECK();
-  // wide re-run (one-warp blocks, as many as queries up to WIDE_MAX_WARPS)
+  // wide re-run (one-warp blocks, as many as queries up to WIDE_MAX_WARPS): the
+  // seed arrays in shared memory (their merges move the whole live array), the
+  // visited table in global memory
   const int wwarps = std::min(WIDE_MAX_WARPS, nq);
+  WarpLayout Lw = L;
+  Lw.s = WIDE_SEEDS;
+  Lw.h = 0;
   DVec<int32_t> wvis((size_t)wwarps * WIDE_VIS, st);
-  DVec<uint64_t> wseeds((size_t)wwarps * 2 * WIDE_SEEDS, st);
-  Redo wide{counts.p, list1.p, counts.p + 1, list2.p, nullptr, wseeds.p, wvis.p, 0, WIDE_SEEDS, WIDE_VIS};
-  k_search<QUANT><<<wwarps, 32, L.bytes(), st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base, meta, L,
-                                                 nullptr, 0, out_idx, out_dist, dstats, wide, PASS_WIDE);
+  Redo wide{counts.p, list1.p, counts.p + 1, list2.p, nullptr, nullptr, wvis.p, 0, WIDE_SEEDS, WIDE_VIS};
+  k_search<QUANT><<<wwarps, 32, Lw.bytes(), st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base, meta, Lw,
+                                                  nullptr, 0, out_idx, out_dist, dstats, wide, PASS_WIDE);
   RINND_LAUNCH_CHECK();
   // exact re-run
   const long long words = ((long long)(ix.N + 31) / 32 + 3) / 4 * 4;  // 16-byte multiple per warp

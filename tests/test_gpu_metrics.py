@@ -83,21 +83,30 @@ def test_generic_build_recall_matches_oracle(rb, orc, name):
     ok = gi >= 0
     want = orc.distance_pairs(kind, np.repeat(X, k, 0), X[np.where(ok, gi, 0).reshape(-1)]).reshape(n, k)
     np.testing.assert_allclose(gd[ok], want[ok], rtol=1e-5, atol=1e-6)
-    oix = orc.OracleIndex(X, n_neighbors=k, distance_kind=kind, correction=orc.CORR_NONE,
-                          angular=name in ("correlation", "true_angular", "tsss"), random_seed=4)
+    ang = name in ("correlation", "true_angular", "tsss")
+    oix = orc.OracleIndex(X, n_neighbors=k, distance_kind=kind, correction=orc.CORR_NONE, angular=ang,
+                          random_seed=4)
     oi, _ = oix.neighbor_graph
-    # tie-aware recall: a found neighbor counts when its distance is within the
-    # k-th smallest (binary metrics such as jaccard have many exactly tied
-    # distances, so which tied ids a build keeps is arrival order)
-    kth = np.sort(dist, axis=1)[:, k - 1:k]
+    if name != "jaccard":
+        assert recall(gi[rows], truth) >= recall(oi[rows], truth) - 0.005
+    else:
+        # Binary sets: most distances are exactly tied, so which tied ids a build
+        # keeps follows arrival order and one build's recall varies by about a
+        # point.  Tie-aware recall (a neighbor counts when its distance is within
+        # the k-th smallest) over every row, averaged over three builds each.
+        all_rows = np.arange(n)
+        full = np.stack([orc.distance_pairs(kind, np.repeat(X[i:i + 1], n, 0), X) for i in all_rows])
+        full[all_rows, all_rows] = np.inf
+        kth = np.sort(full, axis=1)[:, k - 1:k]
 
-    def tie_recall(found):
-        f = found[rows]
-        d = np.take_along_axis(dist, np.where(f >= 0, f, 0), axis=1)
-        return float(np.mean((f >= 0) & (d <= kth)))
+        def tie_recall(found):
+            dd = np.take_along_axis(full, np.where(found >= 0, found, 0), axis=1)
+            return float(np.mean((found >= 0) & (dd <= kth)))
 
-    assert tie_recall(gi) >= tie_recall(oi) - 0.005, (tie_recall(gi), tie_recall(oi), ix.build_info["iterations"],
-                                                      oix.iterations, ix.build_info["pushes_accepted"])
-    assert recall(gi[rows], truth) >= recall(oi[rows], truth) - 0.02
+        g = np.mean([tie_recall(rb.RINND(X, metric=name, n_neighbors=k, random_state=s).neighbor_graph[0])
+                     for s in (4, 5, 6)])
+        o = np.mean([tie_recall(orc.OracleIndex(X, n_neighbors=k, distance_kind=kind, correction=orc.CORR_NONE,
+                                                angular=ang, random_seed=s).neighbor_graph[0]) for s in (4, 5, 6)])
+        assert g >= o - 0.005, (g, o)
     ids, _ = ix.query(X[:200], k=5)
     assert (ids[:, 0] >= 0).all()
