@@ -72,7 +72,9 @@ def test_generic_build_recall_matches_oracle(rb, orc, name):
     X = data_for(name, n, d, seed=61)
     if name == "jaccard":  # distinct enough sets for a meaningful neighbor order
         X = (np.random.default_rng(61).random((n, 64)) < 0.15).astype(np.float32)
-    ix = rb.RINND(X, metric=name, n_neighbors=k, random_state=4)
+    # n_trees = 8 on both sides: the Python class derives 7 from n = 4000
+    # (lib.rs:1200-1204), the oracle's builder default is 8 (index.rs:475-494)
+    ix = rb.RINND(X, metric=name, n_neighbors=k, random_state=4, n_trees=8)
     gi, gd = ix.neighbor_graph
     assert ix.build_info["join_form"] == rb._lib.JOIN_CHUNKED_FP32
     rows = np.arange(0, n, 8)
@@ -103,7 +105,7 @@ def test_generic_build_recall_matches_oracle(rb, orc, name):
             dd = np.take_along_axis(full, np.where(found >= 0, found, 0), axis=1)
             return float(np.mean((found >= 0) & (dd <= kth)))
 
-        g = np.mean([tie_recall(rb.RINND(X, metric=name, n_neighbors=k, random_state=s).neighbor_graph[0])
+        g = np.mean([tie_recall(rb.RINND(X, metric=name, n_neighbors=k, random_state=s, n_trees=8).neighbor_graph[0])
                      for s in (4, 5, 6)])
         o = np.mean([tie_recall(orc.OracleIndex(X, n_neighbors=k, distance_kind=kind, correction=orc.CORR_NONE,
                                                 angular=ang, random_seed=s).neighbor_graph[0]) for s in (4, 5, 6)])
