@@ -381,9 +381,11 @@ RINND_EXPORT int rinnd_search_stats_get(rinnd_index* idx, uint64_t* evaluations,
                                         uint64_t* visited_overflows, int32_t reset);
 /* All search counters since the last reset (8 words): evaluations, expansions,
  * visited-table overflows, spill-frontier overflows, queries re-run with the
- * wide bounded state, queries re-run with the exact state, 0, 0.  A query is
- * re-run when its bounded shared-memory state could have changed its result
- * (see rinnd_query); the re-run's result is the one returned. */
+ * wide bounded state, queries re-run with the exact state, query runs that
+ * used the second-level (global-memory) visited table, query runs that moved
+ * seeds to the global-memory back store.  A query is re-run when its bounded
+ * state could have changed its result (see rinnd_query); the re-run's result
+ * is the one returned. */
 RINND_EXPORT int rinnd_search_counters(rinnd_index* idx, uint64_t* out, int32_t reset);
 
 /* ---- storage info (crates/rinnd/src/lib.rs:1028-1077) ---------------------- */

@@ -379,12 +379,13 @@ class RINND:
 
     def search_stats(self, reset=False) -> dict:
         """Distance evaluations, node expansions, visited-table and spill-frontier
-        overflows, and the queries re-run with the wide and with the exact state,
+        overflows, the queries re-run with the wide and with the exact state, and
+        the query runs that used the global-memory visited table or seed store,
         of the searches since the build (or the last reset)."""
         v = (ctypes.c_uint64 * 8)()
         L.check(L.lib.rinnd_search_counters(self._h, v, int(bool(reset))))
         return {"evaluations": v[0], "expansions": v[1], "visited_overflows": v[2], "frontier_overflows": v[3],
-                "wide_reruns": v[4], "exact_reruns": v[5]}
+                "wide_reruns": v[4], "exact_reruns": v[5], "visited_spills": v[6], "seed_spills": v[7]}
 
     @property
     def build_info(self) -> dict:

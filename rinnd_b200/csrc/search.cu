@@ -18,20 +18,27 @@
 // exact int8 dot with the reference's scaling (quantized.rs:26-40, greedy.rs:384-390)
 // followed by an optional exact FP32 rerank of the leading results (index.rs:103-126).
 //
-// Per-warp state lives in shared memory: the query, the result list (sorted by
-// (distance, id)), the seed set as a sorted array merged warp-parallel with each
-// batch of accepted neighbors, and an open-addressing visited table.  Both are
-// bounded (S seeds, a fixed table), while the reference's seed heap and visited
-// bitset are not.  Dropping the farthest seeds changes nothing unless the
-// unbounded search would pop one of them (it ranks before a seed that is popped
-// while still within the bound, or the seeds run out while it is); such a
-// query, or one with an id the table cannot place within 32 probes, is
-// recorded and re-run from scratch, first with a wider bounded state in global
-// memory and, if that overflows too, with state sized to the index (a visited
-// bitset of N bits and seed arrays of N entries), so every query's result is
-// the one of the unbounded search.
+// Per-warp state: the query, the result list (sorted by (distance, id)) and
+// the front of the seed queue (a sorted array merged warp-parallel with each
+// batch of accepted neighbors) in shared memory; the rest of the seed queue
+// (an unsorted back store) and a second visited table in global memory,
+// behind a first table in shared memory.  Seeds the traversal can no longer
+// pop (distance >= bound with a full result list) are dropped.  The state is
+// still bounded, while the reference's seed heap and visited set are not:
+// dropping seeds from a full back store changes nothing unless the unbounded
+// search would pop one of them (it ranks before a seed that is popped while
+// still within the bound, or the seeds run out while it is); such a query, or
+// one with an id neither table can place within 32 probes, is recorded and
+// re-run from scratch, first with larger bounded state and, if that overflows
+// too, with state sized to the index (a visited bitset of N bits and a back
+// store of N seeds), so every query's result is the one of the unbounded
+// search.
 // Neighbor and tie order follow (distance, id); the reference's BinaryHeap
 // orders exact distance ties by its internal layout.
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "dist.cuh"
 #include "engine.h"
 
@@ -47,9 +54,10 @@ struct WarpLayout {
   __host__ __device__ size_t res_off() const { return (size_t)dp * 4; }
   __host__ __device__ size_t seed_off() const { return res_off() + (size_t)kmax * 8; }
   __host__ __device__ size_t batch_off() const { return seed_off() + (size_t)2 * s * 8; }
-  __host__ __device__ size_t vis_off() const { return batch_off() + 34 * 8; }  // batch + smallest dropped seed
+  __host__ __device__ size_t vis_off() const { return batch_off() + 64 * 8; }  // batch + keys leaving the front
   __host__ __device__ size_t fr_off() const { return vis_off() + (size_t)h * 4; }
-  __host__ __device__ size_t bytes() const { return fr_off() + (size_t)f * 8; }
+  // a warp's region is a multiple of 16 bytes (the tables are cleared with 16-byte stores)
+  __host__ __device__ size_t bytes() const { return (fr_off() + (size_t)f * 8 + 15) & ~(size_t)15; }
 };
 
 __host__ __device__ __forceinline__ int seed_capacity(int width) {
@@ -111,32 +119,60 @@ struct QRng {
   }
 };
 
-// Visited set (VisitedSet::check_and_mark): returns true if id was already
-// present.  Bounded form: an open-addressing table of h entries; an id that
-// finds no free slot within HASH_PROBES probes is counted, treated as visited
-// and marks the search as lost (it will be re-run exactly).  Exact form: a
-// bitset of N bits (bits != null).
+// Visited set (VisitedSet::check_and_mark).  Exact form: a bitset of N bits
+// (bits != null).  Bounded form: an open-addressing table of h ids (shared
+// memory, or global memory for widths above 32) backed by a second global table
+// of h2 ids that a query clears when it first needs it.  An id that finds no
+// free slot within HASH_PROBES probes of either table is counted, treated as
+// visited and marks the search as lost (it is re-run with a larger state).
 struct Visited {
   int32_t* tab;
   int h;
+  int32_t* tab2;  // second level (null: none)
+  int h2;
   uint32_t* bits;
-  bool lost;
+  bool lost;       // warp-uniform
+  bool tab2_live;  // warp-uniform: tab2 cleared for this query
 };
-__device__ __forceinline__ bool visited_check_and_mark(Visited& v, int32_t id, unsigned long long* overflow) {
+
+// 0: id inserted, 1: id present, 2: no free slot within HASH_PROBES probes
+__device__ __forceinline__ int table_mark(int32_t* tab, int h, int32_t id) {
+  uint32_t pos = ((uint32_t)id * 2654435761u) & (uint32_t)(h - 1);
+  for (int p = 0; p < HASH_PROBES; ++p) {
+    const int32_t old = atomicCAS(&tab[pos], -1, id);
+    if (old == -1) return 0;
+    if (old == id) return 1;
+    pos = (pos + 1) & (uint32_t)(h - 1);
+  }
+  return 2;
+}
+
+// Whole warp: marks id on the lanes with `have` and returns, on those lanes,
+// whether it was already visited.  An id whose probes of the first table are
+// all taken goes to the second: the first table never frees a slot, so its
+// later lookups take the same path.
+__device__ __forceinline__ bool visited_mark(Visited& v, int32_t id, bool have, unsigned long long* overflow) {
   if (v.bits) {
+    if (!have) return false;
     const uint32_t m = 1u << (id & 31);
     return (atomicOr(&v.bits[id >> 5], m) & m) != 0u;
   }
-  uint32_t pos = ((uint32_t)id * 2654435761u) & (uint32_t)(v.h - 1);
-  for (int p = 0; p < HASH_PROBES; ++p) {
-    int32_t old = atomicCAS(&v.tab[pos], -1, id);
-    if (old == -1) return false;
-    if (old == id) return true;
-    pos = (pos + 1) & (uint32_t)(v.h - 1);
+  int r = have ? table_mark(v.tab, v.h, id) : 0;
+  if (__any_sync(0xffffffffu, r == 2)) {
+    if (v.tab2) {
+      if (!v.tab2_live) {
+        const int lane = threadIdx.x & 31;
+        int4* t4 = reinterpret_cast<int4*>(v.tab2);
+        for (int t = lane; t < v.h2 / 4; t += 32) t4[t] = make_int4(-1, -1, -1, -1);
+        __syncwarp();
+        v.tab2_live = true;
+      }
+      if (r == 2) r = table_mark(v.tab2, v.h2, id);
+    }
+    if (r == 2) atomicAdd(overflow, 1ull);
+    if (__any_sync(0xffffffffu, r == 2)) v.lost = true;
   }
-  atomicAdd(overflow, 1ull);
-  v.lost = true;
-  return true;
+  return r != 0;
 }
 
 // Visited-table entries of a query of result width w: shared memory up to w = 32,
@@ -245,48 +281,145 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
   return v;
 }
 
-// Merge the sorted batch (one key per lane, ascending, ~0 = none; nb valid) into
-// the sorted seed array A[head, tail) -> C[0, min(na + nb, S)); the two arrays
-// are `stride` entries apart (stride >= S).  Entries merged beyond S are
-// dropped; min_drop (warp-uniform) keeps the smallest dropped key, which the
+// Seed queue: the reference's unbounded min-heap of seeds (greedy.rs:165-201)
+// as a sorted front in shared memory and an unsorted back store in global
+// memory, with every front key < fence <= every back key.  The front's first
+// key is the queue's minimum while the front is non-empty; an empty front is
+// refilled with the smallest back keys.  Keys the traversal can no longer pop
+// are dropped: with a full result list the traversal stops at the first seed
+// whose distance is >= bound, and the bound never grows once the list is full
+// (for a finite epsilon >= 0), so a key with distance >= bound is never popped
+// ("prunable": key >= cut, cut = fkey(bound) << 32; keys of NaN distance are
+// kept).  A full back store drops keys; min_drop keeps the smallest, which the
 // traversal compares with the seeds it pops and its final bound.
-__device__ __forceinline__ void seeds_merge(uint64_t* seeds, uint64_t* bbuf, int stride, int S, int& cur,
-                                            int& head, int& tail, uint64_t bkey, int nb, uint64_t& min_drop) {
+struct SeedQueue {
+  uint64_t* front;  // two arrays of S entries `stride` apart; live: [head, tail) of array cur
+  int stride, S, cur, head, tail;
+  uint64_t* back;  // B entries of this warp's global memory; live: [0, nback)
+  int B, nback;
+  uint64_t fence, min_drop;
+  bool spilled;
+};
+
+__device__ __forceinline__ bool key_prunable(uint64_t key, uint64_t cut) {
+  return key >= cut && (uint32_t)(key >> 32) <= KEY_INF;
+}
+
+__device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
+  for (int o = 16; o; o >>= 1) {
+    const uint64_t x = __shfl_xor_sync(0xffffffffu, v, o);
+    v = x < v ? x : v;
+  }
+  return v;
+}
+
+// Appends the keys of the lanes with `take` to the back store at w (capacity
+// cap), in lane order; keys beyond cap are dropped into min_drop.
+__device__ __forceinline__ void back_append(SeedQueue& s, uint64_t key, bool take, int& w, int cap) {
   const int lane = threadIdx.x & 31;
-  if (nb == 0) return;
-  const bool drops = tail - head + nb > S;
+  const unsigned m = __ballot_sync(0xffffffffu, take);
+  if (!m) return;
+  const int pos = w + __popc(m & ((1u << lane) - 1u));
+  const bool drop = take && pos >= cap;
+  if (take && !drop) s.back[pos] = key;
+  if (__any_sync(0xffffffffu, drop)) {
+    const uint64_t d = warp_min64(drop ? key : ~0ull);
+    s.min_drop = d < s.min_drop ? d : s.min_drop;
+  }
+  w = min(cap, w + __popc(m));
+  s.spilled = true;
+}
+
+// Merges the sorted batch (one key per lane, ascending; the first nb lanes
+// valid, all below the fence) into the front.  Entries merged beyond S leave
+// the front: they are returned on lanes [0, E) in order (E is returned) and
+// the fence becomes the smallest of them if that is lower.  Then prunable keys
+// are cut off the front's end.
+__device__ __forceinline__ int front_merge(SeedQueue& s, uint64_t* bbuf, uint64_t bkey, int nb, uint64_t cut,
+                                           uint64_t& evicted) {
+  const int lane = threadIdx.x & 31;
+  uint64_t* ebuf = bbuf + 32;
   bbuf[lane] = bkey;
   __syncwarp();
-  const uint64_t* A = seeds + (size_t)cur * stride;
-  uint64_t* C = seeds + (size_t)(cur ^ 1) * stride;
-  const int na = tail - head;
+  const uint64_t* A = s.front + (size_t)s.cur * s.stride;
+  uint64_t* C = s.front + (size_t)(s.cur ^ 1) * s.stride;
+  const int na = s.tail - s.head, S = s.S;
   for (int i = lane; i < na; i += 32) {  // out = i + #(b < a)
-    uint64_t a = A[head + i];
+    const uint64_t a = A[s.head + i];
     int lo = 0, hi = nb;
     while (lo < hi) {
-      int mid = (lo + hi) >> 1;
+      const int mid = (lo + hi) >> 1;
       if (bbuf[mid] < a) lo = mid + 1; else hi = mid;
     }
-    int o = i + lo;
-    if (o < S) C[o] = a;
-    else if (o == S) bbuf[32] = a;  // the smallest dropped entry
+    const int o = i + lo;
+    if (o < S) C[o] = a; else ebuf[o - S] = a;
   }
   if (lane < nb) {  // out = j + #(a <= b)
-    uint64_t b = bkey;
     int lo = 0, hi = na;
     while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (A[head + mid] <= b) lo = mid + 1; else hi = mid;
+      const int mid = (lo + hi) >> 1;
+      if (A[s.head + mid] <= bkey) lo = mid + 1; else hi = mid;
     }
-    int o = lane + lo;
-    if (o < S) C[o] = b;
-    else if (o == S) bbuf[32] = b;
+    const int o = lane + lo;
+    if (o < S) C[o] = bkey; else ebuf[o - S] = bkey;
   }
   __syncwarp();
-  if (drops) min_drop = min(min_drop, bbuf[32]);
-  cur ^= 1;
-  head = 0;
-  tail = min(na + nb, S);
+  const int total = na + nb;
+  const int E = total > S ? total - S : 0;  // <= nb <= 32, as na <= S
+  evicted = lane < E ? ebuf[lane] : ~0ull;
+  if (E > 0 && ebuf[0] < s.fence) s.fence = ebuf[0];
+  __syncwarp();
+  s.cur ^= 1;
+  s.head = 0;
+  s.tail = min(total, S);
+  if (s.tail > 0 && key_prunable(C[s.tail - 1], cut)) {  // no NaN key at the end: cut the prunable run
+    int lo = 0, hi = s.tail - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (C[mid] < cut) lo = mid + 1; else hi = mid;
+    }
+    s.tail = lo;
+  }
+  return E;
+}
+
+// Pushes a sorted batch (ascending, one key per lane, the first nb valid):
+// keys below the fence merge into the front, the others and the front's
+// overflow go to the back store, prunable ones nowhere.
+__device__ __forceinline__ void seeds_push(SeedQueue& s, uint64_t* bbuf, uint64_t sorted, int nb, uint64_t cut) {
+  const int lane = threadIdx.x & 31;
+  if (nb == 0) return;
+  const int nf = __popc(__ballot_sync(0xffffffffu, lane < nb && sorted < s.fence));
+  back_append(s, sorted, lane >= nf && lane < nb && !key_prunable(sorted, cut), s.nback, s.B);
+  if (nf == 0) return;
+  uint64_t ev;
+  const int E = front_merge(s, bbuf, sorted, nf, cut, ev);
+  if (E > 0) back_append(s, ev, lane < E && !key_prunable(ev, cut), s.nback, s.B);
+}
+
+// Refills the empty front with the smallest back keys: the back store is
+// merged into the front 32 keys at a time, and what leaves the front is
+// written back in place (never past the keys read so far), so the back store
+// ends with the rest and the fence with the smallest of them.
+__device__ void seeds_refill(SeedQueue& s, uint64_t* bbuf, uint64_t cut) {
+  const int lane = threadIdx.x & 31;
+  const int n = s.nback;
+  s.head = s.tail = 0;
+  s.fence = ~0ull;
+  int w = 0;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    uint64_t key = c0 + lane < n ? s.back[c0 + lane] : ~0ull;
+    if (key_prunable(key, cut)) key = ~0ull;
+    const int nb = __popc(__ballot_sync(0xffffffffu, key != ~0ull));
+    if (nb == 0) continue;
+    const uint64_t sorted = warp_sort32(key);
+    uint64_t ev;
+    const int E = front_merge(s, bbuf, sorted, nb, cut, ev);
+    if (E > 0) back_append(s, ev, lane < E && !key_prunable(ev, cut), w, n);
+  }
+  __syncwarp();
+  s.nback = w;
+  if (w == 0) s.fence = ~0ull;
 }
 
 // tree_query_scale of a quantized query (lib.rs:283-296): max|q| / 127 of the
@@ -397,29 +530,31 @@ __device__ void tree_search_leaves(const SearchIndex& ix, int root, int budget, 
 // k: result-list width; k_out: entries written to oi/od; rerank (QUANT only):
 // number of leading results re-ordered by exact FP32 distance before output;
 // rng_seed: the query's random stream.
-// X (re-runs; all null in the first pass): this warp's global-memory state
-// used instead of the shared-memory one -- the wide form (a larger bounded
-// visited table and seed arrays) or the exact form (a visited bitset of N bits
-// and seed arrays of N entries, which cannot overflow).  Returns true when a
-// bounded state overflowed.
-struct ExactState {
-  uint32_t* bits;     // exact form: visited bitset of N bits
-  uint64_t* seeds;    // two seed arrays of seed_cap entries each
-  int seed_cap;
-  int32_t* vis;       // wide form: open-addressing visited table of vis_cap entries
-  int vis_cap;
+// W: this warp's global-memory state for the pass: the first-level visited
+// table when the layout has none in shared memory (vis1), the second-level
+// table (vis2, or null), the seed back store (back), and in the exact pass a
+// visited bitset of N bits (bits; the tables are then unused) with a back store
+// of N entries, neither of which can overflow.  Returns true when a bounded
+// state could have changed the result (the query is then re-run).
+struct WarpScratch {
+  int32_t* vis1;
+  int vis1_cap;
+  int32_t* vis2;
+  int vis2_cap;
+  uint64_t* back;
+  int back_cap;
+  uint32_t* bits;
 };
 template <bool QUANT>
 __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_t* Q8row,
                            float qinv, uint64_t rng_seed, int k, int k_out, int rerank, float eps,
-                           const WarpLayout& L, unsigned char* wsm, int32_t* gvis, ExactState X, int32_t* oi,
+                           const WarpLayout& L, unsigned char* wsm, const WarpScratch& W, int32_t* oi,
                            float* od, unsigned long long* stats) {
   const int lane = threadIdx.x & 31;
   float* q = reinterpret_cast<float*>(wsm + L.q_off());
   uint64_t* res = reinterpret_cast<uint64_t*>(wsm + L.res_off());
-  uint64_t* seeds = X.seeds ? X.seeds : reinterpret_cast<uint64_t*>(wsm + L.seed_off());
-  const int sstride = X.seeds ? X.seed_cap : L.s;  // seed arrays: entries apart
-  int32_t* vis = reinterpret_cast<int32_t*>(wsm + L.vis_off());
+  uint64_t* seeds = reinterpret_cast<uint64_t*>(wsm + L.seed_off());
+  int32_t* vis = W.vis1 ? W.vis1 : reinterpret_cast<int32_t*>(wsm + L.vis_off());
   uint64_t* bbuf = reinterpret_cast<uint64_t*>(wsm + L.batch_off());
   int8_t* q8 = reinterpret_cast<int8_t*>(q);  // QUANT: codes stored in the query slot
   if (QUANT) {
@@ -428,39 +563,35 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   } else {
     for (int t = lane; t < ix.Dp; t += 32) q[t] = t < ix.D ? Qrow[t] : 0.f;
   }
-  const int vcap = X.vis ? X.vis_cap : visited_capacity(k);
-  if (gvis) vis = gvis;  // global-memory table of this warp
-  if (X.vis) vis = X.vis;
-  Visited V{vis, vcap, X.bits, false};
-  if (X.bits) {
-    for (int t = lane; t < (ix.N + 31) / 32; t += 32) X.bits[t] = 0u;
+  const int vcap = W.vis1 ? W.vis1_cap : L.h;
+  Visited V{vis, vcap, W.vis2, W.vis2_cap, W.bits, false, false};
+  if (W.bits) {
+    uint4* b4 = reinterpret_cast<uint4*>(W.bits);  // words padded to a multiple of 4
+    for (long long t = lane; t < ((long long)ix.N + 127) / 128; t += 32) b4[t] = make_uint4(0u, 0u, 0u, 0u);
   } else {
-    for (int t = lane; t < vcap; t += 32) vis[t] = -1;
+    int4* v4 = reinterpret_cast<int4*>(vis);  // capacities are multiples of 4
+    for (int t = lane; t < vcap / 4; t += 32) v4[t] = make_int4(-1, -1, -1, -1);
   }
   __syncwarp();
   QRng rng(rng_seed);
-  // seed-set capacity from this query's own width (not the batch's), so a
-  // query's result does not depend on the queries it is batched with
-  const int scap = X.seed_cap > 0 ? X.seed_cap : seed_capacity(k);
+  SeedQueue sq{seeds, L.s, L.s, 0, 0, 0, W.back, W.back_cap, 0, ~0ull, ~0ull, false};
   // Dropped seeds change the result only if the unbounded search would pop
   // one: when a popped seed ranks after the smallest dropped one while that
   // one is still within the bound, or the seeds run out while it is.
-  uint64_t min_drop = ~0ull;
   bool lost = false;  // the bounded state may have changed the result (warp-uniform)
-  int rc = 0, cur = 0, head = 0, tail = 0;
+  int rc = 0;
   unsigned long long evals = 0, expansions = 0;
   unsigned long long* overflow = &stats[2];
   const float min_d = ix.min_distance;
   auto bound_of = [&](float mx) { return __fadd_rn(mx, __fmul_rn(eps, __fsub_rn(mx, min_d))); };
+  // seeds are pruned against the bound only where the bound cannot grow again
+  const bool prune_ok = eps >= 0.f && eps <= 3.402823466e38f && fabsf(min_d) <= 3.402823466e38f;
+  auto cut_of = [&](float b) { return prune_ok && rc >= k ? (uint64_t)fkey(b) << 32 : ~0ull; };
 
   // ---- unconditional pushes of a list of candidate ids (leaves, random fill) ----
   auto push_all = [&](int32_t my_id, bool have) {
-    bool fresh = false;
-    float d = 0.f;
-    if (have) {
-      fresh = !visited_check_and_mark(V, my_id, overflow);
-      if (fresh) d = dist_to<QUANT>(ix, q, q8, qinv, my_id);
-    }
+    const bool fresh = !visited_mark(V, my_id, have, overflow) && have;
+    const float d = fresh ? dist_to<QUANT>(ix, q, q8, qinv, my_id) : 0.f;
     unsigned m = __ballot_sync(0xffffffffu, fresh);
     evals += __popc(m);
     uint64_t bkey = fresh ? rkey(d, my_id) : ~0ull;
@@ -473,7 +604,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
       result_push(res, rc, k, dj, ij);
     }
     uint64_t sorted = warp_sort32(bkey);
-    seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(m), min_drop);
+    seeds_push(sq, bbuf, sorted, __popc(m), ~0ull);
   };
 
   // ---- tree seeding (greedy.rs:70-146): the points of the leaves each tree's
@@ -498,7 +629,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   }
   // ---- fill_random (greedy.rs:148-163) ----
   {
-    int need = k - (tail - head);
+    int need = k - (sq.tail - sq.head + sq.nback);
     for (int r0 = 0; r0 < need; r0 += 32) {
       int32_t id = -1;
       // draws in sequence order (every lane runs the stream); lane r takes draw r0 + r
@@ -510,8 +641,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
       bool fresh = false;
       for (int r = 0; r < 32 && r0 + r < need; ++r) {
         int32_t x = __shfl_sync(0xffffffffu, id, r);
-        bool f = false;
-        if (lane == 0) f = !visited_check_and_mark(V, x, overflow);
+        bool f = !visited_mark(V, x, lane == 0, overflow);
         f = __shfl_sync(0xffffffffu, f, 0);
         if (lane == r) fresh = f;
       }
@@ -526,20 +656,25 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
         result_push(res, rc, k, __shfl_sync(0xffffffffu, d, j), __shfl_sync(0xffffffffu, id, j));
       }
       uint64_t sorted = warp_sort32(fresh ? rkey(d, id) : ~0ull);
-      seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(m), min_drop);
+      seeds_push(sq, bbuf, sorted, __popc(m), ~0ull);
     }
   }
   // ---- traverse (greedy.rs:165-201) ----
   float mx = result_max(res, rc);
   float bound = bound_of(mx);
   bool stopped = false;
-  while (head < tail) {
-    uint64_t top = seeds[(size_t)cur * sstride + head];
-    ++head;
+  while (true) {
+    if (sq.head == sq.tail) {
+      if (sq.nback == 0) break;
+      seeds_refill(sq, bbuf, cut_of(bound));
+      if (sq.head == sq.tail) break;
+    }
+    const uint64_t top = sq.front[(size_t)sq.cur * sq.stride + sq.head];
+    ++sq.head;
     float vd = fkey_inv((uint32_t)(top >> 32));
     int32_t v = (int32_t)(uint32_t)top;
-    if (top > min_drop) {  // the unbounded search reaches the dropped seed first
-      if (!(rc >= k && fkey_inv((uint32_t)(min_drop >> 32)) >= bound)) lost = true;
+    if (top > sq.min_drop) {  // the unbounded search reaches the dropped seed first
+      if (!(rc >= k && fkey_inv((uint32_t)(sq.min_drop >> 32)) >= bound)) lost = true;
     }
     if (rc >= k && vd >= bound) {
       stopped = true;
@@ -549,13 +684,13 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
     // only matters after a visited-table overflow, where it bounds the loop.
     if (expansions >= (unsigned long long)ix.N + 64) break;
     // a bounded pass stops as soon as its result is known to need the re-run
-    if (!X.bits && (lost || __any_sync(0xffffffffu, V.lost))) break;
+    if (!W.bits && (lost || V.lost)) break;
     ++expansions;
     int s = ix.indptr[v], e = ix.indptr[v + 1];
     for (int c0 = s; c0 < e; c0 += 32) {
       int c = c0 + lane;
       int32_t nb = c < e ? ix.indices[c] : -1;
-      bool fresh = nb >= 0 && !visited_check_and_mark(V, nb, overflow);
+      const bool fresh = !visited_mark(V, nb, nb >= 0, overflow) && nb >= 0;
       float d = fresh ? dist_to<QUANT>(ix, q, q8, qinv, nb) : 0.f;
       unsigned m = __ballot_sync(0xffffffffu, fresh);
       evals += __popc(m);
@@ -576,18 +711,19 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
       }
       bool acc = (acc_mask >> lane) & 1u;
       uint64_t sorted = warp_sort32(acc ? rkey(d, nb) : ~0ull);
-      seeds_merge(seeds, bbuf, sstride, scap, cur, head, tail, sorted, __popc(acc_mask), min_drop);
+      seeds_push(sq, bbuf, sorted, __popc(acc_mask), cut_of(bound));
     }
   }
   // seeds ran out: the unbounded search would go on with a dropped seed
   // within the bound
-  if (!stopped && min_drop != ~0ull && !(rc >= k && fkey_inv((uint32_t)(min_drop >> 32)) >= bound)) lost = true;
+  if (!stopped && sq.min_drop != ~0ull && !(rc >= k && fkey_inv((uint32_t)(sq.min_drop >> 32)) >= bound))
+    lost = true;
   // ---- exact rerank of the first `rerank` results (index.rs:103-126): exact
   // FP32 distance to the FP32 query, sorted by (distance, id) ----
   int nres = rc;
   if (QUANT && rerank > 0) {
     const int m = min(rc, rerank);
-    uint64_t* tmp = seeds;  // the seed arrays (2 S >= 512 entries) are free after the traversal
+    uint64_t* tmp = seeds;  // the front's arrays (2 S >= 512 entries) are free after the traversal
     for (int e = lane; e < m; e += 32) {
       const int32_t id = (int32_t)(uint32_t)res[e];
       tmp[e] = rkey(exact_distance(ix.kind, Qrow, ix.X + (size_t)id * ix.Dp, ix.D), id);
@@ -618,55 +754,58 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   if (lane == 0) {
     atomicAdd(&stats[0], evals);
     atomicAdd(&stats[1], expansions);
+    if (V.tab2_live) atomicAdd(&stats[6], 1ull);
+    if (sq.spilled) atomicAdd(&stats[7], 1ull);
   }
   __syncwarp();
   return __any_sync(0xffffffffu, lost || V.lost);
 }
 
-// Queries a bounded search could not finish: a launch appends their indices to
-// (count_out, list_out), and the next launch re-runs the queries of
-// (count_in, list_in) with per-warp global-memory state: the wide pass a
-// visited table of vis_cap entries and seed arrays of seed_cap entries, the
-// exact pass a bitset of N bits (words_per_warp words) and seed arrays of N.
-struct Redo {
+// One pass of the search over a set of queries: all nq (list_in null) or
+// list_in[0, *count_in); warps take queries from the counter `next` one at a
+// time.  A query whose bounded state could have changed its result is
+// appended to (count_out, list_out) for the next pass (none in the exact
+// pass).  Per-warp global state: first-level visited tables of vis1_cap ids
+// (null: the layout's shared-memory table), second-level tables of vis2_cap
+// ids (null: none), seed back stores of back_cap keys and, in the exact pass,
+// visited bitsets of `words` words.
+struct PassState {
   const unsigned int* count_in;
   const int32_t* list_in;
   unsigned int* count_out;
   int32_t* list_out;
-  uint32_t* xbits;
-  uint64_t* xseeds;
-  int32_t* xvis;
-  long long words_per_warp;
-  int seed_cap, vis_cap;
+  unsigned int* next;
+  int32_t* vis1;
+  int vis1_cap;
+  int32_t* vis2;
+  int vis2_cap;
+  uint64_t* back;
+  int back_cap;
+  uint32_t* bits;
+  long long words;
 };
-enum SearchPass { PASS_BOUNDED = 0, PASS_WIDE = 1, PASS_EXACT = 2 };
 
 template <bool QUANT>
 __global__ void __launch_bounds__(WPB * 32)
     k_search(SearchIndex ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k, int k_out,
-             int rerank, float eps, uint64_t qid_base, QueryMeta meta, WarpLayout L, int32_t* gvis, int gcap,
-             int32_t* out_idx, float* out_dist, unsigned long long* stats, Redo redo, int pass) {
+             int rerank, float eps, uint64_t qid_base, QueryMeta meta, WarpLayout L, PassState P,
+             int32_t* out_idx, float* out_dist, unsigned long long* stats) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   unsigned char* wsm = smem + (size_t)w * L.bytes();
-  const int wpb = blockDim.x >> 5;  // warps per block (the re-runs launch one-warp blocks)
-  const long long gw = (long long)blockIdx.x * wpb + w;
-  int32_t* my_gvis = gvis ? gvis + (size_t)gw * gcap : nullptr;
-  ExactState X{nullptr, nullptr, 0, nullptr, 0};
-  if (pass == PASS_WIDE) {  // seeds in shared memory (the launch's layout holds seed_cap), table in global
-    X.seed_cap = redo.seed_cap;
-    X.vis = redo.xvis + (size_t)gw * redo.vis_cap;
-    X.vis_cap = redo.vis_cap;
-  } else if (pass == PASS_EXACT) {
-    X.bits = redo.xbits + (size_t)gw * redo.words_per_warp;
-    X.seeds = redo.xseeds + (size_t)gw * 2 * ix.N;
-    X.seed_cap = ix.N;
-  }
-  const int total_warps = gridDim.x * wpb;
-  const int n_run = pass == PASS_BOUNDED ? nq : (int)min((unsigned int)nq, *redo.count_in);
-  for (int t = (int)gw; t < n_run; t += total_warps) {
-    const int qi = pass == PASS_BOUNDED ? t : redo.list_in[t];
+  const size_t gw = (size_t)blockIdx.x * (blockDim.x >> 5) + w;  // the re-runs launch one-warp blocks
+  WarpScratch W{P.vis1 ? P.vis1 + gw * P.vis1_cap : nullptr, P.vis1_cap,
+                P.vis2 ? P.vis2 + gw * P.vis2_cap : nullptr, P.vis2_cap,
+                P.back + gw * P.back_cap, P.back_cap,
+                P.bits ? P.bits + gw * P.words : nullptr};
+  const int n_run = P.list_in ? (int)min((unsigned int)nq, *P.count_in) : nq;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = (int)atomicAdd(P.next, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= n_run) break;
+    const int qi = P.list_in ? P.list_in[t] : t;
     int qk = k, qko = k_out, qr = rerank;
     float qe = eps;
     // FP32 queries seed with seed + query index (index.rs:165); quantized
@@ -682,9 +821,9 @@ __global__ void __launch_bounds__(WPB * 32)
       off = meta.out_off[qi];
     }
     const bool lost = search_one<QUANT>(ix, Q + (size_t)qi * ix.Dp, QUANT ? Q8 + (size_t)qi * ix.Dq : nullptr,
-                                        QUANT ? qinv[qi] : 0.f, ix.seed + stream, qk, qko, qr, qe, L, wsm, my_gvis, X,
+                                        QUANT ? qinv[qi] : 0.f, ix.seed + stream, qk, qko, qr, qe, L, wsm, W,
                                         out_idx + off, out_dist + off, stats);
-    if (lost && pass != PASS_EXACT && lane == 0) redo.list_out[atomicAdd(redo.count_out, 1u)] = qi;
+    if (lost && P.list_out && lane == 0) P.list_out[atomicAdd(P.count_out, 1u)] = qi;
   }
 }
 
@@ -735,27 +874,39 @@ WarpLayout layout_for(const SearchIndex& ix, int k) {
   return L;
 }
 
-// Per-warp global-memory visited tables of a launch whose widest query does
-// not fit the shared-memory table (freed stream-ordered after the launch).
-struct GlobalVisited {
-  DVec<int32_t> buf;
-  int cap = 0;
-  GlobalVisited(const WarpLayout& L, int blocks, cudaStream_t st) {
-    if (L.h > 0) return;
-    cap = visited_capacity(L.kmax);
-    buf.alloc((size_t)blocks * WPB * cap, st);
-  }
-  int32_t* p() const { return buf.p; }
-};
+// Blocks of `kernel` resident on the current device at once (cached).
+int resident_blocks(const void* kernel, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, size_t, int>, int> cache;
+  int dev = 0;
+  RINND_CUDA(cudaGetDevice(&dev));
+  const auto key = std::make_tuple(kernel, threads, smem, dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int per_sm = 0, sms = 0;
+  RINND_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+  RINND_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int r = std::max(1, per_sm) * std::max(1, sms);
+  cache[key] = r;
+  return r;
+}
 
-// Per-warp state of the re-runs.  Wide pass: a visited table of WIDE_VIS
-// entries in global memory and seed arrays of WIDE_SEEDS entries in shared
-// memory (128 KB: one such block per SM).
-// Exact pass: a visited bitset of N bits and two seed arrays of N entries; as
+// Per-warp global state of the passes.  Bounded pass: as many warps as are
+// resident (at most FIRST_BYTES of state), a second-level visited table of
+// 4x the shared table (2x the global first-level table for widths above 32)
+// and a back store of 16 S seeds.  Wide pass (queries the bounded pass lost):
+// WIDE_WARPS one-warp blocks with the same front (a merge costs S / 32 steps
+// a lane, so a larger front slows every expansion) and a visited table of
+// WIDE_VIS1 ids in shared memory, a second-level table of WIDE_VIS2 ids and a
+// back store of WIDE_BACK seeds.  Exact pass (queries the wide pass
+// lost): a visited bitset of N bits and a back store of N seeds per warp, as
 // many warps as fit EXACT_BYTES (at least one, at most EXACT_MAX_WARPS).
-constexpr int WIDE_VIS = 1 << 15;
-constexpr int WIDE_SEEDS = 1 << 13;
-constexpr int WIDE_MAX_WARPS = 148 * 8;
+constexpr size_t FIRST_BYTES = 512ull << 20;
+constexpr int WIDE_WARPS = 148;
+constexpr int WIDE_VIS1 = 1 << 13;
+constexpr int WIDE_VIS2 = 1 << 17;
+constexpr int WIDE_BACK = 1 << 15;
 constexpr size_t EXACT_BYTES = 256ull << 20;
 constexpr int EXACT_MAX_WARPS = 128;
 
@@ -775,37 +926,52 @@ template <bool QUANT>
 void run_search(const SearchIndex& ix, const float* Q, const int8_t* Q8, const float* qinv, int nq, int k, int k_out,
                 int rerank, float eps, uint64_t qid_base, const QueryMeta& meta, const WarpLayout& L,
                 int32_t* out_idx, float* out_dist, cudaStream_t st, unsigned long long* dstats) {
-  const int blocks = std::min((nq + WPB - 1) / WPB, 148 * 8);
-  GlobalVisited gv(L, blocks, st);
-  DVec<unsigned int> counts(2, st);
+  const void* kern = reinterpret_cast<const void*>(k_search<QUANT>);
+  // counts: [0] wide list, [1] exact list, [2..4] work counters of the passes
+  DVec<unsigned int> counts(8, st);
   counts.fill_bytes(0);
   DVec<int32_t> list1((size_t)nq, st), list2((size_t)nq, st);
-  Redo redo{nullptr, nullptr, counts.p, list1.p, nullptr, nullptr, nullptr, 0, 0, 0};
+
+  // bounded pass
+  const int vis1 = L.h > 0 ? 0 : visited_capacity(L.kmax);
+  const int vis2 = L.h > 0 ? 4 * L.h : 2 * vis1;
+  const int back = 16 * L.s;
+  const size_t per_warp = (size_t)vis1 * 4 + (size_t)vis2 * 4 + (size_t)back * 8;
+  int blocks = std::min((nq + WPB - 1) / WPB, resident_blocks(kern, WPB * 32, L.bytes() * WPB));
+  blocks = std::max(1, std::min<int>(blocks, (int)(FIRST_BYTES / (per_warp * WPB))));
+  const size_t warps = (size_t)blocks * WPB;
+  DVec<int32_t> v1(warps * vis1, st), v2(warps * vis2, st);
+  DVec<uint64_t> bk(warps * back, st);
+  PassState p1{nullptr, nullptr, counts.p, list1.p, counts.p + 2, v1.p, vis1, v2.p, vis2, bk.p, back, nullptr, 0};
   k_search<QUANT><<<blocks, WPB * 32, L.bytes() * WPB, st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base,
-                                                             meta, L, gv.p(), gv.cap, out_idx, out_dist, dstats, redo,
-                                                             PASS_BOUNDED);
+                                                             meta, L, p1, out_idx, out_dist, dstats);
   RINND_LAUNCH_CHECK();
-  // wide re-run (one-warp blocks, as many as queries up to WIDE_MAX_WARPS): the
-  // seed arrays in shared memory (their merges move the whole live array), the
-  // visited table in global memory
-  const int wwarps = std::min(WIDE_MAX_WARPS, nq);
+
+  // wide pass
   WarpLayout Lw = L;
-  Lw.s = WIDE_SEEDS;
-  Lw.h = 0;
-  DVec<int32_t> wvis((size_t)wwarps * WIDE_VIS, st);
-  Redo wide{counts.p, list1.p, counts.p + 1, list2.p, nullptr, nullptr, wvis.p, 0, WIDE_SEEDS, WIDE_VIS};
+  Lw.h = WIDE_VIS1;
+  const int wwarps = std::min(WIDE_WARPS, nq);
+  DVec<int32_t> wv2((size_t)wwarps * WIDE_VIS2, st);
+  DVec<uint64_t> wbk((size_t)wwarps * WIDE_BACK, st);
+  PassState p2{counts.p, list1.p, counts.p + 1, list2.p, counts.p + 3, nullptr, 0, wv2.p, WIDE_VIS2,
+               wbk.p, WIDE_BACK, nullptr, 0};
   k_search<QUANT><<<wwarps, 32, Lw.bytes(), st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base, meta, Lw,
-                                                  nullptr, 0, out_idx, out_dist, dstats, wide, PASS_WIDE);
+                                                  p2, out_idx, out_dist, dstats);
   RINND_LAUNCH_CHECK();
-  // exact re-run
+
+  // exact pass
+  WarpLayout Lx = L;
+  Lx.h = 0;
   const long long words = ((long long)(ix.N + 31) / 32 + 3) / 4 * 4;  // 16-byte multiple per warp
-  const size_t per_warp = (size_t)words * 4 + (size_t)2 * ix.N * 8;
-  const int xwarps = std::min(nq, (int)std::max<size_t>(1, std::min<size_t>(EXACT_BYTES / per_warp, EXACT_MAX_WARPS)));
+  const size_t x_per_warp = (size_t)words * 4 + (size_t)ix.N * 8;
+  const int xwarps =
+      std::min(nq, (int)std::max<size_t>(1, std::min<size_t>(EXACT_BYTES / x_per_warp, EXACT_MAX_WARPS)));
   DVec<uint32_t> xbits((size_t)xwarps * words, st);
-  DVec<uint64_t> xseeds((size_t)xwarps * 2 * ix.N, st);
-  Redo exact{counts.p + 1, list2.p, nullptr, nullptr, xbits.p, xseeds.p, nullptr, words, ix.N, 0};
-  k_search<QUANT><<<xwarps, 32, L.bytes(), st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base, meta, L,
-                                                 nullptr, 0, out_idx, out_dist, dstats, exact, PASS_EXACT);
+  DVec<uint64_t> xbk((size_t)xwarps * ix.N, st);
+  PassState p3{counts.p + 1, list2.p, nullptr, nullptr, counts.p + 4, nullptr, 0, nullptr, 0,
+               xbk.p, ix.N, xbits.p, words};
+  k_search<QUANT><<<xwarps, 32, Lx.bytes(), st>>>(ix, Q, Q8, qinv, nq, k, k_out, rerank, eps, qid_base, meta, Lx,
+                                                  p3, out_idx, out_dist, dstats);
   RINND_LAUNCH_CHECK();
   k_count_reruns<<<1, 32, 0, st>>>(counts.p, dstats);
   RINND_LAUNCH_CHECK();
