@@ -54,7 +54,8 @@ struct WarpLayout {
   __host__ __device__ size_t res_off() const { return (size_t)dp * 4; }
   __host__ __device__ size_t seed_off() const { return res_off() + (size_t)kmax * 8; }
   __host__ __device__ size_t batch_off() const { return seed_off() + (size_t)2 * s * 8; }
-  __host__ __device__ size_t vis_off() const { return batch_off() + 64 * 8; }  // batch + keys leaving the front
+  // batch, keys leaving the front, keys staged for the front by a refill
+  __host__ __device__ size_t vis_off() const { return batch_off() + 96 * 8; }
   __host__ __device__ size_t fr_off() const { return vis_off() + (size_t)h * 4; }
   // a warp's region is a multiple of 16 bytes (the tables are cleared with 16-byte stores)
   __host__ __device__ size_t bytes() const { return (fr_off() + (size_t)f * 8 + 15) & ~(size_t)15; }
@@ -122,12 +123,14 @@ struct QRng {
 // Visited set (VisitedSet::check_and_mark).  Exact form: a bitset of N bits
 // (bits != null).  Bounded form: an open-addressing table of h ids (shared
 // memory, or global memory for widths above 32) backed by a second global table
-// of h2 ids that a query clears when it first needs it.  An id that finds no
+// of h2 ids that a query clears when it first needs it.  The first table takes
+// new ids until it holds 2/3 h (so that a lookup's probe run stays short);
+// after that an id absent from it goes to the second.  An id that finds no
 // free slot within HASH_PROBES probes of either table is counted, treated as
 // visited and marks the search as lost (it is re-run with a larger state).
 struct Visited {
   int32_t* tab;
-  int h;
+  int h, n1;      // n1: ids the first table holds (warp-uniform)
   int32_t* tab2;  // second level (null: none)
   int h2;
   uint32_t* bits;
@@ -135,29 +138,36 @@ struct Visited {
   bool tab2_live;  // warp-uniform: tab2 cleared for this query
 };
 
-// 0: id inserted, 1: id present, 2: no free slot within HASH_PROBES probes
-__device__ __forceinline__ int table_mark(int32_t* tab, int h, int32_t id) {
-  uint32_t pos = ((uint32_t)id * 2654435761u) & (uint32_t)(h - 1);
+__device__ __forceinline__ uint32_t vis_slot(int32_t id, int h) {
+  return __umulhi((uint32_t)id * 2654435761u, (uint32_t)h);
+}
+
+// insert: 0 id inserted, 1 id present, 2 no free slot within HASH_PROBES probes.
+// lookup (!insert, no lane inserts meanwhile): 1 present, 2 absent.
+__device__ __forceinline__ int table_mark(int32_t* tab, int h, int32_t id, bool insert) {
+  uint32_t pos = vis_slot(id, h);
   for (int p = 0; p < HASH_PROBES; ++p) {
-    const int32_t old = atomicCAS(&tab[pos], -1, id);
-    if (old == -1) return 0;
+    const int32_t old = insert ? atomicCAS(&tab[pos], -1, id) : tab[pos];
+    if (old == -1) return insert ? 0 : 2;
     if (old == id) return 1;
-    pos = (pos + 1) & (uint32_t)(h - 1);
+    pos = pos + 1 == (uint32_t)h ? 0u : pos + 1;
   }
   return 2;
 }
 
 // Whole warp: marks id on the lanes with `have` and returns, on those lanes,
-// whether it was already visited.  An id whose probes of the first table are
-// all taken goes to the second: the first table never frees a slot, so its
-// later lookups take the same path.
+// whether it was already visited.  An id is held by one table only: the first
+// table never frees a slot, so an id it did not take (no free slot within
+// HASH_PROBES probes, or the table closed) is never found there later either.
 __device__ __forceinline__ bool visited_mark(Visited& v, int32_t id, bool have, unsigned long long* overflow) {
   if (v.bits) {
     if (!have) return false;
     const uint32_t m = 1u << (id & 31);
     return (atomicOr(&v.bits[id >> 5], m) & m) != 0u;
   }
-  int r = have ? table_mark(v.tab, v.h, id) : 0;
+  const bool open1 = v.n1 < v.h - v.h / 3;
+  int r = have ? table_mark(v.tab, v.h, id, open1) : 1;
+  if (open1) v.n1 += __popc(__ballot_sync(0xffffffffu, r == 0));
   if (__any_sync(0xffffffffu, r == 2)) {
     if (v.tab2) {
       if (!v.tab2_live) {
@@ -167,20 +177,20 @@ __device__ __forceinline__ bool visited_mark(Visited& v, int32_t id, bool have, 
         __syncwarp();
         v.tab2_live = true;
       }
-      if (r == 2) r = table_mark(v.tab2, v.h2, id);
+      if (r == 2) r = table_mark(v.tab2, v.h2, id, true);
     }
     if (r == 2) atomicAdd(overflow, 1ull);
     if (__any_sync(0xffffffffu, r == 2)) v.lost = true;
   }
-  return r != 0;
+  return have && r != 0;
 }
 
-// Visited-table entries of a query of result width w: shared memory up to w = 32,
-// beyond that a per-warp region of global memory (a search of width w
-// evaluates on the order of 100 w nodes).  A query's capacity depends on its
-// own width only, so its result does not depend on the queries batched with it.
+// First-level visited-table entries for result width w: shared memory up to
+// w = 32 (3072 entries keep three 4-warp blocks on an SM), beyond that a
+// per-warp region of global memory (a search of width w evaluates on the order
+// of 100 w nodes).
 __host__ __device__ __forceinline__ int visited_capacity(int width) {
-  if (width <= 32) return 4096;
+  if (width <= 32) return 3072;
   int h = 8192;
   while (h < 128 * width) h <<= 1;
   return h;
@@ -397,11 +407,11 @@ __device__ __forceinline__ void seeds_push(SeedQueue& s, uint64_t* bbuf, uint64_
   if (E > 0) back_append(s, ev, lane < E && !key_prunable(ev, cut), s.nback, s.B);
 }
 
-// Refills the empty front with the smallest back keys: the back store is
-// merged into the front 32 keys at a time, and what leaves the front is
-// written back in place (never past the keys read so far), so the back store
-// ends with the rest and the fence with the smallest of them.
-__device__ void seeds_refill(SeedQueue& s, uint64_t* bbuf, uint64_t cut) {
+// Refills the empty front by merging the whole back store through it, 32
+// keys at a time; what leaves the front is written back in place (never past
+// the keys read so far), so the back store ends with the rest and the fence
+// with the smallest of them.  Used when no threshold is found.
+__device__ void seeds_refill_merge(SeedQueue& s, uint64_t* bbuf, uint64_t cut) {
   const int lane = threadIdx.x & 31;
   const int n = s.nback;
   s.head = s.tail = 0;
@@ -420,6 +430,102 @@ __device__ void seeds_refill(SeedQueue& s, uint64_t* bbuf, uint64_t cut) {
   __syncwarp();
   s.nback = w;
   if (w == 0) s.fence = ~0ull;
+}
+
+constexpr int BACK_UNROLL = 8;  // 32-key chunks of the back store loaded at once
+
+// Number of back keys below hi that are not prunable (whole warp).
+__device__ __forceinline__ int back_count(const SeedQueue& s, uint64_t hi, uint64_t cut) {
+  const int lane = threadIdx.x & 31;
+  int c = 0;
+  for (int c0 = 0; c0 < s.nback; c0 += 32 * BACK_UNROLL) {
+    uint64_t key[BACK_UNROLL];
+#pragma unroll
+    for (int u = 0; u < BACK_UNROLL; ++u) {
+      const int p = c0 + 32 * u + lane;
+      key[u] = p < s.nback ? s.back[p] : ~0ull;
+    }
+#pragma unroll
+    for (int u = 0; u < BACK_UNROLL; ++u) c += __popc(__ballot_sync(0xffffffffu, key[u] < hi && !key_prunable(key[u], cut)));
+  }
+  return c;
+}
+
+// Refills the empty front with the back keys below a threshold hi chosen so
+// that at most S of them (about S / 2) qualify: hi follows a sorted sample of
+// up to 32 qualifying keys (each lane takes the first one on its stride of
+// the back store), and is narrowed with a new sample while more than S keys
+// lie below it.  One pass then moves the keys below hi into the front, in
+// sorted batches of 32 staged in shared memory, and compacts the others in
+// place; hi becomes the fence.  Prunable keys are dropped.  Without a
+// threshold after four samples the whole back store is merged through.
+__device__ void seeds_refill(SeedQueue& s, uint64_t* bbuf, uint64_t cut) {
+  const int lane = threadIdx.x & 31;
+  const int n = s.nback;
+  if (n == 0) return;
+  uint64_t hi = ~0ull;
+  int c = n;  // an upper bound of the keys below hi
+  for (int round = 0; c > s.S; ++round) {
+    if (round == 4) {
+      seeds_refill_merge(s, bbuf, cut);
+      return;
+    }
+    uint64_t smp = ~0ull;
+    for (int p = lane; p < n; p += 32) {
+      const uint64_t key = s.back[p];
+      if (key < hi && !key_prunable(key, cut)) {
+        smp = key;
+        break;
+      }
+    }
+    const int ns = __popc(__ballot_sync(0xffffffffu, smp != ~0ull));
+    if (ns == 0) {  // every key prunable (c counted none) or none below hi
+      c = 0;
+      break;
+    }
+    const uint64_t sorted = warp_sort32(smp);
+    // about (r + 1) / ns of the c keys lie at or below the sample's r-th key
+    const int r = max(0, min(ns - 1, (int)(((long long)(s.S / 2) * ns) / c) - 1));
+    const uint64_t t = __shfl_sync(0xffffffffu, sorted, r);
+    hi = t + 1;  // t is a key (distinct, never ~0)
+    c = back_count(s, hi, cut);
+  }
+  uint64_t* stage = bbuf + 64;
+  int staged = 0, w = 0;
+  s.head = s.tail = 0;
+  s.fence = ~0ull;
+  auto flush = [&]() {
+    const uint64_t key = lane < staged ? stage[lane] : ~0ull;
+    __syncwarp();
+    uint64_t ev;
+    front_merge(s, bbuf, warp_sort32(key), staged, cut, ev);  // at most S keys in all: nothing leaves
+    staged = 0;
+  };
+  for (int c0 = 0; c0 < n; c0 += 32 * BACK_UNROLL) {
+    uint64_t keys[BACK_UNROLL];
+#pragma unroll
+    for (int u = 0; u < BACK_UNROLL; ++u) {
+      const int p = c0 + 32 * u + lane;
+      keys[u] = p < n ? s.back[p] : ~0ull;
+    }
+    __syncwarp();  // every chunk read before the in-place writes (w stays at or below c0 + 32 u)
+#pragma unroll
+    for (int u = 0; u < BACK_UNROLL; ++u) {
+      const uint64_t key = keys[u];
+      const bool live = key != ~0ull && !key_prunable(key, cut);
+      const bool sel = live && key < hi;
+      back_append(s, key, live && !sel, w, n);
+      const unsigned sm = __ballot_sync(0xffffffffu, sel);
+      if (staged + __popc(sm) > 32) flush();
+      if (sel) stage[staged + __popc(sm & ((1u << lane) - 1u))] = key;
+      staged += __popc(sm);
+      __syncwarp();
+    }
+  }
+  if (staged > 0) flush();
+  __syncwarp();
+  s.nback = w;
+  s.fence = w > 0 ? hi : ~0ull;
 }
 
 // tree_query_scale of a quantized query (lib.rs:283-296): max|q| / 127 of the
@@ -564,7 +670,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
     for (int t = lane; t < ix.Dp; t += 32) q[t] = t < ix.D ? Qrow[t] : 0.f;
   }
   const int vcap = W.vis1 ? W.vis1_cap : L.h;
-  Visited V{vis, vcap, W.vis2, W.vis2_cap, W.bits, false, false};
+  Visited V{vis, vcap, 0, W.vis2, W.vis2_cap, W.bits, false, false};
   if (W.bits) {
     uint4* b4 = reinterpret_cast<uint4*>(W.bits);  // words padded to a multiple of 4
     for (long long t = lane; t < ((long long)ix.N + 127) / 128; t += 32) b4[t] = make_uint4(0u, 0u, 0u, 0u);
@@ -663,6 +769,8 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
   float mx = result_max(res, rc);
   float bound = bound_of(mx);
   bool stopped = false;
+  int32_t pv = -1, pnb = -1;  // predicted next seed, this lane's first neighbor of it
+  int ps = 0, pe = 0;         // its CSR range
   while (true) {
     if (sq.head == sq.tail) {
       if (sq.nback == 0) break;
@@ -686,26 +794,64 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
     // a bounded pass stops as soon as its result is known to need the re-run
     if (!W.bits && (lost || V.lost)) break;
     ++expansions;
-    int s = ix.indptr[v], e = ix.indptr[v + 1];
+    int s, e;
+    int32_t nb_first;
+    if (v == pv) {  // loaded one expansion ahead
+      s = ps;
+      e = pe;
+      nb_first = pnb;
+    } else {
+      s = ix.indptr[v];
+      e = ix.indptr[v + 1];
+      nb_first = s + lane < e ? ix.indices[s + lane] : -1;
+    }
+    // the likely next seed (the front's first key, unless this expansion
+    // pushes a smaller one): its CSR range now, its first neighbors after the
+    // expansion, so that their latency overlaps this expansion
+    pv = sq.head < sq.tail ? (int32_t)(uint32_t)sq.front[(size_t)sq.cur * sq.stride + sq.head] : -1;
+    if (pv >= 0) {
+      ps = ix.indptr[pv];
+      pe = ix.indptr[pv + 1];
+    }
     for (int c0 = s; c0 < e; c0 += 32) {
       int c = c0 + lane;
-      int32_t nb = c < e ? ix.indices[c] : -1;
+      int32_t nb = c0 == s ? nb_first : (c < e ? ix.indices[c] : -1);
       const bool fresh = !visited_mark(V, nb, nb >= 0, overflow) && nb >= 0;
       float d = fresh ? dist_to<QUANT>(ix, q, q8, qinv, nb) : 0.f;
       unsigned m = __ballot_sync(0xffffffffu, fresh);
       evals += __popc(m);
       unsigned acc_mask = 0;
-      unsigned mm = m;
-      while (mm) {
-        int j = __ffs(mm) - 1;
-        mm &= mm - 1;
-        float dj = __shfl_sync(0xffffffffu, d, j);
-        if (dj < bound) {
-          int32_t ij = __shfl_sync(0xffffffffu, nb, j);
-          acc_mask |= 1u << j;
-          if (result_push(res, rc, k, dj, ij)) {
+      if (rc >= k) {
+        // With a full result list the maximum and the bound only shrink, and a
+        // neighbor enters the list only below the current maximum: those run in
+        // order; every neighbor is accepted against the bound left by the
+        // insertions of the neighbors before it (the reference's sequential test).
+        float my_bound = bound;
+        unsigned ins = __ballot_sync(0xffffffffu, fresh && d < mx);
+        while (ins) {
+          const int j = __ffs(ins) - 1;
+          ins &= ins - 1;
+          const float dj = __shfl_sync(0xffffffffu, d, j);
+          if (dj < bound && result_push(res, rc, k, dj, __shfl_sync(0xffffffffu, nb, j))) {
             mx = result_max(res, rc);
             bound = bound_of(mx);
+            if (lane > j) my_bound = bound;
+          }
+        }
+        acc_mask = __ballot_sync(0xffffffffu, fresh && d < my_bound);
+      } else {
+        unsigned mm = m;
+        while (mm) {
+          int j = __ffs(mm) - 1;
+          mm &= mm - 1;
+          float dj = __shfl_sync(0xffffffffu, d, j);
+          if (dj < bound) {
+            int32_t ij = __shfl_sync(0xffffffffu, nb, j);
+            acc_mask |= 1u << j;
+            if (result_push(res, rc, k, dj, ij)) {
+              mx = result_max(res, rc);
+              bound = bound_of(mx);
+            }
           }
         }
       }
@@ -713,6 +859,7 @@ __device__ bool search_one(const SearchIndex& ix, const float* Qrow, const int8_
       uint64_t sorted = warp_sort32(acc ? rkey(d, nb) : ~0ull);
       seeds_push(sq, bbuf, sorted, __popc(acc_mask), cut_of(bound));
     }
+    if (pv >= 0) pnb = ps + lane < pe ? ix.indices[ps + lane] : -1;
   }
   // seeds ran out: the unbounded search would go on with a dropped seed
   // within the bound
@@ -894,15 +1041,15 @@ int resident_blocks(const void* kernel, int threads, size_t smem) {
 
 // Per-warp global state of the passes.  Bounded pass: as many warps as are
 // resident (at most FIRST_BYTES of state), a second-level visited table of
-// 4x the shared table (2x the global first-level table for widths above 32)
-// and a back store of 16 S seeds.  Wide pass (queries the bounded pass lost):
+// 16x the shared table (4x the global first-level table for widths above 32)
+// and a back store of 64 S seeds.  Wide pass (queries the bounded pass lost):
 // WIDE_WARPS one-warp blocks with the same front (a merge costs S / 32 steps
 // a lane, so a larger front slows every expansion) and a visited table of
 // WIDE_VIS1 ids in shared memory, a second-level table of WIDE_VIS2 ids and a
 // back store of WIDE_BACK seeds.  Exact pass (queries the wide pass
 // lost): a visited bitset of N bits and a back store of N seeds per warp, as
 // many warps as fit EXACT_BYTES (at least one, at most EXACT_MAX_WARPS).
-constexpr size_t FIRST_BYTES = 512ull << 20;
+constexpr size_t FIRST_BYTES = 1024ull << 20;
 constexpr int WIDE_WARPS = 148;
 constexpr int WIDE_VIS1 = 1 << 13;
 constexpr int WIDE_VIS2 = 1 << 17;
@@ -934,8 +1081,8 @@ void run_search(const SearchIndex& ix, const float* Q, const int8_t* Q8, const f
 
   // bounded pass
   const int vis1 = L.h > 0 ? 0 : visited_capacity(L.kmax);
-  const int vis2 = L.h > 0 ? 4 * L.h : 2 * vis1;
-  const int back = 16 * L.s;
+  const int vis2 = L.h > 0 ? 16 * L.h : 4 * vis1;
+  const int back = 64 * L.s;
   const size_t per_warp = (size_t)vis1 * 4 + (size_t)vis2 * 4 + (size_t)back * 8;
   int blocks = std::min((nq + WPB - 1) / WPB, resident_blocks(kern, WPB * 32, L.bytes() * WPB));
   blocks = std::max(1, std::min<int>(blocks, (int)(FIRST_BYTES / (per_warp * WPB))));
