@@ -427,7 +427,7 @@ __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, cons
        e += (unsigned long long)gridDim.x * blockDim.x) {
     const unsigned long long x = spread ? spread_entry(e, n) : e;
     uint32_t r = urow[x];
-    if (row_push(slots + (size_t)r * kp, k, thr + r, ukey[x], &counters[1])) {
+    if (row_push_fast(slots + (size_t)r * kp, k, thr + r, ukey[x], &counters[1])) {
       ++mine;
       tally.add(ic, r);
     }
@@ -456,7 +456,7 @@ __global__ void k_apply_regions(const uint32_t* urow, const uint64_t* ukey, cons
   // in order are cheaper than spread ones)
   for (unsigned int e = part * blockDim.x + threadIdx.x; e < cnt; e += sub * blockDim.x) {
     const uint32_t row = urow[base + e];
-    if (row_push(slots + (size_t)row * kp, k, thr + row, ukey[base + e], &counters[1])) {
+    if (row_push_fast(slots + (size_t)row * kp, k, thr + row, ukey[base + e], &counters[1])) {
       ++mine;
       tally.add(ic, row);
     }
@@ -534,15 +534,19 @@ __global__ void __launch_bounds__(NT)
 // pushes) nor on which endpoint's row holds the edge, so a candidate offered
 // twice carries one key and the lists are a function of the rows' contents:
 // runs (and join precisions) from equal rows sample alike.
-__device__ __forceinline__ uint32_t cand_priority(uint64_t seed, int iter, int row, int32_t id) {
+// salt = cand_salt(seed, iter), computed once per iteration on the host.
+__host__ __device__ __forceinline__ uint64_t cand_salt(uint64_t seed, int iter) {
+  return seed ^ mix64(0xC0DE0000ull + (uint64_t)iter);
+}
+__device__ __forceinline__ uint32_t cand_priority(uint64_t salt, int row, int32_t id) {
   const uint32_t lo = (uint32_t)min(row, (int)id), hi = (uint32_t)max(row, (int)id);
   const uint64_t edge = ((uint64_t)lo << 32) | hi;
-  return (uint32_t)(mix64(seed ^ mix64(0xC0DE0000ull + (uint64_t)iter) ^ edge) >> 33);
+  return (uint32_t)(mix64(salt ^ edge) >> 33);
 }
 
 template <int P>
 __global__ void k_cand_forward(const uint64_t* slots, int N, int k, int kp, int c, int cp, uint64_t* cnew,
-                               uint64_t* cold, uint32_t* thr_new, uint32_t* thr_old, uint64_t seed, int iter,
+                               uint64_t* cold, uint32_t* thr_new, uint32_t* thr_old, uint64_t salt,
                                GroupRows grp) {
   __shared__ uint64_t buf[4][P];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -569,7 +573,7 @@ __global__ void k_cand_forward(const uint64_t* slots, int N, int k, int kp, int 
         uint64_t sl = slots[(size_t)row * kp + j];
         int32_t id = slot_id(sl);
         if (id >= 0 && slot_new(sl) == flag)
-          key = ((uint64_t)cand_priority(seed, iter, row, id) << 32) | (uint32_t)id;
+          key = ((uint64_t)cand_priority(salt, row, id) << 32) | (uint32_t)id;
       }
       n += __popc(__ballot_sync(0xffffffffu, key != ~0ull));
       b[j] = key;
@@ -617,20 +621,24 @@ __global__ void k_cand_forward(const uint64_t* slots, int N, int k, int kp, int 
   }
 }
 
+// One warp per row (lane = slot): each of the row's entries is offered to its
+// neighbor's list.
 __global__ void k_cand_reverse(const uint64_t* slots, int N, int k, int kp, int c, int cp, uint64_t* cnew,
-                               uint64_t* cold, uint32_t* thr_new, uint32_t* thr_old, uint64_t seed, int iter,
+                               uint64_t* cold, uint32_t* thr_new, uint32_t* thr_old, uint64_t salt,
                                unsigned long long* contention, GroupRows grp) {
-  long long total = (long long)N * k;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    int32_t i = (int32_t)(e / k);
-    int j = (int)(e % k);
-    uint64_t sl = slots[(size_t)i * kp + j];
-    int32_t id = slot_id(sl);
-    if (id < 0 || grp.frozen(i)) continue;  // (a frozen row's neighbors are frozen rows too)
-    const bool nw = slot_new(sl);
-    uint64_t key = ((uint64_t)cand_priority(seed, iter, i, id) << 32) | (uint32_t)i;
-    row_push_fast((nw ? cnew : cold) + (size_t)id * cp, c, (nw ? thr_new : thr_old) + id, key, contention);
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < N; r += nwarps) {
+    const int32_t i = (int32_t)r;
+    if (grp.frozen(i)) continue;  // (a frozen row's neighbors are frozen rows too)
+    for (int j = lane; j < k; j += 32) {
+      const uint64_t sl = slots[(size_t)i * kp + j];
+      const int32_t id = slot_id(sl);
+      if (id < 0) continue;
+      const bool nw = slot_new(sl);
+      const uint64_t key = ((uint64_t)cand_priority(salt, i, id) << 32) | (uint32_t)i;
+      row_push_fast((nw ? cnew : cold) + (size_t)id * cp, c, (nw ? thr_new : thr_old) + id, key, contention);
+    }
   }
 }
 
@@ -823,21 +831,21 @@ void build_candidates(KnnState& s, uint64_t seed, int iter, cudaStream_t st) {
   candidates_reserve(s, st);
   uint32_t* thr_new = s.cthr.p;
   uint32_t* thr_old = s.cthr.p + s.N;
+  const uint64_t salt = cand_salt(seed, iter);
   const int grid = (s.N + 3) / 4;
   if (s.k <= 32)
     k_cand_forward<32><<<grid, 128, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p,
-                                             thr_new, thr_old, seed, iter, s.group_rows());
+                                             thr_new, thr_old, salt, s.group_rows());
   else if (s.k <= 64)
     k_cand_forward<64><<<grid, 128, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p,
-                                             thr_new, thr_old, seed, iter, s.group_rows());
+                                             thr_new, thr_old, salt, s.group_rows());
   else
     k_cand_forward<128><<<grid, 128, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p,
-                                              thr_new, thr_old, seed, iter, s.group_rows());
+                                              thr_new, thr_old, salt, s.group_rows());
   RINND_LAUNCH_CHECK();
-  long long total = (long long)s.N * s.k;
-  k_cand_reverse<<<grid_for(total, 256, 148 * 64), 256, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.c, s.cp,
-                                                                s.cand_new.p, s.cand_old.p, thr_new, thr_old,
-                                                                seed, iter, &s.counters.p[1], s.group_rows());
+  k_cand_reverse<<<grid_for((long long)s.N * 32, 256, 148 * 64), 256, 0, st>>>(
+      s.slots.p, s.N, s.k, s.kp, s.c, s.cp, s.cand_new.p, s.cand_old.p, thr_new, thr_old, salt, &s.counters.p[1],
+      s.group_rows());
   RINND_LAUNCH_CHECK();
   k_mark_old<<<grid_for((long long)s.N * 32, 256), 256, 0, st>>>(s.slots.p, s.N, s.k, s.kp, s.cand_new.p,
                                                                  s.c, s.cp);
