@@ -628,7 +628,7 @@ def run_serving(args, world, rank, local_rank):
     def serve(ix, reqs, rate_qps=None):
         """Submits the requests (all at once, or Poisson at rate_qps queries/s) and collects
         them; returns (wall seconds, server stats)."""
-        srv = rinnd_b200.Server(ix, max_batch_queries=4096, max_inflight=4, quantized=True)
+        srv = rinnd_b200.Server(ix, quantized=True)  # default batch shape: 32768 queries, 8 in flight
         ids = []
         done = []
 

@@ -344,8 +344,8 @@ RINND_EXPORT int rinnd_quantize_rows(const float* data, int64_t n, int32_t d, in
  * with the server's widths (quantized = 1, a quantized index) run alone.  The
  * index must outlive the server; submit and poll may be called from any thread. */
 typedef struct rinnd_server_params {
-  int32_t max_batch_queries;     /* queries per device batch, default 4096             */
-  int32_t max_inflight;          /* batches on the device at once, default 4           */
+  int32_t max_batch_queries;     /* queries per device batch, default 32768            */
+  int32_t max_inflight;          /* batches on the device at once, default 8           */
   int32_t max_k;                 /* largest k accepted, default 256 (sizes the buffers) */
   int32_t quantized;             /* 1: int8 search (+ exact rerank) on a quantized index */
   int32_t candidate_width;       /* quantized widths, rules of core/index.rs:55-89      */

@@ -499,7 +499,7 @@ class Server:
     index's widths, for a quantized index) run alone.  The index is kept alive
     by the server."""
 
-    def __init__(self, index, max_batch_queries=4096, max_inflight=4, max_k=256, max_pending_queries=1 << 22,
+    def __init__(self, index, max_batch_queries=32768, max_inflight=8, max_k=256, max_pending_queries=1 << 22,
                  quantized=None):
         self._s = None
         self.index = index

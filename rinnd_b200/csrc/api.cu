@@ -1137,8 +1137,8 @@ int rinnd_search_stats_get(rinnd_index* idx, uint64_t* evaluations, uint64_t* ex
 int rinnd_server_params_default(rinnd_server_params* p) {
   if (!p) return fail(RINND_ERR_INVALID, "params must not be null");
   std::memset(p, 0, sizeof(*p));
-  p->max_batch_queries = 4096;
-  p->max_inflight = 4;
+  p->max_batch_queries = 32768;
+  p->max_inflight = 8;
   p->max_k = 256;
   p->max_pending_queries = 1ll << 22;
   return RINND_OK;
