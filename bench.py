@@ -17,7 +17,10 @@ data path); the max over ranks of the device-timed region is reported.
 --impl reference: the reference's CPU algorithm (the C++ restatement under
 oracle/, all host threads) on the same full workload, one build per step.
 The default run also builds that oracle index once (the `cpu_baseline` leg)
-and reports its recall beside the GPU's, on the same sample and queries.
+and reports its recall beside the GPU's, on the same sample and queries, and
+(one GPU) adds `forms`: the batched form (512 indices, two warm-up calls, one
+timed) and the serving form (10M x 96, int8 per-vector width 100 server,
+2 s per offered load) in compact runs of --workload batched / serving.
 """
 from __future__ import annotations
 
@@ -71,6 +74,8 @@ def parse_args():
                          "BF16 join forms at 1M x 960 cosine with distance error vs FP64")
     ap.add_argument("--serve-n", type=int, default=10_000_000, help="serving workload: index size")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="serving workload: seconds per offered load")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="build workload: skip the compact batched and serving measurements added to the line")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"],
                     help="local-join tiles of the timed builds (the precision form is also reported beside fp32)")
     ap.add_argument("--join-tuning", default="table", choices=["table", "fixed", "retune"],
@@ -238,10 +243,11 @@ def batched_specs(n_items, seed=0):
     return specs
 
 
-def run_batched(args, world, rank, local_rank):
+def run_batched(args, world, rank, local_rank, emit=True):
     """The batched form: this rank's longest-first share of the indices built
     in one rinnd_build_many call from device-resident data; timed with CUDA
-    events, max over ranks; beside it the same share built one index at a time."""
+    events, max over ranks; beside it the same share built one index at a time.
+    Returns the line (rank 0)."""
     import datetime
 
     import torch
@@ -388,9 +394,11 @@ def run_batched(args, world, rank, local_rank):
             "speedup_vs_one_at_a_time": t_one / t_batch, "speedup_vs_stream_per_index": t_streams / t_batch,
             "groups": groups, "quality": quality,
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+    return line if rank == 0 else None
 
 
 PREC_D, PREC_K, PREC_SAMPLE = 960, 15, 4000
@@ -561,7 +569,7 @@ def run_precision(args, world, rank, local_rank):
         dist.destroy_process_group()
 
 
-def run_serving(args, world, rank, local_rank):
+def run_serving(args, world, rank, local_rank, emit=True, compact=False):
     """The serving form on one GPU (replicas per rank otherwise): a 10M x 96
     index of L2-normalised Gaussian-mixture rows (1000 clusters), cosine, k=30,
     built with the BF16 join (FP32 recheck); int8 per-dimension search codes
@@ -569,7 +577,9 @@ def run_serving(args, world, rank, local_rank):
     Request sizes are log-uniform in [1, 4096], k in {10, 100}, epsilon 0.1,
     arrivals Poisson at 0.5 / 0.8 / 0.95 of the measured saturated QPS.  Beside
     it, the plain FP32 search (no codes, no server) at several epsilons and
-    widths, to compare throughput at equal recall@10."""
+    widths, to compare throughput at equal recall@10.  compact: the per-vector
+    int8 server alone (the one the value is taken from when it reaches recall
+    0.95), for the summary inside the default bench line.  Returns the line."""
     import torch
 
     import rinnd_b200
@@ -695,8 +705,8 @@ def run_serving(args, world, rank, local_rank):
 
     # the per-dimension codes the configuration names, at the widest width the
     # search takes, and the per-vector int8 codes at width 100
-    servers = [serving_config("int8 per-dimension (sq8d)", L.Q8_PER_DIMENSION, 256, 256),
-               serving_config("int8 per-vector (int8)", L.Q8_PER_VECTOR_COSINE, 100, 100)]
+    servers = [] if compact else [serving_config("int8 per-dimension (sq8d)", L.Q8_PER_DIMENSION, 256, 256)]
+    servers.append(serving_config("int8 per-vector (int8)", L.Q8_PER_VECTOR_COSINE, 100, 100))
     # the plain FP32 search (rinnd_query_device, 10k queries) at several operating
     # points: result width k (top 10 of it scored) and epsilon
     fp32_points = []
@@ -718,6 +728,7 @@ def run_serving(args, world, rank, local_rank):
         srv_cfg["plain_fp32_at_equal_recall"] = max(reach, key=lambda pnt: pnt["qps"]) if reach else None
     at_target = [c for c in servers if c["recall@10"] >= 0.95]
     head = max(at_target, key=lambda c: c["saturated"]["qps"]) if at_target else servers[0]
+    line = None
     if rank == 0:
         line = {
             "metric": "serving QPS and p50/p99 latency at recall@10 (10M x 96, int8 + FP32 rerank)",
@@ -732,8 +743,10 @@ def run_serving(args, world, rank, local_rank):
             "build_s": t_build, "servers": servers, "recall_sample_queries": ns,
             "plain_fp32_search": fp32_points,
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     L.check(L.lib.rinnd_free(h))
+    return line
 
 
 def main():
@@ -993,6 +1006,22 @@ def main():
             quality["parity_query_recall_gap"] = quality["query_recall@10"] - quality["oracle_query_recall@10"]
         del oix
 
+    # ---- the batched and serving forms, compact, on one GPU: their numbers in
+    # this line (the full workloads: --workload batched / serving) ----
+    forms = {}
+    if world == 1 and rank == 0 and not args.no_forms:
+        del X_dev, Q_dev
+        torch.cuda.empty_cache()
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup, sub.check_items, sub.precision, sub.serve_seconds = 1, 2, 4, "fp32", 2.0
+        for name, fn in (("batched", lambda: run_batched(sub, 1, 0, local_rank, emit=False)),
+                         ("serving", lambda: run_serving(sub, 1, 0, local_rank, emit=False, compact=True))):
+            try:
+                forms[name] = fn()
+            except Exception as exc:  # reported in the line, the build numbers stand
+                forms[name] = {"error": f"{type(exc).__name__}: {exc}"}
+            torch.cuda.empty_cache()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
@@ -1018,6 +1047,7 @@ def main():
             "phases_ms": {"forest": inf.ms_forest, "leaf_init": inf.ms_leaf_init, "iterations": inf.ms_iterations,
                           "candidates": inf.ms_candidates, "join": inf.ms_join, "sort": inf.ms_sort,
                           "graph": inf.ms_graph, "total": inf.ms_total},
+            **({"forms": forms} if forms else {}),
         }
         print(json.dumps(line), flush=True)
     if world > 1:
