@@ -19,8 +19,10 @@ oracle/, all host threads) on the same full workload, one build per step.
 The default run also builds that oracle index once (the `cpu_baseline` leg)
 and reports its recall beside the GPU's, on the same sample and queries, and
 (one GPU) adds `forms`: the batched form (512 indices, two warm-up calls, one
-timed) and the serving form (10M x 96, int8 per-vector width 100 server,
-2 s per offered load) in compact runs of --workload batched / serving.
+timed), the serving form (10M x 96, int8 per-vector width 100 server, 2 s per
+offered load) and the precision form (1M x 960 cosine, FP32 and BF16 builds,
+without the oracle parity sizes) in compact runs of --workload batched /
+serving / precision.
 """
 from __future__ import annotations
 
@@ -405,14 +407,16 @@ PREC_D, PREC_K, PREC_SAMPLE = 960, 15, 4000
 PREC_PARITY_SIZES = (20_000, 100_000)
 
 
-def run_precision(args, world, rank, local_rank):
+def run_precision(args, world, rank, local_rank, emit=True, compact=False):
     """The precision workload: N x 960 rows with entries |N(0,1)|^1.5,
     L2-normalised, cosine, k=15, built with FP32 join tiles and with the BF16
     precision form (which falls back to FP32 tiles where its tensor-core join
     does not apply; `join_form` says which kernel ran).  Reports each form's
     build points/s, recall@15 against FP64 exact kNN on a seeded sample of rows,
     and the error of the reported neighbor distances against the same pairs'
-    cosine distances recomputed in FP64.  Replicas on N > 1 ranks."""
+    cosine distances recomputed in FP64.  Replicas on N > 1 ranks.  compact:
+    without the oracle parity builds (for the default bench line).  Returns
+    the line (rank 0)."""
     import datetime
 
     import torch
@@ -507,7 +511,7 @@ def run_precision(args, world, rank, local_rank):
     # n_s rows, for each n_s in PREC_PARITY_SIZES, is the yardstick: both builds
     # see the same rows and are scored on the same seeded sample of them.
     parity = []
-    if rank == 0 and not args.no_recall:
+    if rank == 0 and not args.no_recall and not compact:
         import oracle
 
         for n_s in [m for m in PREC_PARITY_SIZES if m <= n]:
@@ -564,9 +568,11 @@ def run_precision(args, world, rank, local_rank):
             "bf16_speedup_vs_fp32": forms["fp32"]["ms_per_build"] / forms["bf16"]["ms_per_build"],
             "parity_by_size": parity,
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+    return line if rank == 0 else None
 
 
 def run_serving(args, world, rank, local_rank, emit=True, compact=False):
@@ -1015,7 +1021,8 @@ def main():
         sub = argparse.Namespace(**vars(args))
         sub.steps, sub.warmup, sub.check_items, sub.precision, sub.serve_seconds = 1, 2, 4, "fp32", 2.0
         for name, fn in (("batched", lambda: run_batched(sub, 1, 0, local_rank, emit=False)),
-                         ("serving", lambda: run_serving(sub, 1, 0, local_rank, emit=False, compact=True))):
+                         ("serving", lambda: run_serving(sub, 1, 0, local_rank, emit=False, compact=True)),
+                         ("precision", lambda: run_precision(sub, 1, 0, local_rank, emit=False, compact=True))):
             try:
                 forms[name] = fn()
             except Exception as exc:  # reported in the line, the build numbers stand
