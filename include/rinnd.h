@@ -405,6 +405,25 @@ RINND_EXPORT int rinnd_storage_info_get(const rinnd_index* idx, rinnd_storage_in
  * reference accumulation order, core/distance/*.rs. */
 RINND_EXPORT int rinnd_distance_pairs(int32_t kind, const float* a, const float* b, int64_t n_pairs, int32_t d,
                          float* out);
+/* Brute-force exact kNN.  No counterpart in the reference, which has no exact
+ * pass; its recall criteria are measured against these neighbors.  For each of
+ * nq query rows, the k data rows of smallest (distance, id), ascending, padded
+ * with (-1, +inf) when n < k.  data: n x d floats with row stride ld_data,
+ * queries: nq x d with stride ld_queries; on the current device when on_device
+ * != 0 (outputs are then device pointers too), else host memory.
+ * distance_kind: RINND_DIST_SQEUCLIDEAN, _MANHATTAN, _INNER_PRODUCT, _COSINE or
+ * _DIRECT_COSINE.  precision: RINND_BRUTE_FP32 (the FP32 join's per-pair
+ * arithmetic, so distances equal the build's) or RINND_BRUTE_FP64 (every term
+ * in double: the checker the FP32 form's ids are compared with).  exclude_ids
+ * (nullable, nq entries): query i leaves out data row exclude_ids[i] (the kNN
+ * graph of the data itself).  k in [1, 128]. */
+#define RINND_BRUTE_FP32 0
+#define RINND_BRUTE_FP64 2
+RINND_EXPORT int rinnd_brute_force_knn(const float* data, int64_t n, int64_t ld_data, const float* queries,
+                                       int64_t nq, int64_t ld_queries, int32_t d, int32_t k, int32_t distance_kind,
+                                       int32_t precision, const int32_t* exclude_ids, int32_t on_device,
+                                       int32_t* out_idx, float* out_dist);
+
 /* SearchGraph::from_dense_diversified (core/graph/search_graph.rs:263-360) on a
  * host kNN graph (n x k, ascending rows, -1 padding) over host data (n x d).
  * indices must hold n * round(mult * k) entries; *nnz receives the edge count. */

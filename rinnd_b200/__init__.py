@@ -74,6 +74,45 @@ def device_count() -> int:
     return L.device_count()
 
 
+_BRUTE_METRICS = {"sqeuclidean": (L.DIST_SQEUCLIDEAN, False), "euclidean": (L.DIST_SQEUCLIDEAN, True),
+                  "l2": (L.DIST_SQEUCLIDEAN, True), "manhattan": (L.DIST_MANHATTAN, False),
+                  "l1": (L.DIST_MANHATTAN, False), "taxicab": (L.DIST_MANHATTAN, False),
+                  "cosine": (L.DIST_COSINE, False), "inner_product": (L.DIST_INNER_PRODUCT, False),
+                  "dot": (L.DIST_INNER_PRODUCT, False)}
+
+
+def brute_force_knn(data, queries, k=10, metric="sqeuclidean", precision="fp32", exclude_self=False):
+    """Exact k nearest data rows of every query row, by (distance, id) ascending
+    (no counterpart in the reference; its recall criteria are measured against
+    these).  precision "fp32" computes each distance with the build's FP32 join
+    arithmetic, "fp64" in double (the checker).  exclude_self leaves out data
+    row i for query i (queries must then be the data rows themselves).
+    Returns (int32[nq, k], float32[nq, k]), padded with (-1, inf) when k > n."""
+    if metric not in _BRUTE_METRICS:
+        raise ValueError(f"Unknown metric for brute force: {metric}")
+    kind, take_sqrt = _BRUTE_METRICS[metric]
+    X = np.ascontiguousarray(_as_f32_2d(data, "data"))
+    Q = np.ascontiguousarray(_as_f32_2d(queries, "queries"))
+    if Q.shape[1] != X.shape[1]:
+        raise ValueError(f"Query dimension {Q.shape[1]} does not match data dimension {X.shape[1]}")
+    if precision not in ("fp32", "fp64"):
+        raise ValueError("precision must be 'fp32' or 'fp64'")
+    nq = Q.shape[0]
+    excl = None
+    if exclude_self:
+        if nq > X.shape[0]:
+            raise ValueError("exclude_self needs the queries to be the first rows of the data")
+        excl = np.arange(nq, dtype=np.int32)
+    oi = np.empty((nq, int(k)), np.int32)
+    od = np.empty((nq, int(k)), np.float32)
+    L.check(L.lib.rinnd_brute_force_knn(L.ptr(X), X.shape[0], X.shape[1], L.ptr(Q), nq, Q.shape[1], X.shape[1],
+                                        int(k), kind, L.BRUTE_FP32 if precision == "fp32" else L.BRUTE_FP64,
+                                        L.ptr(excl) if excl is not None else None, 0, L.ptr(oi), L.ptr(od)))
+    if take_sqrt:
+        od = np.sqrt(od)
+    return oi, od
+
+
 def _as_f32_2d(a, what="data") -> np.ndarray:
     a = np.asarray(a)
     if a.dtype != np.float32:

@@ -30,6 +30,7 @@ Q8_PER_VECTOR_COSINE, Q8_GLOBAL_SYMMETRIC, Q8_PER_VECTOR_SYMMETRIC, Q8_PER_DIMEN
 PRECISION_FP32, PRECISION_BF16 = range(2)
 TUNE_TABLE, TUNE_FIXED, TUNE_RETUNE = range(3)
 JOIN_CHUNKED_FP32, JOIN_PIPELINED_FP32, JOIN_TENSOR_BF16 = range(3)  # rinnd_build_info.join_form
+BRUTE_FP32, BRUTE_FP64 = 0, 2  # rinnd_brute_force_knn precision
 
 _i32, _i64, _u64, _f32, _f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_float, ctypes.c_double
 _P = ctypes.c_void_p
@@ -131,6 +132,7 @@ SIGNATURES = {
     "rinnd_server_destroy": (ctypes.c_int, [_P]),
     "rinnd_storage_info_get": (ctypes.c_int, [_P, _P]),
     "rinnd_distance_pairs": (ctypes.c_int, [_i32, _P, _P, _i64, _i32, _P]),
+    "rinnd_brute_force_knn": (ctypes.c_int, [_P, _i64, _i64, _P, _i64, _i64, _i32, _i32, _i32, _i32, _P, _i32, _P, _P]),
     "rinnd_search_graph_from_knn": (ctypes.c_int, [_P, _P, _P, _i32, _i32, _i32, _i32, _f32, _P, _P, _P, _P]),
     "rinnd_heap_push_batch": (ctypes.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rinnd_nndescent_step": (ctypes.c_int, [_P, _i64, _i32, _i32, _i32, _i32, _i32, _u64, _i32, _P, _P, _P, _P, _P]),

@@ -1487,6 +1487,56 @@ int rinnd_distance_pairs(int32_t kind, const float* a, const float* b, int64_t n
   });
 }
 
+int rinnd_brute_force_knn(const float* data, int64_t n, int64_t ld_data, const float* queries, int64_t nq,
+                          int64_t ld_queries, int32_t d, int32_t k, int32_t distance_kind, int32_t precision,
+                          const int32_t* exclude_ids, int32_t on_device, int32_t* out_idx, float* out_dist) {
+  return guarded([&] {
+    require(n >= 1 && nq >= 0 && d >= 1, "invalid shape");
+    require(n < (int64_t)INT32_MAX - 1 && nq < (int64_t)INT32_MAX, "too many rows");
+    require(ld_data >= d && ld_queries >= d, "row stride smaller than the dimension");
+    require(k >= 1 && k <= 128, "k must be in [1, 128]");
+    require(precision == RINND_BRUTE_FP32 || precision == RINND_BRUTE_FP64, "precision must be FP32 or FP64");
+    require(distance_kind >= 0 && distance_kind < DK_COUNT && brute_supported(distance_kind),
+            "brute force supports squared Euclidean, Manhattan, inner product, cosine and direct cosine");
+    if (nq == 0) return;
+    require(data && queries && out_idx && out_dist, "pointers must not be null");
+    int dev = 0;
+    if (on_device) RINND_CUDA(cudaGetDevice(&dev));
+    ensure_device(dev);
+    StreamGuard sg;
+    const int Dp = round_up(d, 4);
+    DVec<float> X, Q;
+    load_rows(data, on_device != 0, n, d, ld_data, Dp, X, sg.s);
+    load_rows(queries, on_device != 0, nq, d, ld_queries, Dp, Q, sg.s);
+    DVec<int32_t> ex, oi;
+    DVec<float> od;
+    const int32_t* excl = nullptr;
+    if (exclude_ids) {
+      if (on_device) {
+        excl = exclude_ids;
+      } else {
+        ex.alloc((size_t)nq, sg.s);
+        RINND_CUDA(cudaMemcpyAsync(ex.p, exclude_ids, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, sg.s));
+        excl = ex.p;
+      }
+    }
+    int32_t* pi = out_idx;
+    float* pd = out_dist;
+    if (!on_device) {
+      oi.alloc((size_t)nq * k, sg.s);
+      od.alloc((size_t)nq * k, sg.s);
+      pi = oi.p;
+      pd = od.p;
+    }
+    brute_force_knn(Q.p, (int)nq, X.p, n, Dp, k, distance_kind, precision, excl, pi, pd, sg.s);
+    if (!on_device) {
+      oi.to_host(out_idx, (size_t)nq * k);
+      od.to_host(out_dist, (size_t)nq * k);
+    }
+    RINND_CUDA(cudaStreamSynchronize(sg.s));
+  });
+}
+
 int rinnd_search_graph_from_knn(const int32_t* knn_idx, const float* knn_dist, const float* data, int32_t n,
                                 int32_t k, int32_t d, int32_t kind, float mult, int32_t* indptr,
                                 int32_t* indices, int64_t* nnz, float* min_distance) {

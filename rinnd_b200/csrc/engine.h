@@ -267,6 +267,13 @@ void greedy_search_packed(const SearchIndex& ix, const float* Q, const int8_t* Q
 // rows; with Q8, their int8 codes route over the int8 routing trees): up to
 // `budget` leaves (start, end) per query into out_leaves (nq x budget x 2) and
 // the count into out_counts.
+// ---- brute-force exact kNN (brute.cu) ---------------------------------------
+// Q: nq x Dp, X: n x Dp (device, Dp a multiple of 4); precision 0 FP32, 2 FP64;
+// excl (nullable): per query a row to leave out.  out: nq x k, ascending.
+bool brute_supported(int kind);
+void brute_force_knn(const float* Q, int nq, const float* X, long long n, int Dp, int k, int kind, int precision,
+                     const int32_t* excl, int32_t* out_idx, float* out_dist, cudaStream_t st);
+
 void tree_leaves(const SearchIndex& ix, const float* Q, const int8_t* Q8, int nq, int tree, int budget,
                  uint64_t qid_base, int32_t* out_leaves, int32_t* out_counts, cudaStream_t st,
                  unsigned long long* dstats);

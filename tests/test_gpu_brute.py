@@ -1,0 +1,129 @@
+"""Brute-force exact kNN (rinnd_brute_force_knn) against exact references.
+
+The FP64 form is checked against numpy in float64 on small inputs, and the
+FP32 form against the FP64 form at larger ones: "bit-exact ids wherever the
+distances are untied" -- a query's ids must match position by position when
+the FP64 distances of its first k + 1 neighbors are separated by more than
+8 FP32 ulps of the computation's magnitude (the distance itself for sums of
+non-negative terms, |x| |q| for the inner product, 1 for the cosine distance
+1 - cos, whose FP32 error is of the order of ulp(1) however small it is), and
+its FP32 distances must lie within 1e-5 of the FP64 ones on that scale.  The FP32 form computes each distance with the build's join
+arithmetic, so its distances also agree with the reference's distance
+functions (the oracle) within the build's 1e-5 tolerance.
+"""
+import numpy as np
+import pytest
+
+from helpers import gmm
+
+pytestmark = pytest.mark.gpu
+
+METRICS = ["sqeuclidean", "manhattan", "inner_product", "cosine"]
+
+
+def numpy_knn(X, Q, k, metric, exclude_self=False):
+    X = X.astype(np.float64)
+    Q = Q.astype(np.float64)
+    if metric == "sqeuclidean":  # the expansion in float64: far below the ties' 1e-12 threshold here
+        D = (Q * Q).sum(1)[:, None] + (X * X).sum(1)[None, :] - 2.0 * (Q @ X.T)
+    elif metric == "manhattan":
+        D = np.abs(Q[:, None, :] - X[None, :, :]).sum(-1)
+    elif metric == "inner_product":
+        D = -(Q @ X.T)
+    else:
+        den = np.sqrt((Q * Q).sum(1)[:, None] * (X * X).sum(1)[None, :])
+        D = np.where(den < 1e-12, 1.0, 1.0 - np.clip((Q @ X.T) / np.maximum(den, 1e-300), -1.0, 1.0))
+    if exclude_self:
+        D[np.arange(len(Q)), np.arange(len(Q))] = np.inf
+    ids = np.arange(X.shape[0])
+    order = np.stack([np.lexsort((ids, row)) for row in D])
+    return order[:, :k].astype(np.int32), np.take_along_axis(D, order[:, :k + 1], 1)
+
+
+def untied(d, rel, scale=None):
+    """Rows whose first len(d[0]) distances are each separated by more than
+    rel x scale (scale: the distances' magnitudes unless given)."""
+    gaps = np.diff(d, axis=1)
+    scale = np.maximum(np.abs(d[:, 1:]) if scale is None else scale[:, 1:], 1e-30)
+    return np.all(gaps > rel * scale, axis=1)
+
+
+@pytest.mark.parametrize("metric", METRICS)
+def test_fp64_equals_numpy_float64(rb, metric):
+    rng = np.random.default_rng(3)
+    X = rng.normal(0.0, 1.0, (3000, 37)).astype(np.float32)
+    Q = rng.normal(0.0, 1.0, (150, 37)).astype(np.float32)
+    gi, gd = rb.brute_force_knn(X, Q, k=10, metric=metric, precision="fp64")
+    ni, nd = numpy_knn(X, Q, 10, metric)
+    ok = untied(nd, 1e-12)
+    assert ok.mean() > 0.99
+    np.testing.assert_array_equal(gi[ok], ni[ok])
+    np.testing.assert_allclose(gd, nd[:, :10].astype(np.float32), rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("metric", METRICS)
+def test_fp32_ids_match_fp64_wherever_untied(rb, orc, metric):
+    X = gmm(60000, 128, 50, seed=21)
+    Q = gmm(60000 + 1500, 128, 50, seed=21)[60000:]
+    fi, fd = rb.brute_force_knn(X, Q, k=15, metric=metric, precision="fp32")
+    di, dd = rb.brute_force_knn(X, Q, k=16, metric=metric, precision="fp64")
+    # the FP64 distances of the first k + 1 neighbors, as float64 from the checker's ids
+    Xd, Qd = X.astype(np.float64), Q.astype(np.float64)
+    nb = Xd[di]
+    if metric == "sqeuclidean":
+        d64 = ((nb - Qd[:, None, :]) ** 2).sum(-1)
+        scale = np.abs(d64)
+    elif metric == "manhattan":
+        d64 = np.abs(nb - Qd[:, None, :]).sum(-1)
+        scale = np.abs(d64)
+    elif metric == "inner_product":
+        d64 = -(nb * Qd[:, None, :]).sum(-1)
+        scale = np.sqrt((nb * nb).sum(-1) * (Qd * Qd).sum(-1)[:, None])
+    else:
+        d64 = 1.0 - (nb * Qd[:, None, :]).sum(-1) / np.sqrt((nb * nb).sum(-1) * (Qd * Qd).sum(-1)[:, None])
+        scale = np.maximum(np.abs(d64), 1.0)
+    ok = untied(d64, 8 * 2.0 ** -23, scale)
+    assert ok.mean() > 0.5, ok.mean()
+    np.testing.assert_array_equal(fi[ok], di[ok, :15])
+    err = np.abs(fd.astype(np.float64) - d64[:, :15]) / np.maximum(scale[:, :15], 1e-30)
+    assert err.max() < 1e-5, err.max()
+    # every reported FP32 distance against the reference's distance function (the oracle)
+    kinds = {"sqeuclidean": orc.SQEUCLIDEAN, "manhattan": orc.MANHATTAN, "inner_product": orc.INNER_PRODUCT,
+             "cosine": orc.COSINE}
+    rows = np.repeat(np.arange(len(Q)), 15)
+    ref = orc.distance_pairs(kinds[metric], np.ascontiguousarray(Q[rows]), np.ascontiguousarray(X[fi.reshape(-1)]))
+    np.testing.assert_allclose(fd.reshape(-1), ref, rtol=1e-5, atol=1e-5)
+
+
+def test_exclude_self_and_split_rows(rb):
+    X = gmm(20000, 64, 20, seed=5)
+    # the data's own kNN graph: no row is its own neighbor
+    gi, gd = rb.brute_force_knn(X, X[:500], k=12, metric="sqeuclidean", exclude_self=True)
+    assert not np.any(gi == np.arange(500)[:, None])
+    ni, nd = numpy_knn(X, X[:500], 12, "sqeuclidean", exclude_self=True)
+    ok = untied(nd, 8 * 2.0 ** -23)
+    np.testing.assert_array_equal(gi[ok], ni[ok])
+    # a few queries (their rows split over many CTAs and merged) give the same
+    # results as inside a large batch (one CTA per query tile)
+    Q = gmm(20000 + 3000, 64, 20, seed=5)[20000:]
+    bi, bd = rb.brute_force_knn(X, Q, k=12)
+    for sel in (np.arange(3), np.arange(1000, 1037)):
+        si, sd = rb.brute_force_knn(X, Q[sel], k=12)
+        np.testing.assert_array_equal(si, bi[sel])
+        np.testing.assert_array_equal(sd.view(np.uint32), bd[sel].view(np.uint32))
+
+
+def test_k_above_n_and_errors(rb):
+    rng = np.random.default_rng(1)
+    X = rng.normal(0.0, 1.0, (5, 8)).astype(np.float32)
+    Q = rng.normal(0.0, 1.0, (4, 8)).astype(np.float32)
+    gi, gd = rb.brute_force_knn(X, Q, k=8)
+    assert np.all(np.sort(gi[:, :5], axis=1) == np.arange(5))
+    assert np.all(gi[:, 5:] == -1) and np.all(np.isinf(gd[:, 5:]))
+    assert np.all(np.diff(gd[:, :5], axis=1) >= 0)
+    with pytest.raises(ValueError):
+        rb.brute_force_knn(X, Q, k=129)
+    with pytest.raises(ValueError):
+        rb.brute_force_knn(X, Q, k=3, metric="hamming")
+    with pytest.raises(ValueError):
+        rb.brute_force_knn(X, Q[:, :7], k=3)
