@@ -4,12 +4,13 @@
 // neighbors are what its recall criteria are measured against.  For each
 // query the k rows of smallest (distance, id), in that order.
 //
-// Tiles.  A CTA holds 32 queries and walks its share of the rows in chunks
-// of 64 (the rows of a large call are split over gridDim.y CTAs per query
-// tile when there are few query tiles, and the splits merged after).  Query
-// and row tiles are staged in shared memory 64 dimensions at a time, so any D
-// fits; each thread accumulates a 2 x 4 block of (query, row) pairs.  Two
-// arithmetics:
+// Tiles.  A CTA holds 64 queries (FP32; 32 in FP64) and walks its share of
+// the rows in chunks of 64 (the rows of a large call are split over gridDim.y
+// CTAs per query tile when there are few query tiles, and the splits merged
+// after).  Query and row tiles are staged in shared memory 64 dimensions at a
+// time, so any D fits; each thread accumulates a 4 x 4 (2 x 4) block of
+// (query, row) pairs, its rows 16 apart so a warp's 16-byte reads of them
+// spread over all banks.  Two arithmetics:
 //   FP32: the FP32 join's per-pair arithmetic (join_dist_fp32: packed
 //     accumulators over dimension pairs (4q, 4q+1) and (4q+2, 4q+3), summed at
 //     the end; dot forms finalized with FP32 squared norms), so a distance
@@ -31,12 +32,12 @@ namespace {
 
 using namespace joinc;
 
-constexpr int BF_QT = 32;   // queries per CTA
 constexpr int BF_RT = 64;   // rows per chunk
-constexpr int BF_NT = 256;  // threads; thread t: queries 2 (t / 16) .. +1, rows 4 (t % 16) .. +3
+constexpr int BF_NT = 256;  // threads: thread t takes queries QT/16 (t / 16) + i and rows t % 16 + 16 j, j < 4
 constexpr int BF_KC = 64;   // dimensions staged at a time
 constexpr int BF_KS = BF_KC + 4;  // staged row stride (floats): conflict-free 16-byte reads
 constexpr int BF_KMAX = 128;      // largest k
+enum BfMode { BF_SQ = 0, BF_MAN = 1, BF_DOT = 2 };
 
 template <typename T>
 struct BfKey {
@@ -94,38 +95,39 @@ struct BfArgs {
   float* out_dist;
 };
 
-template <typename T, bool DIFF>
+template <typename T, int MODE, int QT>
 __global__ void __launch_bounds__(BF_NT) k_brute(BfArgs a) {
+  constexpr int QPT = QT / 16;  // queries per thread
   extern __shared__ __align__(16) unsigned char smem[];
-  float* sq = reinterpret_cast<float*>(smem);                  // BF_QT x BF_KS
-  float* sx = sq + BF_QT * BF_KS;                               // BF_RT x BF_KS
-  BfKey<T>* cand = reinterpret_cast<BfKey<T>*>(sx + BF_RT * BF_KS);  // BF_QT x BF_RT
-  BfKey<T>* list = cand + BF_QT * BF_RT;                        // BF_QT x k
-  int* ccount = reinterpret_cast<int*>(list + (size_t)BF_QT * a.k);  // BF_QT
-  int* lcount = ccount + BF_QT;                                 // BF_QT
-  BfKey<T>* thr = reinterpret_cast<BfKey<T>*>(lcount + BF_QT + 2);   // BF_QT (16-byte aligned: 66 ints)
+  float* sq = reinterpret_cast<float*>(smem);                  // QT x BF_KS
+  float* sx = sq + QT * BF_KS;                                  // BF_RT x BF_KS
+  BfKey<T>* cand = reinterpret_cast<BfKey<T>*>(sx + BF_RT * BF_KS);  // QT x BF_RT
+  BfKey<T>* list = cand + QT * BF_RT;                           // QT x k
+  int* ccount = reinterpret_cast<int*>(list + (size_t)QT * a.k);  // QT
+  int* lcount = ccount + QT;                                    // QT
+  BfKey<T>* thr = reinterpret_cast<BfKey<T>*>(lcount + QT + 2);     // QT (8-byte aligned)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int q0 = blockIdx.x * BF_QT;
+  const int q0 = blockIdx.x * QT;
   const long long per = (a.n + a.splits - 1) / a.splits;
   const long long r_lo = (long long)blockIdx.y * per, r_hi = min(a.n, r_lo + per);
-  const int tq = 2 * (tid >> 4), tr = 4 * (tid & 15);
+  const int tq = QPT * (tid >> 4), tr = tid & 15;
   const T* qn = reinterpret_cast<const T*>(a.qn);
   const T* xn = reinterpret_cast<const T*>(a.xn);
-  if (tid < BF_QT) {
-    ccount[tid] = 0;
-    lcount[tid] = 0;
-    thr[tid] = key_max<T>();
+  for (int t = tid; t < QT; t += BF_NT) {
+    ccount[t] = 0;
+    lcount[t] = 0;
+    thr[t] = key_max<T>();
   }
   __syncthreads();
-  int32_t my_excl[2];
+  int32_t my_excl[QPT];
 #pragma unroll
-  for (int i = 0; i < 2; ++i) my_excl[i] = (a.excl && q0 + tq + i < a.nq) ? a.excl[q0 + tq + i] : -1;
+  for (int i = 0; i < QPT; ++i) my_excl[i] = (a.excl && q0 + tq + i < a.nq) ? a.excl[q0 + tq + i] : -1;
   for (long long r0 = r_lo; r0 < r_hi; r0 += BF_RT) {
-    // ---- distances of the 32 x 64 tile, 64 dimensions at a time ----
-    unsigned long long accf[2][4];
-    T accd[2][4];
+    // ---- distances of the QT x 64 tile, 64 dimensions at a time ----
+    unsigned long long accf[QPT][4];
+    T accd[QPT][4];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < QPT; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         accf[i][j] = 0ull;
@@ -134,7 +136,7 @@ __global__ void __launch_bounds__(BF_NT) k_brute(BfArgs a) {
     for (int k0 = 0; k0 < a.Dp; k0 += BF_KC) {
       const int kc = min(BF_KC, a.Dp - k0);  // a multiple of 4
       __syncthreads();
-      for (int e = tid; e < BF_QT * (BF_KC / 4); e += BF_NT) {
+      for (int e = tid; e < QT * (BF_KC / 4); e += BF_NT) {
         const int qi = e / (BF_KC / 4), c = 4 * (e % (BF_KC / 4));
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (c < kc && q0 + qi < a.nq) v = *reinterpret_cast<const float4*>(a.Q + (size_t)(q0 + qi) * a.Dp + k0 + c);
@@ -148,62 +150,67 @@ __global__ void __launch_bounds__(BF_NT) k_brute(BfArgs a) {
       }
       __syncthreads();
       for (int c = 0; c < kc; c += 4) {
-        float4 qv[2], xv[4];
+        if constexpr (sizeof(T) == 4) {
+          // join_dist_fp32's arithmetic on (x0, x1) and (x2, x3) as packed pairs
+          ulonglong2 qv[QPT], xv[4];
 #pragma unroll
-        for (int i = 0; i < 2; ++i) qv[i] = *reinterpret_cast<const float4*>(sq + (tq + i) * BF_KS + c);
+          for (int i = 0; i < QPT; ++i) qv[i] = *reinterpret_cast<const ulonglong2*>(sq + (tq + i) * BF_KS + c);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) xv[j] = *reinterpret_cast<const float4*>(sx + (tr + j) * BF_KS + c);
+          for (int j = 0; j < 4; ++j) xv[j] = *reinterpret_cast<const ulonglong2*>(sx + (tr + 16 * j) * BF_KS + c);
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+          for (int i = 0; i < QPT; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            if constexpr (sizeof(T) == 4) {
-              // join_dist_fp32's arithmetic: (x0, x1) and (x2, x3) as packed pairs
-              const unsigned long long q01 = ((unsigned long long)__float_as_uint(qv[i].y) << 32) | __float_as_uint(qv[i].x);
-              const unsigned long long q23 = ((unsigned long long)__float_as_uint(qv[i].w) << 32) | __float_as_uint(qv[i].z);
-              const unsigned long long x01 = ((unsigned long long)__float_as_uint(xv[j].y) << 32) | __float_as_uint(xv[j].x);
-              const unsigned long long x23 = ((unsigned long long)__float_as_uint(xv[j].w) << 32) | __float_as_uint(xv[j].z);
-              if (DIFF) {
-                if (a.kind == DK_SQEUCLIDEAN) {
-                  const unsigned long long d01 = f2_sub(x01, q01), d23 = f2_sub(x23, q23);
-                  accf[i][j] = f2_fma(d01, d01, accf[i][j]);
-                  accf[i][j] = f2_fma(d23, d23, accf[i][j]);
-                } else {
-                  const unsigned long long absmask = 0x7FFFFFFF7FFFFFFFull;
-                  accf[i][j] = f2_add(accf[i][j], f2_sub(x01, q01) & absmask);
-                  accf[i][j] = f2_add(accf[i][j], f2_sub(x23, q23) & absmask);
-                }
+            for (int j = 0; j < 4; ++j) {
+              if (MODE == BF_SQ) {
+                const unsigned long long d01 = f2_sub(xv[j].x, qv[i].x), d23 = f2_sub(xv[j].y, qv[i].y);
+                accf[i][j] = f2_fma(d01, d01, accf[i][j]);
+                accf[i][j] = f2_fma(d23, d23, accf[i][j]);
+              } else if (MODE == BF_MAN) {
+                const unsigned long long absmask = 0x7FFFFFFF7FFFFFFFull;
+                accf[i][j] = f2_add(accf[i][j], f2_sub(xv[j].x, qv[i].x) & absmask);
+                accf[i][j] = f2_add(accf[i][j], f2_sub(xv[j].y, qv[i].y) & absmask);
               } else {
-                accf[i][j] = f2_fma(x01, q01, accf[i][j]);
-                accf[i][j] = f2_fma(x23, q23, accf[i][j]);
+                accf[i][j] = f2_fma(xv[j].x, qv[i].x, accf[i][j]);
+                accf[i][j] = f2_fma(xv[j].y, qv[i].y, accf[i][j]);
               }
-            } else {
+            }
+        } else {
+          float4 qv[QPT], xv[4];
+#pragma unroll
+          for (int i = 0; i < QPT; ++i) qv[i] = *reinterpret_cast<const float4*>(sq + (tq + i) * BF_KS + c);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) xv[j] = *reinterpret_cast<const float4*>(sx + (tr + 16 * j) * BF_KS + c);
+#pragma unroll
+          for (int i = 0; i < QPT; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
               const float xs[4] = {xv[j].x, xv[j].y, xv[j].z, xv[j].w};
               const float qs[4] = {qv[i].x, qv[i].y, qv[i].z, qv[i].w};
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
                 const T dx = (T)xs[u] - (T)qs[u];
-                if (DIFF) accd[i][j] = a.kind == DK_SQEUCLIDEAN ? fma(dx, dx, accd[i][j]) : accd[i][j] + fabs(dx);
+                if (MODE == BF_SQ) accd[i][j] = fma(dx, dx, accd[i][j]);
+                else if (MODE == BF_MAN) accd[i][j] = accd[i][j] + fabs(dx);
                 else accd[i][j] = fma((T)xs[u], (T)qs[u], accd[i][j]);
               }
             }
-          }
+        }
       }
     }
     // ---- keys that beat the query's k-th key -> the query's staging list ----
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < QPT; ++i) {
       const int qi = tq + i;
       if (q0 + qi >= a.nq) continue;
       const BfKey<T> t = thr[qi];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const long long r = r0 + tr + j;
+        const long long r = r0 + tr + 16 * j;
         if (r >= r_hi || (int32_t)r == my_excl[i]) continue;
         T d;
         if constexpr (sizeof(T) == 4) d = f2_sum(accf[i][j]);
         else d = accd[i][j];
-        if (!DIFF) d = bf_finalize<T>(a.kind, d, xn[r], qn[q0 + qi]);
+        if (MODE == BF_DOT) d = bf_finalize<T>(a.kind, d, xn[r], qn[q0 + qi]);
         if (d != d) d = (T)INFINITY;  // NaN ranks last
         const BfKey<T> key{d, (int32_t)r};
         if (key_less(key, t)) cand[qi * BF_RT + atomicAdd(&ccount[qi], 1)] = key;
@@ -211,7 +218,7 @@ __global__ void __launch_bounds__(BF_NT) k_brute(BfArgs a) {
     }
     __syncthreads();
     // ---- merge: warp w takes queries w, w + 8, ... ----
-    for (int qi = warp; qi < BF_QT; qi += BF_NT / 32) {
+    for (int qi = warp; qi < QT; qi += BF_NT / 32) {
       const int nc = ccount[qi];
       if (nc == 0) continue;
       BfKey<T>* c = cand + qi * BF_RT;
@@ -267,7 +274,7 @@ __global__ void __launch_bounds__(BF_NT) k_brute(BfArgs a) {
     __syncthreads();
   }
   // ---- results ----
-  for (int qi = warp; qi < BF_QT; qi += BF_NT / 32) {
+  for (int qi = warp; qi < QT; qi += BF_NT / 32) {
     if (q0 + qi >= a.nq) continue;
     const BfKey<T>* L = list + (size_t)qi * a.k;
     const int nl = lcount[qi];
@@ -317,18 +324,29 @@ __global__ void k_brute_merge(const BfKey<T>* __restrict__ part, int nq, int spl
   }
 }
 
-template <typename T>
+template <typename T, int QT>
 size_t bf_smem(int k) {
-  return (size_t)(BF_QT + BF_RT) * BF_KS * 4 + (size_t)BF_QT * (BF_RT + k) * sizeof(BfKey<T>) +
-         (size_t)(2 * BF_QT + 2) * 4 + (size_t)BF_QT * sizeof(BfKey<T>);
+  return (size_t)(QT + BF_RT) * BF_KS * 4 + (size_t)QT * (BF_RT + k) * sizeof(BfKey<T>) + (size_t)(2 * QT + 2) * 4 +
+         (size_t)QT * sizeof(BfKey<T>);
 }
 
+template <typename T, int MODE, int QT>
+void brute_launch(const BfArgs& a, int qtiles, cudaStream_t st) {
+  const size_t smem = bf_smem<T, QT>(a.k);
+  set_smem_limit_once(reinterpret_cast<const void*>(k_brute<T, MODE, QT>), 200 * 1024);
+  k_brute<T, MODE, QT><<<dim3((unsigned)qtiles, (unsigned)a.splits), BF_NT, smem, st>>>(a);
+  RINND_LAUNCH_CHECK();
+}
+
+// FP32: 64 queries a CTA (4 x 4 pairs a thread); FP64: 32 (2 x 4), its keys
+// being twice as wide.
 template <typename T>
 void brute_run(const float* Q, int nq, const float* X, long long n, int Dp, int k, int kind, const int32_t* excl,
                int32_t* out_idx, float* out_dist, cudaStream_t st) {
-  const bool diff = !bf_dot_kind(kind);
+  constexpr int QT = sizeof(T) == 4 ? 64 : 32;
+  const int mode = kind == DK_SQEUCLIDEAN ? BF_SQ : (kind == DK_MANHATTAN ? BF_MAN : BF_DOT);
   DVec<T> qn, xn;
-  if (!diff) {
+  if (mode == BF_DOT) {
     qn.alloc((size_t)nq, st);
     xn.alloc((size_t)n, st);
     k_bf_norms<T><<<(unsigned)(((long long)nq * 32 + 255) / 256), 256, 0, st>>>(Q, nq, Dp, qn.p);
@@ -336,20 +354,16 @@ void brute_run(const float* Q, int nq, const float* X, long long n, int Dp, int 
     k_bf_norms<T><<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(X, n, Dp, xn.p);
     RINND_LAUNCH_CHECK();
   }
-  const int qtiles = (nq + BF_QT - 1) / BF_QT;
-  // enough CTAs for two waves of 2 per SM, rows split over CTAs of one query tile
+  const int qtiles = (nq + QT - 1) / QT;
+  // enough CTAs for a few waves, rows split over the CTAs of one query tile
   int splits = 1;
   while (splits < 32 && (long long)qtiles * splits < 148 * 4 && (long long)splits * 4 * BF_RT < n) splits *= 2;
-  const size_t smem = bf_smem<T>(k);
-  const void* kern = diff ? reinterpret_cast<const void*>(k_brute<T, true>) : reinterpret_cast<const void*>(k_brute<T, false>);
-  set_smem_limit_once(kern, 200 * 1024);
   DVec<BfKey<T>> part;
   if (splits > 1) part.alloc((size_t)nq * splits * k, st);
   BfArgs a{Q, X, qn.p, xn.p, excl, n, nq, Dp, k, kind, splits, part.p, out_idx, out_dist};
-  const dim3 grid((unsigned)qtiles, (unsigned)splits);
-  if (diff) k_brute<T, true><<<grid, BF_NT, smem, st>>>(a);
-  else k_brute<T, false><<<grid, BF_NT, smem, st>>>(a);
-  RINND_LAUNCH_CHECK();
+  if (mode == BF_SQ) brute_launch<T, BF_SQ, QT>(a, qtiles, st);
+  else if (mode == BF_MAN) brute_launch<T, BF_MAN, QT>(a, qtiles, st);
+  else brute_launch<T, BF_DOT, QT>(a, qtiles, st);
   if (splits > 1) {
     k_brute_merge<T><<<(unsigned)((nq * 32 + 255) / 256), 256, 0, st>>>(part.p, nq, splits, k, out_idx, out_dist);
     RINND_LAUNCH_CHECK();
