@@ -18,8 +18,9 @@ data path); the max over ranks of the device-timed region is reported.
 oracle/, all host threads) on the same full workload, one build per step.
 The default run also builds that oracle index once (the `cpu_baseline` leg)
 and reports its recall beside the GPU's, on the same sample and queries, and
-(one GPU) adds `forms`: the batched form (512 indices, two warm-up calls, one
-timed), the serving form (10M x 96, int8 per-vector width 100 server, 2 s per
+(one GPU) adds `forms`: brute-force exact kNN of the same queries against the
+same rows (FP32 and the FP64 checker), the batched form (512 indices, two
+warm-up calls, one timed), the serving form (10M x 96, int8 per-vector width 100 server, 2 s per
 offered load) and the precision form (1M x 960 cosine, FP32 and BF16 builds,
 without the oracle parity sizes) in compact runs of --workload batched /
 serving / precision.
@@ -1016,6 +1017,10 @@ def main():
     # this line (the full workloads: --workload batched / serving) ----
     forms = {}
     if world == 1 and rank == 0 and not args.no_forms:
+        try:
+            forms["brute_force"] = brute_force_form(L, X_dev, Q_dev, QK)
+        except Exception as exc:  # reported in the line, the build numbers stand
+            forms["brute_force"] = {"error": f"{type(exc).__name__}: {exc}"}
         del X_dev, Q_dev
         torch.cuda.empty_cache()
         sub = argparse.Namespace(**vars(args))
@@ -1059,6 +1064,44 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def brute_force_form(L, X_dev, Q_dev, k):
+    """Brute-force exact kNN of the build workload's queries against its rows
+    (rinnd_brute_force_knn, squared Euclidean): the FP32 form (the build's join
+    arithmetic), the BF16 tensor-core form (Gram-tile filter + FP32 recheck)
+    and the FP64 checker, each timed after a warm-up call (synchronized host
+    clock around the call); whether the BF16 form's results are the FP32
+    form's bit for bit, and how many queries' id lists FP32 and FP64 agree on."""
+    import torch
+
+    nq, n, d = Q_dev.shape[0], X_dev.shape[0], X_dev.shape[1]
+    out, ids, dists = {"workload": f"{nq} queries x {n} rows x {d}, k={k}, sqeuclidean, device-resident"}, {}, {}
+    for name, prec in (("fp32", L.BRUTE_FP32), ("bf16", L.BRUTE_BF16), ("fp64", L.BRUTE_FP64)):
+        oi = torch.empty((nq, k), dtype=torch.int32, device=X_dev.device)
+        od = torch.empty((nq, k), dtype=torch.float32, device=X_dev.device)
+
+        def call():
+            L.check(L.lib.rinnd_brute_force_knn(ctypes.c_void_p(X_dev.data_ptr()), n, d, ctypes.c_void_p(Q_dev.data_ptr()),
+                                                nq, d, d, k, L.DIST_SQEUCLIDEAN, prec, None, 1,
+                                                ctypes.c_void_p(oi.data_ptr()), ctypes.c_void_p(od.data_ptr())))
+
+        call()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        call()
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        ids[name] = oi.cpu().numpy()
+        dists[name] = od.cpu().numpy()
+        out[name] = {"ms": 1000.0 * t, "qps": nq / t, "tflops_2qnd": 2.0 * nq * n * d / t / 1e12}
+    # FP32 SIMT work: a subtraction and a fused multiply-add per element pair
+    out["fp32"]["fp32_simt_fraction_of_nominal"] = 3.0 * nq * n * d / (out["fp32"]["ms"] / 1000.0) / 74.4e12
+    out["fp32_id_lists_equal_to_fp64"] = float(np.mean(np.all(ids["fp32"] == ids["fp64"], axis=1)))
+    out["bf16_results_equal_to_fp32"] = bool(np.array_equal(ids["bf16"], ids["fp32"]) and
+                                             np.array_equal(dists["bf16"].view(np.uint32), dists["fp32"].view(np.uint32)))
+    out["bf16"]["speedup_vs_fp32"] = out["fp32"]["ms"] / out["bf16"]["ms"]
+    return out
 
 
 def _exact_rows(Xd, xx, rows, k, dev):

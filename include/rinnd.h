@@ -413,11 +413,16 @@ RINND_EXPORT int rinnd_distance_pairs(int32_t kind, const float* a, const float*
  * != 0 (outputs are then device pointers too), else host memory.
  * distance_kind: RINND_DIST_SQEUCLIDEAN, _MANHATTAN, _INNER_PRODUCT, _COSINE or
  * _DIRECT_COSINE.  precision: RINND_BRUTE_FP32 (the FP32 join's per-pair
- * arithmetic, so distances equal the build's) or RINND_BRUTE_FP64 (every term
- * in double: the checker the FP32 form's ids are compared with).  exclude_ids
+ * arithmetic, so distances equal the build's), RINND_BRUTE_BF16 (BF16
+ * tensor-core Gram tiles filter the pairs with a rigorous lower bound and the
+ * survivors are recomputed in that FP32 arithmetic: the FP32 form's results,
+ * for d <= 128, k <= 32 and squared Euclidean or a dot form; other shapes are
+ * rejected) or RINND_BRUTE_FP64 (every term in double: the checker the FP32
+ * form's ids are compared with).  exclude_ids
  * (nullable, nq entries): query i leaves out data row exclude_ids[i] (the kNN
  * graph of the data itself).  k in [1, 128]. */
 #define RINND_BRUTE_FP32 0
+#define RINND_BRUTE_BF16 1
 #define RINND_BRUTE_FP64 2
 RINND_EXPORT int rinnd_brute_force_knn(const float* data, int64_t n, int64_t ld_data, const float* queries,
                                        int64_t nq, int64_t ld_queries, int32_t d, int32_t k, int32_t distance_kind,

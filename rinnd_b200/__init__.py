@@ -85,7 +85,10 @@ def brute_force_knn(data, queries, k=10, metric="sqeuclidean", precision="fp32",
     """Exact k nearest data rows of every query row, by (distance, id) ascending
     (no counterpart in the reference; its recall criteria are measured against
     these).  precision "fp32" computes each distance with the build's FP32 join
-    arithmetic, "fp64" in double (the checker).  exclude_self leaves out data
+    arithmetic; "bf16" filters the pairs on the tensor cores (BF16 Gram tiles,
+    a rigorous lower bound) and recomputes the survivors in that FP32
+    arithmetic, giving the FP32 results (dimension <= 128, k <= 32, not
+    Manhattan); "fp64" computes in double (the checker).  exclude_self leaves out data
     row i for query i (queries must then be the data rows themselves).
     Returns (int32[nq, k], float32[nq, k]), padded with (-1, inf) when k > n."""
     if metric not in _BRUTE_METRICS:
@@ -95,8 +98,9 @@ def brute_force_knn(data, queries, k=10, metric="sqeuclidean", precision="fp32",
     Q = np.ascontiguousarray(_as_f32_2d(queries, "queries"))
     if Q.shape[1] != X.shape[1]:
         raise ValueError(f"Query dimension {Q.shape[1]} does not match data dimension {X.shape[1]}")
-    if precision not in ("fp32", "fp64"):
-        raise ValueError("precision must be 'fp32' or 'fp64'")
+    precisions = {"fp32": L.BRUTE_FP32, "bf16": L.BRUTE_BF16, "fp64": L.BRUTE_FP64}
+    if precision not in precisions:
+        raise ValueError("precision must be 'fp32', 'bf16' or 'fp64'")
     nq = Q.shape[0]
     excl = None
     if exclude_self:
@@ -106,7 +110,7 @@ def brute_force_knn(data, queries, k=10, metric="sqeuclidean", precision="fp32",
     oi = np.empty((nq, int(k)), np.int32)
     od = np.empty((nq, int(k)), np.float32)
     L.check(L.lib.rinnd_brute_force_knn(L.ptr(X), X.shape[0], X.shape[1], L.ptr(Q), nq, Q.shape[1], X.shape[1],
-                                        int(k), kind, L.BRUTE_FP32 if precision == "fp32" else L.BRUTE_FP64,
+                                        int(k), kind, precisions[precision],
                                         L.ptr(excl) if excl is not None else None, 0, L.ptr(oi), L.ptr(od)))
     if take_sqrt:
         od = np.sqrt(od)

@@ -30,7 +30,7 @@ Q8_PER_VECTOR_COSINE, Q8_GLOBAL_SYMMETRIC, Q8_PER_VECTOR_SYMMETRIC, Q8_PER_DIMEN
 PRECISION_FP32, PRECISION_BF16 = range(2)
 TUNE_TABLE, TUNE_FIXED, TUNE_RETUNE = range(3)
 JOIN_CHUNKED_FP32, JOIN_PIPELINED_FP32, JOIN_TENSOR_BF16 = range(3)  # rinnd_build_info.join_form
-BRUTE_FP32, BRUTE_FP64 = 0, 2  # rinnd_brute_force_knn precision
+BRUTE_FP32, BRUTE_BF16, BRUTE_FP64 = 0, 1, 2  # rinnd_brute_force_knn precision
 
 _i32, _i64, _u64, _f32, _f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_float, ctypes.c_double
 _P = ctypes.c_void_p

@@ -1495,7 +1495,8 @@ int rinnd_brute_force_knn(const float* data, int64_t n, int64_t ld_data, const f
     require(n < (int64_t)INT32_MAX - 1 && nq < (int64_t)INT32_MAX, "too many rows");
     require(ld_data >= d && ld_queries >= d, "row stride smaller than the dimension");
     require(k >= 1 && k <= 128, "k must be in [1, 128]");
-    require(precision == RINND_BRUTE_FP32 || precision == RINND_BRUTE_FP64, "precision must be FP32 or FP64");
+    require(precision == RINND_BRUTE_FP32 || precision == RINND_BRUTE_BF16 || precision == RINND_BRUTE_FP64,
+            "precision must be FP32, BF16 or FP64");
     require(distance_kind >= 0 && distance_kind < DK_COUNT && brute_supported(distance_kind),
             "brute force supports squared Euclidean, Manhattan, inner product, cosine and direct cosine");
     if (nq == 0) return;

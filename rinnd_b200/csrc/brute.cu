@@ -23,9 +23,28 @@
 // its split by binary search); the k-th key then filters the next chunks.
 // Metrics: squared Euclidean and Manhattan (difference form), inner product,
 // cosine and direct cosine (dot form).
+//
+// Tensor-core form (BF16 filter + FP32 recheck; D <= 128, k <= 32; squared
+// Euclidean and the dot forms).  Rows and queries get a BF16 copy written in
+// the tcgen05 operand layout (K-major core matrices, no swizzle), one 128-row
+// tile after another, with per row |b|^2 and a bound e >= |b - x| of its
+// rounding error.  A CTA holds 128 queries as the A operand and streams 128-row
+// tiles as B, each arriving with one bulk copy on an mbarrier (two stages);
+// one thread issues the M = 128, N = 128 MMAs (FP32 accumulate) into two
+// tensor-memory accumulators; eight epilogue warps each read 64 columns of
+// their lane quadrant (lane = query).  A pair survives when its lower bound --
+// the local join's (join_tc.cu): squared Euclidean |b_i - b_j| from the Gram
+// value with its FP32 error and the rows' rounding bounds, dot forms from an
+// upper bound of the dot -- beats the k-th key of the query's list; survivors
+// are recomputed with the FP32 form's arithmetic and inserted by (distance,
+// id).  Each (query, epilogue half) keeps its own list and the two are merged
+// at the end, so the results equal the FP32 form's exactly.
+#include <cuda_bf16.h>
+
 #include "dist.cuh"
 #include "engine.h"
 #include "join_common.cuh"
+#include "tcgen05.cuh"
 
 namespace rinnd {
 namespace {
@@ -370,6 +389,335 @@ void brute_run(const float* Q, int nq, const float* X, long long n, int Dp, int 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core form
+// ---------------------------------------------------------------------------
+constexpr int TC_M = 128;       // queries per CTA (tensor-memory lanes)
+constexpr int TC_N = 128;       // rows per tile (accumulator columns)
+constexpr int TC_KPMAX = 128;   // padded dimension limit
+constexpr int TC_KMAX = 32;     // k limit
+constexpr int TC_NEPI = 8;      // epilogue warps: lane quadrant warp % 4, column half (warp - 2) / 4
+constexpr int TC_NT = 32 * (2 + TC_NEPI);
+
+// BF16 copy of rows 0..n_pad-1 (rows >= n zero) in the tiled operand layout:
+// tile t = rows 128 t.., at t * 128 Kp elements; element (r, k) of a tile at
+// byte (r / 8) SBO + (k / 8) 128 + (r % 8) 16 + (k % 8) 2, SBO = (Kp / 8) 128.
+// info[r] = (|b_r|^2, e_r >= |b_r - x_r|), one warp per row.
+__global__ void k_bf16_tiled(const float* __restrict__ X, long long n, long long n_pad, int Dp, int Kp,
+                             __nv_bfloat16* __restrict__ out, float2* __restrict__ info) {
+  const long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n_pad) return;
+  const long long tile = r / TC_N;
+  const int rr = (int)(r % TC_N);
+  const size_t sbo = (size_t)(Kp / 8) * 128;
+  unsigned char* base = reinterpret_cast<unsigned char*>(out) + (size_t)tile * TC_N * Kp * 2 + (size_t)(rr / 8) * sbo +
+                        (size_t)(rr % 8) * 16;
+  float bn = 0.f, ee = 0.f;
+  for (int k = lane; k < Kp; k += 32) {
+    const float x = (r < n && k < Dp) ? X[(size_t)r * Dp + k] : 0.f;
+    const __nv_bfloat16 b = __float2bfloat16_rn(x);
+    const float bf = __bfloat162float(b);
+    *reinterpret_cast<__nv_bfloat16*>(base + (size_t)(k / 8) * 128 + (k % 8) * 2) = b;
+    bn = fmaf(bf, bf, bn);
+    const float d = bf - x;  // exact: b is x rounded to 8 significant bits
+    ee = fmaf(d, d, ee);
+  }
+  for (int o = 16; o; o >>= 1) {
+    bn += __shfl_xor_sync(0xffffffffu, bn, o);
+    ee += __shfl_xor_sync(0xffffffffu, ee, o);
+  }
+  // the FP32 sum of squares is within Kp 2^-24 of its value; 2^-10 covers it and the sqrt
+  if (lane == 0) info[r] = make_float2(bn, sqrtf(ee) * 1.0009765625f + 1e-30f);
+}
+
+struct TcArgs {
+  const __nv_bfloat16* Qb;  // tiled BF16 queries
+  const float2* qinfo;
+  const float* Q;           // FP32 queries, nq x Dp
+  const float* qn;          // FP32 squared norms (dot forms)
+  const __nv_bfloat16* Xb;  // tiled BF16 rows
+  const float2* xinfo;
+  const float* X;
+  const float* xn;
+  const int32_t* excl;
+  long long n;
+  int nq, Dp, Kp, k, kind, splits, ntiles;
+  BfKey<float>* out_key;  // splits > 1: nq x splits x k
+  int32_t* out_idx;
+  float* out_dist;
+  int* err;
+};
+
+__host__ __device__ inline size_t tc_smem(int Kp, int k) {
+  return (size_t)3 * TC_N * Kp * 2 + (size_t)TC_M * 2 * k * sizeof(BfKey<float>) + 16 * 8 + 16 + TC_M * 2 * 4;
+}
+
+// Bounded wait whose outcome is the same in every lane of the warp.
+__device__ __forceinline__ bool warp_wait_tc(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  return __all_sync(0xffffffffu, wait_or_abort(bar, parity, abort_flag));
+}
+
+template <bool SQ>
+__global__ void __launch_bounds__(TC_NT) k_brute_tc(TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const uint32_t tile_bytes = (uint32_t)(TC_N * a.Kp * 2);
+  unsigned char* A = smem;
+  unsigned char* Bst = smem + tile_bytes;  // two stages
+  BfKey<float>* lists = reinterpret_cast<BfKey<float>*>(smem + 3 * (size_t)tile_bytes);  // (query, half) x k
+  uint64_t* bar = reinterpret_cast<uint64_t*>(lists + (size_t)TC_M * 2 * a.k);
+  uint64_t* a_full = bar;
+  uint64_t* tile_full = bar + 1;   // [2]
+  uint64_t* tile_empty = bar + 3;  // [2]
+  uint64_t* mma_done = bar + 5;    // [2]
+  uint64_t* tmem_empty = bar + 7;  // [2]
+  uint64_t* drain = bar + 9;
+  int* ints = reinterpret_cast<int*>(bar + 16);
+  volatile int* abort_flag = ints;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ints + 1);
+  int* lcnt = ints + 4;  // entries of each (query, half) list
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int per = (a.ntiles + a.splits - 1) / a.splits;
+  const int t_lo = blockIdx.y * per;
+  const int nt = max(0, min(a.ntiles, t_lo + per) - t_lo);
+  if (tid == 0) {
+    mbar_init(a_full, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&tile_full[i], 1);
+      mbar_init(&tile_empty[i], 1);
+      mbar_init(&mma_done[i], 1);
+      mbar_init(&tmem_empty[i], TC_NEPI);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 1) umma::tmem_alloc(tmem_slot, 2 * TC_N);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t taddr = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------ producer ------------------------------
+    if (lane == 0) {
+      bool ok = true;
+      int issued = 0;
+      mbar_arrive_expect_tx(a_full, tile_bytes);
+      bulk_g2s(A, a.Qb + (size_t)blockIdx.x * TC_M * a.Kp, tile_bytes, a_full);
+      for (int t = 0; t < nt; ++t) {
+        const int s = t & 1;
+        if (t >= 2 && !(ok = wait_or_abort(&tile_empty[s], (uint32_t)((t >> 1) - 1) & 1u, abort_flag))) break;
+        mbar_arrive_expect_tx(&tile_full[s], tile_bytes);
+        bulk_g2s(Bst + (size_t)s * tile_bytes, a.Xb + (size_t)(t_lo + t) * TC_N * a.Kp, tile_bytes, &tile_full[s]);
+        issued = t + 1;
+      }
+      if (!ok) {
+        *abort_flag = 1;
+        atomicExch(a.err, 1);
+      }
+      // no copy may land after the CTA exits: wait (bounded) for the last ones issued
+      mbar_wait_bounded(a_full, 0u, WAIT_POLLS);
+      for (int t = max(0, issued - 2); t < issued; ++t)
+        mbar_wait_bounded(&tile_full[t & 1], (uint32_t)(t >> 1) & 1u, WAIT_POLLS);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------ MMA issuer ------------------------------
+    if (lane == 0) {
+      bool ok = wait_or_abort(a_full, 0u, abort_flag);
+      const uint32_t idesc = umma::idesc_bf16_f32(TC_M, TC_N);
+      const uint32_t sbo = (uint32_t)(a.Kp / 8) * 128u;
+      const uint32_t a0 = smem_addr(A), b0 = smem_addr(Bst);
+      for (int t = 0; ok && t < nt; ++t) {
+        const int s = t & 1;
+        if (!(ok = wait_or_abort(&tile_full[s], (uint32_t)(t >> 1) & 1u, abort_flag))) break;
+        if (t >= 2 && !(ok = wait_or_abort(&tmem_empty[s], (uint32_t)((t >> 1) - 1) & 1u, abort_flag))) break;
+        umma::fence_after_sync();
+        for (int kk = 0; kk < a.Kp / 16; ++kk) {
+          const uint64_t ad = umma::smem_desc(a0 + 256u * kk, 128u, sbo);
+          const uint64_t bd = umma::smem_desc(b0 + (uint32_t)s * tile_bytes + 256u * kk, 128u, sbo);
+          umma::mma_bf16(taddr + (uint32_t)(TC_N * s), ad, bd, idesc, kk > 0);
+        }
+        umma::commit(&tile_empty[s]);  // the stage is free once these MMAs completed
+        umma::commit(&mma_done[s]);
+      }
+      if (!ok) {
+        *abort_flag = 1;
+        atomicExch(a.err, 1);
+      }
+      // no MMA may run once the tensor memory is freed: a last commit tracks every MMA issued
+      umma::commit(drain);
+      mbar_wait_bounded(drain, 0u, WAIT_POLLS);
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------ epilogue ------------------------------
+    const int quad = warp & 3, half = (warp - 2) >> 2;
+    const int qi = 32 * quad + lane;
+    const int q = blockIdx.x * TC_M + qi;
+    const bool qv = q < a.nq;
+    BfKey<float>* L = lists + ((size_t)qi * 2 + half) * a.k;
+    int cnt = 0;
+    BfKey<float> thr = key_max<float>();
+    const float2 qinf = qv ? a.qinfo[q] : make_float2(0.f, 0.f);
+    const float bn_q = qinf.x, e_q = qinf.y;
+    const float xn_q = (!SQ && qv) ? a.qn[q] : 0.f;
+    const float bt = sqrtf(bn_q);
+    const int32_t excl = (a.excl && qv) ? a.excl[q] : -1;
+    const float* qrow = a.Q + (size_t)(qv ? q : 0) * a.Dp;
+    const float gam = SQ ? (float)a.Kp * 1.9073486328125e-06f + 9.5367431640625e-07f   // Kp 2^-19 + 2^-20
+                         : (float)a.Kp * 9.5367431640625e-07f + 9.5367431640625e-07f;  // Kp 2^-20 + 2^-20
+    float sthr = INFINITY;  // squared Euclidean: sqrt(T (1 + 2^-11)) of the list's k-th distance T
+    for (int t = 0; t < nt; ++t) {
+      const int b = t & 1;
+      if (!warp_wait_tc(&mma_done[b], (uint32_t)(t >> 1) & 1u, abort_flag)) {
+        if (lane == 0) {
+          *abort_flag = 1;
+          atomicExch(a.err, 1);
+        }
+        break;
+      }
+      umma::fence_after_sync();
+      uint32_t g[64];
+      const uint32_t ta = taddr + ((uint32_t)(32 * quad) << 16) + (uint32_t)(TC_N * b + 64 * half);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) umma::ld_32x32b_x16(ta + 16u * c, g + 16 * c);
+      umma::wait_ld();
+      umma::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tmem_empty[b]);  // this warp's reads of the accumulator are done
+      const long long row0 = (long long)(t_lo + t) * TC_N + 64 * half;
+      // survivors of the filter against the list's k-th key at the tile's start
+      unsigned long long keepm = 0ull;
+#pragma unroll
+      for (int j = 0; j < 64; ++j) {
+        const long long row = row0 + j;
+        const float G = __uint_as_float(g[j]);
+        const float2 xi = row < a.n ? __ldg(a.xinfo + row) : make_float2(0.f, 0.f);
+        bool keep;
+        if (SQ) {
+          const float sum = bn_q + xi.x;
+          const float x = sum - 2.0f * G - gam * sum;
+          const float c = sthr + e_q + xi.y;
+          keep = fmaxf(x, 0.f) < c * c;
+        } else {
+          const float bj = sqrtf(xi.x);
+          const float ub = G + e_q * bj + xi.y * (bt + e_q) + gam * bt * bj;
+          float lb = finalize_dot(a.kind, ub, row < a.n ? __ldg(a.xn + row) : 0.f, xn_q);
+          lb = lb - fabsf(lb) * 4.8828125e-4f - 1e-30f;
+          keep = lb < thr.d;
+        }
+        keepm |= (unsigned long long)(keep && row < a.n) << j;
+      }
+      if (!qv) keepm = 0ull;
+      while (keepm) {
+        const int j = __ffsll((long long)keepm) - 1;
+        keepm &= keepm - 1;
+        const long long row = row0 + j;
+        if ((int32_t)row == excl) continue;
+        // exact FP32 recheck: the FP32 form's arithmetic (row first)
+        float d = join_dist_fp32(a.kind, a.X + (size_t)row * a.Dp, qrow, a.Dp);
+        if (!SQ) d = finalize_dot(a.kind, d, __ldg(a.xn + row), xn_q);
+        if (d != d) d = INFINITY;
+        const BfKey<float> key{d, (int32_t)row};
+        if (!key_less(key, thr)) continue;
+        int p = cnt < a.k ? cnt : a.k - 1;  // the slot the key may take
+        while (p > 0 && key_less(key, L[p - 1])) {
+          L[p] = L[p - 1];
+          --p;
+        }
+        L[p] = key;
+        if (cnt < a.k) ++cnt;
+        if (cnt == a.k) {
+          thr = L[a.k - 1];
+          sthr = SQ ? sqrtf(thr.d * 1.00048828125f) : 0.f;
+        }
+      }
+    }
+    lcnt[qi * 2 + half] = cnt;  // the two halves' lists of a query are merged after the barrier
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 1) umma::tmem_dealloc(taddr, 2 * TC_N);
+  if (warp >= 2 && ((warp - 2) >> 2) == 0) {
+    const int qi = 32 * (warp & 3) + lane;
+    const int q = blockIdx.x * TC_M + qi;
+    if (q < a.nq) {
+      const BfKey<float>* L0 = lists + (size_t)qi * 2 * a.k;
+      const BfKey<float>* L1 = L0 + a.k;
+      const int n0 = lcnt[qi * 2], n1 = lcnt[qi * 2 + 1];
+      int i0 = 0, i1 = 0;
+      for (int p = 0; p < a.k; ++p) {
+        BfKey<float> key{INFINITY, -1};
+        if (i0 < n0 && (i1 >= n1 || key_less(L0[i0], L1[i1]))) key = L0[i0++];
+        else if (i1 < n1) key = L1[i1++];
+        if (a.splits > 1) {
+          a.out_key[((size_t)q * a.splits + blockIdx.y) * a.k + p] = key;
+        } else {
+          a.out_idx[(size_t)q * a.k + p] = key.id;
+          a.out_dist[(size_t)q * a.k + p] = key.d;
+        }
+      }
+    }
+  }
+}
+
+bool tc_supported(int kind, int Dp, int k) {
+  return (kind == DK_SQEUCLIDEAN || bf_dot_kind(kind)) && (Dp + 15) / 16 * 16 <= TC_KPMAX && k <= TC_KMAX;
+}
+
+void brute_tc_run(const float* Q, int nq, const float* X, long long n, int Dp, int k, int kind, const int32_t* excl,
+                  int32_t* out_idx, float* out_dist, cudaStream_t st) {
+  const int Kp = (Dp + 15) / 16 * 16;
+  const long long ntiles = (n + TC_N - 1) / TC_N;
+  const int qtiles = (nq + TC_M - 1) / TC_M;
+  if (ntiles > 0x7FFFFFFF) throw std::invalid_argument("brute force: too many rows");
+  DVec<__nv_bfloat16> Xb((size_t)ntiles * TC_N * Kp, st), Qb((size_t)qtiles * TC_M * Kp, st);
+  DVec<float2> xinfo((size_t)ntiles * TC_N, st), qinfo((size_t)qtiles * TC_M, st);
+  k_bf16_tiled<<<(unsigned)((ntiles * TC_N * 32 + 255) / 256), 256, 0, st>>>(X, n, ntiles * TC_N, Dp, Kp, Xb.p, xinfo.p);
+  RINND_LAUNCH_CHECK();
+  k_bf16_tiled<<<(unsigned)(((long long)qtiles * TC_M * 32 + 255) / 256), 256, 0, st>>>(Q, nq, (long long)qtiles * TC_M,
+                                                                                       Dp, Kp, Qb.p, qinfo.p);
+  RINND_LAUNCH_CHECK();
+  DVec<float> qn, xn;
+  const bool sq = kind == DK_SQEUCLIDEAN;
+  if (!sq) {
+    qn.alloc((size_t)nq, st);
+    xn.alloc((size_t)n, st);
+    k_bf_norms<float><<<(unsigned)(((long long)nq * 32 + 255) / 256), 256, 0, st>>>(Q, nq, Dp, qn.p);
+    RINND_LAUNCH_CHECK();
+    k_bf_norms<float><<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(X, n, Dp, xn.p);
+    RINND_LAUNCH_CHECK();
+  }
+  // one CTA per SM (its shared memory): row tiles split so that every SM has work
+  int splits = 1;
+  while (splits < 32 && (long long)qtiles * splits < 148 && (long long)splits * 4 < ntiles) splits *= 2;
+  DVec<BfKey<float>> part;
+  if (splits > 1) part.alloc((size_t)nq * splits * k, st);
+  DVec<int> err(1, st);
+  err.fill_bytes(0);
+  TcArgs a{Qb.p, qinfo.p, Q, qn.p, Xb.p, xinfo.p, X, xn.p, excl, n, nq, Dp, Kp, k, kind, splits, (int)ntiles,
+           part.p, out_idx, out_dist, err.p};
+  // at least 116 KB: at most two CTAs (2 x 256 tensor-memory columns) share an SM
+  const size_t smem = std::max<size_t>(tc_smem(Kp, k), 116 * 1024);
+  const void* kern = sq ? reinterpret_cast<const void*>(k_brute_tc<true>) : reinterpret_cast<const void*>(k_brute_tc<false>);
+  set_smem_limit_once(kern, 227 * 1024);
+  const dim3 grid((unsigned)qtiles, (unsigned)splits);
+  if (sq) k_brute_tc<true><<<grid, TC_NT, smem, st>>>(a);
+  else k_brute_tc<false><<<grid, TC_NT, smem, st>>>(a);
+  RINND_LAUNCH_CHECK();
+  if (splits > 1) {
+    k_brute_merge<float><<<(unsigned)(((long long)nq * 32 + 255) / 256), 256, 0, st>>>(part.p, nq, splits, k, out_idx,
+                                                                                       out_dist);
+    RINND_LAUNCH_CHECK();
+  }
+  int h_err = 0;
+  RINND_CUDA(cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  RINND_CUDA(cudaStreamSynchronize(st));
+  if (h_err) throw std::runtime_error("brute force: a tensor-core pipeline wait timed out");
+}
+
 }  // namespace
 
 bool brute_supported(int kind) {
@@ -382,9 +730,18 @@ void brute_force_knn(const float* Q, int nq, const float* X, long long n, int Dp
   if (k < 1 || k > BF_KMAX) throw std::invalid_argument("brute force: k must be in [1, 128]");
   if (!brute_supported(kind)) throw std::invalid_argument("brute force: unsupported distance kind");
   if (Dp % 4 != 0) throw std::invalid_argument("brute force: row stride must be a multiple of 4");
-  if (precision == 2) brute_run<double>(Q, nq, X, n, Dp, k, kind, excl, out_idx, out_dist, st);
-  else if (precision == 0) brute_run<float>(Q, nq, X, n, Dp, k, kind, excl, out_idx, out_dist, st);
-  else throw std::invalid_argument("brute force: precision must be 0 (FP32) or 2 (FP64)");
+  if (precision == 2) {
+    brute_run<double>(Q, nq, X, n, Dp, k, kind, excl, out_idx, out_dist, st);
+  } else if (precision == 0) {
+    brute_run<float>(Q, nq, X, n, Dp, k, kind, excl, out_idx, out_dist, st);
+  } else if (precision == 1) {
+    if (!tc_supported(kind, Dp, k))
+      throw std::invalid_argument(
+          "brute force: the BF16 tensor-core form takes D <= 128, k <= 32 and squared Euclidean or a dot form");
+    brute_tc_run(Q, nq, X, n, Dp, k, kind, excl, out_idx, out_dist, st);
+  } else {
+    throw std::invalid_argument("brute force: precision must be 0 (FP32), 1 (BF16 tensor cores) or 2 (FP64)");
+  }
 }
 
 }  // namespace rinnd

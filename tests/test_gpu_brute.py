@@ -127,3 +127,24 @@ def test_k_above_n_and_errors(rb):
         rb.brute_force_knn(X, Q, k=3, metric="hamming")
     with pytest.raises(ValueError):
         rb.brute_force_knn(X, Q[:, :7], k=3)
+
+
+@pytest.mark.parametrize("metric,d", [("sqeuclidean", 128), ("sqeuclidean", 37), ("inner_product", 96),
+                                      ("cosine", 64)])
+def test_bf16_tensor_core_form_equals_fp32(rb, metric, d):
+    """The tensor-core form filters with BF16 Gram tiles and rechecks in the
+    FP32 form's arithmetic: its results are the FP32 form's, bit for bit."""
+    X = gmm(40000, d, 40, seed=8)
+    Q = gmm(40000 + 700, d, 40, seed=8)[40000:]
+    for k, sel in ((10, slice(None)), (32, slice(0, 5))):  # 5 queries: rows split over many CTAs
+        fi, fd = rb.brute_force_knn(X, Q[sel], k=k, metric=metric, precision="fp32")
+        ti, td = rb.brute_force_knn(X, Q[sel], k=k, metric=metric, precision="bf16")
+        np.testing.assert_array_equal(ti, fi)
+        np.testing.assert_array_equal(td.view(np.uint32), fd.view(np.uint32))
+    # the data's own graph, self excluded
+    fi, fd = rb.brute_force_knn(X, X[:300], k=15, metric=metric, precision="fp32", exclude_self=True)
+    ti, td = rb.brute_force_knn(X, X[:300], k=15, metric=metric, precision="bf16", exclude_self=True)
+    np.testing.assert_array_equal(ti, fi)
+    np.testing.assert_array_equal(td.view(np.uint32), fd.view(np.uint32))
+    with pytest.raises(ValueError):
+        rb.brute_force_knn(X, Q, k=33, metric=metric, precision="bf16")
