@@ -309,8 +309,10 @@ __global__ void __launch_bounds__(BF_NT) k_brute(BfArgs a) {
   }
 }
 
-// The splits' sorted lists of one query -> its first k keys (warp per query):
-// repeatedly the smallest head, found by a warp reduction over the splits.
+// The splits' sorted lists of one query -> its first k keys (warp per query;
+// lane l holds the heads of splits l, l + 32, l + 64, l + 96): repeatedly the
+// smallest head, by a reduction within the lane and then over the warp.
+constexpr int BF_MAXSPLIT = 128;
 template <typename T>
 __global__ void k_brute_merge(const BfKey<T>* __restrict__ part, int nq, int splits, int k, int32_t* out_idx,
                               float* out_dist) {
@@ -318,12 +320,27 @@ __global__ void k_brute_merge(const BfKey<T>* __restrict__ part, int nq, int spl
   const int lane = threadIdx.x & 31;
   if (q >= nq) return;
   const BfKey<T>* P = part + (size_t)q * splits * k;
-  int head = 0;  // this lane's position in split `lane` (splits <= 32)
+  int head[BF_MAXSPLIT / 32] = {0, 0, 0, 0};
+  auto head_key = [&](int u) {
+    const int sp = lane + 32 * u;
+    BfKey<T> key{(T)INFINITY, 0x7FFFFFFF};
+    if (sp < splits && head[u] < k) {
+      key = P[(size_t)sp * k + head[u]];
+      if (key.id < 0) key = BfKey<T>{(T)INFINITY, 0x7FFFFFFF};
+    }
+    return key;
+  };
   for (int p = 0; p < k; ++p) {
-    BfKey<T> mine = (lane < splits && head < k) ? P[(size_t)lane * k + head] : BfKey<T>{(T)INFINITY, -1};
-    if (mine.id < 0) mine = BfKey<T>{(T)INFINITY, 0x7FFFFFFF};
-    BfKey<T> best = mine;
-    int src = lane;
+    BfKey<T> best = head_key(0);
+    int src = lane;  // split number of the best head
+#pragma unroll
+    for (int u = 1; u < BF_MAXSPLIT / 32; ++u) {
+      const BfKey<T> h = head_key(u);
+      if (key_less(h, best)) {
+        best = h;
+        src = lane + 32 * u;
+      }
+    }
     for (int o = 16; o; o >>= 1) {
       const T od = __shfl_xor_sync(0xffffffffu, best.d, o);
       const int32_t oi = __shfl_xor_sync(0xffffffffu, best.id, o);
@@ -334,13 +351,46 @@ __global__ void k_brute_merge(const BfKey<T>* __restrict__ part, int nq, int spl
         src = os;
       }
     }
-    if (lane == src) ++head;
+#pragma unroll
+    for (int u = 0; u < BF_MAXSPLIT / 32; ++u)
+      if (src == lane + 32 * u) ++head[u];
     if (lane == 0) {
       const bool empty = best.id == 0x7FFFFFFF;
       out_idx[(size_t)q * k + p] = empty ? -1 : best.id;
       out_dist[(size_t)q * k + p] = empty ? __int_as_float(0x7f800000) : (float)best.d;
     }
   }
+}
+
+// Row splits per query tile: the fewest in [1, 128] (the merge kernel's limit,
+// and at least `min_tiles` row tiles a split) whose CTAs fill 90 % of the
+// resident slots over their waves -- a grid that barely exceeds the slots
+// would double the time with its last wave -- else the count that fills them
+// best.  Fewer splits keep the per-CTA start (the first tile's keys all enter
+// the lists) and the merge small.
+int choose_splits(long long qtiles, long long row_tiles, int slots, int min_tiles) {
+  int best = 1;
+  double best_eff = 0.0;
+  for (int s = 1; s <= BF_MAXSPLIT; ++s) {
+    if (s > 1 && (long long)s * min_tiles > row_tiles) break;
+    const long long ctas = qtiles * s;
+    const long long waves = (ctas + slots - 1) / slots;
+    const double eff = (double)ctas / (double)(waves * slots);
+    if (eff >= 0.9) return s;
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = s;
+    }
+  }
+  return best;
+}
+
+int resident_slots(const void* kernel, int threads, size_t smem) {
+  int dev = 0, per_sm = 0, sms = 0;
+  RINND_CUDA(cudaGetDevice(&dev));
+  RINND_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+  RINND_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return std::max(1, per_sm) * std::max(1, sms);
 }
 
 template <typename T, int QT>
@@ -350,9 +400,15 @@ size_t bf_smem(int k) {
 }
 
 template <typename T, int MODE, int QT>
-void brute_launch(const BfArgs& a, int qtiles, cudaStream_t st) {
+void brute_launch(BfArgs& a, int qtiles, DVec<BfKey<T>>& part, cudaStream_t st) {
   const size_t smem = bf_smem<T, QT>(a.k);
-  set_smem_limit_once(reinterpret_cast<const void*>(k_brute<T, MODE, QT>), 200 * 1024);
+  const void* kern = reinterpret_cast<const void*>(k_brute<T, MODE, QT>);
+  set_smem_limit_once(kern, 200 * 1024);
+  a.splits = choose_splits(qtiles, (a.n + BF_RT - 1) / BF_RT, resident_slots(kern, BF_NT, smem), 4);
+  if (a.splits > 1) {
+    part.alloc((size_t)a.nq * a.splits * a.k, st);
+    a.out_key = part.p;
+  }
   k_brute<T, MODE, QT><<<dim3((unsigned)qtiles, (unsigned)a.splits), BF_NT, smem, st>>>(a);
   RINND_LAUNCH_CHECK();
 }
@@ -374,17 +430,13 @@ void brute_run(const float* Q, int nq, const float* X, long long n, int Dp, int 
     RINND_LAUNCH_CHECK();
   }
   const int qtiles = (nq + QT - 1) / QT;
-  // enough CTAs for a few waves, rows split over the CTAs of one query tile
-  int splits = 1;
-  while (splits < 32 && (long long)qtiles * splits < 148 * 4 && (long long)splits * 4 * BF_RT < n) splits *= 2;
   DVec<BfKey<T>> part;
-  if (splits > 1) part.alloc((size_t)nq * splits * k, st);
-  BfArgs a{Q, X, qn.p, xn.p, excl, n, nq, Dp, k, kind, splits, part.p, out_idx, out_dist};
-  if (mode == BF_SQ) brute_launch<T, BF_SQ, QT>(a, qtiles, st);
-  else if (mode == BF_MAN) brute_launch<T, BF_MAN, QT>(a, qtiles, st);
-  else brute_launch<T, BF_DOT, QT>(a, qtiles, st);
-  if (splits > 1) {
-    k_brute_merge<T><<<(unsigned)((nq * 32 + 255) / 256), 256, 0, st>>>(part.p, nq, splits, k, out_idx, out_dist);
+  BfArgs a{Q, X, qn.p, xn.p, excl, n, nq, Dp, k, kind, 1, nullptr, out_idx, out_dist};
+  if (mode == BF_SQ) brute_launch<T, BF_SQ, QT>(a, qtiles, part, st);
+  else if (mode == BF_MAN) brute_launch<T, BF_MAN, QT>(a, qtiles, part, st);
+  else brute_launch<T, BF_DOT, QT>(a, qtiles, part, st);
+  if (a.splits > 1) {
+    k_brute_merge<T><<<(unsigned)((nq * 32 + 255) / 256), 256, 0, st>>>(part.p, nq, a.splits, k, out_idx, out_dist);
     RINND_LAUNCH_CHECK();
   }
 }
@@ -690,19 +742,17 @@ void brute_tc_run(const float* Q, int nq, const float* X, long long n, int Dp, i
     k_bf_norms<float><<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(X, n, Dp, xn.p);
     RINND_LAUNCH_CHECK();
   }
-  // one CTA per SM (its shared memory): row tiles split so that every SM has work
-  int splits = 1;
-  while (splits < 32 && (long long)qtiles * splits < 148 && (long long)splits * 4 < ntiles) splits *= 2;
+  // at least 116 KB: at most two CTAs (2 x 256 tensor-memory columns) share an SM
+  const size_t smem = std::max<size_t>(tc_smem(Kp, k), 116 * 1024);
+  const void* kern = sq ? reinterpret_cast<const void*>(k_brute_tc<true>) : reinterpret_cast<const void*>(k_brute_tc<false>);
+  set_smem_limit_once(kern, 227 * 1024);
+  const int splits = choose_splits(qtiles, ntiles, resident_slots(kern, TC_NT, smem), 8);
   DVec<BfKey<float>> part;
   if (splits > 1) part.alloc((size_t)nq * splits * k, st);
   DVec<int> err(1, st);
   err.fill_bytes(0);
   TcArgs a{Qb.p, qinfo.p, Q, qn.p, Xb.p, xinfo.p, X, xn.p, excl, n, nq, Dp, Kp, k, kind, splits, (int)ntiles,
            part.p, out_idx, out_dist, err.p};
-  // at least 116 KB: at most two CTAs (2 x 256 tensor-memory columns) share an SM
-  const size_t smem = std::max<size_t>(tc_smem(Kp, k), 116 * 1024);
-  const void* kern = sq ? reinterpret_cast<const void*>(k_brute_tc<true>) : reinterpret_cast<const void*>(k_brute_tc<false>);
-  set_smem_limit_once(kern, 227 * 1024);
   const dim3 grid((unsigned)qtiles, (unsigned)splits);
   if (sq) k_brute_tc<true><<<grid, TC_NT, smem, st>>>(a);
   else k_brute_tc<false><<<grid, TC_NT, smem, st>>>(a);
