@@ -640,13 +640,23 @@ __global__ void __launch_bounds__(TC_NT) k_brute_tc(TcArgs a) {
       __syncwarp();
       if (lane == 0) mbar_arrive(&tmem_empty[b]);  // this warp's reads of the accumulator are done
       const long long row0 = (long long)(t_lo + t) * TC_N + 64 * half;
+      // the 64 columns' row terms, one column a lane per 32, passed by shuffles
+      float2 xi_l[2];
+      float xn_l[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long long row = row0 + 32 * h + lane;
+        xi_l[h] = row < a.n ? __ldg(a.xinfo + row) : make_float2(0.f, 0.f);
+        xn_l[h] = (!SQ && row < a.n) ? __ldg(a.xn + row) : 0.f;
+      }
       // survivors of the filter against the list's k-th key at the tile's start
       unsigned long long keepm = 0ull;
 #pragma unroll
       for (int j = 0; j < 64; ++j) {
         const long long row = row0 + j;
         const float G = __uint_as_float(g[j]);
-        const float2 xi = row < a.n ? __ldg(a.xinfo + row) : make_float2(0.f, 0.f);
+        const float2 xi = make_float2(__shfl_sync(0xffffffffu, xi_l[j >> 5].x, j & 31),
+                                      __shfl_sync(0xffffffffu, xi_l[j >> 5].y, j & 31));
         bool keep;
         if (SQ) {
           const float sum = bn_q + xi.x;
@@ -656,7 +666,7 @@ __global__ void __launch_bounds__(TC_NT) k_brute_tc(TcArgs a) {
         } else {
           const float bj = sqrtf(xi.x);
           const float ub = G + e_q * bj + xi.y * (bt + e_q) + gam * bt * bj;
-          float lb = finalize_dot(a.kind, ub, row < a.n ? __ldg(a.xn + row) : 0.f, xn_q);
+          float lb = finalize_dot(a.kind, ub, __shfl_sync(0xffffffffu, xn_l[j >> 5], j & 31), xn_q);
           lb = lb - fabsf(lb) * 4.8828125e-4f - 1e-30f;
           keep = lb < thr.d;
         }
