@@ -327,10 +327,17 @@ __global__ void k_diversify_rev(const int32_t* rev_ptr, const uint64_t* rev_key,
   const int row = blockIdx.x * WARPS + w;
   if (row >= N) return;
   int nret = 0;
-  for (int e = rev_ptr[row]; e < rev_ptr[row + 1]; ++e) {
+  const int e_end = rev_ptr[row + 1];
+  for (int e = rev_ptr[row]; e < e_end; ++e) {
     uint64_t key = rev_key[e];
     int32_t j = (int32_t)(uint32_t)key;
     float dij = fkey_inv((uint32_t)(key >> 32));
+    // warm L1 with the next candidate's row while this one is checked (the
+    // candidate's row is the chain's global load; retained rows mostly hit L1)
+    if (e + 1 < e_end && lane * 128 < Dp * 4) {
+      const char* nxt = reinterpret_cast<const char*>(X + (size_t)(int32_t)(uint32_t)rev_key[e + 1] * Dp) + lane * 128;
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(nxt));
+    }
     bool pruned = pruned_by_retained<KIND>(s_id[w], s_d[w], nret, j, dij, X, D, Dp, kind, pd, row);
     if (!pruned) {
       if (lane == 0) {
