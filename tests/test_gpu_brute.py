@@ -148,3 +148,25 @@ def test_bf16_tensor_core_form_equals_fp32(rb, metric, d):
     np.testing.assert_array_equal(td.view(np.uint32), fd.view(np.uint32))
     with pytest.raises(ValueError):
         rb.brute_force_knn(X, Q, k=33, metric=metric, precision="bf16")
+
+
+def test_bf16_tensor_core_form_edge_shapes(rb):
+    """One partial row tile, query counts off the 128-query tile, dimensions
+    that need padding, k = 1, and all-zero rows under the cosine distance (its
+    1.0 for a zero norm): the tensor-core form's results are the FP32 form's."""
+    rng = np.random.default_rng(12)
+    for n, d, nq, k in ((50, 5, 3, 1), (50, 5, 3, 8), (129, 17, 130, 4), (1000, 128, 257, 32)):
+        X = rng.normal(0.0, 1.0, (n, d)).astype(np.float32)
+        Q = rng.normal(0.0, 1.0, (nq, d)).astype(np.float32)
+        for metric in ("sqeuclidean", "inner_product", "cosine"):
+            fi, fd = rb.brute_force_knn(X, Q, k=k, metric=metric, precision="fp32")
+            ti, td = rb.brute_force_knn(X, Q, k=k, metric=metric, precision="bf16")
+            np.testing.assert_array_equal(ti, fi, err_msg=f"{metric} n={n} d={d} nq={nq} k={k}")
+            np.testing.assert_array_equal(td.view(np.uint32), fd.view(np.uint32))
+    X = rng.normal(0.0, 1.0, (300, 24)).astype(np.float32)
+    X[::7] = 0.0
+    Q = np.concatenate([rng.normal(0.0, 1.0, (20, 24)), np.zeros((2, 24))]).astype(np.float32)
+    fi, fd = rb.brute_force_knn(X, Q, k=10, metric="cosine", precision="fp32")
+    ti, td = rb.brute_force_knn(X, Q, k=10, metric="cosine", precision="bf16")
+    np.testing.assert_array_equal(ti, fi)
+    np.testing.assert_array_equal(td.view(np.uint32), fd.view(np.uint32))
