@@ -170,3 +170,30 @@ def test_bf16_tensor_core_form_edge_shapes(rb):
     ti, td = rb.brute_force_knn(X, Q, k=10, metric="cosine", precision="bf16")
     np.testing.assert_array_equal(ti, fi)
     np.testing.assert_array_equal(td.view(np.uint32), fd.view(np.uint32))
+
+
+def test_device_pointers_equal_host_path(rb):
+    """rinnd_brute_force_knn with device-resident inputs, outputs and excluded
+    ids (on_device = 1) gives the host path's results, in each form."""
+    import ctypes
+
+    import torch
+
+    from rinnd_b200 import _lib as L
+
+    X = gmm(30000, 96, 30, seed=4)
+    Q = X[:700].copy()
+    dev = torch.device("cuda", 0)
+    Xd, Qd = torch.from_numpy(X).to(dev), torch.from_numpy(Q).to(dev)
+    ex = torch.arange(700, dtype=torch.int32, device=dev)
+    for prec in ("fp32", "bf16", "fp64"):
+        hi, hd = rb.brute_force_knn(X, Q, k=12, precision=prec, exclude_self=True)
+        oi = torch.empty((700, 12), dtype=torch.int32, device=dev)
+        od = torch.empty((700, 12), dtype=torch.float32, device=dev)
+        code = {"fp32": L.BRUTE_FP32, "bf16": L.BRUTE_BF16, "fp64": L.BRUTE_FP64}[prec]
+        L.check(L.lib.rinnd_brute_force_knn(ctypes.c_void_p(Xd.data_ptr()), 30000, 96, ctypes.c_void_p(Qd.data_ptr()),
+                                            700, 96, 96, 12, L.DIST_SQEUCLIDEAN, code,
+                                            ctypes.c_void_p(ex.data_ptr()), 1, ctypes.c_void_p(oi.data_ptr()),
+                                            ctypes.c_void_p(od.data_ptr())))
+        np.testing.assert_array_equal(oi.cpu().numpy(), hi)
+        np.testing.assert_array_equal(od.cpu().numpy().view(np.uint32), hd.view(np.uint32))
