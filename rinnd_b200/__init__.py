@@ -81,14 +81,16 @@ _BRUTE_METRICS = {"sqeuclidean": (L.DIST_SQEUCLIDEAN, False), "euclidean": (L.DI
                   "dot": (L.DIST_INNER_PRODUCT, False)}
 
 
-def brute_force_knn(data, queries, k=10, metric="sqeuclidean", precision="fp32", exclude_self=False):
+def brute_force_knn(data, queries, k=10, metric="sqeuclidean", precision="auto", exclude_self=False):
     """Exact k nearest data rows of every query row, by (distance, id) ascending
     (no counterpart in the reference; its recall criteria are measured against
     these).  precision "fp32" computes each distance with the build's FP32 join
     arithmetic; "bf16" filters the pairs on the tensor cores (BF16 Gram tiles,
     a rigorous lower bound) and recomputes the survivors in that FP32
     arithmetic, giving the FP32 results (dimension <= 128, k <= 32, not
-    Manhattan); "fp64" computes in double (the checker).  exclude_self leaves out data
+    Manhattan); "auto" (default) takes "bf16" where it applies and "fp32"
+    elsewhere -- the same results either way; "fp64" computes in double (the
+    checker).  exclude_self leaves out data
     row i for query i (queries must then be the data rows themselves).
     Returns (int32[nq, k], float32[nq, k]), padded with (-1, inf) when k > n."""
     if metric not in _BRUTE_METRICS:
@@ -99,8 +101,10 @@ def brute_force_knn(data, queries, k=10, metric="sqeuclidean", precision="fp32",
     if Q.shape[1] != X.shape[1]:
         raise ValueError(f"Query dimension {Q.shape[1]} does not match data dimension {X.shape[1]}")
     precisions = {"fp32": L.BRUTE_FP32, "bf16": L.BRUTE_BF16, "fp64": L.BRUTE_FP64}
+    if precision == "auto":
+        precision = "bf16" if (X.shape[1] <= 128 and int(k) <= 32 and kind != L.DIST_MANHATTAN) else "fp32"
     if precision not in precisions:
-        raise ValueError("precision must be 'fp32', 'bf16' or 'fp64'")
+        raise ValueError("precision must be 'auto', 'fp32', 'bf16' or 'fp64'")
     nq = Q.shape[0]
     excl = None
     if exclude_self:
