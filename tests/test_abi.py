@@ -181,3 +181,30 @@ def test_join_tile_table_rejects_shapes_that_do_not_exist():
     L.check(L.lib.rinnd_join_tile_table_clear())
     L.check(L.lib.rinnd_join_tile_table(None, 0, ctypes.byref(n)))
     assert n.value == 0
+
+
+def test_brute_force_arguments_rejected_before_any_device_work():
+    """rinnd_brute_force_knn validates shapes, k, precision and the metric
+    before touching a device; the Python wrapper raises ValueError for the same."""
+    from rinnd_b200 import _lib as L
+    import rinnd_b200
+
+    x = np.zeros((4, 3), np.float32)
+    oi = np.empty((4, 2), np.int32)
+    od = np.empty((4, 2), np.float32)
+
+    def call(k=2, kind=L.DIST_SQEUCLIDEAN, prec=L.BRUTE_FP32, n=4, d=3):
+        return L.lib.rinnd_brute_force_knn(L.ptr(x), n, d, L.ptr(x), 4, d, d, k, kind, prec, None, 0, L.ptr(oi),
+                                           L.ptr(od))
+
+    assert call(k=0) == L.ERR_INVALID and "k must be" in L.last_error()
+    assert call(k=129) == L.ERR_INVALID
+    assert call(prec=7) == L.ERR_INVALID and "precision" in L.last_error()
+    assert call(kind=L.DIST_HAMMING) == L.ERR_INVALID and "brute force supports" in L.last_error()
+    assert call(n=0) == L.ERR_INVALID
+    with pytest.raises(ValueError, match="Unknown metric"):
+        rinnd_b200.brute_force_knn(x, x, k=2, metric="hamming")
+    with pytest.raises(ValueError, match="does not match"):
+        rinnd_b200.brute_force_knn(x, x[:, :2], k=2)
+    with pytest.raises(ValueError, match="precision"):
+        rinnd_b200.brute_force_knn(x, x, k=2, precision="fp16")
