@@ -60,9 +60,10 @@ def test_search_equals_oracle_search_on_the_same_index(rb, orc, leaf_budget, eps
 def test_search_equals_oracle_search_on_long_traversals(rb, orc, eps):
     """Tight clusters on the unit sphere: distances within a cluster
     concentrate, so with a wide epsilon a query's bound covers much of its
-    cluster and its search expands hundreds to thousands of seeds -- the path that expands seeds in
-    speculative groups, spills seeds to the back store and visited ids to the
-    global table.  Results still equal the oracle's on the same index."""
+    cluster and its search expands hundreds to thousands of seeds -- the path
+    that refills the sorted seed front from the unsorted back store and spills
+    visited ids to the global table.  Results still equal the oracle's on the
+    same index."""
     rng = np.random.default_rng(9)
     centers = rng.normal(0.0, 10.0, (10, 64))
     X = centers[rng.integers(0, 10, 20000)] + rng.normal(0.0, 1.0, (20000, 64))
@@ -75,7 +76,7 @@ def test_search_equals_oracle_search_on_long_traversals(rb, orc, eps):
     gi, gd = ix.query(Q, k=10, epsilon=eps)
     oi, od = oix.query(Q, k=10, epsilon=eps)
     st = ix.search_stats()
-    assert st["expansions"] > 200 * len(Q), st  # long traversals: grouped expansions ran
+    assert st["expansions"] > 200 * len(Q), st  # long traversals did run
     bad = np.nonzero(~np.all(gi == oi, axis=1))[0]
     assert len(bad) == 0, (len(bad), bad[:5], gi[bad[:2]], oi[bad[:2]])
     np.testing.assert_array_equal(gd.view(np.uint32), od.view(np.uint32))
