@@ -236,9 +236,9 @@ __device__ __forceinline__ int row_push_hi_first(uint64_t* row, int k, uint32_t*
   return row_push_raw(row, k, thr, key, contention);
 }
 
-// The push of the reverse candidate offers: rows of up to 32 slots take the
-// register-snapshot form (faster there; in the update-application kernel its
-// registers cost more occupancy than the shorter scan saves).
+// The push of the reverse candidate offers and of the update application: rows
+// of up to 32 slots take the register-snapshot form, longer rows the chunked
+// scan.
 __device__ __forceinline__ int row_push_fast(uint64_t* row, int k, uint32_t* thr, uint64_t key,
                                              unsigned long long* contention) {
   if (thr != nullptr && (uint32_t)(key >> 32) >= __ldcg(thr)) return 0;
@@ -246,6 +246,43 @@ __device__ __forceinline__ int row_push_fast(uint64_t* row, int k, uint32_t* thr
   if (k <= 32) return row_push_small<32>(row, k, thr, key, contention);
   return row_push(row, k, thr, key, contention);
 }
+
+// Pushes that passed their row's bound, compacted per warp so that the row
+// scans of row_push_fast start together on 32 queued updates instead of on
+// whichever lanes of a 32-update slice passed.  `t` and `key` are this warp's
+// 64 entries in shared memory.  append() queues the lanes whose `pass` is set
+// and, once 32 are queued, hands one entry to every lane (returns true,
+// warp-uniformly); drain() hands the rest to lanes below n.  Call both with
+// the whole warp.
+struct WarpQueue {
+  uint32_t* t;
+  uint64_t* key;
+  int n;
+  __device__ __forceinline__ bool append(bool pass, uint32_t ti, uint64_t ki, uint32_t& to, uint64_t& ko) {
+    const int lane = threadIdx.x & 31;
+    const unsigned bal = __ballot_sync(0xffffffffu, pass);
+    if (pass) {
+      const int pos = n + __popc(bal & ((1u << lane) - 1));
+      t[pos] = ti;
+      key[pos] = ki;
+    }
+    n += __popc(bal);
+    __syncwarp();
+    if (n < 32) return false;
+    n -= 32;
+    to = t[n + lane];
+    ko = key[n + lane];
+    __syncwarp();
+    return true;
+  }
+  __device__ __forceinline__ bool drain(uint32_t& to, uint64_t& ko) const {
+    const int lane = threadIdx.x & 31;
+    if (lane >= n) return false;
+    to = t[lane];
+    ko = key[lane];
+    return true;
+  }
+};
 
 // Per-index accounting of a grouped build (several indices' rows in one set of
 // heaps): an accepted push into row r adds 1 to changes[row_item[r]].  Both

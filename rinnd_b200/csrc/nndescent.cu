@@ -438,7 +438,10 @@ __global__ void k_apply_updates(const uint32_t* urow, const uint64_t* ukey, cons
 }
 
 // k_apply_updates for the region form: region r of the buffer holds rcnt[r]
-// updates from entry r * rsize; `sub` blocks share a region.
+// updates from entry r * rsize; `sub` blocks share a region.  Updates under
+// their row's bound are queued per warp and pushed 32 at a time (WarpQueue;
+// 1.77 -> 1.60 ms per launch at 400k x 128, k = 30; the same queue in the
+// reverse candidate offers was slower at 1M).  Launched with 256 threads.
 __global__ void k_apply_regions(const uint32_t* urow, const uint64_t* ukey, const uint32_t* rcnt, int nreg,
                                 unsigned int rsize, int sub, const unsigned long long* count, uint64_t* slots,
                                 uint32_t* thr, int k, int kp, unsigned long long* counters, ItemCount ic) {
@@ -452,15 +455,33 @@ __global__ void k_apply_regions(const uint32_t* urow, const uint64_t* ukey, cons
   const size_t base = (size_t)r * rsize;
   unsigned int mine = 0;
   ItemTally tally;
-  // (in order: the join's updates rarely share rows within a warp, and reads
-  // in order are cheaper than spread ones)
-  for (unsigned int e = part * blockDim.x + threadIdx.x; e < cnt; e += sub * blockDim.x) {
-    const uint32_t row = urow[base + e];
-    if (row_push_fast(slots + (size_t)row * kp, k, thr + row, ukey[base + e], &counters[1])) {
+  __shared__ uint32_t q_row[8][64];
+  __shared__ uint64_t q_key[8][64];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpQueue q{q_row[w], q_key[w], 0};
+  uint32_t row;
+  uint64_t key;
+  auto push = [&]() {
+    if (row_push_fast(slots + (size_t)row * kp, k, thr + row, key, &counters[1])) {
       ++mine;
       tally.add(ic, row);
     }
+  };
+  // (in order: the join's updates rarely share rows within a warp, and reads
+  // in order are cheaper than spread ones)
+  for (unsigned int e0 = part * blockDim.x + w * 32; e0 < cnt; e0 += sub * blockDim.x) {
+    const unsigned int e = e0 + lane;
+    bool pass = false;
+    uint32_t rr = 0;
+    uint64_t kk = 0;
+    if (e < cnt) {
+      rr = urow[base + e];
+      kk = ukey[base + e];
+      pass = (uint32_t)(kk >> 32) < __ldcg(thr + rr);
+    }
+    if (q.append(pass, rr, kk, row, key)) push();
   }
+  if (q.drain(row, key)) push();
   tally.flush(ic);
   for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&counters[0], (unsigned long long)mine);

@@ -62,18 +62,22 @@ def test_distance_pairs_match_reference_order(rb, orc, dim):
             assert np.array_equal(g.view(np.uint32), r.view(np.uint32)), (kind, np.abs(g - r).max())
 
 
-def test_heap_push_batch_matches_sequential(rb, orc):
+@pytest.mark.parametrize("k", [12, 20, 30, 32, 48])
+def test_heap_push_batch_matches_sequential(rb, orc, k):
     """Concurrent checked_flagged_push == the reference's sequential application
-    (final row sets are the k smallest distinct ids offered)."""
+    (final row sets are the k smallest distinct ids offered), for rows of one,
+    two and three 16-slot line groups and a full last group (k = 32)."""
     from rinnd_b200 import _lib as L
 
     rng = np.random.default_rng(3)
-    n, k, n_ops = 200, 12, 60000
+    n, n_ops = 200, 60000
     rows = rng.integers(0, n, n_ops).astype(np.int32)
     ids = rng.integers(0, 400, n_ops).astype(np.int32)
-    # one distance per (row, id), as in NN-Descent where d(p, q) is a function of the pair
-    h = (rows.astype(np.uint64) * np.uint64(2654435761) + ids.astype(np.uint64) * np.uint64(40503)) % np.uint64(1 << 20)
-    dists = (h.astype(np.float32) / np.float32(1 << 20)) * np.float32(10.0)
+    # one distance per (row, id), as in NN-Descent where d(p, q) is a function of
+    # the pair, distinct within a row (ids < the prime modulus), so the k smallest
+    # leave no tie at a row's boundary for arrival order to decide
+    h = (rows.astype(np.uint64) * np.uint64(7919) + ids.astype(np.uint64) * np.uint64(104729)) % np.uint64(1000003)
+    dists = (h.astype(np.float32) / np.float32(1000003)) * np.float32(10.0)
     flags = ((h >> np.uint64(7)) & np.uint64(1)).astype(np.uint8)  # also a function of the pair
     oi, od, of, _ = orc.neighbor_heap_apply(n, k, rows, ids, dists, flags)
     gi = np.empty((n, k), np.int32)
