@@ -104,51 +104,63 @@ __global__ void k_fill_segmap(const long long* seg_gstart, const long long* seg_
 // builder.rs:312-348 partition_inplace side decision for every tree's position
 // of a point: margin = dot(point, hyperplane) + offset in the reference's dot
 // order (builder.rs:11-60, exact_dot_a); |margin| < 1e-8 -> random side; else
-// margin < 0 -> left.  One warp per point reads the point's row once per level
-// for all trees: 4 trees at a time, 8 lanes per dot, lane t carrying the
-// reference's accumulator chain t (elements 8c + t, c in order), the same
-// horizontal-sum tree over shuffles and the remainder added by lane 0 -- the
-// margins are bit-identical to exact_dot_a's.  inv[t N + p] is point p's
-// position in tree t; positions of finished leaves (segment -1) get side 0.
+// margin < 0 -> left.  Two lanes per (point, tree) pair, a warp over 16
+// consecutive pairs (a point's trees are neighbors, so its row is read once
+// from DRAM per level): lane q carries the reference's accumulator chains
+// 4q .. 4q + 3 (elements 8c + 4q + i, c in order) with 16-byte loads of the
+// row and the hyperplane (rows are 4-float padded and 16-byte aligned), the
+// pair's lanes combine the eight chains in the reference's horizontal-sum tree
+// ((s4 + s0) + (s5 + s1)) + ((s6 + s2) + (s7 + s3)) and lane 0 adds the
+// remainder -- the margins are bit-identical to exact_dot_a's.  inv[t N + p] is
+// point p's position in tree t; positions of finished leaves (segment -1) get
+// side 0.
 __global__ void k_margins(const int32_t* seg_of, const int32_t* inv, int N, int T, const float* X, int D, int Dp,
                           const float* hp, const float* off, uint64_t seed, int depth, int32_t* is_left) {
-  const int lane = threadIdx.x & 31, grp = lane >> 3, t8 = lane & 7;
+  const int lane = threadIdx.x & 31, q = lane & 1;
   const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   const int chunks = D >> 3;
-  for (long long pid = warp; pid < N; pid += nwarps) {
+  const long long total = (long long)N * T;
+  for (long long u0 = warp * 16; u0 < total; u0 += nwarps * 16) {
+    const long long u = u0 + (lane >> 1);
+    long long g = -1;
+    int sg = -1, pid = 0, t = 0;
+    if (u < total) {
+      pid = (int)(u / T);
+      t = (int)(u - (long long)pid * T);
+      g = (long long)t * N + inv[(size_t)t * N + pid];
+      sg = seg_of[g];
+    }
     const float* x = X + (size_t)pid * Dp;
-    for (int t0 = 0; t0 < T; t0 += 4) {
-      const int t = t0 + grp;
-      long long g = -1;
-      int sg = -1;
-      if (t < T) {
-        g = (long long)t * N + inv[(size_t)t * N + pid];
-        sg = seg_of[g];
+    const float* h = hp + (size_t)(sg >= 0 ? sg : 0) * Dp;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    if (sg >= 0) {
+      const float4* x4 = reinterpret_cast<const float4*>(x) + q;
+      const float4* h4 = reinterpret_cast<const float4*>(h) + q;
+      for (int c = 0; c < chunks; ++c) {
+        const float4 xa = __ldg(x4 + 2 * c), ha = __ldg(h4 + 2 * c);
+        s0 = __fmaf_rn(xa.x, ha.x, s0);
+        s1 = __fmaf_rn(xa.y, ha.y, s1);
+        s2 = __fmaf_rn(xa.z, ha.z, s2);
+        s3 = __fmaf_rn(xa.w, ha.w, s3);
       }
-      const float* h = hp + (size_t)(sg >= 0 ? sg : 0) * Dp;
-      float acc = 0.f;
-      if (sg >= 0)
-        for (int c = 0; c < chunks; ++c) acc = __fmaf_rn(x[8 * c + t8], h[8 * c + t8], acc);
-      // hsum_a: ((s4 + s0) + (s5 + s1)) + ((s6 + s2) + (s7 + s3))
-      const float up4 = __shfl_down_sync(0xffffffffu, acc, 4, 8);
-      const float a = __fadd_rn(up4, acc);
-      const float up1 = __shfl_down_sync(0xffffffffu, a, 1, 8);
-      const float b = __fadd_rn(a, up1);
-      const float up2 = __shfl_down_sync(0xffffffffu, b, 2, 8);
-      if (t8 == 0 && g >= 0) {
-        int left = 0;
-        if (sg >= 0) {
-          float r = __fadd_rn(b, up2);
-          for (int i = chunks * 8; i < D; ++i) r = __fadd_rn(r, __fmul_rn(x[i], h[i]));
-          const float margin = __fadd_rn(r, off[sg]);
-          if (fabsf(margin) < 1e-8f)
-            left = (int)(hash3(seed ^ 0x7a11u, ((uint64_t)t << 32) | (uint32_t)depth, (uint64_t)pid) >> 63);
-          else
-            left = margin < 0.f;
-        }
-        is_left[g] = left;
+    }
+    // lane 0 of the pair receives chains 4..7 from lane 1
+    const float p0 = __shfl_xor_sync(0xffffffffu, s0, 1), p1 = __shfl_xor_sync(0xffffffffu, s1, 1);
+    const float p2 = __shfl_xor_sync(0xffffffffu, s2, 1), p3 = __shfl_xor_sync(0xffffffffu, s3, 1);
+    if (q == 0 && g >= 0) {
+      int left = 0;
+      if (sg >= 0) {
+        const float a0 = __fadd_rn(p0, s0), a1 = __fadd_rn(p1, s1), a2 = __fadd_rn(p2, s2), a3 = __fadd_rn(p3, s3);
+        float r = __fadd_rn(__fadd_rn(a0, a1), __fadd_rn(a2, a3));
+        for (int i = chunks * 8; i < D; ++i) r = __fadd_rn(r, __fmul_rn(x[i], h[i]));
+        const float margin = __fadd_rn(r, off[sg]);
+        if (fabsf(margin) < 1e-8f)
+          left = (int)(hash3(seed ^ 0x7a11u, ((uint64_t)t << 32) | (uint32_t)depth, (uint64_t)pid) >> 63);
+        else
+          left = margin < 0.f;
       }
+      is_left[g] = left;
     }
   }
 }
