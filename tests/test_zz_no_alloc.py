@@ -125,3 +125,55 @@ def test_noalloc_invalid_pushes_fail_like_the_allocating_entry_point():
     ni2, nd2, _, _ = noalloc(L, torch, n, k, rows, ok_ids, dists, flags)
     np.testing.assert_array_equal(ni2, ai)
     np.testing.assert_array_equal(nd2.view(np.uint32), ad.view(np.uint32))
+
+
+def test_noalloc_takes_no_device_memory():
+    """Every device allocation of the library is a cudaMallocAsync from the
+    device's default memory pool; the pool's high-water mark of memory in use,
+    reset before the calls, shows that the allocation-free entry point takes
+    none (not even transiently), while the allocating entry point, measured
+    the same way, does."""
+    torch = pytest.importorskip("torch")
+    cudart = pytest.importorskip("cuda.bindings.runtime")
+    cudrv = pytest.importorskip("cuda.bindings.driver")
+    from rinnd_b200 import _lib as L
+
+    ok = cudart.cudaError_t.cudaSuccess
+    high_attr = cudart.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh
+    cur_attr = cudart.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent
+    err, pool = cudart.cudaDeviceGetDefaultMemPool(0)
+    assert err == ok
+
+    def attr(a):
+        err, v = cudart.cudaMemPoolGetAttribute(pool, a)
+        assert err == ok
+        return int(v)
+
+    def reset_high():
+        (err,) = cudart.cudaMemPoolSetAttribute(pool, high_attr, cudrv.cuuint64_t(0))
+        assert err == ok
+
+    n, k = 1000, 30
+    rows, ids, dists, flags = make_pushes(31, n, k, 120000, 3000)
+    ref = noalloc(L, torch, n, k, rows, ids, dists, flags)  # first call on the device: resolves the scratch
+    dev = torch.device("cuda", 0)
+    t_rows, t_ids = torch.from_numpy(rows).to(dev), torch.from_numpy(ids).to(dev)
+    t_d, t_f = torch.from_numpy(dists).to(dev), torch.from_numpy(flags).to(dev)
+    oi = torch.empty((n, k), dtype=torch.int32, device=dev)
+    od = torch.empty((n, k), dtype=torch.float32, device=dev)
+    of = torch.empty((n, k), dtype=torch.uint8, device=dev)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    torch.cuda.synchronize(dev)
+    base = attr(cur_attr)
+    reset_high()
+    for _ in range(2):
+        L.check(L.lib.rinnd_heap_push_batch_noalloc(n, k, rows.size, p(t_rows), p(t_ids), p(t_d), p(t_f), p(oi),
+                                                    p(od), p(of), None, stream))
+    torch.cuda.synchronize(dev)
+    assert attr(high_attr) <= base and attr(cur_attr) == base, (attr(high_attr), base)
+    np.testing.assert_array_equal(oi.cpu().numpy(), ref[0])
+    # the measurement sees allocations: the allocating entry point's buffers raise the mark
+    reset_high()
+    allocating(L, n, k, rows, ids, dists, flags)
+    assert attr(high_attr) > base
